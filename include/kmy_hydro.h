@@ -1,0 +1,153 @@
+/* kmy_hydro.h -- C ABI of the B200 finite-volume update (kamayan hydro path).
+ *
+ * Plain C types only: no CUDA, torch or C++ types cross this boundary.  Every
+ * entry point returns a kmy_status code; no C++ exception escapes.  A context
+ * owns one mesh, its device-resident stage containers and one CUDA stream; it
+ * is not thread-safe (use one context per host thread).
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the kamayan source tree).
+ */
+#ifndef KMY_HYDRO_H_
+#define KMY_HYDRO_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* TaskStatus / PARTHENON_FAIL analogue (driver/kamayan_driver_types.hpp:19-20). */
+typedef enum {
+  KMY_OK = 0,
+  KMY_ERR_BAD_PARAM = 1, /* unknown option, bad size or name */
+  KMY_ERR_OOM = 2,       /* device allocation failed */
+  KMY_ERR_NONFINITE = 3, /* NaN/inf or non-positive density/pressure detected */
+  KMY_ERR_TIMEOUT = 4,   /* a bounded device wait gave up */
+  KMY_ERR_CUDA = 5,      /* CUDA runtime error (see kmy_last_error) */
+  KMY_ERR_STATE = 6      /* call out of order (e.g. no state yet) */
+} kmy_status;
+
+typedef struct kmy_ctx kmy_ctx;
+
+/* Mesh description returned by kmy_get_info.  Arrays are (i, j, k) ordered. */
+typedef struct {
+  int ndim;
+  int nblocks;
+  int nx[3];        /* interior cells per meshblock */
+  int nghost;       /* ghost cells in each active dimension */
+  int ncells_pad[3];/* ghost-padded cells per block: nx + 2*nghost (1 if inactive) */
+  int nfaces_pad[3];/* face array dims: ncells_pad + 1 in active dims */
+  int nblocks_dim[3];
+  int ncons;        /* cell conserved components: 5 hydro, 8 with CT */
+  int mhd;          /* 0 off, 1 constrained transport */
+  int nstages;      /* RK stages of the integrator */
+  int precision;    /* 64 or 32: arithmetic/storage type of the bulk update */
+  double xmin[3], xmax[3], dx[3];
+} kmy_info;
+
+/* Create a context from a Parthenon input deck (`<block>` headers with
+ * `key = value` lines, and `block/key = value` override lines).  Accepted keys
+ * mirror the reference's runtime parameters: <parthenon/mesh> (nx*, x*min/max,
+ * *_bc, nghost), <parthenon/meshblock> (nx*), <parthenon/time> (integrator,
+ * tlim, nlim, dt_*), <hydro> (reconstruction, slope_limiter, riemann, cfl,
+ * ReconstructionVars, ReconstructionStrategy, EMF_averaging), <physics> (MHD),
+ * <material/single> (gamma, Abar, eos_type), <eos> (mode_init), plus
+ * <kamayan_b200> (precision = fp64|fp32).  Unknown option values fail with
+ * KMY_ERR_BAD_PARAM.
+ * Replaces: InitEnv/InitPackages parameter setup (src/kamayan/kamayan.cpp:20-138),
+ * hydro::SetupParams (src/physics/hydro/hydro.cpp:51-92),
+ * grid::SetupParams (src/grid/grid.cpp:169-262),
+ * driver::SetupParams (src/driver/kamayan_driver.cpp:23-81). */
+int kmy_create(const char *deck, int device, kmy_ctx **out);
+int kmy_destroy(kmy_ctx *ctx);
+/* Message of the last failing call on this context ("" if none). */
+const char *kmy_last_error(const kmy_ctx *ctx);
+int kmy_get_info(const kmy_ctx *ctx, kmy_info *out);
+
+/* Bind the context to a caller-owned cudaStream_t (NULL = context's own). */
+int kmy_set_stream(kmy_ctx *ctx, void *cuda_stream);
+/* Block until all work queued on the context's stream is finished. */
+int kmy_sync(kmy_ctx *ctx);
+
+/* ---- state in Parthenon MeshData layout -------------------------------------
+ * Cell variables: n = nblocks * prod(ncells_pad) doubles, block-major then
+ * (k, j, i) with i fastest.  Face variable "mag": comp = face direction, n =
+ * nblocks * prod(nfaces_pad).  Names are the reference field names
+ * (src/kamayan/fields.hpp:177-210): "dens", "momentum"(3), "ener", "magc"(3),
+ * "mag"(face, 3), "velocity"(3), "pres", "bulk modulus", "eint", "temp",
+ * "divb".  Containers: "base", the stage names "1", "2", ... and "dUdt"
+ * (src/driver/kamayan_driver.cpp:140-143).  Primitives are shared by all
+ * containers.  Export fills ghost zones first (boundary exchange semantics). */
+int kmy_import_var(kmy_ctx *ctx, const char *container, const char *var, int comp,
+                   const double *host, size_t n);
+int kmy_export_var(kmy_ctx *ctx, const char *container, const char *var, int comp,
+                   double *host, size_t n);
+/* Mark imported state complete: prims of "base" are taken as given (as after
+ * the reference's MeshPostInitialization), ghosts are filled, dt is estimated.
+ * Replaces: the driver initialisation path (EstimateTimestep after pgen). */
+int kmy_finalize_import(kmy_ctx *ctx);
+
+/* Device problem generators: "isentropic_vortex", "kelvin_helmholtz",
+ * "orszag_tang", "blast", "sedov".  Problem parameters come from the deck.
+ * Replaces: ProblemGenerator + MeshPostInitialization
+ * (src/problems/isentropic_vortex.cpp:307-377, src/problems/sedov.cpp:104-143,
+ *  src/physics/hydro/primconsflux.cpp:145-148, src/physics/material_properties/eos/eos.cpp:165-168). */
+int kmy_pgen(kmy_ctx *ctx, const char *problem);
+
+/* ---- per-task entry points (KamayanUnit callback slots) -------------------- */
+/* hydro::AddFluxTasks -> CalculateFluxes (src/physics/hydro/hydro_add_flux_tasks.cpp:36-264) */
+int kmy_compute_fluxes(kmy_ctx *ctx, const char *md0);
+/* hydro::AddFluxTasks -> CalculateEMF (src/physics/hydro/hydro_add_flux_tasks.cpp:405-442) */
+int kmy_compute_emf(kmy_ctx *ctx, const char *md0);
+/* grid::FluxesToDuDt (src/grid/grid.cpp:348-351; src/grid/grid_update.hpp:15-137) */
+int kmy_flux_divergence(kmy_ctx *ctx, const char *md0, const char *dudt);
+/* grid::ApplyDuDt (src/grid/grid.cpp:353-423) */
+int kmy_apply_dudt(kmy_ctx *ctx, const char *base, const char *md0, const char *md1,
+                   const char *dudt, double beta, double dt);
+/* hydro::PreparePrimitive + eos::PreparePrimitive (src/physics/hydro/primconsflux.cpp:152-155,
+ * src/physics/material_properties/eos/eos.cpp:164) */
+int kmy_prepare_primitive(kmy_ctx *ctx, const char *md1);
+/* Parthenon AddBoundaryExchangeTasks on one level (kamayan_driver.cpp:150-151) */
+int kmy_fill_ghosts(kmy_ctx *ctx, const char *md);
+/* hydro::EstimateTimeStepMesh (src/physics/hydro/hydro_time_step.cpp:67-70) */
+int kmy_estimate_dt(kmy_ctx *ctx, const char *md, double *dt_out);
+/* hydro::FillDerived, div B (src/physics/hydro/hydro.cpp:191-194) */
+int kmy_fill_derived(kmy_ctx *ctx, const char *md);
+/* One RK stage through the per-task kernels above, in the reference task order
+ * (KamayanDriver::BuildTaskListRKStage, src/driver/kamayan_driver.cpp:186-248). */
+int kmy_task_stage(kmy_ctx *ctx, int stage, double dt);
+
+/* ---- fused path -----------------------------------------------------------
+ * One RK stage in a single fused launch (reconstruction, Riemann flux, flux
+ * divergence and the low-storage update; dt estimate fused into the last
+ * stage).  Same results as kmy_task_stage within FP64 rounding. */
+int kmy_rk_stage(kmy_ctx *ctx, int stage, double dt);
+/* One time step at the current dt (all stages) followed by the dt controller
+ * (Parthenon EvolutionDriver semantics).  dt_taken may be NULL. */
+int kmy_step(kmy_ctx *ctx, double *dt_taken);
+/* Step until tlim or nlim steps (nlim < 0: no limit). */
+int kmy_evolve(kmy_ctx *ctx, double tlim, int nlim, int *nsteps);
+/* Simulation clock: time, next dt, last dt estimate, cycle count. */
+int kmy_get_time(const kmy_ctx *ctx, double *time, double *dt, double *dt_est, int *ncycle);
+/* Override the dt used by the next kmy_step (e.g. to replay a reference run). */
+int kmy_set_dt(kmy_ctx *ctx, double dt);
+/* Select the stepping path used by kmy_step/kmy_evolve: 0 = fused, 1 = tasks. */
+int kmy_set_path(kmy_ctx *ctx, int path);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+/* L1 error of dens/velocity/pres against the initial isentropic vortex,
+ * (src/problems/isentropic_vortex.hpp:150-200).  var: 0 dens, 1 velocity, 2 pres. */
+int kmy_vortex_error(kmy_ctx *ctx, int var, int comp, double *out);
+/* Compensated (Kahan-Babuska) FP64 sums of the conserved variables over the
+ * interior of `md` times the cell volume: out[0..ncons-1]. */
+int kmy_conserved_sums(kmy_ctx *ctx, const char *md, double *out);
+
+/* Number of this library's kernels launched on the context since creation. */
+int kmy_launch_count(const kmy_ctx *ctx, int64_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KMY_HYDRO_H_ */

@@ -1,0 +1,247 @@
+"""kamayan_b200 -- B200-native finite-volume update for kamayan's hydro path.
+
+Python host layer over the C ABI in ``include/kmy_hydro.h`` (loaded with
+ctypes from ``kamayan_b200/lib/libkmy_hydro.so``).  The compute path is the
+CUDA library only: if the shared library is missing, importing the bindings
+raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from .deck import Deck, deck_text  # noqa: F401
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libkmy_hydro.so"
+
+STATUS = {
+    0: "OK",
+    1: "BAD_PARAM",
+    2: "OOM",
+    3: "NONFINITE",
+    4: "TIMEOUT",
+    5: "CUDA",
+    6: "STATE",
+}
+
+# Every entry point declared in include/kmy_hydro.h.
+EXPORTS = (
+    "kmy_create", "kmy_destroy", "kmy_last_error", "kmy_get_info", "kmy_set_stream", "kmy_sync",
+    "kmy_import_var", "kmy_export_var", "kmy_finalize_import", "kmy_pgen",
+    "kmy_compute_fluxes", "kmy_compute_emf", "kmy_flux_divergence", "kmy_apply_dudt",
+    "kmy_prepare_primitive", "kmy_fill_ghosts", "kmy_estimate_dt", "kmy_fill_derived",
+    "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_get_time", "kmy_set_dt",
+    "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
+)
+
+
+class KmyError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("ndim", ctypes.c_int), ("nblocks", ctypes.c_int), ("nx", ctypes.c_int * 3),
+        ("nghost", ctypes.c_int), ("ncells_pad", ctypes.c_int * 3),
+        ("nfaces_pad", ctypes.c_int * 3), ("nblocks_dim", ctypes.c_int * 3),
+        ("ncons", ctypes.c_int), ("mhd", ctypes.c_int), ("nstages", ctypes.c_int),
+        ("precision", ctypes.c_int), ("xmin", ctypes.c_double * 3), ("xmax", ctypes.c_double * 3),
+        ("dx", ctypes.c_double * 3),
+    ]
+
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def lib() -> ctypes.CDLL:
+    """Load libkmy_hydro.so (built by ``kamayan_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m kamayan_b200.build` first")
+        L = ctypes.CDLL(str(LIB_PATH))
+        vp, cp, i, d, sz = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+        L.kmy_create.argtypes = [cp, i, ctypes.POINTER(vp)]
+        L.kmy_destroy.argtypes = [vp]
+        L.kmy_last_error.restype = cp
+        L.kmy_last_error.argtypes = [vp]
+        L.kmy_get_info.argtypes = [vp, ctypes.POINTER(Info)]
+        L.kmy_set_stream.argtypes = [vp, vp]
+        L.kmy_sync.argtypes = [vp]
+        L.kmy_import_var.argtypes = [vp, cp, cp, i, _dp, sz]
+        L.kmy_export_var.argtypes = [vp, cp, cp, i, _dp, sz]
+        L.kmy_finalize_import.argtypes = [vp]
+        L.kmy_pgen.argtypes = [vp, cp]
+        for n in ("kmy_compute_fluxes", "kmy_compute_emf", "kmy_prepare_primitive",
+                  "kmy_fill_ghosts", "kmy_fill_derived"):
+            getattr(L, n).argtypes = [vp, cp]
+        L.kmy_flux_divergence.argtypes = [vp, cp, cp]
+        L.kmy_apply_dudt.argtypes = [vp, cp, cp, cp, cp, d, d]
+        L.kmy_estimate_dt.argtypes = [vp, cp, _dp]
+        L.kmy_task_stage.argtypes = [vp, i, d]
+        L.kmy_rk_stage.argtypes = [vp, i, d]
+        L.kmy_step.argtypes = [vp, _dp]
+        L.kmy_evolve.argtypes = [vp, d, i, ctypes.POINTER(i)]
+        L.kmy_get_time.argtypes = [vp, _dp, _dp, _dp, ctypes.POINTER(i)]
+        L.kmy_set_dt.argtypes = [vp, d]
+        L.kmy_set_path.argtypes = [vp, i]
+        L.kmy_vortex_error.argtypes = [vp, i, i, _dp]
+        L.kmy_conserved_sums.argtypes = [vp, cp, _dp]
+        L.kmy_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class Solver:
+    """One mesh with its device-resident stage containers (one ``kmy_ctx``)."""
+
+    def __init__(self, deck: str | Deck, device: int = 0):
+        text = deck.text() if isinstance(deck, Deck) else deck
+        h = ctypes.c_void_p()
+        rc = lib().kmy_create(text.encode(), device, ctypes.byref(h))
+        if rc:
+            raise KmyError(rc, "kmy_create rejected the deck (see stderr)")
+        self._h = h
+        info = Info()
+        self._check(lib().kmy_get_info(self._h, ctypes.byref(info)))
+        self.info = info
+        self.ndim = info.ndim
+        self.nblocks = info.nblocks
+        self.cell_shape = (info.nblocks, info.ncells_pad[2], info.ncells_pad[1], info.ncells_pad[0])
+        self.face_shape = (info.nblocks, info.nfaces_pad[2], info.nfaces_pad[1], info.nfaces_pad[0])
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().kmy_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise KmyError(rc, lib().kmy_last_error(self._h).decode())
+
+    # --- state ---
+    def _shape(self, var: str):
+        return self.face_shape if var == "mag" else self.cell_shape
+
+    def export(self, var: str, comp: int = 0, container: str = "base") -> np.ndarray:
+        out = np.empty(self._shape(var), dtype=np.float64)
+        self._check(lib().kmy_export_var(self._h, container.encode(), var.encode(), comp,
+                                         _ptr(out), out.size))
+        return out
+
+    def import_(self, var: str, arr, comp: int = 0, container: str = "base") -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        self._check(lib().kmy_import_var(self._h, container.encode(), var.encode(), comp,
+                                         _ptr(a), a.size))
+
+    def finalize_import(self) -> None:
+        self._check(lib().kmy_finalize_import(self._h))
+
+    def pgen(self, problem: str) -> None:
+        self._check(lib().kmy_pgen(self._h, problem.encode()))
+
+    # --- stepping ---
+    def step(self) -> float:
+        dt = ctypes.c_double()
+        self._check(lib().kmy_step(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def evolve(self, tlim: float, nlim: int = -1) -> int:
+        n = ctypes.c_int()
+        self._check(lib().kmy_evolve(self._h, tlim, nlim, ctypes.byref(n)))
+        return n.value
+
+    def rk_stage(self, stage: int, dt: float = -1.0) -> None:
+        self._check(lib().kmy_rk_stage(self._h, stage, dt))
+
+    def task_stage(self, stage: int, dt: float) -> None:
+        self._check(lib().kmy_task_stage(self._h, stage, dt))
+
+    def set_path(self, path: str) -> None:
+        self._check(lib().kmy_set_path(self._h, {"fused": 0, "tasks": 1}[path]))
+
+    def set_dt(self, dt: float) -> None:
+        self._check(lib().kmy_set_dt(self._h, dt))
+
+    def sync(self) -> None:
+        self._check(lib().kmy_sync(self._h))
+
+    @property
+    def time(self) -> dict:
+        t, dt, est = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        n = ctypes.c_int()
+        self._check(lib().kmy_get_time(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(est),
+                                       ctypes.byref(n)))
+        return dict(time=t.value, dt=dt.value, dt_est=est.value, ncycle=n.value)
+
+    # --- per-task entry points ---
+    def compute_fluxes(self, md0: str) -> None:
+        self._check(lib().kmy_compute_fluxes(self._h, md0.encode()))
+
+    def compute_emf(self, md0: str) -> None:
+        self._check(lib().kmy_compute_emf(self._h, md0.encode()))
+
+    def flux_divergence(self, md0: str, dudt: str = "dUdt") -> None:
+        self._check(lib().kmy_flux_divergence(self._h, md0.encode(), dudt.encode()))
+
+    def apply_dudt(self, base: str, md0: str, md1: str, dudt: str, beta: float, dt: float) -> None:
+        self._check(lib().kmy_apply_dudt(self._h, base.encode(), md0.encode(), md1.encode(),
+                                         dudt.encode(), beta, dt))
+
+    def prepare_primitive(self, md1: str) -> None:
+        self._check(lib().kmy_prepare_primitive(self._h, md1.encode()))
+
+    def fill_ghosts(self, md: str = "base") -> None:
+        self._check(lib().kmy_fill_ghosts(self._h, md.encode()))
+
+    def estimate_dt(self, md: str = "base") -> float:
+        out = ctypes.c_double()
+        self._check(lib().kmy_estimate_dt(self._h, md.encode(), ctypes.byref(out)))
+        return out.value
+
+    def fill_derived(self, md: str = "base") -> None:
+        self._check(lib().kmy_fill_derived(self._h, md.encode()))
+
+    # --- diagnostics ---
+    def vortex_error(self, var: str = "dens", comp: int = 0) -> float:
+        out = ctypes.c_double()
+        self._check(lib().kmy_vortex_error(self._h, {"dens": 0, "velocity": 1, "pres": 2}[var], comp,
+                                           ctypes.byref(out)))
+        return out.value
+
+    def conserved_sums(self, md: str = "base") -> np.ndarray:
+        out = np.zeros(self.info.ncons)
+        self._check(lib().kmy_conserved_sums(self._h, md.encode(), _ptr(out)))
+        return out
+
+    @property
+    def launch_count(self) -> int:
+        n = ctypes.c_int64()
+        self._check(lib().kmy_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    def interior(self, arr: np.ndarray) -> np.ndarray:
+        i = self.info
+        g = i.nghost
+        g2 = g if i.ndim > 1 else 0
+        g3 = g if i.ndim > 2 else 0
+        return arr[:, g3:g3 + i.nx[2], g2:g2 + i.nx[1], g:g + i.nx[0]]

@@ -1,0 +1,714 @@
+// kmy_api.cu -- C ABI of libkmy_hydro: contexts, deck parameters, MeshData
+// import/export and the RK driver (stage sequencing + device dt controller).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <sstream>
+
+#include "../../include/kmy_hydro.h"
+#include "kmy_internal.hpp"
+
+using kmy::Container;
+
+namespace kmy {
+
+int cuda_check(kmy_ctx *c, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return KMY_OK;
+  c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return KMY_ERR_OOM;
+  return KMY_ERR_CUDA;
+}
+
+double Params::real(const std::string &k, double d) const {
+  auto it = deck.find(k);
+  return it == deck.end() ? d : std::strtod(it->second.c_str(), nullptr);
+}
+int Params::integer(const std::string &k, int d) const {
+  auto it = deck.find(k);
+  return it == deck.end() ? d : std::atoi(it->second.c_str());
+}
+std::string Params::str(const std::string &k, const std::string &d) const {
+  auto it = deck.find(k);
+  return it == deck.end() ? d : it->second;
+}
+
+// Parthenon input-deck syntax: "<block>" headers, "key = value" lines, '#'
+// comments, and "block/key = value" lines that name their block themselves.
+static void parse_deck(const char *text, std::map<std::string, std::string> &kv) {
+  std::istringstream in(text ? text : "");
+  std::string line, block;
+  auto trim = [](const std::string &s) {
+    size_t a = s.find_first_not_of(" \t\r\n");
+    if (a == std::string::npos) return std::string();
+    size_t b = s.find_last_not_of(" \t\r\n");
+    return s.substr(a, b - a + 1);
+  };
+  while (std::getline(in, line)) {
+    auto hash = line.find('#');
+    if (hash != std::string::npos) line = line.substr(0, hash);
+    line = trim(line);
+    if (line.empty()) continue;
+    if (line.front() == '<' && line.back() == '>') {
+      block = trim(line.substr(1, line.size() - 2));
+      continue;
+    }
+    auto eq = line.find('=');
+    if (eq == std::string::npos) continue;
+    std::string key = trim(line.substr(0, eq)), val = trim(line.substr(eq + 1));
+    if (key.find('/') != std::string::npos) kv[key] = val;
+    else kv[block + "/" + key] = val;
+  }
+}
+
+static int bc_kind(const std::string &s, bool &ok) {
+  if (s == "periodic") return BC_PERIODIC;
+  if (s == "outflow") return BC_OUTFLOW;
+  if (s == "reflect" || s == "reflecting") return BC_REFLECT;
+  ok = false;
+  return BC_OUTFLOW;
+}
+
+static bool one_of(const std::string &v, std::initializer_list<const char *> opts) {
+  for (auto o : opts)
+    if (v == o) return true;
+  return false;
+}
+
+// Validates and fills ctx->prm / ctx->m.  Mirrors the option lists of the
+// reference's AddParm calls (hydro.cpp:55-90, grid.cpp:175-228,
+// kamayan_driver.cpp:25-80, eos.cpp:32-49, physics.cpp:20-23).
+static int setup_params(kmy_ctx *c, const char *deck) {
+  Params &p = c->prm;
+  parse_deck(deck, p.deck);
+  auto bad = [&](const std::string &msg) {
+    c->err = msg;
+    return int(KMY_ERR_BAD_PARAM);
+  };
+  const std::string rc = p.str("hydro/reconstruction", "fog");
+  if (!one_of(rc, {"fog", "plm", "ppm", "wenoz"})) return bad("hydro/reconstruction: " + rc);
+  p.recon = rc == "plm" ? PLM : rc == "ppm" ? PPM : rc == "wenoz" ? WENOZ : FOG;
+  const std::string sl = p.str("hydro/slope_limiter", "minmod");
+  if (!one_of(sl, {"minmod", "van_leer", "mc"})) return bad("hydro/slope_limiter: " + sl);
+  p.limiter = sl == "mc" ? MC : sl == "van_leer" ? VAN_LEER : MINMOD;
+  const std::string rs = p.str("hydro/riemann", "hll");
+  if (!one_of(rs, {"hll", "hllc"})) return bad("hydro/riemann: " + rs);
+  p.riemann = rs == "hllc" ? HLLC : HLL;
+  if (!one_of(p.str("hydro/ReconstructionVars", "primitive"), {"primitive"}))
+    return bad("hydro/ReconstructionVars");
+  if (!one_of(p.str("hydro/ReconstructionStrategy", "scratchpad"), {"scratchpad", "scratchvar"}))
+    return bad("hydro/ReconstructionStrategy");
+  if (!one_of(p.str("hydro/EMF_averaging", "arithmetic"), {"arithmetic"}))
+    return bad("hydro/EMF_averaging");
+  p.cfl = p.real("hydro/cfl", 0.8);
+  const std::string mhd = p.str("physics/MHD", "off");
+  if (!one_of(mhd, {"off", "ct"})) return bad("physics/MHD: " + mhd);
+  p.mhd = mhd == "ct";
+  if (p.str("physics/fluid", "oneT") != "oneT") return bad("physics/fluid: only oneT is implemented");
+  if (p.str("geometry/geometry", "cartesian") != "cartesian")
+    return bad("geometry/geometry: only cartesian is supported");
+  if (p.str("material/single/eos_type", "gamma") != "gamma") return bad("material/single/eos_type");
+  if (!one_of(p.str("eos/mode_init", "dens_pres"), {"dens_pres"}))
+    return bad("eos/mode_init: only dens_pres is supported");
+  p.gamma = p.real("material/single/gamma", 5.0 / 3.0);
+  p.Abar = p.real("material/single/Abar", 1.0);
+  const std::string prec = p.str("kamayan_b200/precision", "fp64");
+  if (!one_of(prec, {"fp64", "fp32"})) return bad("kamayan_b200/precision: " + prec);
+  p.precision = prec == "fp32" ? 32 : 64;
+
+  const std::string integ = p.str("parthenon/time/integrator", "rk2");
+  if (integ == "rk1") p.beta = {1.0};
+  else if (integ == "rk2") p.beta = {1.0, 0.5};
+  else if (integ == "rk3") p.beta = {1.0, 0.25, 2.0 / 3.0};
+  else return bad("parthenon/time/integrator: " + integ);
+  const int ns = int(p.beta.size());
+  p.stage_name.assign(ns + 1, "base");
+  for (int s = 1; s < ns; s++) p.stage_name[s] = std::to_string(s);
+
+  const double big = std::numeric_limits<double>::max();
+  p.tp.tlim = p.real("parthenon/time/tlim", big);
+  p.tp.nlim = p.integer("parthenon/time/nlim", -1);
+  p.tp.dt_factor = p.real("parthenon/time/dt_factor", 2.0);
+  p.tp.dt_init = p.real("parthenon/time/dt_init", big);
+  p.tp.dt_ceil = p.real("parthenon/time/dt_ceil", big);
+  p.tp.dt_user = p.real("parthenon/time/dt_user", big);
+  p.tp.dt_floor = p.real("parthenon/time/dt_floor", std::numeric_limits<double>::min());
+
+  const std::string refine = p.str("parthenon/mesh/refinement", "none");
+  if (!one_of(refine, {"none", "static", "adaptive"})) return bad("parthenon/mesh/refinement");
+  if (refine != "none" && p.integer("parthenon/mesh/numlevel", 1) > 1)
+    return bad("parthenon/mesh/refinement: multi-level meshes use the AMR entry points");
+
+  MeshDesc &m = c->m;
+  const char *ax[3] = {"1", "2", "3"};
+  for (int i = 0; i < 3; i++) {
+    m.mesh_nx[i] = p.integer(std::string("parthenon/mesh/nx") + ax[i], 32);
+    m.nx[i] = p.integer(std::string("parthenon/meshblock/nx") + ax[i], m.mesh_nx[i]);
+    m.xmin[i] = p.real(std::string("parthenon/mesh/x") + ax[i] + "min", 0.0);
+    const double xmax = p.real(std::string("parthenon/mesh/x") + ax[i] + "max", 1.0);
+    bool ok = true;
+    m.bc[i][0] = bc_kind(p.str(std::string("parthenon/mesh/ix") + ax[i] + "_bc", "outflow"), ok);
+    m.bc[i][1] = bc_kind(p.str(std::string("parthenon/mesh/ox") + ax[i] + "_bc", "outflow"), ok);
+    if (!ok) return bad(std::string("parthenon/mesh boundary condition along x") + ax[i]);
+    m.dx[i] = xmax - m.xmin[i];  // divided below
+  }
+  m.ndim = m.mesh_nx[2] > 1 ? 3 : (m.mesh_nx[1] > 1 ? 2 : 1);
+  for (int i = m.ndim; i < 3; i++) m.nx[i] = m.mesh_nx[i] = 1;
+  const int ng = p.integer("parthenon/mesh/nghost", 4);
+  const int need = ReconWidthRuntime(p.recon) + 1 + (p.mhd ? 1 : 0);
+  if (ng < need) return bad("parthenon/mesh/nghost too small for the reconstruction");
+  m.nb = 1;
+  for (int i = 0; i < 3; i++) {
+    if (m.nx[i] <= 0 || m.mesh_nx[i] % m.nx[i] != 0)
+      return bad("parthenon/mesh nx must be a multiple of parthenon/meshblock nx");
+    if (i < m.ndim && m.nx[i] < ng) return bad("meshblock smaller than nghost");
+    if ((m.bc[i][0] == BC_PERIODIC) != (m.bc[i][1] == BC_PERIODIC))
+      return bad("periodic boundaries must be periodic on both sides");
+    m.nbx[i] = m.mesh_nx[i] / m.nx[i];
+    m.nb *= m.nbx[i];
+    m.g[i] = i < m.ndim ? ng : 0;
+    m.np[i] = m.nx[i] + 2 * m.g[i];
+    m.nf[i] = m.np[i] + (i < m.ndim ? 1 : 0);
+    m.dx[i] = m.dx[i] / double(m.mesh_nx[i]);
+  }
+  m.P = (long long)m.np[0] * m.np[1] * m.np[2];
+  m.Pf = (long long)m.nf[0] * m.nf[1] * m.nf[2];
+  m.area[0] = m.dx[1] * m.dx[2];
+  m.area[1] = m.dx[0] * m.dx[2];
+  m.area[2] = m.dx[0] * m.dx[1];
+  m.vol = m.dx[0] * m.dx[1] * m.dx[2];
+  p.tp.cfl_over_ndim = p.cfl / double(m.ndim);
+
+  const double kboltz = 1.380649e-16;
+  c->eos.cv = p.gamma * kboltz / p.Abar;
+  c->eos.gm1 = p.gamma - 1.0;
+  c->ncc = p.mhd ? 8 : 5;
+  c->esz = p.precision == 32 ? 4 : 8;
+  return KMY_OK;
+}
+
+static int dalloc(kmy_ctx *c, void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return KMY_OK;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "cudaMalloc of " + std::to_string(bytes) + " bytes failed";
+    return KMY_ERR_OOM;
+  }
+  c->allocations.push_back(*p);
+  return cuda_check(c, cudaMemsetAsync(*p, 0, bytes, c->stream), "memset");
+}
+
+static int make_container(kmy_ctx *c, const std::string &name) {
+  Container ct;
+  const MeshDesc &m = c->m;
+  const size_t n = size_t(m.nb) * m.P, nf = size_t(m.nb) * m.Pf;
+  int rc = dalloc(c, &ct.cc, c->esz * c->ncc * n);
+  if (!rc && c->esz == 4) rc = dalloc(c, &ct.ener_lo, 4 * n);
+  if (!rc && c->prm.mhd) rc = dalloc(c, &ct.fc, c->esz * 3 * nf);
+  if (!rc && c->prm.mhd) rc = dalloc(c, &ct.emf, c->esz * 3 * nf);
+  if (rc) return rc;
+  c->md[name] = ct;
+  return KMY_OK;
+}
+
+}  // namespace kmy
+
+using namespace kmy;
+
+static Container *find_container(kmy_ctx *c, const char *name) {
+  auto it = c->md.find(name ? name : "");
+  if (it == c->md.end()) {
+    c->err = std::string("unknown container ") + (name ? name : "(null)");
+    return nullptr;
+  }
+  return &it->second;
+}
+
+// ----------------------------------------------------------------------------
+// staging conversions between host doubles and device storage
+__global__ void k_store_cells(const double *src, void *dst, float *lo, size_t n, int f32) {
+  size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const double v = src[i];
+  if (f32) {
+    const float hi = float(v);
+    static_cast<float *>(dst)[i] = hi;
+    if (lo) lo[i] = float(v - double(hi));
+  } else {
+    static_cast<double *>(dst)[i] = v;
+  }
+}
+__global__ void k_load_cells(const void *src, const float *lo, double *dst, size_t n, int f32) {
+  size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  if (f32) {
+    double v = double(static_cast<const float *>(src)[i]);
+    if (lo) v += double(lo[i]);
+    dst[i] = v;
+  } else {
+    dst[i] = static_cast<const double *>(src)[i];
+  }
+}
+
+// Resolve (container, var, comp) to device storage.
+struct VarRef {
+  void *p = nullptr;
+  float *lo = nullptr;
+  bool is_double = false;
+  size_t n = 0;
+};
+
+static int resolve(kmy_ctx *c, const char *container, const char *var, int comp, VarRef &r) {
+  const MeshDesc &m = c->m;
+  const size_t n = size_t(m.nb) * m.P, nf = size_t(m.nb) * m.Pf;
+  const std::string v(var ? var : "");
+  auto shared = [&](int slot) {
+    r.p = static_cast<char *>(c->prim) + c->esz * n * slot;
+    r.n = n;
+    return int(KMY_OK);
+  };
+  if (v == "velocity" && comp >= 0 && comp < 3) return shared(PVEL0 + comp);
+  if (v == "pres") return shared(PPRES);
+  if (v == "bulk modulus") return shared(PBMOD);
+  if (v == "eint") return shared(PEINT);
+  if (v == "temp") return shared(PTEMP);
+  if (v == "divb" && c->prm.mhd) {
+    r.p = c->divb;
+    r.is_double = true;
+    r.n = n;
+    return KMY_OK;
+  }
+  Container *ct = find_container(c, container);
+  if (!ct) return KMY_ERR_BAD_PARAM;
+  auto cell = [&](int slot) {
+    r.p = static_cast<char *>(ct->cc) + c->esz * n * slot;
+    r.n = n;
+    return int(KMY_OK);
+  };
+  if (v == "dens") return cell(CDENS);
+  if (v == "momentum" && comp >= 0 && comp < 3) return cell(CMOM0 + comp);
+  if (v == "ener") {
+    r.lo = static_cast<float *>(ct->ener_lo);
+    return cell(CENER);
+  }
+  if (v == "magc" && c->prm.mhd && comp >= 0 && comp < 3) return cell(CMAGC0 + comp);
+  if (v == "mag" && c->prm.mhd && comp >= 0 && comp < 3) {
+    r.p = static_cast<char *>(ct->fc) + c->esz * nf * comp;
+    r.n = nf;
+    return KMY_OK;
+  }
+  c->err = "unknown variable " + v + " (comp " + std::to_string(comp) + ")";
+  return KMY_ERR_BAD_PARAM;
+}
+
+// Materialise the reference-visible state of "base" after fused steps:
+// primitives from PreparePrimitive and filled ghosts.
+static int materialize(kmy_ctx *c) {
+  if (c->prims_valid) return KMY_OK;
+  Container &b = c->md["base"];
+  int rc = launch_prepare_primitive(c, b);
+  if (!rc) rc = launch_fill_ghosts(c, b);
+  if (!rc) c->prims_valid = true;
+  return rc;
+}
+
+extern "C" {
+
+int kmy_create(const char *deck, int device, kmy_ctx **out) {
+  if (!out) return KMY_ERR_BAD_PARAM;
+  *out = nullptr;
+  auto *c = new kmy_ctx();
+  c->device = device;
+  int rc = setup_params(c, deck);
+  if (rc) {
+    std::fprintf(stderr, "kmy_create: %s\n", c->err.c_str());
+    delete c;
+    return rc;
+  }
+  rc = cuda_check(c, cudaSetDevice(device), "cudaSetDevice");
+  if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+  if (rc) {
+    std::fprintf(stderr, "kmy_create: %s\n", c->err.c_str());
+    delete c;
+    return rc;
+  }
+  c->own_stream = true;
+  const size_t n = size_t(c->m.nb) * c->m.P;
+  for (size_t s = 0; s + 1 < c->prm.stage_name.size() && !rc; s++)
+    if (!c->md.count(c->prm.stage_name[s])) rc = make_container(c, c->prm.stage_name[s]);
+  if (!rc) rc = make_container(c, "dUdt");
+  if (!rc) rc = dalloc(c, &c->prim, c->esz * NPRIM * n);
+  if (!rc && c->prm.mhd) rc = dalloc(c, reinterpret_cast<void **>(&c->divb), 8 * n);
+  if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&c->clock), sizeof(DevClock));
+  if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&c->scratch), 8 * 64);
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "create sync");
+  if (rc) {
+    std::fprintf(stderr, "kmy_create: %s\n", c->err.c_str());
+    kmy_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return KMY_OK;
+}
+
+int kmy_destroy(kmy_ctx *c) {
+  if (!c) return KMY_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void *p : c->allocations) cudaFree(p);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return KMY_OK;
+}
+
+const char *kmy_last_error(const kmy_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int kmy_get_info(const kmy_ctx *c, kmy_info *o) {
+  if (!c || !o) return KMY_ERR_BAD_PARAM;
+  const MeshDesc &m = c->m;
+  o->ndim = m.ndim;
+  o->nblocks = m.nb;
+  for (int i = 0; i < 3; i++) {
+    o->nx[i] = m.nx[i];
+    o->ncells_pad[i] = m.np[i];
+    o->nfaces_pad[i] = m.nf[i];
+    o->nblocks_dim[i] = m.nbx[i];
+    o->xmin[i] = m.xmin[i];
+    o->dx[i] = m.dx[i];
+    o->xmax[i] = m.xmin[i] + m.dx[i] * m.mesh_nx[i];
+  }
+  o->nghost = m.g[0];
+  o->ncons = c->ncc;
+  o->mhd = c->prm.mhd ? 1 : 0;
+  o->nstages = int(c->prm.beta.size());
+  o->precision = c->prm.precision;
+  return KMY_OK;
+}
+
+int kmy_set_stream(kmy_ctx *c, void *s) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  if (s) {
+    cudaStreamSynchronize(c->stream);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    c->stream = static_cast<cudaStream_t>(s);
+    c->own_stream = false;
+  }
+  return KMY_OK;
+}
+
+int kmy_sync(kmy_ctx *c) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+}
+
+int kmy_import_var(kmy_ctx *c, const char *container, const char *var, int comp,
+                   const double *host, size_t n) {
+  if (!c || !host) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  VarRef r;
+  int rc = resolve(c, container, var, comp, r);
+  if (rc) return rc;
+  if (n != r.n) {
+    c->err = "size mismatch: expected " + std::to_string(r.n);
+    return KMY_ERR_BAD_PARAM;
+  }
+  if (r.is_double || c->esz == 8)
+    return cuda_check(c, cudaMemcpyAsync(r.p, host, n * 8, cudaMemcpyHostToDevice, c->stream),
+                      "import copy") ||
+           cuda_check(c, cudaStreamSynchronize(c->stream), "import sync");
+  double *stage = nullptr;
+  rc = cuda_check(c, cudaMallocAsync(reinterpret_cast<void **>(&stage), n * 8, c->stream), "stage");
+  if (rc) return rc;
+  rc = cuda_check(c, cudaMemcpyAsync(stage, host, n * 8, cudaMemcpyHostToDevice, c->stream), "import");
+  if (!rc) {
+    k_store_cells<<<unsigned((n + 255) / 256), 256, 0, c->stream>>>(stage, r.p, r.lo, n, 1);
+    c->launches++;
+    rc = cuda_check(c, cudaGetLastError(), "k_store_cells");
+  }
+  cudaFreeAsync(stage, c->stream);
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "import sync");
+  c->prims_valid = true;
+  return rc;
+}
+
+int kmy_export_var(kmy_ctx *c, const char *container, const char *var, int comp, double *host,
+                   size_t n) {
+  if (!c || !host) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  VarRef r;
+  int rc = resolve(c, container, var, comp, r);
+  if (rc) return rc;
+  if (n != r.n) {
+    c->err = "size mismatch: expected " + std::to_string(r.n);
+    return KMY_ERR_BAD_PARAM;
+  }
+  rc = materialize(c);
+  if (rc) return rc;
+  if (r.is_double || c->esz == 8)
+    return cuda_check(c, cudaMemcpyAsync(host, r.p, n * 8, cudaMemcpyDeviceToHost, c->stream),
+                      "export copy") ||
+           cuda_check(c, cudaStreamSynchronize(c->stream), "export sync");
+  double *stage = nullptr;
+  rc = cuda_check(c, cudaMallocAsync(reinterpret_cast<void **>(&stage), n * 8, c->stream), "stage");
+  if (rc) return rc;
+  k_load_cells<<<unsigned((n + 255) / 256), 256, 0, c->stream>>>(r.p, r.lo, stage, n, 1);
+  c->launches++;
+  rc = cuda_check(c, cudaGetLastError(), "k_load_cells");
+  if (!rc) rc = cuda_check(c, cudaMemcpyAsync(host, stage, n * 8, cudaMemcpyDeviceToHost, c->stream), "export");
+  cudaFreeAsync(stage, c->stream);
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "export sync");
+  return rc;
+}
+
+int kmy_finalize_import(kmy_ctx *c) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  Container &b = c->md["base"];
+  int rc = launch_fill_ghosts(c, b);
+  if (!rc && c->prm.mhd) rc = launch_fill_derived(c, b);
+  if (!rc) rc = launch_estimate_dt(c, b, true);
+  if (!rc) rc = launch_dt_controller(c, 1);
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "finalize");
+  c->prims_valid = true;
+  return rc;
+}
+
+int kmy_pgen(kmy_ctx *c, const char *problem) {
+  if (!c || !problem) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  int rc = launch_pgen(c, problem);
+  if (rc) return rc;
+  Container &b = c->md["base"];
+  rc = launch_eos_init(c, b);
+  if (!rc) rc = launch_convert_to_conserved(c, b);
+  if (!rc) rc = launch_fill_ghosts(c, b);
+  if (!rc && c->prm.mhd) rc = launch_fill_derived(c, b);
+  if (!rc) rc = launch_estimate_dt(c, b, true);
+  if (!rc) rc = launch_dt_controller(c, 1);
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "pgen");
+  c->prims_valid = true;
+  return rc;
+}
+
+#define KMY_CONTAINER(var, name)          \
+  Container *var = find_container(c, name); \
+  if (!var) return KMY_ERR_BAD_PARAM;
+
+int kmy_compute_fluxes(kmy_ctx *c, const char *md0) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  KMY_CONTAINER(a, md0);
+  return launch_compute_fluxes(c, *a);
+}
+int kmy_compute_emf(kmy_ctx *c, const char *md0) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  KMY_CONTAINER(a, md0);
+  return launch_compute_emf(c, *a);
+}
+int kmy_flux_divergence(kmy_ctx *c, const char *md0, const char *dudt) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  KMY_CONTAINER(a, md0);
+  KMY_CONTAINER(d, dudt);
+  return launch_flux_divergence(c, *a, *d);
+}
+int kmy_apply_dudt(kmy_ctx *c, const char *base, const char *md0, const char *md1,
+                   const char *dudt, double beta, double dt) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  KMY_CONTAINER(b, base);
+  KMY_CONTAINER(a0, md0);
+  KMY_CONTAINER(a1, md1);
+  KMY_CONTAINER(d, dudt);
+  return launch_apply_dudt(c, *b, *a0, *a1, *d, beta, dt, nullptr);
+}
+int kmy_prepare_primitive(kmy_ctx *c, const char *md1) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  KMY_CONTAINER(a, md1);
+  return launch_prepare_primitive(c, *a);
+}
+int kmy_fill_ghosts(kmy_ctx *c, const char *md) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  KMY_CONTAINER(a, md);
+  return launch_fill_ghosts(c, *a);
+}
+int kmy_estimate_dt(kmy_ctx *c, const char *md, double *dt_out) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  KMY_CONTAINER(a, md);
+  int rc = launch_estimate_dt(c, *a, true);
+  if (rc) return rc;
+  DevClock h;
+  rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "dt");
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "dt sync");
+  if (rc) return rc;
+  double dtmin;
+  std::memcpy(&dtmin, &h.dtmin_bits, 8);
+  if (dt_out) *dt_out = dtmin * c->prm.tp.cfl_over_ndim;
+  return KMY_OK;
+}
+int kmy_fill_derived(kmy_ctx *c, const char *md) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  KMY_CONTAINER(a, md);
+  return launch_fill_derived(c, *a);
+}
+
+// One stage through the per-task kernels, reference task order.  dt is read
+// from the device clock when dt < 0.
+static int task_stage(kmy_ctx *c, int stage, double dt) {
+  const auto &nm = c->prm.stage_name;
+  const int ns = int(c->prm.beta.size());
+  Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
+  Container &du = c->md["dUdt"];
+  if (!c->prims_valid) {
+    // primitives of md0 are needed with ghosts (fused steps leave them stale)
+    int rc = launch_prepare_primitive(c, md0);
+    if (!rc) rc = launch_fill_ghosts(c, md0);
+    if (rc) return rc;
+    c->prims_valid = true;
+  }
+  int rc = launch_compute_fluxes(c, md0);
+  if (!rc) rc = launch_compute_emf(c, md0);
+  if (!rc) rc = launch_flux_divergence(c, md0, du);
+  if (!rc) rc = launch_apply_dudt(c, base, md0, md1, du, c->prm.beta[stage - 1], dt,
+                                  dt < 0 ? &c->clock->dt : nullptr);
+  if (!rc) rc = launch_prepare_primitive(c, md1);
+  if (!rc && stage == ns) {
+    rc = launch_estimate_dt(c, base, true);
+    if (!rc && c->prm.mhd) rc = launch_fill_derived(c, base);
+  }
+  if (!rc) rc = launch_fill_ghosts(c, md1);
+  return rc;
+}
+
+int kmy_task_stage(kmy_ctx *c, int stage, double dt) {
+  if (!c || stage < 1 || stage > int(c->prm.beta.size())) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  return task_stage(c, stage, dt);
+}
+
+static int fused_stage(kmy_ctx *c, int stage) {
+  const auto &nm = c->prm.stage_name;
+  const int ns = int(c->prm.beta.size());
+  Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
+  const bool stored = stage == 1 && c->prims_valid;
+  int rc = launch_fused_stage(c, base, md0, md1, c->prm.beta[stage - 1], stored, stage == ns);
+  c->prims_valid = false;
+  return rc;
+}
+
+int kmy_rk_stage(kmy_ctx *c, int stage, double dt) {
+  if (!c || stage < 1 || stage > int(c->prm.beta.size())) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  if (dt >= 0) {
+    int rc = cuda_check(c, cudaMemcpyAsync(&c->clock->dt, &dt, 8, cudaMemcpyHostToDevice, c->stream), "dt");
+    if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "dt sync");
+    if (rc) return rc;
+  }
+  if (c->prm.mhd) {
+    c->err = "the fused stage covers hydro; use kmy_task_stage for constrained transport";
+    return KMY_ERR_BAD_PARAM;
+  }
+  return fused_stage(c, stage);
+}
+
+static int step_async(kmy_ctx *c) {
+  const int ns = int(c->prm.beta.size());
+  int rc = KMY_OK;
+  const bool fused = c->path == 0 && !c->prm.mhd;
+  for (int s = 1; s <= ns && !rc; s++) rc = fused ? fused_stage(c, s) : task_stage(c, s, -1.0);
+  if (!rc) rc = launch_dt_controller(c, 0);
+  return rc;
+}
+
+int kmy_step(kmy_ctx *c, double *dt_taken) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  int rc = step_async(c);
+  if (rc) return rc;
+  DevClock h;
+  rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "step");
+  if (rc) return rc;
+  if (dt_taken) *dt_taken = h.dt_taken;
+  if (h.status) {
+    c->err = "non-finite or non-positive time-step estimate";
+    return KMY_ERR_NONFINITE;
+  }
+  return KMY_OK;
+}
+
+int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  c->prm.tp.tlim = tlim;
+  int rc = launch_dt_controller(c, 2);  // clamp the pending dt to tlim
+  int n = 0;
+  DevClock h{};
+  while (!rc) {
+    const int chunk = 8;
+    for (int i = 0; i < chunk && !rc && (nlim < 0 || n < nlim); i++, n++) rc = step_async(c);
+    if (rc) break;
+    rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
+    if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "evolve");
+    if (rc) break;
+    if (h.status) {
+      c->err = "non-finite or non-positive time-step estimate";
+      rc = KMY_ERR_NONFINITE;
+      break;
+    }
+    if (h.done || (nlim >= 0 && n >= nlim)) break;
+  }
+  if (nsteps) *nsteps = h.ncycle;
+  return rc;
+}
+
+int kmy_get_time(const kmy_ctx *c, double *time, double *dt, double *dt_est, int *ncycle) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  DevClock h;
+  cudaError_t e = cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return KMY_ERR_CUDA;
+  if (time) *time = h.time;
+  if (dt) *dt = h.dt;
+  if (dt_est) *dt_est = h.dt_est;
+  if (ncycle) *ncycle = h.ncycle;
+  return KMY_OK;
+}
+
+int kmy_set_dt(kmy_ctx *c, double dt) {
+  if (!c || !(dt > 0)) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  int rc = cuda_check(c, cudaMemcpyAsync(&c->clock->dt, &dt, 8, cudaMemcpyHostToDevice, c->stream), "dt");
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "dt");
+  return rc;
+}
+
+int kmy_set_path(kmy_ctx *c, int path) {
+  if (!c || (path != 0 && path != 1)) return KMY_ERR_BAD_PARAM;
+  c->path = path;
+  return KMY_OK;
+}
+
+int kmy_vortex_error(kmy_ctx *c, int var, int comp, double *out) {
+  if (!c || !out || var < 0 || var > 2) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  int rc = materialize(c);
+  if (!rc) rc = launch_vortex_error(c, var, comp, out);
+  return rc;
+}
+
+int kmy_conserved_sums(kmy_ctx *c, const char *md, double *out) {
+  if (!c || !out) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  KMY_CONTAINER(a, md);
+  return launch_conserved_sums(c, *a, out);
+}
+
+int kmy_launch_count(const kmy_ctx *c, int64_t *out) {
+  if (!c || !out) return KMY_ERR_BAD_PARAM;
+  *out = c->launches;
+  return KMY_OK;
+}
+
+}  // extern "C"

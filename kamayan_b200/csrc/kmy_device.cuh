@@ -1,0 +1,404 @@
+// kmy_device.cuh -- per-cell / per-face arithmetic of the hydro update.
+//
+// Device restatements of the reference's inline functions, templated on the
+// arithmetic type R (double for the FP64 path, float for the FP32 bulk path).
+// Expressions keep the reference's operation order; nvcc may contract a*b+c
+// into FMA, which moves results by at most an ulp per operation.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+namespace kmy {
+
+enum Recon : int { FOG = 0, PLM = 1, PPM = 2, WENOZ = 3 };
+enum Limiter : int { MINMOD = 0, VAN_LEER = 1, MC = 2 };
+enum RiemannSolver : int { HLL = 0, HLLC = 1 };
+enum BoundaryKind : int { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2 };
+
+// slots of a conserved state
+enum : int { CDENS = 0, CMOM0 = 1, CMOM1 = 2, CMOM2 = 3, CENER = 4, CMAGC0 = 5 };
+// slots of a reconstructed (primitive) state, hydro_types.hpp:61-77 order
+enum : int { RDENS = 0, RVEL0 = 1, RVEL1 = 2, RVEL2 = 3, RPRES = 4, RBMOD = 5, REINT = 6, RMAGC0 = 7 };
+// shared primitive arrays in device storage (density lives with the conserved)
+enum : int { PVEL0 = 0, PVEL1 = 1, PVEL2 = 2, PPRES = 3, PBMOD = 4, PEINT = 5, PTEMP = 6, NPRIM = 7 };
+
+template <typename R> struct Lim;
+template <> struct Lim<double> {
+  static __host__ __device__ constexpr double tiny() { return DBL_MIN; }
+};
+template <> struct Lim<float> {
+  static __host__ __device__ constexpr float tiny() { return FLT_MIN; }
+};
+
+template <typename R> __device__ __forceinline__ R kmin(R a, R b) { return (b < a) ? b : a; }
+template <typename R> __device__ __forceinline__ R kmax(R a, R b) { return (a < b) ? b : a; }
+template <typename R> __device__ __forceinline__ R sq(R x) { return x * x; }
+
+// reconstruction.hpp:24-39
+template <typename R>
+__device__ __forceinline__ R LimitedSlope(int limiter, R a, R b) {
+  if (limiter == MC) {
+    return (copysign(R(1), a) + copysign(R(1), b)) *
+           kmin(fabs(a), kmin(R(.25) * fabs(a + b), fabs(b)));
+  } else if (limiter == VAN_LEER) {
+    if (a * b > R(0)) return R(2) * a * b / (a + b);
+    return R(0);
+  }
+  return R(0.5) * (copysign(R(1), a) + copysign(R(1), b)) * kmin(fabs(a), fabs(b));
+}
+
+// Stencil half-width each reconstruction reads (cells c-W .. c+W).
+template <int RECON> struct ReconWidth { static constexpr int value = 0; };
+template <> struct ReconWidth<PLM> { static constexpr int value = 1; };
+template <> struct ReconWidth<PPM> { static constexpr int value = 2; };
+template <> struct ReconWidth<WENOZ> { static constexpr int value = 2; };
+
+__host__ __device__ inline int ReconWidthRuntime(int recon) {
+  return recon == FOG ? 0 : recon == PLM ? 1 : 2;
+}
+
+// reconstruction.hpp:11-142: both face values of the cell at s[0] (s indexed
+// -W..W through the pointer arithmetic of the caller: s[o] = value at c+o).
+template <int RECON, typename R>
+__device__ __forceinline__ void Reconstruct(int limiter, const R (&s)[5], R &vM, R &vP) {
+  // s[0..4] hold offsets -2..2
+  const R s0 = s[2];
+  if constexpr (RECON == FOG) {
+    vM = s0;
+    vP = s0;
+  } else if constexpr (RECON == PLM) {
+    const R dvL = s0 - s[1];
+    const R dvR = s[3] - s0;
+    const R del = LimitedSlope(limiter, dvL, dvR);
+    vM = s0 - R(0.5) * del;
+    vP = s0 + R(0.5) * del;
+  } else if constexpr (RECON == PPM) {
+    const R dv_p = LimitedSlope(limiter, s[4] - s[3], s[3] - s0);
+    const R dv_0 = LimitedSlope(limiter, s[3] - s0, s0 - s[1]);
+    const R dv_m = LimitedSlope(limiter, s0 - s[1], s[1] - s[0]);
+    const R sixth = R(1.) / R(6.);
+    vM = R(0.5) * (s[1] + s0) - sixth * (dv_0 - dv_m);
+    vP = R(0.5) * (s0 + s[3]) - sixth * (dv_p - dv_0);
+    if ((vP - s0) * (s0 - vM) <= R(0)) {
+      vM = s0;
+      vP = s0;
+    }
+    if (-(vP - vM) * (vP - vM) > R(6) * (vP - vM) * (s0 - R(0.5) * (vP + vM))) {
+      vP = R(3) * s0 - R(2) * vM;
+    }
+    if ((vP - vM) * (vP - vM) < R(6) * (vP - vM) * (s0 - R(0.5) * (vP + vM))) {
+      vM = R(3) * s0 - R(2) * vP;
+    }
+  } else {
+    const R sixth = R(1.) / R(6.);
+    // eno predictions at +1/2 (pm=+1) and -1/2 (pm=-1)
+    const R ep0 = sixth * (-s[4] + R(5) * s[3] + R(2) * s0);
+    const R ep1 = sixth * (R(2) * s[3] + R(5) * s0 - s[1]);
+    const R ep2 = sixth * (R(11) * s0 - R(7) * s[1] + R(2) * s[0]);
+    const R em0 = sixth * (-s[0] + R(5) * s[1] + R(2) * s0);
+    const R em1 = sixth * (R(2) * s[1] + R(5) * s0 - s[3]);
+    const R em2 = sixth * (R(11) * s0 - R(7) * s[3] + R(2) * s[4]);
+    const R c1312 = R(13.) / R(12.);
+    const R b0 = c1312 * sq(s[0] - R(2) * s[1] + s0) + R(0.25) * sq(s[0] - R(4) * s[1] + R(3) * s0);
+    const R b1 = c1312 * sq(s[1] - R(2) * s0 + s[3]) + R(0.25) * sq(s[1] - s[3]);
+    const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
+    const R eps = R(1.e-36);
+    const R tau = fabs(b2 - b0);
+    const R q0 = R(1) + sq(tau / (eps + b0));
+    const R q1 = R(1) + sq(tau / (eps + b1));
+    const R q2 = R(1) + sq(tau / (eps + b2));
+    {  // pm = -1: w0 uses beta0, w2 uses beta2
+      const R w0 = R(3) * q0, w1 = R(6) * q1, w2 = R(1) * q2;
+      const R norm = w0 + w1 + w2;
+      vM = (w0 * em0 + w1 * em1 + w2 * em2) / norm;
+    }
+    {  // pm = +1: w0 uses beta2, w2 uses beta0
+      const R w0 = R(3) * q2, w1 = R(6) * q1, w2 = R(1) * q0;
+      const R norm = w0 + w1 + w2;
+      vP = (w0 * ep0 + w1 * ep1 + w2 * ep2) / norm;
+    }
+  }
+}
+
+// Value at the plus face only (for the cell left of a face).
+template <int RECON, typename R>
+__device__ __forceinline__ R ReconstructPlus(int limiter, const R (&s)[5]) {
+  if constexpr (RECON == WENOZ) {
+    const R s0 = s[2];
+    const R sixth = R(1.) / R(6.);
+    const R ep0 = sixth * (-s[4] + R(5) * s[3] + R(2) * s0);
+    const R ep1 = sixth * (R(2) * s[3] + R(5) * s0 - s[1]);
+    const R ep2 = sixth * (R(11) * s0 - R(7) * s[1] + R(2) * s[0]);
+    const R c1312 = R(13.) / R(12.);
+    const R b0 = c1312 * sq(s[0] - R(2) * s[1] + s0) + R(0.25) * sq(s[0] - R(4) * s[1] + R(3) * s0);
+    const R b1 = c1312 * sq(s[1] - R(2) * s0 + s[3]) + R(0.25) * sq(s[1] - s[3]);
+    const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
+    const R eps = R(1.e-36);
+    const R tau = fabs(b2 - b0);
+    const R w0 = R(3) * (R(1) + sq(tau / (eps + b2)));
+    const R w1 = R(6) * (R(1) + sq(tau / (eps + b1)));
+    const R w2 = R(1) * (R(1) + sq(tau / (eps + b0)));
+    const R norm = w0 + w1 + w2;
+    return (w0 * ep0 + w1 * ep1 + w2 * ep2) / norm;
+  } else {
+    R vM, vP;
+    Reconstruct<RECON, R>(limiter, s, vM, vP);
+    return vP;
+  }
+}
+
+// Value at the minus face only (for the cell right of a face).
+template <int RECON, typename R>
+__device__ __forceinline__ R ReconstructMinus(int limiter, const R (&s)[5]) {
+  if constexpr (RECON == WENOZ) {
+    const R s0 = s[2];
+    const R sixth = R(1.) / R(6.);
+    const R em0 = sixth * (-s[0] + R(5) * s[1] + R(2) * s0);
+    const R em1 = sixth * (R(2) * s[1] + R(5) * s0 - s[3]);
+    const R em2 = sixth * (R(11) * s0 - R(7) * s[3] + R(2) * s[4]);
+    const R c1312 = R(13.) / R(12.);
+    const R b0 = c1312 * sq(s[0] - R(2) * s[1] + s0) + R(0.25) * sq(s[0] - R(4) * s[1] + R(3) * s0);
+    const R b1 = c1312 * sq(s[1] - R(2) * s0 + s[3]) + R(0.25) * sq(s[1] - s[3]);
+    const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
+    const R eps = R(1.e-36);
+    const R tau = fabs(b2 - b0);
+    const R w0 = R(3) * (R(1) + sq(tau / (eps + b0)));
+    const R w1 = R(6) * (R(1) + sq(tau / (eps + b1)));
+    const R w2 = R(1) * (R(1) + sq(tau / (eps + b2)));
+    const R norm = w0 + w1 + w2;
+    return (w0 * em0 + w1 * em1 + w2 * em2) / norm;
+  } else {
+    R vM, vP;
+    Reconstruct<RECON, R>(limiter, s, vM, vP);
+    return vM;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// primconsflux.hpp:21-138 on register states.  V: reconstructed layout
+// (RDENS..REINT [+RMAGC0..2]); U/F: conserved layout (CDENS..CENER [+CMAGC0..2]).
+template <bool MHD, typename R>
+__device__ __forceinline__ R TotalPres(const R *V) {
+  R pres = V[RPRES];
+  if constexpr (MHD) {
+    pres += R(0.5) * (V[RMAGC0] * V[RMAGC0] + V[RMAGC0 + 1] * V[RMAGC0 + 1] +
+                      V[RMAGC0 + 2] * V[RMAGC0 + 2]);
+  }
+  return pres;
+}
+
+template <bool MHD, typename R>
+__device__ __forceinline__ R FastSpeed(int dir1, const R *V) {
+  const R idens = R(1.) / V[RDENS];
+  const R a2 = idens * V[RBMOD];
+  R cfast2;
+  if constexpr (!MHD) {
+    cfast2 = a2;
+  } else {
+    const R bb2 = V[RMAGC0 + dir1] * V[RMAGC0 + dir1] * idens;
+    R b2 = R(0);
+    for (int dir = 0; dir < 3; dir++) b2 += V[RMAGC0 + dir] * V[RMAGC0 + dir];
+    b2 *= idens;
+    cfast2 = R(0.5) * ((a2 + b2) + sqrt((a2 - b2) * (a2 - b2) + R(4) * a2 * (b2 - bb2)));
+  }
+  return sqrt(cfast2);
+}
+
+template <bool MHD, typename R>
+__device__ __forceinline__ void Prim2Cons(const R *V, R *U) {
+  U[CDENS] = V[RDENS];
+  R emag = R(0), ekin = R(0);
+#pragma unroll
+  for (int dir = 0; dir < 3; dir++) {
+    U[CMOM0 + dir] = V[RDENS] * V[RVEL0 + dir];
+    ekin += V[RVEL0 + dir] * V[RVEL0 + dir];
+    if constexpr (MHD) {
+      U[CMAGC0 + dir] = V[RMAGC0 + dir];
+      emag += V[RMAGC0 + dir] * V[RMAGC0 + dir];
+    }
+  }
+  const R eint = V[REINT] * V[RDENS];
+  ekin *= R(0.5) * V[RDENS];
+  emag *= R(0.5);
+  U[CENER] = eint + ekin + emag;
+}
+
+template <bool MHD, int DIR1, typename R>
+__device__ __forceinline__ void Prim2Flux(const R *V, R *F) {
+  constexpr int DIR2 = (DIR1 + 1) % 3;
+  constexpr int DIR3 = (DIR1 + 2) % 3;
+  F[CDENS] = V[RDENS] * V[RVEL0 + DIR1];
+  R ptot = V[RPRES];
+  R B2 = R(0), uB = R(0), ekin = R(0);
+#pragma unroll
+  for (int dir = 0; dir < 3; dir++) {
+    F[CMOM0 + dir] = F[CDENS] * V[RVEL0 + dir];
+    ekin += V[RVEL0 + dir] * V[RVEL0 + dir];
+    if constexpr (MHD) {
+      B2 += V[RMAGC0 + dir] * V[RMAGC0 + dir];
+      uB += V[RVEL0 + dir] * V[RMAGC0 + dir];
+      F[CMOM0 + dir] -= V[RMAGC0 + DIR1] * V[RMAGC0 + dir];
+    }
+  }
+  ekin *= R(0.5) * V[RDENS];
+  const R emag = R(0.5) * B2;
+  ptot += R(0.5) * B2;
+  const R etot = V[REINT] * V[RDENS] + ekin + emag;
+  F[CMOM0 + DIR1] += ptot;
+  F[CENER] = (etot + ptot) * V[RVEL0 + DIR1];
+  if constexpr (MHD) {
+    F[CENER] -= uB * V[RMAGC0 + DIR1];
+    F[CMAGC0 + DIR1] = R(0);
+    F[CMAGC0 + DIR2] = V[RVEL0 + DIR1] * V[RMAGC0 + DIR2] - V[RVEL0 + DIR2] * V[RMAGC0 + DIR1];
+    F[CMAGC0 + DIR3] = V[RVEL0 + DIR1] * V[RMAGC0 + DIR3] - V[RVEL0 + DIR3] * V[RMAGC0 + DIR1];
+  }
+}
+
+// riemann_solver.hpp:20-57 (HLL) and :59-149 (HLLC) for the face normal DIR1.
+template <int RIEMANN, bool MHD, int DIR1, typename R>
+__device__ __forceinline__ void RiemannFlux(const R *vL, const R *vR, R *flux) {
+  constexpr int DIR2 = (DIR1 + 1) % 3;
+  constexpr int DIR3 = (DIR1 + 2) % 3;
+  constexpr int NC = MHD ? 8 : 5;
+  const R cfL = FastSpeed<MHD>(DIR1, vL);
+  const R cfR = FastSpeed<MHD>(DIR1, vR);
+  const R tiny = Lim<R>::tiny();
+  const R sL = kmin(-tiny, kmin(vL[RVEL0 + DIR1] - cfL, vR[RVEL0 + DIR1] - cfR));
+  const R sR = kmax(tiny, kmax(vL[RVEL0 + DIR1] + cfL, vR[RVEL0 + DIR1] + cfR));
+  const R sRmsLi = R(1.0) / (sR - sL);
+  R UL[NC], UR[NC], FL[NC], FR[NC];
+  Prim2Cons<MHD>(vL, UL);
+  Prim2Cons<MHD>(vR, UR);
+  Prim2Flux<MHD, DIR1>(vR, FR);
+  Prim2Flux<MHD, DIR1>(vL, FL);
+  if constexpr (RIEMANN == HLL) {
+#pragma unroll
+    for (int v = 0; v < NC; v++)
+      flux[v] = sRmsLi * (sR * FL[v] - sL * FR[v] + sR * sL * (UR[v] - UL[v]));
+  } else {
+    const R total_presL = TotalPres<MHD>(vL);
+    const R total_presR = TotalPres<MHD>(vR);
+    R ustar = total_presR - total_presL + UL[CMOM0 + DIR1] * (sL - vL[RVEL0 + DIR1]) -
+              UR[CMOM0 + DIR1] * (sR - vR[RVEL0 + DIR1]);
+    ustar = ustar / (vL[RDENS] * (sL - vL[RVEL0 + DIR1]) - vR[RDENS] * (sR - vR[RVEL0 + DIR1]));
+    const R pstar =
+        R(0.5) * (total_presL + total_presR +
+                  vL[RDENS] * (sL - vL[RVEL0 + DIR1]) * (ustar - vL[RVEL0 + DIR1]) +
+                  vR[RDENS] * (sR - vR[RVEL0 + DIR1]) * (ustar - vR[RVEL0 + DIR1]));
+    R UsL[NC], UsR[NC];
+    auto hllc_state = [&](R S, const R *U, R Pu, R *Us) {
+      const R susi = R(1.) / (S - ustar + tiny);
+      Us[CDENS] = susi * (S * U[CDENS] - U[CMOM0 + DIR1]);
+      Us[CMOM0 + DIR1] = Us[CDENS] * ustar;
+      Us[CMOM0 + DIR2] = U[CMOM0 + DIR2] * Us[CDENS] / U[CDENS];
+      Us[CMOM0 + DIR3] = U[CMOM0 + DIR3] * Us[CDENS] / U[CDENS];
+      Us[CENER] = U[CENER] * Us[CDENS] / U[CDENS] + susi * (pstar * ustar - Pu);
+      if constexpr (MHD) {
+        const R sRsLi = R(1.) / (sR - sL);
+        auto hll = [&](int v) { return sRsLi * (sR * UR[v] - sL * UL[v] + FL[v] - FR[v]); };
+        Us[CMAGC0 + DIR1] = hll(CMAGC0 + DIR1);
+        Us[CMAGC0 + DIR2] = hll(CMAGC0 + DIR2);
+        Us[CMAGC0 + DIR3] = hll(CMAGC0 + DIR3);
+        Us[CMOM0 + DIR2] -=
+            (Us[CMAGC0 + DIR1] * Us[CMAGC0 + DIR2] - U[CMAGC0 + DIR1] * U[CMAGC0 + DIR2]) * susi;
+        Us[CMOM0 + DIR3] -=
+            (Us[CMAGC0 + DIR1] * Us[CMAGC0 + DIR3] - U[CMAGC0 + DIR1] * U[CMAGC0 + DIR3]) * susi;
+        Us[CENER] -= susi * (Us[CMAGC0 + DIR1] *
+                                 (Us[CMAGC0 + DIR1] * hll(CMOM0 + DIR1) +
+                                  Us[CMAGC0 + DIR2] * hll(CMOM0 + DIR2) +
+                                  Us[CMAGC0 + DIR3] * hll(CMOM0 + DIR3)) /
+                                 hll(CDENS) -
+                             U[CMAGC0 + DIR1] *
+                                 (U[CMAGC0 + DIR1] * U[CMOM0 + DIR1] +
+                                  U[CMAGC0 + DIR2] * U[CMOM0 + DIR2] +
+                                  U[CMAGC0 + DIR3] * U[CMOM0 + DIR3]) /
+                                 U[CDENS]);
+      }
+    };
+    hllc_state(sL, UL, total_presL * vL[RVEL0 + DIR1], UsL);
+    hllc_state(sR, UR, total_presR * vR[RVEL0 + DIR1], UsR);
+    const R biasL = -kmin(-tiny, copysign(R(1), ustar));
+    const R biasR = kmax(tiny, copysign(R(1), ustar));
+#pragma unroll
+    for (int v = 0; v < NC; v++)
+      flux[v] = biasR * (FL[v] + sL * (UsL[v] - UL[v])) + biasL * (FR[v] + sR * (UsR[v] - UR[v]));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ideal-gas EOS (singularity::IdealGas as used at equation_of_state.hpp:40-64).
+struct EosParams {
+  double gm1;  // gamma - 1
+  double cv;   // gamma * kB / Abar
+};
+
+// ener mode: rho, sie -> T, P, bulk modulus
+template <typename R>
+__device__ __forceinline__ void EosEner(const EosParams &e, R rho, R sie, R &temp, R &pres,
+                                        R &bmod) {
+  const R gm1 = R(e.gm1);
+  pres = kmax(R(0), gm1 * rho * sie);
+  temp = kmax(R(0), sie / R(e.cv));
+  bmod = kmax(R(0), (gm1 + R(1)) * gm1 * rho * sie);
+}
+
+// Cons2Prim (primconsflux.hpp:76-98) + ener-mode EOS on one cell.  E is passed
+// in double so the FP32 path recovers e_int = E - e_kin - e_mag in FP64.
+template <bool MHD, typename R>
+__device__ __forceinline__ void Cons2PrimEos(const EosParams &eos, R dens, R m0, R m1, R m2,
+                                             double ener, const R *B, R *V) {
+  const R idens = R(1.0) / dens;
+  V[RDENS] = dens;
+  V[RVEL0] = idens * m0;
+  V[RVEL1] = idens * m1;
+  V[RVEL2] = idens * m2;
+  R sie;
+  if constexpr (sizeof(R) == sizeof(double)) {
+    R ekin = R(0), emag = R(0);
+    ekin += V[RVEL0] * V[RVEL0];
+    ekin += V[RVEL1] * V[RVEL1];
+    ekin += V[RVEL2] * V[RVEL2];
+    if constexpr (MHD) {
+      for (int d = 0; d < 3; d++) emag += B[d] * B[d];
+    }
+    ekin *= R(0.5) * dens;
+    emag *= R(0.5);
+    const R eint = R(ener) - ekin - emag;
+    sie = idens * eint;
+  } else {
+    // FP32 storage: kinetic and magnetic energies and the subtraction in FP64
+    const double dd = double(dens);
+    const double id = 1.0 / dd;
+    const double u0 = id * double(m0), u1 = id * double(m1), u2 = id * double(m2);
+    double ekin = (u0 * u0 + u1 * u1 + u2 * u2) * (0.5 * dd);
+    double emag = 0.0;
+    if constexpr (MHD) {
+      for (int d = 0; d < 3; d++) emag += double(B[d]) * double(B[d]);
+      emag *= 0.5;
+    }
+    sie = R(id * (ener - ekin - emag));
+  }
+  V[REINT] = sie;
+  R temp;
+  EosEner(eos, dens, sie, temp, V[RPRES], V[RBMOD]);
+  if constexpr (MHD) {
+    V[RMAGC0] = B[0];
+    V[RMAGC0 + 1] = B[1];
+    V[RMAGC0 + 2] = B[2];
+  }
+}
+
+// splitmix64 (Steele, Lea & Flood 2014) as a counter-based generator.
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__host__ __device__ __forceinline__ double kh_uniform(uint64_t seed, uint64_t gidx, int comp) {
+  const uint64_t h = splitmix64(splitmix64(seed) ^ (gidx * 2u + uint64_t(comp)));
+  return double(h >> 11) * 0x1.0p-53;
+}
+
+}  // namespace kmy

@@ -1,0 +1,332 @@
+// kmy_fused.cuh -- one RK stage of the hydro update in a single launch.
+//
+// Each CTA owns a brick of interior cells of one meshblock.  For every active
+// direction it stages the brick, extended by H cells along that direction,
+// into shared memory as primitives (cons->prim + EOS on the fly), evaluates
+// the face fluxes of that direction (reconstruction of all seven primitives at
+// both cells of the face + Riemann solver), and accumulates the flux
+// divergence of its own cells in registers.  The epilogue applies the
+// low-storage RK update and, on the last stage, reduces the CFL time step.
+//
+// Ghost zones are not read: a halo cell is fetched from the interior of the
+// block that owns it on the uniform mesh (periodic wrap, outflow clamp,
+// reflect mirror with a sign flip), which is what the boundary exchange would
+// have copied into the ghost zone.  The stage therefore reads U_stage once
+// from HBM (halo re-reads hit L2), reads U_base for stages >= 2 and writes
+// U_new, with no separate primitive, flux, dU/dt or ghost-exchange passes.
+//
+// Arithmetic per cell/face is the same as the per-task kernels
+// (kmy_tasks.cu), which follow hydro_add_flux_tasks.cpp:36-264,
+// grid_update.hpp:15-57, grid.cpp:353-381, primconsflux.cpp:82-142 and
+// hydro_time_step.cpp:19-64.
+#pragma once
+
+#include "../../include/kmy_hydro.h"
+#include "kmy_internal.hpp"
+
+namespace kmy {
+
+template <int NDIM, int RECON>
+struct FusedShape {
+  static constexpr int W = ReconWidth<RECON>::value;
+  static constexpr int H = W + 1;
+  static constexpr int B[3] = {NDIM == 3 ? 8 : NDIM == 2 ? 16 : 128, NDIM == 3 ? 8 : NDIM == 2 ? 16 : 1,
+                               NDIM == 3 ? 8 : 1};
+  static constexpr int NT = 256;
+  static constexpr int NCELL = B[0] * B[1] * B[2];
+  static constexpr int CPT = (NCELL + NT - 1) / NT;
+  static constexpr int region(int d) { return (B[d] + 2 * H) * (NCELL / B[d]); }
+  static constexpr int faces(int d) { return (B[d] + 1) * (NCELL / B[d]); }
+  static constexpr int cmax(int a, int b) { return a > b ? a : b; }
+  static constexpr int REG_MAX =
+      cmax(region(0), cmax(NDIM > 1 ? region(1) : 0, NDIM > 2 ? region(2) : 0));
+  static constexpr int FACE_MAX =
+      cmax(faces(0), cmax(NDIM > 1 ? faces(1) : 0, NDIM > 2 ? faces(2) : 0));
+  static constexpr int NR = 7;
+  static constexpr int NC = 5;
+  template <typename S>
+  static constexpr size_t smem_bytes() {
+    return sizeof(S) * (size_t(NR) * REG_MAX + size_t(NC) * FACE_MAX);
+  }
+};
+
+template <typename S>
+struct FusedArgs {
+  MeshDesc m;
+  EosParams eos;
+  int limiter;
+  const S *u0;
+  const float *u0lo;
+  const S *ub;
+  const float *ublo;
+  S *u1;
+  float *u1lo;
+  const S *prim;
+  int stored;
+  int last;
+  double beta;
+  DevClock *clock;
+  int nbr[3];
+};
+
+__device__ __forceinline__ int fz_map(int G, int N, int bc, bool &flip) {
+  if (G >= 0 && G < N) return G;
+  if (bc == BC_PERIODIC) return ((G % N) + N) % N;
+  if (bc == BC_OUTFLOW) return G < 0 ? 0 : N - 1;
+  flip = !flip;
+  return G < 0 ? -G - 1 : 2 * N - G - 1;
+}
+
+// Load the primitive state of block-interior cell (l0,l1,l2) of block at
+// logical location lx (coordinates may lie up to H cells outside the block).
+template <typename S>
+__device__ __forceinline__ void fz_load_prim(const FusedArgs<S> &a, const int lx[3], int l0, int l1,
+                                             int l2, S *V) {
+  const MeshDesc &m = a.m;
+  const int l[3] = {l0, l1, l2};
+  int sb = 0, mult = 1, loc[3];
+  bool flip[3] = {false, false, false};
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const int G = lx[d] * m.nx[d] + l[d];
+    const int M = fz_map(G, m.mesh_nx[d], m.bc[d][G < 0 ? 0 : 1], flip[d]);
+    const int ob = M / m.nx[d];
+    sb += ob * mult;
+    mult *= m.nbx[d];
+    loc[d] = M - ob * m.nx[d] + m.g[d];
+  }
+  const long long NP = (long long)m.nb * m.P;
+  const long long n = (long long)sb * m.P + ((long long)loc[2] * m.np[1] + loc[1]) * m.np[0] + loc[0];
+  const S dens = a.u0[n];
+  if (a.stored) {
+    V[RDENS] = dens;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const S v = a.prim[(PVEL0 + d) * NP + n];
+      V[RVEL0 + d] = flip[d] ? -v : v;
+    }
+    V[RPRES] = a.prim[PPRES * NP + n];
+    V[RBMOD] = a.prim[PBMOD * NP + n];
+    V[REINT] = a.prim[PEINT * NP + n];
+  } else {
+    S mo[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const S v = a.u0[(CMOM0 + d) * NP + n];
+      mo[d] = flip[d] ? -v : v;
+    }
+    double e = double(a.u0[CENER * NP + n]);
+    if constexpr (sizeof(S) == 4) e += double(a.u0lo[n]);
+    Cons2PrimEos<false, S>(a.eos, dens, mo[0], mo[1], mo[2], e, nullptr, V);
+  }
+}
+
+template <typename S, int NDIM, int RECON, int RIEMANN, int DIR>
+__device__ __forceinline__ void fz_direction(const FusedArgs<S> &a, const int lx[3], const int o[3],
+                                             S *sp, S *sf, S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
+  using Sh = FusedShape<NDIM, RECON>;
+  constexpr int H = Sh::H, W = Sh::W;
+  constexpr int B0 = Sh::B[0], B1 = Sh::B[1], B2 = Sh::B[2];
+  constexpr int E0 = B0 + (DIR == 0 ? 2 * H : 0);
+  constexpr int E1 = B1 + (DIR == 1 ? 2 * H : 0);
+  constexpr int E2 = B2 + (DIR == 2 ? 2 * H : 0);
+  constexpr int NREG = E0 * E1 * E2;
+  constexpr int RM = Sh::REG_MAX, FM = Sh::FACE_MAX;
+  const int tid = threadIdx.x;
+
+  // 1. stage primitives of the direction-extended brick
+  for (int q = tid; q < NREG; q += Sh::NT) {
+    const int x = q % E0, y = (q / E0) % E1, z = q / (E0 * E1);
+    const int l0 = o[0] + x - (DIR == 0 ? H : 0);
+    const int l1 = o[1] + y - (DIR == 1 ? H : 0);
+    const int l2 = o[2] + z - (DIR == 2 ? H : 0);
+    S V[7];
+    fz_load_prim<S>(a, lx, l0, l1, l2, V);
+#pragma unroll
+    for (int r = 0; r < 7; r++) sp[r * RM + q] = V[r];
+  }
+  __syncthreads();
+
+  // 2. face fluxes of this direction
+  constexpr int NFACE = (DIR == 0 ? B0 + 1 : B0) * (DIR == 1 ? B1 + 1 : B1) * (DIR == 2 ? B2 + 1 : B2);
+  constexpr int F0 = DIR == 0 ? B0 + 1 : B0, F1 = DIR == 1 ? B1 + 1 : B1;
+  constexpr int ST = DIR == 0 ? 1 : DIR == 1 ? E0 : E0 * E1;  // region stride along DIR
+  for (int it = tid; it < NFACE; it += Sh::NT) {
+    const int x = it % F0, y = (it / F0) % F1, z = it / (F0 * F1);
+    // region coordinate of the face's high cell
+    const int hx = x + (DIR == 0 ? H : 0), hy = y + (DIR == 1 ? H : 0), hz = z + (DIR == 2 ? H : 0);
+    const int hq = hx + E0 * (hy + E1 * hz);
+    S vL[7], vR[7];
+#pragma unroll
+    for (int r = 0; r < 7; r++) {
+      S line[2 * W + 2];
+#pragma unroll
+      for (int q = 0; q < 2 * W + 2; q++) line[q] = sp[r * RM + hq + (q - 1 - W) * ST];
+      S sl[5], sr[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        const int ol = q - 2 + W, orr = q - 1 + W;
+        sl[q] = (ol >= 0 && ol < 2 * W + 2) ? line[ol] : S(0);
+        sr[q] = (orr >= 0 && orr < 2 * W + 2) ? line[orr] : S(0);
+      }
+      vL[r] = ReconstructPlus<RECON, S>(a.limiter, sl);
+      vR[r] = ReconstructMinus<RECON, S>(a.limiter, sr);
+    }
+    S F[5];
+    RiemannFlux<RIEMANN, false, DIR, S>(vL, vR, F);
+#pragma unroll
+    for (int v = 0; v < 5; v++) sf[v * FM + it] = F[v];
+  }
+  __syncthreads();
+
+  // 3. divergence contribution of this direction for the owned cells
+  const S A = S(a.m.area[DIR]);
+#pragma unroll
+  for (int s = 0; s < Sh::CPT; s++) {
+    const int c = tid + s * Sh::NT;
+    if (c < Sh::NCELL) {
+      const int x = c % B0, y = (c / B0) % B1, z = c / (B0 * B1);
+      int lo, hi;
+      if (DIR == 0) {
+        lo = x + (B0 + 1) * (y + B1 * z);
+        hi = lo + 1;
+      } else if (DIR == 1) {
+        lo = x + B0 * (y + (B1 + 1) * z);
+        hi = lo + B0;
+      } else {
+        lo = x + B0 * (y + B1 * z);
+        hi = lo + B0 * B1;
+      }
+#pragma unroll
+      for (int v = 0; v < 5; v++) du[s][v] -= (A * sf[v * FM + hi] - A * sf[v * FM + lo]);
+    }
+  }
+  __syncthreads();
+}
+
+template <typename S, int NDIM, int RECON, int RIEMANN>
+__global__ void __launch_bounds__(256) k_fused_stage(FusedArgs<S> a) {
+  using Sh = FusedShape<NDIM, RECON>;
+  const DevClock *clk = a.clock;
+  if (clk->done) return;
+  const double dt = clk->dt;
+  extern __shared__ __align__(16) unsigned char kmy_smem[];
+  S *sp = reinterpret_cast<S *>(kmy_smem);
+  S *sf = sp + Sh::NR * Sh::REG_MAX;
+
+  const MeshDesc &m = a.m;
+  const int nbrick = a.nbr[0] * a.nbr[1] * a.nbr[2];
+  const int b = blockIdx.x / nbrick;
+  const int br = blockIdx.x - b * nbrick;
+  const int o[3] = {(br % a.nbr[0]) * Sh::B[0], ((br / a.nbr[0]) % a.nbr[1]) * Sh::B[1],
+                    (br / (a.nbr[0] * a.nbr[1])) * Sh::B[2]};
+  const int lx[3] = {b % m.nbx[0], (b / m.nbx[0]) % m.nbx[1], b / (m.nbx[0] * m.nbx[1])};
+
+  S du[Sh::CPT][5];
+#pragma unroll
+  for (int s = 0; s < Sh::CPT; s++)
+#pragma unroll
+    for (int v = 0; v < 5; v++) du[s][v] = S(0);
+
+  fz_direction<S, NDIM, RECON, RIEMANN, 0>(a, lx, o, sp, sf, du);
+  if constexpr (NDIM > 1) fz_direction<S, NDIM, RECON, RIEMANN, 1>(a, lx, o, sp, sf, du);
+  if constexpr (NDIM > 2) fz_direction<S, NDIM, RECON, RIEMANN, 2>(a, lx, o, sp, sf, du);
+
+  // epilogue: low-storage update of the owned interior cells
+  const long long NP = (long long)m.nb * m.P;
+  const S vol = S(m.vol);
+  const S bt = S(a.beta);
+  double dtl = INFINITY;
+#pragma unroll
+  for (int s = 0; s < Sh::CPT; s++) {
+    const int c = threadIdx.x + s * Sh::NT;
+    if (c >= Sh::NCELL) continue;
+    const int x = c % Sh::B[0], y = (c / Sh::B[0]) % Sh::B[1], z = c / (Sh::B[0] * Sh::B[1]);
+    const int l0 = o[0] + x, l1 = o[1] + y, l2 = o[2] + z;
+    if (l0 >= m.nx[0] || l1 >= m.nx[1] || l2 >= m.nx[2]) continue;
+    const long long n = (long long)b * m.P +
+                        ((long long)(l2 + m.g[2]) * m.np[1] + (l1 + m.g[1])) * m.np[0] + (l0 + m.g[0]);
+    S un[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const S dudt = du[s][v] / vol;
+      if (sizeof(S) == 4 && v == CENER) {
+        double eb = double(a.ub[CENER * NP + n]), e0 = double(a.u0[CENER * NP + n]);
+        if constexpr (sizeof(S) == 4) {
+          eb += double(a.ublo[n]);
+          e0 += double(a.u0lo[n]);
+        }
+        const double e1 = (a.beta * eb + (1.0 - a.beta) * e0) + a.beta * dt * double(dudt);
+        const float hi = float(e1);
+        a.u1[CENER * NP + n] = S(hi);
+        if constexpr (sizeof(S) == 4) a.u1lo[n] = float(e1 - double(hi));
+        un[v] = S(hi);
+        continue;
+      }
+      const S x0 = bt * a.ub[v * NP + n] + (S(1.0) - bt) * a.u0[v * NP + n];
+      un[v] = x0 + bt * S(dt) * dudt;
+      a.u1[v * NP + n] = un[v];
+    }
+    if (a.last) {
+      double e = double(un[CENER]);
+      if constexpr (sizeof(S) == 4) e += double(a.u1lo[n]);
+      S V[7];
+      Cons2PrimEos<false, S>(a.eos, un[CDENS], un[CMOM0], un[CMOM1], un[CMOM2], e, nullptr, V);
+#pragma unroll
+      for (int dir = 0; dir < NDIM; dir++) {
+        const S cf = FastSpeed<false>(dir, V);
+        double xv = double(S(m.dx[dir]) / (fabs(V[RVEL0 + dir]) + cf));
+        if (xv != xv) xv = 0.0;
+        dtl = xv < dtl ? xv : dtl;
+      }
+    }
+  }
+  if (a.last) {
+    for (int q = 16; q > 0; q >>= 1) dtl = fmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, q));
+    __shared__ double wmin[Sh::NT / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) wmin[warp] = dtl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = wmin[0];
+      for (int w = 1; w < Sh::NT / 32; w++) v = fmin(v, wmin[w]);
+      if (!(v >= 0.0)) v = 0.0;
+      atomicMin(&a.clock->dtmin_bits, (unsigned long long)__double_as_longlong(v));
+    }
+  }
+}
+
+template <typename S, int NDIM, int RECON, int RIEMANN>
+int fused_launch(kmy_ctx *c, FusedArgs<S> a) {
+  using Sh = FusedShape<NDIM, RECON>;
+  const MeshDesc &m = c->m;
+  for (int d = 0; d < 3; d++) a.nbr[d] = (m.nx[d] + Sh::B[d] - 1) / Sh::B[d];
+  const long long grid = (long long)a.nbr[0] * a.nbr[1] * a.nbr[2] * m.nb;
+  const size_t smem = Sh::template smem_bytes<S>();
+  auto kern = k_fused_stage<S, NDIM, RECON, RIEMANN>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return cuda_check(c, e, "fused smem attribute");
+  kern<<<unsigned(grid), Sh::NT, smem, c->stream>>>(a);
+  c->launches++;
+  return cuda_check(c, cudaGetLastError(), "fused stage");
+}
+
+template <typename S>
+int fused_dispatch(kmy_ctx *c, FusedArgs<S> a) {
+  const int nd = c->m.ndim, rec = c->prm.recon, rie = c->prm.riemann;
+#define KMY_FZ(ND, RC)                                               \
+  if (nd == ND && rec == RC) {                                       \
+    return rie == HLL ? fused_launch<S, ND, RC, HLL>(c, a)           \
+                      : fused_launch<S, ND, RC, HLLC>(c, a);         \
+  }
+#define KMY_FZ_ND(ND) KMY_FZ(ND, FOG) KMY_FZ(ND, PLM) KMY_FZ(ND, PPM) KMY_FZ(ND, WENOZ)
+  KMY_FZ_ND(1)
+  KMY_FZ_ND(2)
+  KMY_FZ_ND(3)
+#undef KMY_FZ_ND
+#undef KMY_FZ
+  c->err = "no fused kernel for this configuration";
+  return KMY_ERR_BAD_PARAM;
+}
+
+}  // namespace kmy

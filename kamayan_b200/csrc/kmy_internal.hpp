@@ -1,0 +1,129 @@
+// kmy_internal.hpp -- host-side context, mesh description and kernel entry
+// points shared by the translation units of libkmy_hydro.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "kmy_device.cuh"
+
+namespace kmy {
+
+// Uniform single-level mesh, passed by value to every kernel.  Block b sits at
+// logical location (b % nbx0, (b / nbx0) % nbx1, b / (nbx0 nbx1)); arrays are
+// Parthenon MeshData layout: [var][block][k][j][i] over the ghost-padded block.
+struct MeshDesc {
+  int ndim;
+  int nb;
+  int nx[3];       // interior cells per block
+  int g[3];        // ghosts per dim (0 if inactive)
+  int np[3];       // padded cells per dim
+  int nf[3];       // padded face dims (np + 1 in active dims)
+  int nbx[3];      // blocks per dim
+  int mesh_nx[3];  // cells across the mesh
+  int bc[3][2];    // BoundaryKind per dim and side
+  long long P;     // padded cells per block
+  long long Pf;    // padded faces per block (one element)
+  double dx[3];
+  double xmin[3];
+  // cartesian geometry (Parthenon UniformCartesian products)
+  double area[3];  // dy*dz, dx*dz, dx*dy
+  double vol;      // dx*dy*dz
+};
+
+// Device-resident simulation clock.  The dt controller runs on the device so
+// that a whole step (all stages + controller) needs no host round trip.
+struct DevClock {
+  double time;
+  double dt;        // dt of the next step
+  double dt_est;    // last CFL estimate (already times cfl/ndim)
+  double dt_taken;  // dt of the last completed step
+  unsigned long long dtmin_bits;  // atomic min of dx/(|v|+c) (bit pattern of a positive double)
+  int ncycle;
+  int done;         // time >= tlim: stage kernels become no-ops
+  int status;       // KMY_ERR_NONFINITE when the estimate was not finite/positive
+};
+
+struct TimeParams {
+  double tlim, dt_factor, dt_init, dt_ceil, dt_user, dt_floor;
+  double cfl_over_ndim;
+  int nlim;
+};
+
+struct Params {
+  int recon = FOG, limiter = MINMOD, riemann = HLL;
+  bool mhd = false;
+  double cfl = 0.8, gamma = 5.0 / 3.0, Abar = 1.0;
+  std::vector<double> beta;
+  std::vector<std::string> stage_name;
+  int precision = 64;
+  TimeParams tp{};
+  std::map<std::string, std::string> deck;
+  double real(const std::string &k, double d) const;
+  int integer(const std::string &k, int d) const;
+  std::string str(const std::string &k, const std::string &d) const;
+};
+
+struct Container {
+  void *cc = nullptr;     // [ncc][nb][P] of S
+  void *ener_lo = nullptr;// [nb][P] float low word of E (FP32 path only)
+  void *fc = nullptr;     // [3][nb][Pf] face "mag" (CT only)
+  void *emf = nullptr;    // [3][nb][Pf] edge EMFs (CT only)
+};
+
+}  // namespace kmy
+
+struct kmy_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  kmy::Params prm;
+  kmy::MeshDesc m{};
+  kmy::EosParams eos{};
+  int ncc = 5;
+  size_t esz = 8;  // bytes per stored real
+  std::map<std::string, kmy::Container> md;
+  void *prim = nullptr;   // [NPRIM][nb][P] shared primitives (S)
+  void *flux = nullptr;   // [3][ncc][nb][Pf] face fluxes (S), shared by all containers
+  double *divb = nullptr; // [nb][P]
+  kmy::DevClock *clock = nullptr;  // device
+  double *scratch = nullptr;       // reduction scratch (device)
+  bool prims_valid = false;  // stored prims match "base" (after pgen/import/tasks)
+  int path = 0;              // 0 fused, 1 tasks
+  int64_t launches = 0;
+  std::string err;
+  std::vector<void *> allocations;
+};
+
+namespace kmy {
+
+// ---- kernels (kmy_tasks.cu) ----
+int launch_fill_ghosts(kmy_ctx *c, Container &ct);
+int launch_compute_fluxes(kmy_ctx *c, Container &md0);
+int launch_compute_emf(kmy_ctx *c, Container &md0);
+int launch_flux_divergence(kmy_ctx *c, Container &md0, Container &dudt);
+int launch_apply_dudt(kmy_ctx *c, Container &base, Container &md0, Container &md1,
+                      Container &dudt, double beta, double dt, const double *dt_dev);
+int launch_prepare_primitive(kmy_ctx *c, Container &md1);
+int launch_estimate_dt(kmy_ctx *c, Container &md, bool reset);
+int launch_fill_derived(kmy_ctx *c, Container &md);
+int launch_eos_init(kmy_ctx *c, Container &md);
+int launch_convert_to_conserved(kmy_ctx *c, Container &md);
+// mode 0: after a step; 1: initial dt from the estimate; 2: clamp pending dt to tlim
+int launch_dt_controller(kmy_ctx *c, int mode);
+int launch_conserved_sums(kmy_ctx *c, Container &md, double *host_out);
+int launch_vortex_error(kmy_ctx *c, int var, int comp, double *host_out);
+int launch_set_energy_split(kmy_ctx *c, Container &ct);
+// ---- fused stage (kmy_fused.cu) ----
+int launch_fused_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1,
+                       double beta, bool stored_prims, bool last);
+// ---- problem generators (kmy_pgen.cu) ----
+int launch_pgen(kmy_ctx *c, const std::string &problem);
+
+int cuda_check(kmy_ctx *c, cudaError_t e, const char *what);
+
+}  // namespace kmy
