@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 finite-volume update (one JSON line on stdout).
+
+Workload: 3D Kelvin-Helmholtz, gamma 1.4, periodic unit cube, 256^3 cells in
+512 meshblocks of 32^3 with 3 ghost cells, WENO-Z + HLLC, RK3, CFL 0.4,
+synthetic initial state (seeded shear-layer perturbation).  A step is one full
+RK3 time step over the whole mesh (three fused stage launches + the device dt
+controller).  Metric: cell-updates/s = interior cells x steps / time.
+
+``value``: the FP32 bulk path (FP64 energy recovery and sums), all 512 blocks
+batched into one launch per stage, timed with CUDA events on the solver's
+stream.  Beside it: the FP64 fused path, the FP64 per-task path (the
+reference task list, one kernel per task) and the FP32-vs-FP64 density L1.
+``e2e``: the same metric through the C ABI with host buffers: import of the
+initial state from pinned host memory, K x kmy_step (each returns dt to the
+host), export of the final conserved state.
+
+``--impl reference`` times the reference's CPU path (the C++ restatement in
+oracle/, all host threads) on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): the path does not shard here, so every rank runs an
+independent replica; the time is the max over ranks and ``value`` the sum.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s"
+
+
+def args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kmy", choices=["kmy", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="cells per dimension")
+    ap.add_argument("--nb", type=int, default=32, help="meshblock cells per dimension")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tasks", action="store_true", help="skip the per-task FP64 arm")
+    return ap.parse_args()
+
+
+def workload_config(a, n_gpus):
+    nb = (a.n // a.nb) ** 3
+    return {
+        "workload": f"kelvin_helmholtz_3d {a.n}^3 in {nb} blocks of {a.nb}^3, 3 ghosts, "
+                    f"WENO-Z + HLLC, RK3, CFL 0.4",
+        "cells": a.n ** 3,
+        "meshblocks": nb,
+        "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU",
+        "cache": "inputs larger than L2 (256^3 state: 671 MB FP64, 336 MB FP32)",
+    }
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(rows[0][2]),
+                "reasons": sorted(reasons), "samples": len(rows),
+                "power_w_max": max((num(r[3]) or 0.0) for r in rows)}
+
+
+# ---------------------------------------------------------------------------
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def allreduce_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_stages(s, nstages: int, tasks: bool):
+    for st in range(1, nstages + 1):
+        if tasks:
+            s.task_stage(st, -1.0)
+        else:
+            s.rk_stage(st)
+    s.end_step()
+
+
+def time_solver(s, stream, K: int, W: int, ws: int, tasks: bool = False, sampler=None):
+    """Warm up W steps, then time exactly K steps with CUDA events on the solver's stream."""
+    import torch
+
+    ns = s.info.nstages
+    for _ in range(W):
+        run_stages(s, ns, tasks)
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(ns)] for _ in range(K)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    launches0 = s.launch_count
+    if sampler:
+        sampler.start()
+    t0.record(stream)
+    for k in range(K):
+        for st in range(1, ns + 1):
+            ev[k][st - 1][0].record(stream)
+            if tasks:
+                s.task_stage(st, -1.0)
+            else:
+                s.rk_stage(st)
+            ev[k][st - 1][1].record(stream)
+        s.end_step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    barrier(ws)
+    torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    stage_ms = [a.elapsed_time(b) for row in ev for (a, b) in row]
+    clk = s.time
+    if not (clk["dt"] > 0.0 and clk["dt"] < 1e300):
+        raise RuntimeError(f"solver state became non-finite during the timed steps: {clk}")
+    return {"total_ms": total_ms, "stage_ms_avg": sum(stage_ms) / len(stage_ms),
+            "launches": s.launch_count - launches0, "clocks": clocks}
+
+
+def make_solver(a, precision: str, device: int, stream):
+    import kamayan_b200
+    from kamayan_b200 import configs
+
+    s = kamayan_b200.Solver(configs.kh_3d(n=a.n, nb=a.nb, precision=precision), device=device)
+    s.set_stream(stream.cuda_stream)
+    s.pgen("kelvin_helmholtz")
+    return s
+
+
+def e2e_solve(a, device: int, stream, K: int):
+    """Initial state from pinned host memory -> K x kmy_step -> final state to pinned host."""
+    import torch
+
+    import kamayan_b200
+
+    src = make_solver(a, "fp64", device, stream)
+    names_in = [("dens", 0), ("momentum", 0), ("momentum", 1), ("momentum", 2), ("ener", 0),
+                ("velocity", 0), ("velocity", 1), ("velocity", 2), ("pres", 0), ("bulk modulus", 0),
+                ("eint", 0), ("temp", 0)]
+    names_out = names_in[:5]
+    n = 1
+    for x in src.cell_shape:
+        n *= x
+    host_in = {}
+    for v, c in names_in:
+        t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        src.export_ptr(v, t.data_ptr(), n, c)
+        host_in[(v, c)] = t
+    src.close()
+    host_out = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in names_out}
+    from kamayan_b200 import configs
+
+    s = kamayan_b200.Solver(configs.kh_3d(n=a.n, nb=a.nb, precision="fp32"), device=device)
+    s.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for (v, c), t in host_in.items():
+        s.import_ptr(v, t.data_ptr(), n, c)
+    s.finalize_import()
+    for _ in range(K):
+        s.step()
+    for (v, c), t in host_out.items():
+        s.export_ptr(v, t.data_ptr(), n, c)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    s.close()
+    h2d = 8 * n * len(names_in)
+    d2h = 8 * n * len(names_out) + 48 * K
+    return ms, h2d, d2h
+
+
+def load_traffic(precision: str, a):
+    """DRAM bytes per fused-stage launch from the committed ncu summary, scaled to this mesh."""
+    p = ROOT / "profiles" / "fused_stage_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())[precision]
+        return d["bytes_per_cell"] * a.n ** 3
+    except Exception:
+        return None
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(sample_n: int, min_seconds: float, max_steps: int, steps: int = 1):
+    cmd = [sys.executable, "-m", "oracle.cpu_bench", "--workload", "kh_3d", "--n", str(sample_n),
+           "--nb", "32", "--steps", str(steps), "--warmup", "1", "--min-seconds", str(min_seconds),
+           "--max-steps", str(max_steps)]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"error": r.stderr[-400:]}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def main_reference(a):
+    ws, rank, _ = dist_init()
+    if rank != 0:
+        return
+    cb = cpu_baseline(128, 20.0, 200, steps=max(1, min(a.steps, 3)))
+    cfg = workload_config(a, a.gpus)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb.get("value"), "unit": METRIC,
+        "n_gpus": a.gpus, "steps": cb.get("steps"), "warmup": 1, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": cb.get("value"), "unit": METRIC, "cores": cb.get("threads"),
+                         "kind": "port", "sample": cb.get("sample")},
+        "e2e": {"value": cb.get("value"), "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "reference's own build is unavailable (un-vendored Parthenon/Kokkos); "
+                "timed: the C++ restatement of its CPU path, OpenMP over meshblocks",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = args()
+    if a.impl == "reference":
+        return main_reference(a)
+    import torch
+
+    ws, rank, local = dist_init()
+    device = local
+    torch.cuda.set_device(device)
+    stream = torch.cuda.Stream(device=device)
+    K, W = a.steps, max(3, a.warmup)
+    cells = a.n ** 3
+    ns = 3
+
+    # headline: FP32 bulk path, fused stages over all blocks
+    s32 = make_solver(a, "fp32", device, stream)
+    sampler = ClockSampler(device)
+    r32 = time_solver(s32, stream, K, W, ws, sampler=sampler)
+    # FP64 fused
+    s64 = make_solver(a, "fp64", device, stream)
+    r64 = time_solver(s64, stream, K, W, ws)
+    import numpy as np
+
+    d32 = s32.interior(s32.export("dens"))
+    d64 = s64.interior(s64.export("dens"))
+    l1 = float(np.abs(d32 - d64).sum() / np.abs(d64).sum())
+    t32, t64 = s32.time["time"], s64.time["time"]
+    s32.close()
+    s64.close()
+    # FP64 per-task path (the reference task list as separate kernels)
+    rt = None
+    if not a.no_tasks:
+        st = make_solver(a, "fp64", device, stream)
+        st.set_path("tasks")
+        rt = time_solver(st, stream, max(2, K // 4), W, ws, tasks=True)
+        st.close()
+    e2e_ms, h2d, d2h = e2e_solve(a, device, stream, K)
+
+    tot32 = allreduce_max(r32["total_ms"], ws)
+    tot64 = allreduce_max(r64["total_ms"], ws)
+    e2e_ms = allreduce_max(e2e_ms, ws)
+    value = ws * cells * K / (tot32 / 1e3)
+    v64 = ws * cells * K / (tot64 / 1e3)
+    vt = None
+    if rt:
+        Kt = max(2, K // 4)
+        vt = ws * cells * Kt / (allreduce_max(rt["total_ms"], ws) / 1e3)
+
+    # roofline of the dominant kernel (the fused stage): algorithmic bytes per
+    # launch = cells x words x bytes, words = 10 (stage 1) or 15 (stages 2, 3)
+    # (5 conserved words per cell; the FP32 path's extra energy low word is not counted)
+    words_avg = (10 + 15 * (ns - 1)) / ns
+    alg32 = cells * words_avg * 4
+    alg64 = cells * words_avg * 8
+    peak, peak_kind = peaks()
+    ach32 = alg32 / (r32["stage_ms_avg"] / 1e3) / 1e9
+    ach64 = alg64 / (r64["stage_ms_avg"] / 1e3) / 1e9
+    traffic = load_traffic("fp32", a)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": K, "warmup": W,
+        "ms_per_step": tot32 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": workload_config(a, ws),
+        "e2e": {"value": ws * cells * K / (e2e_ms / 1e3), "unit": METRIC,
+                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+                "what": "kmy_import_var (pinned host) + finalize + K x kmy_step + kmy_export_var, FP32"},
+        "gpu_launches": r32["launches"],
+        "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
+                     "frac": ach32 / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_fused_stage<float,3,WENOZ,HLLC>",
+                     "alg_bytes_per_launch": alg32, "launch_ms_avg": r32["stage_ms_avg"]},
+        "clocks": r32["clocks"],
+        "fp64_fused": {"value": v64, "ms_per_step": tot64 / K, "launch_ms_avg": r64["stage_ms_avg"],
+                       "roofline_achieved_gbs": ach64, "frac": ach64 / peak},
+        "fp64_tasks": ({"value": vt, "ms_per_step": rt["total_ms"] / max(2, K // 4)} if rt else None),
+        "l1_density_fp32_vs_fp64": l1,
+        "sim_time_fp32_fp64": [t32, t64],
+    }
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cb = cpu_baseline(128, 10.0, 200)
+        line["cpu_baseline"] = {"value": cb.get("value"), "unit": METRIC, "cores": cb.get("threads"),
+                                "kind": "port", "sample": cb.get("sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

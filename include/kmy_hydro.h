@@ -129,6 +129,11 @@ int kmy_rk_stage(kmy_ctx *ctx, int stage, double dt);
 int kmy_step(kmy_ctx *ctx, double *dt_taken);
 /* Step until tlim or nlim steps (nlim < 0: no limit). */
 int kmy_evolve(kmy_ctx *ctx, double tlim, int nlim, int *nsteps);
+/* Close a step driven stage by stage with kmy_rk_stage: advance the clock by
+ * the step's dt and choose the next dt on the device, without a host round
+ * trip.  Replaces: Parthenon EvolutionDriver time update + SetGlobalTimeStep
+ * after the stage task collections (src/driver/kamayan_driver.cpp:121-155). */
+int kmy_end_step(kmy_ctx *ctx);
 /* Simulation clock: time, next dt, last dt estimate, cycle count. */
 int kmy_get_time(const kmy_ctx *ctx, double *time, double *dt, double *dt_est, int *ncycle);
 /* Override the dt used by the next kmy_step (e.g. to replay a reference run). */

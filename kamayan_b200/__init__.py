@@ -33,7 +33,8 @@ EXPORTS = (
     "kmy_import_var", "kmy_export_var", "kmy_finalize_import", "kmy_pgen",
     "kmy_compute_fluxes", "kmy_compute_emf", "kmy_flux_divergence", "kmy_apply_dudt",
     "kmy_prepare_primitive", "kmy_fill_ghosts", "kmy_estimate_dt", "kmy_fill_derived",
-    "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_get_time", "kmy_set_dt",
+    "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_end_step", "kmy_get_time",
+    "kmy_set_dt",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
 )
 
@@ -88,6 +89,7 @@ def lib() -> ctypes.CDLL:
         L.kmy_rk_stage.argtypes = [vp, i, d]
         L.kmy_step.argtypes = [vp, _dp]
         L.kmy_evolve.argtypes = [vp, d, i, ctypes.POINTER(i)]
+        L.kmy_end_step.argtypes = [vp]
         L.kmy_get_time.argtypes = [vp, _dp, _dp, _dp, ctypes.POINTER(i)]
         L.kmy_set_dt.argtypes = [vp, d]
         L.kmy_set_path.argtypes = [vp, i]
@@ -153,6 +155,15 @@ class Solver:
         self._check(lib().kmy_import_var(self._h, container.encode(), var.encode(), comp,
                                          _ptr(a), a.size))
 
+    def import_ptr(self, var: str, ptr: int, n: int, comp: int = 0, container: str = "base") -> None:
+        """Import n doubles from host address ptr (e.g. a pinned buffer)."""
+        self._check(lib().kmy_import_var(self._h, container.encode(), var.encode(), comp,
+                                         ctypes.cast(ptr, _dp), n))
+
+    def export_ptr(self, var: str, ptr: int, n: int, comp: int = 0, container: str = "base") -> None:
+        self._check(lib().kmy_export_var(self._h, container.encode(), var.encode(), comp,
+                                         ctypes.cast(ptr, _dp), n))
+
     def finalize_import(self) -> None:
         self._check(lib().kmy_finalize_import(self._h))
 
@@ -171,7 +182,15 @@ class Solver:
         return n.value
 
     def rk_stage(self, stage: int, dt: float = -1.0) -> None:
+        """One fused stage; dt < 0 takes the dt held by the device clock."""
         self._check(lib().kmy_rk_stage(self._h, stage, dt))
+
+    def end_step(self) -> None:
+        self._check(lib().kmy_end_step(self._h))
+
+    def set_stream(self, cuda_stream: int) -> None:
+        """Run on a caller-owned cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
+        self._check(lib().kmy_set_stream(self._h, ctypes.c_void_p(cuda_stream)))
 
     def task_stage(self, stage: int, dt: float) -> None:
         self._check(lib().kmy_task_stage(self._h, stage, dt))

@@ -415,10 +415,12 @@ int kmy_import_var(kmy_ctx *c, const char *container, const char *var, int comp,
     c->err = "size mismatch: expected " + std::to_string(r.n);
     return KMY_ERR_BAD_PARAM;
   }
-  if (r.is_double || c->esz == 8)
-    return cuda_check(c, cudaMemcpyAsync(r.p, host, n * 8, cudaMemcpyHostToDevice, c->stream),
-                      "import copy") ||
-           cuda_check(c, cudaStreamSynchronize(c->stream), "import sync");
+  if (r.is_double || c->esz == 8) {
+    rc = cuda_check(c, cudaMemcpyAsync(r.p, host, n * 8, cudaMemcpyHostToDevice, c->stream), "import copy");
+    if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "import sync");
+    c->prims_valid = true;
+    return rc;
+  }
   double *stage = nullptr;
   rc = cuda_check(c, cudaMallocAsync(reinterpret_cast<void **>(&stage), n * 8, c->stream), "stage");
   if (rc) return rc;
@@ -447,10 +449,11 @@ int kmy_export_var(kmy_ctx *c, const char *container, const char *var, int comp,
   }
   rc = materialize(c);
   if (rc) return rc;
-  if (r.is_double || c->esz == 8)
-    return cuda_check(c, cudaMemcpyAsync(host, r.p, n * 8, cudaMemcpyDeviceToHost, c->stream),
-                      "export copy") ||
-           cuda_check(c, cudaStreamSynchronize(c->stream), "export sync");
+  if (r.is_double || c->esz == 8) {
+    rc = cuda_check(c, cudaMemcpyAsync(host, r.p, n * 8, cudaMemcpyDeviceToHost, c->stream), "export copy");
+    if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "export sync");
+    return rc;
+  }
   double *stage = nullptr;
   rc = cuda_check(c, cudaMallocAsync(reinterpret_cast<void **>(&stage), n * 8, c->stream), "stage");
   if (rc) return rc;
@@ -660,6 +663,12 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
   }
   if (nsteps) *nsteps = h.ncycle;
   return rc;
+}
+
+int kmy_end_step(kmy_ctx *c) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  return launch_dt_controller(c, 0);
 }
 
 int kmy_get_time(const kmy_ctx *c, double *time, double *dt, double *dt_est, int *ncycle) {

@@ -58,6 +58,17 @@ __host__ __device__ inline int ReconWidthRuntime(int recon) {
   return recon == FOG ? 0 : recon == PLM ? 1 : 2;
 }
 
+// WENO-Z weight factor 1 + (tau/(eps + beta))^2 (reconstruction.hpp:118-135).
+// In FP32 the ratio is capped at 1e15 so its square stays finite: with
+// eps = 1e-36 a vanishing smoothness indicator gives ratios far beyond the
+// float range, and at 1e15 that stencil already holds the whole weight.
+template <typename R>
+__device__ __forceinline__ R weno_q(R tau, R beta) {
+  R r = tau / (R(1.e-36) + beta);
+  if constexpr (sizeof(R) == 4) r = fminf(r, 1.0e15f);
+  return R(1) + sq(r);
+}
+
 // reconstruction.hpp:11-142: both face values of the cell at s[0] (s indexed
 // -W..W through the pointer arithmetic of the caller: s[o] = value at c+o).
 template <int RECON, typename R>
@@ -105,9 +116,10 @@ __device__ __forceinline__ void Reconstruct(int limiter, const R (&s)[5], R &vM,
     const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
     const R eps = R(1.e-36);
     const R tau = fabs(b2 - b0);
-    const R q0 = R(1) + sq(tau / (eps + b0));
-    const R q1 = R(1) + sq(tau / (eps + b1));
-    const R q2 = R(1) + sq(tau / (eps + b2));
+    (void)eps;
+    const R q0 = weno_q(tau, b0);
+    const R q1 = weno_q(tau, b1);
+    const R q2 = weno_q(tau, b2);
     {  // pm = -1: w0 uses beta0, w2 uses beta2
       const R w0 = R(3) * q0, w1 = R(6) * q1, w2 = R(1) * q2;
       const R norm = w0 + w1 + w2;
@@ -136,9 +148,10 @@ __device__ __forceinline__ R ReconstructPlus(int limiter, const R (&s)[5]) {
     const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
     const R eps = R(1.e-36);
     const R tau = fabs(b2 - b0);
-    const R w0 = R(3) * (R(1) + sq(tau / (eps + b2)));
-    const R w1 = R(6) * (R(1) + sq(tau / (eps + b1)));
-    const R w2 = R(1) * (R(1) + sq(tau / (eps + b0)));
+    (void)eps;
+    const R w0 = R(3) * weno_q(tau, b2);
+    const R w1 = R(6) * weno_q(tau, b1);
+    const R w2 = R(1) * weno_q(tau, b0);
     const R norm = w0 + w1 + w2;
     return (w0 * ep0 + w1 * ep1 + w2 * ep2) / norm;
   } else {
@@ -163,9 +176,10 @@ __device__ __forceinline__ R ReconstructMinus(int limiter, const R (&s)[5]) {
     const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
     const R eps = R(1.e-36);
     const R tau = fabs(b2 - b0);
-    const R w0 = R(3) * (R(1) + sq(tau / (eps + b0)));
-    const R w1 = R(6) * (R(1) + sq(tau / (eps + b1)));
-    const R w2 = R(1) * (R(1) + sq(tau / (eps + b2)));
+    (void)eps;
+    const R w0 = R(3) * weno_q(tau, b0);
+    const R w1 = R(6) * weno_q(tau, b1);
+    const R w2 = R(1) * weno_q(tau, b2);
     const R norm = w0 + w1 + w2;
     return (w0 * em0 + w1 * em1 + w2 * em2) / norm;
   } else {

@@ -69,12 +69,21 @@ struct FusedArgs {
   int nbr[3];
 };
 
+// Global index -> interior index under the physical boundary of that side.
+// The final clamp only matters for partial bricks far outside a tiny mesh;
+// it keeps every access inside the mesh.
 __device__ __forceinline__ int fz_map(int G, int N, int bc, bool &flip) {
   if (G >= 0 && G < N) return G;
-  if (bc == BC_PERIODIC) return ((G % N) + N) % N;
-  if (bc == BC_OUTFLOW) return G < 0 ? 0 : N - 1;
-  flip = !flip;
-  return G < 0 ? -G - 1 : 2 * N - G - 1;
+  int M;
+  if (bc == BC_PERIODIC) {
+    M = ((G % N) + N) % N;
+  } else if (bc == BC_OUTFLOW) {
+    M = G < 0 ? 0 : N - 1;
+  } else {
+    flip = !flip;
+    M = G < 0 ? -G - 1 : 2 * N - G - 1;
+  }
+  return M < 0 ? 0 : (M >= N ? N - 1 : M);
 }
 
 // Load the primitive state of block-interior cell (l0,l1,l2) of block at
