@@ -49,6 +49,8 @@ def args():
     ap.add_argument("--nb", type=int, default=32, help="meshblock cells per dimension")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tasks", action="store_true", help="skip the per-task FP64 arm")
+    ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
+                    help="time one precision only (profiling captures); prints its own line")
     return ap.parse_args()
 
 
@@ -262,7 +264,7 @@ def e2e_solve(a, device: int, stream, K: int):
 
 def load_traffic(precision: str, a):
     """DRAM bytes per fused-stage launch from the committed ncu summary, scaled to this mesh."""
-    p = ROOT / "profiles" / "fused_stage_traffic.json"
+    p = ROOT / "profiles" / "fused_stage_traffic.txt"
     if not p.exists():
         return None
     try:
@@ -323,6 +325,20 @@ def main():
     K, W = a.steps, max(3, a.warmup)
     cells = a.n ** 3
     ns = 3
+
+    if a.only:
+        s1 = make_solver(a, a.only, device, stream)
+        r1 = time_solver(s1, stream, K, W, ws)
+        s1.close()
+        tot = allreduce_max(r1["total_ms"], ws)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": ws * cells * K / (tot / 1e3), "unit": METRIC,
+                              "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": tot / K,
+                              "dtype": "f32" if a.only == "fp32" else "f64",
+                              "launch_ms_avg": r1["stage_ms_avg"], "config": workload_config(a, ws),
+                              "note": "single-precision profiling run; not the headline line"}),
+                  flush=True)
+        return
 
     # headline: FP32 bulk path, fused stages over all blocks
     s32 = make_solver(a, "fp32", device, stream)
