@@ -152,6 +152,25 @@ int kmy_conserved_sums(kmy_ctx *ctx, const char *md, double *out);
 /* Number of this library's kernels launched on the context since creation. */
 int kmy_launch_count(const kmy_ctx *ctx, int64_t *out);
 
+/* Compensated FP64 sums of conserved variables for callers that cannot
+ * allocate device memory (a framework that owns all device memory through its
+ * own pool, or code where an allocation is not allowed or would synchronise
+ * the device).  No counterpart in the reference.  Needs no context and calls
+ * no cudaMalloc/cudaFree: its scratch is a static device array of fixed size
+ * held by every GPU that loads the library.
+ *   cons:   device pointer, [ncons][nblocks][ncells_pad] doubles (MeshData layout)
+ *   out_dev: device pointer to ncons doubles, out_dev[v] = sum over interior
+ *           cells of cons[v] * cell_volume
+ *   stream: cudaStream_t to launch on (NULL = default stream)
+ * ncons above 8 (the scratch array's capacity) returns KMY_ERR_BAD_PARAM.
+ * The first call on a device looks up the scratch array's device address with
+ * that device current; make that first call before any stream capture.  Calls
+ * share the scratch array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+int kmy_conserved_sums_noalloc(const double *cons, int ncons, int nblocks,
+                               const int ncells_pad[3], const int nx[3], const int nghost[3],
+                               double cell_volume, double *out_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,6 +36,7 @@ EXPORTS = (
     "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_end_step", "kmy_get_time",
     "kmy_set_dt",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
+    "kmy_conserved_sums_noalloc",
 )
 
 
@@ -96,6 +97,8 @@ def lib() -> ctypes.CDLL:
         L.kmy_vortex_error.argtypes = [vp, i, i, _dp]
         L.kmy_conserved_sums.argtypes = [vp, cp, _dp]
         L.kmy_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        ip3 = ctypes.POINTER(ctypes.c_int)
+        L.kmy_conserved_sums_noalloc.argtypes = [vp, i, i, ip3, ip3, ip3, d, vp, vp]
         _lib = L
     return _lib
 
