@@ -142,8 +142,9 @@ int kmy_set_dt(kmy_ctx *ctx, double dt);
 int kmy_set_path(kmy_ctx *ctx, int path);
 
 /* ---- diagnostics ----------------------------------------------------------- */
-/* L1 error of dens/velocity/pres against the initial isentropic vortex,
- * (src/problems/isentropic_vortex.hpp:150-200).  var: 0 dens, 1 velocity, 2 pres. */
+/* L1 error of dens/velocity/pres/magc against the initial isentropic vortex
+ * (src/problems/isentropic_vortex.hpp:150-200).  var: 0 dens, 1 velocity,
+ * 2 pres, 3 magc (CT only). */
 int kmy_vortex_error(kmy_ctx *ctx, int var, int comp, double *out);
 /* Compensated (Kahan-Babuska) FP64 sums of the conserved variables over the
  * interior of `md` times the cell volume: out[0..ncons-1]. */

@@ -246,7 +246,7 @@ class Solver:
     # --- diagnostics ---
     def vortex_error(self, var: str = "dens", comp: int = 0) -> float:
         out = ctypes.c_double()
-        self._check(lib().kmy_vortex_error(self._h, {"dens": 0, "velocity": 1, "pres": 2}[var], comp,
+        self._check(lib().kmy_vortex_error(self._h, {"dens": 0, "velocity": 1, "pres": 2, "magc": 3}[var], comp,
                                            ctypes.byref(out)))
         return out.value
 

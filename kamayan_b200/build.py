@@ -26,6 +26,14 @@ NVCC_FLAGS = [
 ]
 
 
+# Per-unit flags.  The FP32 fused stage uses approximate division/square root
+# and flushes denormals: its results are checked against FP64 at an L1 of 1e-5,
+# and the reciprocal/sqrt unit is its busiest pipe.
+EXTRA_FLAGS = {
+    "kmy_fused_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+}
+
+
 def nvcc() -> str:
     for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
         if cand and Path(cand).exists():
@@ -53,7 +61,8 @@ def compile_one(src: Path, verbose_ptxas: bool = False) -> Path:
     obj = BUILD / (src.stem + ".o")
     if not _stale(obj, src) and not verbose_ptxas:
         return obj
-    cmd = [nvcc(), "-ccbin", host_cxx(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), "-ccbin", host_cxx(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src.name, []), "-c", str(src),
+           "-o", str(obj)]
     if verbose_ptxas:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

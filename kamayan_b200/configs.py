@@ -52,6 +52,18 @@ def vortex_2d(n: int = 128, nb: int = 64, recon: str = "plm", limiter: str = "mc
     return d
 
 
+def mhd_vortex_2d(n: int = 64, nb: int = 32, recon: str = "ppm", limiter: str = "mc",
+                  riemann: str = "hll", nghost: int = 4, precision: str = "fp64",
+                  tlim: float = 10.0) -> Deck:
+    """The reference's CT vortex regression (tests/test_suites/mhd_vortex/mhd_vortex.py:37-55)."""
+    d = vortex_2d(n=n, nb=nb, recon=recon, limiter=limiter, riemann=riemann, nghost=nghost,
+                  precision=precision, tlim=tlim)
+    d.set("physics", "MHD", "ct")
+    d.set("isentropic_vortex", "strength", 1.0)
+    d.set("isentropic_vortex", "mhd_strength", 1.0)
+    return d
+
+
 def kh_3d(n: int = 256, nb: int = 32, precision: str = "fp64", recon: str = "wenoz",
           riemann: str = "hllc", integrator: str = "rk3", nghost: int = 3, seed: int = 20240611,
           nlim: int = 200) -> Deck:

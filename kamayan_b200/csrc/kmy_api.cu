@@ -700,7 +700,7 @@ int kmy_set_path(kmy_ctx *c, int path) {
 }
 
 int kmy_vortex_error(kmy_ctx *c, int var, int comp, double *out) {
-  if (!c || !out || var < 0 || var > 2) return KMY_ERR_BAD_PARAM;
+  if (!c || !out || var < 0 || var > 3 || (var == 3 && !c->prm.mhd)) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
   int rc = materialize(c);
   if (!rc) rc = launch_vortex_error(c, var, comp, out);

@@ -305,9 +305,11 @@ __device__ __forceinline__ void RiemannFlux(const R *vL, const R *vR, R *flux) {
       const R susi = R(1.) / (S - ustar + tiny);
       Us[CDENS] = susi * (S * U[CDENS] - U[CMOM0 + DIR1]);
       Us[CMOM0 + DIR1] = Us[CDENS] * ustar;
-      Us[CMOM0 + DIR2] = U[CMOM0 + DIR2] * Us[CDENS] / U[CDENS];
-      Us[CMOM0 + DIR3] = U[CMOM0 + DIR3] * Us[CDENS] / U[CDENS];
-      Us[CENER] = U[CENER] * Us[CDENS] / U[CDENS] + susi * (pstar * ustar - Pu);
+      // U * Us_dens / U_dens with one shared ratio (one division instead of three)
+      const R rho_ratio = Us[CDENS] / U[CDENS];
+      Us[CMOM0 + DIR2] = U[CMOM0 + DIR2] * rho_ratio;
+      Us[CMOM0 + DIR3] = U[CMOM0 + DIR3] * rho_ratio;
+      Us[CENER] = U[CENER] * rho_ratio + susi * (pstar * ustar - Pu);
       if constexpr (MHD) {
         const R sRsLi = R(1.) / (sR - sL);
         auto hll = [&](int v) { return sRsLi * (sR * UR[v] - sL * UL[v] + FL[v] - FR[v]); };

@@ -20,6 +20,7 @@ enum Problem { P_VORTEX = 0, P_KH = 1, P_OT = 2, P_BLAST = 3, P_SEDOV = 4 };
 
 struct PgenParams {
   int problem;
+  int mhd;
   double gamma;
   double p[8];
   unsigned long long seed;
@@ -43,7 +44,19 @@ __global__ void k_pgen_cells(MeshDesc m, PgenParams pp, S *cc, S *prim) {
   const double y = m.xmin[1] + (double(gj) + 0.5) * m.dx[1];
   double dens = 1.0, v0 = 0.0, v1 = 0.0, v2 = 0.0, pres = 1.0;
   const double gamma = pp.gamma;
-  if (pp.problem == P_VORTEX) {
+  if (pp.problem == P_VORTEX && pp.mhd) {
+    // isentropic_vortex.hpp:75-100 (StateMHD); cell B comes from the faces
+    const double pressure = pp.p[1], velx = pp.p[2], vely = pp.p[3], strength = pp.p[4],
+                 mhd_strength = pp.p[5];
+    const double r2 = x * x + y * y;
+    const double dv = strength * exp(0.5 * (1.0 - r2)) / (2.0 * M_PI);
+    const double ex = exp(1.0 - r2);
+    dens = 1.0;
+    pres = pressure + (mhd_strength * mhd_strength / (8.0 * M_PI * M_PI)) * (1.0 - r2) * ex -
+           (strength * strength / (8.0 * M_PI * M_PI)) * ex;
+    v0 = velx - y * dv;
+    v1 = vely + x * dv;
+  } else if (pp.problem == P_VORTEX) {
     const double density = pp.p[0], pressure = pp.p[1], velx = pp.p[2], vely = pp.p[3],
                  strength = pp.p[4];
     const double r2 = x * x + y * y;
@@ -105,6 +118,8 @@ __global__ void k_pgen_faces(MeshDesc m, PgenParams pp, S *fc) {
   const double xc = xf + 0.5 * m.dx[0], yc = yf + 0.5 * m.dx[1];
   const double B0 = 1.0 / sqrt(4.0 * M_PI);
   auto Az = [&](double X, double Y) {
+    if (pp.problem == P_VORTEX)  // isentropic_vortex.hpp:140-144
+      return pp.p[5] / (2. * M_PI) * exp(0.5 * (1.0 - (X * X + Y * Y)));
     if (pp.problem != P_OT) return 0.0;
     return B0 * (cos(4. * M_PI * X) / (4. * M_PI) + cos(2. * M_PI * Y) / (2. * M_PI));
   };
@@ -127,6 +142,8 @@ int launch_pgen(kmy_ctx *c, const std::string &problem) {
     pp.p[2] = p.real("isentropic_vortex/velx", 1.0);
     pp.p[3] = p.real("isentropic_vortex/vely", 1.0);
     pp.p[4] = p.real("isentropic_vortex/strength", 5.0);
+    pp.p[5] = p.real("isentropic_vortex/mhd_strength", 1.0);
+    pp.mhd = p.mhd ? 1 : 0;
   } else if (problem == "kelvin_helmholtz") {
     pp.problem = P_KH;
     pp.p[0] = p.real("kelvin_helmholtz/amplitude", 0.01);

@@ -953,7 +953,7 @@ int launch_conserved_sums(kmy_ctx *c, Container &md, double *out) {
 template <typename S>
 __global__ void k_vortex_err(MeshDesc m, const S *cc, const S *prim, int var, int comp, double gamma,
                              double density, double pressure, double velx, double vely,
-                             double strength, double *part) {
+                             double strength, double mhd_strength, double *part) {
   const long long per = (long long)m.nx[0] * m.nx[1] * m.nx[2];
   const long long tot = per * m.nb;
   const long long NP = (long long)m.nb * m.P;
@@ -974,16 +974,29 @@ __global__ void k_vortex_err(MeshDesc m, const S *cc, const S *prim, int var, in
     const double dv = strength * exp(0.5 * (1.0 - r2)) / (2.0 * M_PI);
     const double T = pressure / density -
                      (gamma - 1.0) * strength * strength * exp(1.0 - r2) / (8.0 * gamma * M_PI * M_PI);
-    const double dens = pow(T, 1.0 / (gamma - 1.0));
+    double dens = pow(T, 1.0 / (gamma - 1.0));
+    double presx = T * dens, Bx = 0.0, By = 0.0;
+    if (mhd_strength >= 0.0) {  // StateMHD (isentropic_vortex.hpp:75-100)
+      const double dB = mhd_strength * exp(0.5 * (1.0 - r2)) / (2.0 * M_PI);
+      const double ex = exp(1.0 - r2);
+      dens = 1.0;
+      presx = pressure + (mhd_strength * mhd_strength / (8.0 * M_PI * M_PI)) * (1.0 - r2) * ex -
+              (strength * strength / (8.0 * M_PI * M_PI)) * ex;
+      Bx = -y * dB;
+      By = +x * dB;
+    }
     double exact, have;
-    if (var == 0) {
+    if (var == 3) {
+      exact = comp == 0 ? Bx : comp == 1 ? By : 0.0;
+      have = double(cc[(CMAGC0 + comp) * NP + n]);
+    } else if (var == 0) {
       exact = dens;
       have = double(cc[n]);
     } else if (var == 1) {
       exact = comp == 0 ? velx - y * dv : comp == 1 ? vely + x * dv : 0.0;
       have = double(prim[(PVEL0 + comp) * NP + n]);
     } else {
-      exact = T * dens;
+      exact = presx;
       have = double(prim[PPRES * NP + n]);
     }
     s += fabs(exact - have) * m.vol;
@@ -1007,12 +1020,13 @@ int launch_vortex_error(kmy_ctx *c, int var, int comp, double *out) {
   const double dn = p.real("isentropic_vortex/density", 1.0), pr = p.real("isentropic_vortex/pressure", 1.0);
   const double vx = p.real("isentropic_vortex/velx", 1.0), vy = p.real("isentropic_vortex/vely", 1.0);
   const double st = p.real("isentropic_vortex/strength", 5.0);
+  const double ms = p.mhd ? p.real("isentropic_vortex/mhd_strength", 1.0) : -1.0;
   if (c->esz == 8)
     k_vortex_err<double><<<kSumBlocks, kThreads, 0, c->stream>>>(m, (const double *)b.cc, (const double *)c->prim,
-                                                                 var, comp, p.gamma, dn, pr, vx, vy, st, part);
+                                                                 var, comp, p.gamma, dn, pr, vx, vy, st, ms, part);
   else
     k_vortex_err<float><<<kSumBlocks, kThreads, 0, c->stream>>>(m, (const float *)b.cc, (const float *)c->prim,
-                                                                var, comp, p.gamma, dn, pr, vx, vy, st, part);
+                                                                var, comp, p.gamma, dn, pr, vx, vy, st, ms, part);
   c->launches++;
   std::vector<double> h(kSumBlocks);
   rc = cuda_check(c, cudaGetLastError(), "vortex err");

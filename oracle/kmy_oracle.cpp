@@ -1083,7 +1083,27 @@ int Sim::pgen(const std::string &problem) {
           const Real x = xcen(b, 0, i), y = xcen(b, 1, j), z = xcen(b, 2, k);
           (void)z;
           Real dens = 1., v0 = 0., v1 = 0., v2 = 0., pres = 1.;
-          if (problem == "isentropic_vortex") {
+          if (problem == "isentropic_vortex" && ph.mhd) {
+            // isentropic_vortex.hpp:75-100 (StateMHD, Balsara 2004)
+            const Real pressure = deck.real("isentropic_vortex/pressure", 1.0);
+            const Real velx = deck.real("isentropic_vortex/velx", 1.0);
+            const Real vely = deck.real("isentropic_vortex/vely", 1.0);
+            const Real strength = deck.real("isentropic_vortex/strength", 5.0);
+            const Real mhd_strength = deck.real("isentropic_vortex/mhd_strength", 1.0);
+            const Real r2 = x * x + y * y;
+            const Real dv = strength * std::exp(0.5 * (1.0 - r2)) / (2.0 * M_PI);
+            const Real dB = mhd_strength * std::exp(0.5 * (1.0 - r2)) / (2.0 * M_PI);
+            const Real ex = std::exp(1.0 - r2);
+            dens = 1.0;
+            pres = pressure + (mhd_strength * mhd_strength / (8.0 * M_PI * M_PI)) * (1.0 - r2) * ex -
+                   (strength * strength / (8.0 * M_PI * M_PI)) * ex;
+            v0 = velx - y * dv;
+            v1 = vely + x * dv;
+            v2 = 0.0;
+            cc(c, CMAGC0, b)[n] = -y * dB;
+            cc(c, CMAGC0 + 1, b)[n] = +x * dB;
+            cc(c, CMAGC0 + 2, b)[n] = 0.0;
+          } else if (problem == "isentropic_vortex") {
             // isentropic_vortex.hpp:31-51
             const Real density = deck.real("isentropic_vortex/density", 1.0);
             const Real pressure = deck.real("isentropic_vortex/pressure", 1.0);
@@ -1150,7 +1170,13 @@ int Sim::pgen(const std::string &problem) {
         }
   if (ph.mhd) {
     // face B from a vector potential (isentropic_vortex.cpp:352-375 pattern)
+    const Real mhd_strength = deck.real("isentropic_vortex/mhd_strength", 1.0);
     auto Az = [&](Real x, Real y) {
+      if (problem == "isentropic_vortex") {  // isentropic_vortex.hpp:140-144
+        const Real r2 = x * x + y * y;
+        const Real ex = std::exp(0.5 * (1.0 - r2));
+        return mhd_strength / (2. * M_PI) * ex;
+      }
       if (problem == "orszag_tang") {
         const Real B0 = 1.0 / std::sqrt(4.0 * M_PI);
         return B0 * (std::cos(4. * M_PI * x) / (4. * M_PI) + std::cos(2. * M_PI * y) / (2. * M_PI));
@@ -1202,16 +1228,31 @@ Real Sim::vortex_error(int var, int comp) {
           const Real T = pressure / density - (gamma - 1.0) * strength * strength *
                                                   std::exp(1.0 - r2) /
                                                   (8.0 * gamma * M_PI * M_PI);
-          const Real dens = std::pow(T, 1.0 / (gamma - 1.0));
+          Real dens = std::pow(T, 1.0 / (gamma - 1.0));
+          Real presx = T * dens;
+          Real Bx = 0.0, By = 0.0;
+          if (ph.mhd) {  // StateMHD (isentropic_vortex.hpp:75-100)
+            const Real mhd_strength = deck.real("isentropic_vortex/mhd_strength", 1.0);
+            const Real dB = mhd_strength * std::exp(0.5 * (1.0 - r2)) / (2.0 * M_PI);
+            const Real ex = std::exp(1.0 - r2);
+            dens = 1.0;
+            presx = pressure + (mhd_strength * mhd_strength / (8.0 * M_PI * M_PI)) * (1.0 - r2) * ex -
+                    (strength * strength / (8.0 * M_PI * M_PI)) * ex;
+            Bx = -y * dB;
+            By = +x * dB;
+          }
           Real exact, have;
-          if (var == 0) {
+          if (var == 3) {
+            exact = comp == 0 ? Bx : comp == 1 ? By : 0.0;
+            have = cc(c, CMAGC0 + comp, b)[n];
+          } else if (var == 0) {
             exact = dens;
             have = cc(c, CDENS, b)[n];
           } else if (var == 1) {
             exact = comp == 0 ? velx - y * dv : comp == 1 ? vely + x * dv : 0.0;
             have = pr(PVEL0 + comp, b)[n];
           } else {
-            exact = T * dens;
+            exact = presx;
             have = pr(PPRES, b)[n];
           }
           err += std::fabs(exact - have) * CellVolume();

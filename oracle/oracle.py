@@ -172,7 +172,7 @@ class OracleSim:
         return dict(time=out[0], dt=out[1], dt_est=out[2], ncycle=int(out[3]))
 
     def vortex_error(self, var: str = "dens", comp: int = 0) -> float:
-        v = {"dens": 0, "velocity": 1, "pres": 2}[var]
+        v = {"dens": 0, "velocity": 1, "pres": 2, "magc": 3}[var]
         return lib().kmyo_vortex_error(self._h, v, comp)
 
     def interior(self, arr: np.ndarray) -> np.ndarray:

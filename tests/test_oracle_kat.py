@@ -111,6 +111,17 @@ def test_vortex_convergence_wenoz(oracle_mod):
     assert min(slopes) > 1.5, slopes
 
 
+def test_mhd_vortex_ct_threshold(oracle_mod):
+    """CT vortex: PPM-MC, HLL, RK2, 64^2, t=10; magx L1 < 0.05 (mhd_vortex.py:25-27,298-299)
+    and div B at round-off."""
+    s = oracle_mod.OracleSim(configs.mhd_vortex_2d().text())
+    s.pgen("isentropic_vortex")
+    s.evolve(10.0)
+    err = s.vortex_error("magc", 0)
+    assert err < 0.05 and np.isfinite(err)
+    assert np.abs(s.interior(s.get("divb"))).max() < 1e-10
+
+
 def test_oracle_thread_count_independent(oracle_mod):
     # the oracle's OpenMP block loops must not change a single bit
     import os
