@@ -49,6 +49,9 @@ def args():
     ap.add_argument("--nb", type=int, default=32, help="meshblock cells per dimension")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tasks", action="store_true", help="skip the per-task FP64 arm")
+    ap.add_argument("--serve", type=int, default=120,
+                    help="requests in the serving-stream measurement (0: skip; 2000 = full stream)")
+    ap.add_argument("--serve-steps", type=int, default=100)
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
                     help="time one precision only (profiling captures); prints its own line")
     return ap.parse_args()
@@ -292,6 +295,29 @@ def cpu_baseline(sample_n: int, min_seconds: float, max_steps: int, steps: int =
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
+def serving_block(a, device: int) -> dict:
+    """Serving stream: saturation capacity, Poisson arrivals at 0.8 x capacity,
+    and the same requests solved one after another without batching."""
+    from kamayan_b200 import serving
+
+    reqs = [serving.make_request(i) for i in range(a.serve)]
+    sat = serving.run_stream(reqs, a.serve_steps, arrivals=None, device=device)
+    mean_work = sum(r.cells for r in reqs) * a.serve_steps / len(reqs)
+    rate = 0.8 * sat["cell_updates_per_s"] / mean_work
+    arrivals = serving.poisson_arrivals(len(reqs), rate, seed=11)
+    poi = serving.run_stream(reqs, a.serve_steps, arrivals=arrivals, device=device)
+    nseq = min(len(reqs), 24)
+    seq = serving.run_sequential(reqs[:nseq], a.serve_steps, device=device)
+    return {
+        "workload": f"{a.serve} requests (seeded mix of vortex/blast, 64^2..128^3, PLM/HLL, PPM/HLLC, "
+                    f"WENO-Z/HLLC, FP32/FP64), {a.serve_steps} RK2 steps each",
+        "saturation": sat,
+        "poisson": dict(poi, offered_load=0.8, rate_per_s=rate),
+        "sequential_per_solve": seq,
+        "batched_over_sequential": sat["cell_updates_per_s"] / seq["cell_updates_per_s"],
+    }
+
+
 def main_reference(a):
     ws, rank, _ = dist_init()
     if rank != 0:
@@ -404,6 +430,8 @@ def main():
         "l1_density_fp32_vs_fp64": l1,
         "sim_time_fp32_fp64": [t32, t64],
     }
+    if a.serve > 0:
+        line["serving"] = serving_block(a, device)
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         cb = cpu_baseline(128, 10.0, 200)
         line["cpu_baseline"] = {"value": cb.get("value"), "unit": METRIC, "cores": cb.get("threads"),

@@ -153,6 +153,35 @@ int kmy_conserved_sums(kmy_ctx *ctx, const char *md, double *out);
 /* Number of this library's kernels launched on the context since creation. */
 int kmy_launch_count(const kmy_ctx *ctx, int64_t *out);
 
+/* ---- serving loop: continuously batched independent solves ----------------
+ * No counterpart in the reference (which runs one mesh per process).  A
+ * server owns one CUDA stream and an HBM budget (a fraction of the free
+ * device memory at creation).  Requests are a deck, a problem generator and a
+ * step count; kmy_server_tick admits queued requests whose footprint fits the
+ * budget, then advances every admitted solve by one RK step with one
+ * persistent launch per stage per kernel class (precision, dimensionality,
+ * reconstruction, Riemann solver), replayed from a CUDA graph.  Hydro decks
+ * with rk2/rk3 only.  Times are host seconds. */
+typedef struct kmy_server kmy_server;
+int kmy_server_create(int device, double hbm_fraction, int use_graphs, kmy_server **out);
+int kmy_server_destroy(kmy_server *srv);
+const char *kmy_server_last_error(const kmy_server *srv);
+int kmy_server_submit(kmy_server *srv, const char *deck, const char *problem, int nsteps,
+                      int64_t *id);
+/* Admit, step every active solve once, retire finished ones. */
+int kmy_server_tick(kmy_server *srv, int *nactive, int *nqueued);
+/* Finished requests since the last poll: id, time-to-solution (submit to
+ * completion), status (KMY_OK or the failure code). */
+int kmy_server_poll(kmy_server *srv, int64_t *ids, double *seconds, int *status, int max, int *n);
+/* Final state of a finished request (MeshData layout, like kmy_export_var). */
+int kmy_server_export(kmy_server *srv, int64_t id, const char *var, int comp, double *host,
+                      size_t n);
+/* Free a finished request's device state. */
+int kmy_server_release(kmy_server *srv, int64_t id);
+/* out[0..7]: active, queued, finished, bytes in use, byte budget, ticks,
+ * cell updates done, kernel launches. */
+int kmy_server_stats(const kmy_server *srv, double *out);
+
 /* Compensated FP64 sums of conserved variables for callers that cannot
  * allocate device memory (a framework that owns all device memory through its
  * own pool, or code where an allocation is not allowed or would synchronise

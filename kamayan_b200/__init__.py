@@ -37,6 +37,9 @@ EXPORTS = (
     "kmy_set_dt",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
     "kmy_conserved_sums_noalloc",
+    "kmy_server_create", "kmy_server_destroy", "kmy_server_last_error", "kmy_server_submit",
+    "kmy_server_tick", "kmy_server_poll", "kmy_server_export", "kmy_server_release",
+    "kmy_server_stats",
 )
 
 
@@ -99,6 +102,17 @@ def lib() -> ctypes.CDLL:
         L.kmy_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         ip3 = ctypes.POINTER(ctypes.c_int)
         L.kmy_conserved_sums_noalloc.argtypes = [vp, i, i, ip3, ip3, ip3, d, vp, vp]
+        i64p = ctypes.POINTER(ctypes.c_int64)
+        L.kmy_server_create.argtypes = [i, d, i, ctypes.POINTER(vp)]
+        L.kmy_server_destroy.argtypes = [vp]
+        L.kmy_server_last_error.restype = cp
+        L.kmy_server_last_error.argtypes = [vp]
+        L.kmy_server_submit.argtypes = [vp, cp, cp, i, i64p]
+        L.kmy_server_tick.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.kmy_server_poll.argtypes = [vp, i64p, _dp, ctypes.POINTER(i), i, ctypes.POINTER(i)]
+        L.kmy_server_export.argtypes = [vp, ctypes.c_int64, cp, i, _dp, sz]
+        L.kmy_server_release.argtypes = [vp, ctypes.c_int64]
+        L.kmy_server_stats.argtypes = [vp, _dp]
         _lib = L
     return _lib
 
@@ -267,3 +281,69 @@ class Solver:
         g2 = g if i.ndim > 1 else 0
         g3 = g if i.ndim > 2 else 0
         return arr[:, g3:g3 + i.nx[2], g2:g2 + i.nx[1], g:g + i.nx[0]]
+
+
+class Server:
+    """Serving loop over the C ABI: continuously batched independent solves."""
+
+    STATS = ("active", "queued", "finished", "bytes_in_use", "budget", "ticks", "cell_updates",
+             "launches")
+
+    def __init__(self, device: int = 0, hbm_fraction: float = 0.8, graphs: bool = True):
+        h = ctypes.c_void_p()
+        rc = lib().kmy_server_create(device, hbm_fraction, int(graphs), ctypes.byref(h))
+        if rc:
+            raise KmyError(rc, "kmy_server_create failed")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().kmy_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise KmyError(rc, lib().kmy_server_last_error(self._h).decode())
+
+    def submit(self, deck, problem: str, nsteps: int) -> int:
+        text = deck.text() if isinstance(deck, Deck) else deck
+        rid = ctypes.c_int64()
+        self._check(lib().kmy_server_submit(self._h, text.encode(), problem.encode(), nsteps,
+                                            ctypes.byref(rid)))
+        return rid.value
+
+    def tick(self) -> tuple[int, int]:
+        a, q = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().kmy_server_tick(self._h, ctypes.byref(a), ctypes.byref(q)))
+        return a.value, q.value
+
+    def poll(self, max_items: int = 4096) -> list[tuple[int, float, int]]:
+        ids = (ctypes.c_int64 * max_items)()
+        secs = (ctypes.c_double * max_items)()
+        st = (ctypes.c_int * max_items)()
+        n = ctypes.c_int()
+        self._check(lib().kmy_server_poll(self._h, ids, secs, st, max_items, ctypes.byref(n)))
+        return [(ids[k], secs[k], st[k]) for k in range(n.value)]
+
+    def export(self, rid: int, var: str, shape, comp: int = 0) -> np.ndarray:
+        out = np.empty(shape, dtype=np.float64)
+        self._check(lib().kmy_server_export(self._h, rid, var.encode(), comp, _ptr(out), out.size))
+        return out
+
+    def release(self, rid: int) -> None:
+        self._check(lib().kmy_server_release(self._h, rid))
+
+    @property
+    def stats(self) -> dict:
+        out = np.zeros(8)
+        self._check(lib().kmy_server_stats(self._h, _ptr(out)))
+        return dict(zip(self.STATS, out.tolist()))

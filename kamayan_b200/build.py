@@ -31,6 +31,9 @@ NVCC_FLAGS = [
 # and the reciprocal/sqrt unit is its busiest pipe.
 EXTRA_FLAGS = {
     "kmy_fused_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+    # same arithmetic as the single-mesh FP32 stage, so a solve gives the same
+    # bits alone and inside a batch
+    "kmy_batch_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
 }
 
 

@@ -187,6 +187,31 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   return KMY_OK;
 }
 
+// Device bytes a fused-path context for `deck` allocates at kmy_create, and
+// the deck's kernel class.  Host-only: parses and validates the deck.
+int deck_footprint(const char *deck, Footprint *out, std::string *err) {
+  kmy_ctx tmp;
+  const int rc = setup_params(&tmp, deck);
+  if (rc) {
+    if (err) *err = tmp.err;
+    return rc;
+  }
+  const MeshDesc &m = tmp.m;
+  const size_t n = size_t(m.nb) * m.P, nf = size_t(m.nb) * m.Pf;
+  const size_t ns = tmp.prm.beta.size();
+  size_t per = tmp.esz * tmp.ncc * n + (tmp.esz == 4 ? 4 * n : 0);
+  if (tmp.prm.mhd) per += 2 * tmp.esz * 3 * nf;
+  out->bytes = ns * per + tmp.esz * NPRIM * n + (tmp.prm.mhd ? 8 * n : 0) + sizeof(DevClock) + 512;
+  out->esz = int(tmp.esz);
+  out->ndim = m.ndim;
+  out->recon = tmp.prm.recon;
+  out->riemann = tmp.prm.riemann;
+  out->nstages = int(ns);
+  out->mhd = tmp.prm.mhd ? 1 : 0;
+  out->cells = (long long)m.mesh_nx[0] * m.mesh_nx[1] * m.mesh_nx[2];
+  return KMY_OK;
+}
+
 static int dalloc(kmy_ctx *c, void **p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return KMY_OK;
@@ -217,10 +242,18 @@ static int make_container(kmy_ctx *c, const std::string &name) {
 
 using namespace kmy;
 
+// Containers by name.  "dUdt" is only needed by the per-task path and is
+// allocated on first use, so fused-only contexts (the serving path) never
+// hold it.
 static Container *find_container(kmy_ctx *c, const char *name) {
-  auto it = c->md.find(name ? name : "");
+  const std::string n(name ? name : "");
+  auto it = c->md.find(n);
+  if (it == c->md.end() && n == "dUdt") {
+    if (make_container(c, "dUdt")) return nullptr;
+    it = c->md.find(n);
+  }
   if (it == c->md.end()) {
-    c->err = std::string("unknown container ") + (name ? name : "(null)");
+    c->err = "unknown container " + n;
     return nullptr;
   }
   return &it->second;
@@ -338,7 +371,6 @@ int kmy_create(const char *deck, int device, kmy_ctx **out) {
   const size_t n = size_t(c->m.nb) * c->m.P;
   for (size_t s = 0; s + 1 < c->prm.stage_name.size() && !rc; s++)
     if (!c->md.count(c->prm.stage_name[s])) rc = make_container(c, c->prm.stage_name[s]);
-  if (!rc) rc = make_container(c, "dUdt");
   if (!rc) rc = dalloc(c, &c->prim, c->esz * NPRIM * n);
   if (!rc && c->prm.mhd) rc = dalloc(c, reinterpret_cast<void **>(&c->divb), 8 * n);
   if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&c->clock), sizeof(DevClock));
@@ -560,8 +592,10 @@ int kmy_fill_derived(kmy_ctx *c, const char *md) {
 static int task_stage(kmy_ctx *c, int stage, double dt) {
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());
+  Container *dup = find_container(c, "dUdt");
+  if (!dup) return KMY_ERR_OOM;
   Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
-  Container &du = c->md["dUdt"];
+  Container &du = *dup;
   if (!c->prims_valid) {
     // primitives of md0 are needed with ghosts (fused steps leave them stale)
     int rc = launch_prepare_primitive(c, md0);
@@ -592,8 +626,19 @@ int kmy_task_stage(kmy_ctx *c, int stage, double dt) {
 static int fused_stage(kmy_ctx *c, int stage) {
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());
-  Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
   const bool stored = stage == 1 && c->prims_valid;
+  if (ns == 1) {
+    // rk1 updates base in place (stage names base -> base).  The fused stage
+    // reads neighbouring bricks' halos while it writes, so it writes a scratch
+    // container and the two swap roles afterwards.
+    if (!c->md.count("1") && make_container(c, "1")) return KMY_ERR_OOM;
+    Container &base = c->md["base"], &out = c->md["1"];
+    int rc = launch_fused_stage(c, base, base, out, c->prm.beta[0], stored, true);
+    if (!rc) std::swap(c->md["base"], c->md["1"]);
+    c->prims_valid = false;
+    return rc;
+  }
+  Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
   int rc = launch_fused_stage(c, base, md0, md1, c->prm.beta[stage - 1], stored, stage == ns);
   c->prims_valid = false;
   return rc;

@@ -1,0 +1,12 @@
+// float instantiations of the batched fused stage (separate unit for parallel builds).
+#include "kmy_batch.cuh"
+
+namespace kmy {
+int batch_stage_f32(cudaStream_t stream, int ndim, int recon, int riemann, const void *desc,
+                   const long long *prefix, const int *n, int stage, int *grid_io) {
+  return batch_stage<float>(stream, ndim, recon, riemann, desc, prefix, n, stage, grid_io);
+}
+int batch_controller_f32(cudaStream_t stream, void *desc, const int *n, int capacity, BatchStatus *st) {
+  return batch_controller<float>(stream, desc, n, capacity, st);
+}
+}  // namespace kmy

@@ -213,20 +213,16 @@ __device__ __forceinline__ void fz_direction(const FusedArgs<S> &a, const int lx
   __syncthreads();
 }
 
+// Brick br of block b for one stage: the whole per-CTA body.  Every thread of
+// the CTA calls it (it synchronises internally).
 template <typename S, int NDIM, int RECON, int RIEMANN>
-__global__ void __launch_bounds__(256) k_fused_stage(FusedArgs<S> a) {
+__device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br, double dt) {
   using Sh = FusedShape<NDIM, RECON>;
-  const DevClock *clk = a.clock;
-  if (clk->done) return;
-  const double dt = clk->dt;
   extern __shared__ __align__(16) unsigned char kmy_smem[];
   S *sp = reinterpret_cast<S *>(kmy_smem);
   S *sf = sp + Sh::NR * Sh::REG_MAX;
 
   const MeshDesc &m = a.m;
-  const int nbrick = a.nbr[0] * a.nbr[1] * a.nbr[2];
-  const int b = blockIdx.x / nbrick;
-  const int br = blockIdx.x - b * nbrick;
   const int o[3] = {(br % a.nbr[0]) * Sh::B[0], ((br / a.nbr[0]) % a.nbr[1]) * Sh::B[1],
                     (br / (a.nbr[0] * a.nbr[1])) * Sh::B[2]};
   const int lx[3] = {b % m.nbx[0], (b / m.nbx[0]) % m.nbx[1], b / (m.nbx[0] * m.nbx[1])};
@@ -302,6 +298,97 @@ __global__ void __launch_bounds__(256) k_fused_stage(FusedArgs<S> a) {
       if (!(v >= 0.0)) v = 0.0;
       atomicMin(&a.clock->dtmin_bits, (unsigned long long)__double_as_longlong(v));
     }
+  }
+}
+
+// One stage of one mesh: one CTA per brick.
+template <typename S, int NDIM, int RECON, int RIEMANN>
+__global__ void __launch_bounds__(256) k_fused_stage(FusedArgs<S> a) {
+  if (a.clock->done) return;
+  const int nbrick = a.nbr[0] * a.nbr[1] * a.nbr[2];
+  const int b = blockIdx.x / nbrick;
+  fused_brick<S, NDIM, RECON, RIEMANN>(a, b, blockIdx.x - b * nbrick, a.clock->dt);
+}
+
+// ---------------------------------------------------------------------------
+// Batched stage over many independent solves of one kernel class (precision,
+// dimensionality, reconstruction, Riemann solver).  The work list is
+// (solve, block, brick) with per-solve offsets prefix[]; a persistent grid
+// strides over it.  The list, its length and every solve's clock live in
+// device memory, so the same launch (and a CUDA graph of it) serves any mix.
+template <typename S>
+struct SolveDesc {
+  MeshDesc m;
+  EosParams eos;
+  TimeParams tp;
+  int limiter;
+  int nstages;
+  int nlim;       // steps after which the solve is done (< 0: none)
+  int stored;     // stage 1 of the next step reads stored primitives (cleared by the controller)
+  S *cont[3];     // containers "base", "1", "2"
+  float *lo[3];   // their FP32 energy low words (FP32 only)
+  const S *prim;
+  double beta[3];
+  DevClock *clock;
+  int nbr[3];
+};
+
+template <typename S>
+__device__ __forceinline__ void batch_args(const SolveDesc<S> &q, int stage, FusedArgs<S> &a) {
+  // stage names base, 1, ..., nstages-1, base (Parthenon low-storage integrators)
+  const int i0 = stage - 1, i1 = stage == q.nstages ? 0 : stage;
+  a.m = q.m;
+  a.eos = q.eos;
+  a.limiter = q.limiter;
+  a.u0 = q.cont[i0];
+  a.u0lo = q.lo[i0];
+  a.ub = q.cont[0];
+  a.ublo = q.lo[0];
+  a.u1 = q.cont[i1];
+  a.u1lo = q.lo[i1];
+  a.prim = q.prim;
+  a.stored = stage == 1 ? q.stored : 0;
+  a.last = stage == q.nstages;
+  a.beta = q.beta[stage - 1];
+  a.clock = q.clock;
+  a.nbr[0] = q.nbr[0];
+  a.nbr[1] = q.nbr[1];
+  a.nbr[2] = q.nbr[2];
+}
+
+template <typename S, int NDIM, int RECON, int RIEMANN>
+__global__ void __launch_bounds__(256) k_fused_batch(const SolveDesc<S> *__restrict__ d,
+                                                     const long long *__restrict__ prefix,
+                                                     const int *nsolves_dev, int stage) {
+  __shared__ FusedArgs<S> sa;
+  __shared__ long long s_base;
+  __shared__ int s_skip;
+  __shared__ double s_dt;
+  const int ns = *nsolves_dev;
+  if (ns <= 0) return;
+  const long long total = prefix[ns];
+  for (long long w = blockIdx.x; w < total; w += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = ns - 1;  // last solve whose offset is <= w
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= w) lo = mid;
+        else hi = mid - 1;
+      }
+      const SolveDesc<S> &q = d[lo];
+      s_base = prefix[lo];
+      s_skip = q.clock->done || stage > q.nstages;
+      s_dt = q.clock->dt;
+      batch_args(q, stage, sa);
+    }
+    __syncthreads();
+    if (!s_skip) {
+      const long long wl = w - s_base;
+      const int nbrick = sa.nbr[0] * sa.nbr[1] * sa.nbr[2];
+      const int b = int(wl / nbrick);
+      fused_brick<S, NDIM, RECON, RIEMANN>(sa, b, int(wl - (long long)b * nbrick), s_dt);
+    }
+    __syncthreads();
   }
 }
 

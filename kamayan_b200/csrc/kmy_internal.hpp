@@ -54,6 +54,29 @@ struct TimeParams {
   int nlim;
 };
 
+// Parthenon EvolutionDriver time update + SetGlobalTimeStep after a step,
+// restated: time += dt, then dt <- min(dt * dt_factor, CFL estimate, ceilings),
+// clamped so the run ends exactly at tlim.  The estimate is the atomic minimum
+// of dx/(|v|+c_f) left by the last stage.
+__device__ __forceinline__ void advance_clock(DevClock *clk, const TimeParams &tp) {
+  const double dtmin = __longlong_as_double((long long)clk->dtmin_bits);
+  const double big = 1.7976931348623157e308;
+  clk->dt_taken = clk->dt;
+  clk->time += clk->dt;
+  clk->ncycle += 1;
+  const double est = dtmin * tp.cfl_over_ndim;
+  clk->dt_est = est;
+  if (!(est > 0.0) || !(est < big)) clk->status = 3;  // KMY_ERR_NONFINITE
+  double nd = clk->dt;
+  if (nd < 0.1 * big) nd *= tp.dt_factor;
+  nd = fmin(nd, est);
+  nd = fmin(nd, tp.dt_ceil);
+  nd = fmin(nd, tp.dt_user);
+  if (clk->time < tp.tlim && (tp.tlim - clk->time) < nd) nd = tp.tlim - clk->time;
+  clk->dt = nd;
+  clk->done = clk->time >= tp.tlim;
+}
+
 struct Params {
   int recon = FOG, limiter = MINMOD, riemann = HLL;
   bool mhd = false;
@@ -125,5 +148,13 @@ int launch_fused_stage(kmy_ctx *c, Container &base, Container &md0, Container &m
 int launch_pgen(kmy_ctx *c, const std::string &problem);
 
 int cuda_check(kmy_ctx *c, cudaError_t e, const char *what);
+
+// Device footprint and kernel class of a deck (kmy_api.cu), for admission.
+struct Footprint {
+  size_t bytes;
+  int esz, ndim, recon, riemann, nstages, mhd;
+  long long cells;
+};
+int deck_footprint(const char *deck, Footprint *out, std::string *err);
 
 }  // namespace kmy

@@ -702,9 +702,8 @@ __global__ void k_dt_controller(DevClock *clk, TimeParams tp, int mode) {
   }
   if (mode == 0) {
     if (clk->done) return;
-    clk->dt_taken = clk->dt;
-    clk->time += clk->dt;
-    clk->ncycle += 1;
+    advance_clock(clk, tp);
+    return;
   } else {
     clk->time = 0.0;
     clk->ncycle = 0;
@@ -724,6 +723,7 @@ __global__ void k_dt_controller(DevClock *clk, TimeParams tp, int mode) {
   if (clk->time < tp.tlim && (tp.tlim - clk->time) < nd) nd = tp.tlim - clk->time;
   clk->dt = nd;
   clk->done = clk->time >= tp.tlim;
+  clk->dtmin_bits = 0x7FF0000000000000ull;  // the next step's CFL minimum starts at +inf
 }
 
 int launch_dt_controller(kmy_ctx *c, int mode) {
