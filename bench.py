@@ -306,7 +306,8 @@ def serving_block(a, device: int) -> dict:
     rate = 0.8 * sat["cell_updates_per_s"] / mean_work
     arrivals = serving.poisson_arrivals(len(reqs), rate, seed=11)
     poi = serving.run_stream(reqs, a.serve_steps, arrivals=arrivals, device=device)
-    nseq = min(len(reqs), 24)
+    # the same requests, one after another, each on its own context (no batching)
+    nseq = len(reqs) if len(reqs) <= 240 else 240
     seq = serving.run_sequential(reqs[:nseq], a.serve_steps, device=device)
     return {
         "workload": f"{a.serve} requests (seeded mix of vortex/blast, 64^2..128^3, PLM/HLL, PPM/HLLC, "

@@ -212,13 +212,28 @@ int deck_footprint(const char *deck, Footprint *out, std::string *err) {
   return KMY_OK;
 }
 
-static int dalloc(kmy_ctx *c, void **p, size_t bytes) {
+// Context memory comes from the device's stream-ordered pool.  The pool keeps
+// freed blocks for reuse (release threshold raised once per device, for this
+// process only), so creating and destroying contexts -- one per request in
+// the serving loop -- does not synchronise the device or return to the driver.
+static void keep_pool(int device) {
+  static bool done[64] = {};
+  if (device < 0 || device >= 64 || done[device]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t threshold = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  done[device] = true;
+}
+
+int dalloc(kmy_ctx *c, void **p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return KMY_OK;
-  cudaError_t e = cudaMalloc(p, bytes);
+  cudaError_t e = cudaMallocAsync(p, bytes, c->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    c->err = "cudaMalloc of " + std::to_string(bytes) + " bytes failed";
+    c->err = "device allocation of " + std::to_string(bytes) + " bytes failed";
     return KMY_ERR_OOM;
   }
   c->allocations.push_back(*p);
@@ -368,6 +383,7 @@ int kmy_create(const char *deck, int device, kmy_ctx **out) {
     return rc;
   }
   c->own_stream = true;
+  keep_pool(device);
   const size_t n = size_t(c->m.nb) * c->m.P;
   for (size_t s = 0; s + 1 < c->prm.stage_name.size() && !rc; s++)
     if (!c->md.count(c->prm.stage_name[s])) rc = make_container(c, c->prm.stage_name[s]);
@@ -388,8 +404,8 @@ int kmy_create(const char *deck, int device, kmy_ctx **out) {
 int kmy_destroy(kmy_ctx *c) {
   if (!c) return KMY_OK;
   cudaSetDevice(c->device);
+  for (void *p : c->allocations) cudaFreeAsync(p, c->stream);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (void *p : c->allocations) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return KMY_OK;

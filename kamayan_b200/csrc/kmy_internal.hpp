@@ -148,6 +148,8 @@ int launch_fused_stage(kmy_ctx *c, Container &base, Container &md0, Container &m
 int launch_pgen(kmy_ctx *c, const std::string &problem);
 
 int cuda_check(kmy_ctx *c, cudaError_t e, const char *what);
+// Zeroed device allocation from the stream-ordered pool, freed with the context.
+int dalloc(kmy_ctx *c, void **p, size_t bytes);
 
 // Device footprint and kernel class of a deck (kmy_api.cu), for admission.
 struct Footprint {

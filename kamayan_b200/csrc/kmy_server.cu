@@ -50,6 +50,7 @@ struct Batch {
   std::vector<Request *> members;
   bool dirty = true;
   int capacity = 0;
+  cudaStream_t stream = nullptr;  // one stream per class: classes overlap on the GPU
   void *d_desc = nullptr;
   long long *d_prefix = nullptr;
   int *d_n = nullptr;
@@ -163,13 +164,13 @@ static int upload(kmy_server *s, Batch &b) {
     }
     prefix[i + 1] = prefix[i] + nbrick * c->m.nb;
   }
-  cudaError_t e = cudaMemcpyAsync(b.d_desc, desc.data(), dsz * n, cudaMemcpyHostToDevice, s->stream);
+  cudaError_t e = cudaMemcpyAsync(b.d_desc, desc.data(), dsz * n, cudaMemcpyHostToDevice, b.stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b.d_prefix, prefix.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice,
-                        s->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(b.d_n, &n, sizeof(int), cudaMemcpyHostToDevice, s->stream);
+                        b.stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b.d_n, &n, sizeof(int), cudaMemcpyHostToDevice, b.stream);
   // the host vectors are released on return: finish the copies first
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
   if (e != cudaSuccess) return srv_fail(s, KMY_ERR_CUDA, cudaGetErrorString(e));
   b.dirty = false;
   return KMY_OK;
@@ -179,14 +180,14 @@ static int upload(kmy_server *s, Batch &b) {
 static int launch_step(kmy_server *s, Batch &b) {
   int rc = 0;
   for (int st = 1; st <= b.nstages && !rc; st++) {
-    rc = b.esz == 8 ? batch_stage_f64(s->stream, b.ndim, b.recon, b.riemann, b.d_desc, b.d_prefix, b.d_n,
+    rc = b.esz == 8 ? batch_stage_f64(b.stream, b.ndim, b.recon, b.riemann, b.d_desc, b.d_prefix, b.d_n,
                                       st, &b.grid)
-                    : batch_stage_f32(s->stream, b.ndim, b.recon, b.riemann, b.d_desc, b.d_prefix, b.d_n,
+                    : batch_stage_f32(b.stream, b.ndim, b.recon, b.riemann, b.d_desc, b.d_prefix, b.d_n,
                                       st, &b.grid);
   }
   if (!rc)
-    rc = b.esz == 8 ? batch_controller_f64(s->stream, b.d_desc, b.d_n, b.capacity, b.d_status)
-                    : batch_controller_f32(s->stream, b.d_desc, b.d_n, b.capacity, b.d_status);
+    rc = b.esz == 8 ? batch_controller_f64(b.stream, b.d_desc, b.d_n, b.capacity, b.d_status)
+                    : batch_controller_f32(b.stream, b.d_desc, b.d_n, b.capacity, b.d_status);
   return rc ? srv_fail(s, KMY_ERR_CUDA, "batched stage launch failed") : KMY_OK;
 }
 
@@ -208,9 +209,9 @@ static int run_batch(kmy_server *s, Batch &b) {
       return rc;
     }
     cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+    cudaError_t e = cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal);
     int rc = e == cudaSuccess ? launch_step(s, b) : KMY_ERR_CUDA;
-    e = cudaStreamEndCapture(s->stream, &g);
+    e = cudaStreamEndCapture(b.stream, &g);
     if (rc || e != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
       return srv_fail(s, KMY_ERR_CUDA, "graph capture failed");
@@ -220,7 +221,7 @@ static int run_batch(kmy_server *s, Batch &b) {
     if (e != cudaSuccess) return srv_fail(s, KMY_ERR_CUDA, "graph instantiation failed");
   }
   s->launches += b.nstages + 1;
-  const cudaError_t e = cudaGraphLaunch(b.graph, s->stream);
+  const cudaError_t e = cudaGraphLaunch(b.graph, b.stream);
   return e == cudaSuccess ? KMY_OK : srv_fail(s, KMY_ERR_CUDA, cudaGetErrorString(e));
 }
 
@@ -259,6 +260,8 @@ static int admit(kmy_server *s) {
       b->recon = r->fp.recon;
       b->riemann = r->fp.riemann;
       b->nstages = r->fp.nstages;
+      if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return srv_fail(s, KMY_ERR_CUDA, "stream creation failed");
       s->batches.push_back(std::move(b));
       bi = int(s->batches.size()) - 1;
     }
@@ -297,7 +300,11 @@ int kmy_server_destroy(kmy_server *s) {
   cudaStreamSynchronize(s->stream);
   for (auto &kv : s->reqs)
     if (kv.second->ctx) kmy_destroy(kv.second->ctx);
-  for (auto &b : s->batches) free_batch_buffers(*b);
+  for (auto &b : s->batches) {
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    free_batch_buffers(*b);
+    if (b->stream) cudaStreamDestroy(b->stream);
+  }
   cudaStreamDestroy(s->stream);
   delete s;
   return KMY_OK;
@@ -337,12 +344,15 @@ int kmy_server_tick(kmy_server *s, int *nactive, int *nqueued) {
     rc = run_batch(s, *b);
     if (rc) return rc;
     cudaMemcpyAsync(b->h_status, b->d_status, sizeof(BatchStatus) * b->members.size(),
-                    cudaMemcpyDeviceToHost, s->stream);
+                    cudaMemcpyDeviceToHost, b->stream);
     any = true;
   }
   if (any) {
-    const cudaError_t e = cudaStreamSynchronize(s->stream);
-    if (e != cudaSuccess) return srv_fail(s, KMY_ERR_CUDA, cudaGetErrorString(e));
+    for (auto &b : s->batches) {
+      if (b->members.empty()) continue;
+      const cudaError_t e = cudaStreamSynchronize(b->stream);
+      if (e != cudaSuccess) return srv_fail(s, KMY_ERR_CUDA, cudaGetErrorString(e));
+    }
     s->ticks++;
   }
   const double t = s->now();

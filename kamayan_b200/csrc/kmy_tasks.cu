@@ -267,12 +267,8 @@ static int compute_fluxes_t(kmy_ctx *c, Container &md0) {
   const MeshDesc &m = c->m;
   if (!c->flux) {
     const size_t bytes = c->esz * 3 * c->ncc * size_t(m.nb) * m.Pf;
-    if (cudaMalloc(&c->flux, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      c->err = "cudaMalloc of the flux arrays failed";
-      return KMY_ERR_OOM;
-    }
-    c->allocations.push_back(c->flux);
+    const int rc = dalloc(c, &c->flux, bytes);
+    if (rc) return rc;
   }
   const S *cc = (const S *)md0.cc, *prim = (const S *)c->prim, *fc = (const S *)md0.fc;
   S *flux = (S *)c->flux;
