@@ -56,6 +56,13 @@ typedef struct {
  * <material/single> (gamma, Abar, eos_type), <eos> (mode_init), plus
  * <kamayan_b200> (precision = fp64|fp32).  Unknown option values fail with
  * KMY_ERR_BAD_PARAM.
+ * Adaptive meshes (hydro): <parthenon/mesh> refinement = adaptive, numlevel
+ * (<= 8), derefine_count, and a <kamayan/refinement0> block with field
+ * (dens|pres|ener), method = loehner, refine_tol, derefine_tol, filter,
+ * max_level (src/grid/grid.cpp:43-48, :90-124; src/grid/grid_refinement.cpp:15-30).
+ * Blocks then carry a level and a logical location (kmy_get_blocks) and the
+ * block count changes as the mesh adapts; the step runs the per-task kernels
+ * with flux correction, Loehner tagging and a remesh after each step.
  * Replaces: InitEnv/InitPackages parameter setup (src/kamayan/kamayan.cpp:20-138),
  * hydro::SetupParams (src/physics/hydro/hydro.cpp:51-92),
  * grid::SetupParams (src/grid/grid.cpp:169-262),
@@ -136,6 +143,13 @@ int kmy_evolve(kmy_ctx *ctx, double tlim, int nlim, int *nsteps);
 int kmy_end_step(kmy_ctx *ctx);
 /* Simulation clock: time, next dt, last dt estimate, cycle count. */
 int kmy_get_time(const kmy_ctx *ctx, double *time, double *dt, double *dt_est, int *ncycle);
+/* Leaf blocks in block order: refinement level (levels[b]) and logical
+ * location at that level (locations[3b..3b+2], i j k).  Fills at most
+ * max_blocks entries; *nblocks receives the block count.  Single-level meshes
+ * report level 0 and the lexicographic location.
+ * Replaces: Parthenon MeshBlock::loc / LogicalLocation of each block of the
+ * MeshData (used by the refinement tasks, src/grid/grid_refinement.cpp:30-152). */
+int kmy_get_blocks(const kmy_ctx *ctx, int *levels, int *locations, int max_blocks, int *nblocks);
 /* Override the dt used by the next kmy_step (e.g. to replay a reference run). */
 int kmy_set_dt(kmy_ctx *ctx, double dt);
 /* Select the stepping path used by kmy_step/kmy_evolve: 0 = fused, 1 = tasks. */

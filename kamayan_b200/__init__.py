@@ -34,7 +34,7 @@ EXPORTS = (
     "kmy_compute_fluxes", "kmy_compute_emf", "kmy_flux_divergence", "kmy_apply_dudt",
     "kmy_prepare_primitive", "kmy_fill_ghosts", "kmy_estimate_dt", "kmy_fill_derived",
     "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_end_step", "kmy_get_time",
-    "kmy_set_dt",
+    "kmy_get_blocks", "kmy_set_dt",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
     "kmy_conserved_sums_noalloc",
     "kmy_server_create", "kmy_server_destroy", "kmy_server_last_error", "kmy_server_submit",
@@ -95,6 +95,7 @@ def lib() -> ctypes.CDLL:
         L.kmy_evolve.argtypes = [vp, d, i, ctypes.POINTER(i)]
         L.kmy_end_step.argtypes = [vp]
         L.kmy_get_time.argtypes = [vp, _dp, _dp, _dp, ctypes.POINTER(i)]
+        L.kmy_get_blocks.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i), i, ctypes.POINTER(i)]
         L.kmy_set_dt.argtypes = [vp, d]
         L.kmy_set_path.argtypes = [vp, i]
         L.kmy_vortex_error.argtypes = [vp, i, i, _dp]
@@ -131,13 +132,40 @@ class Solver:
         if rc:
             raise KmyError(rc, "kmy_create rejected the deck (see stderr)")
         self._h = h
-        info = Info()
-        self._check(lib().kmy_get_info(self._h, ctypes.byref(info)))
-        self.info = info
-        self.ndim = info.ndim
-        self.nblocks = info.nblocks
-        self.cell_shape = (info.nblocks, info.ncells_pad[2], info.ncells_pad[1], info.ncells_pad[0])
-        self.face_shape = (info.nblocks, info.nfaces_pad[2], info.nfaces_pad[1], info.nfaces_pad[0])
+        self._info = Info()
+        self.ndim = self.info.ndim
+
+    # An adaptive mesh changes its block count as it refines, so the mesh
+    # description is read from the context on every use.
+    @property
+    def info(self) -> Info:
+        self._check(lib().kmy_get_info(self._h, ctypes.byref(self._info)))
+        return self._info
+
+    @property
+    def nblocks(self) -> int:
+        return self.info.nblocks
+
+    @property
+    def cell_shape(self) -> tuple:
+        i = self.info
+        return (i.nblocks, i.ncells_pad[2], i.ncells_pad[1], i.ncells_pad[0])
+
+    @property
+    def face_shape(self) -> tuple:
+        i = self.info
+        return (i.nblocks, i.nfaces_pad[2], i.nfaces_pad[1], i.nfaces_pad[0])
+
+    def blocks(self) -> tuple[np.ndarray, np.ndarray]:
+        """Leaf blocks in block order: levels (nb,) and logical locations (nb, 3)."""
+        n = ctypes.c_int()
+        self._check(lib().kmy_get_blocks(self._h, None, None, 0, ctypes.byref(n)))
+        lev = np.zeros(n.value, dtype=np.int32)
+        loc = np.zeros((n.value, 3), dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self._check(lib().kmy_get_blocks(self._h, lev.ctypes.data_as(ip), loc.ctypes.data_as(ip), n.value,
+                                         ctypes.byref(n)))
+        return lev, loc
 
     def close(self) -> None:
         if getattr(self, "_h", None):

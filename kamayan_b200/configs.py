@@ -8,6 +8,8 @@
                  cube, 192^3 in 216 blocks of 32^3 (4 ghosts), PPM+HLL, RK2, CFL 0.3, t=0.5.
 ``blast_2d``     2D blast, gamma 5/3, [-0.5,0.5]^2, 128^2 in 16^2 blocks, PLM+HLLC,
                  RK2, t=0.2 (single-level form of the AMR workload).
+``blast_2d_amr`` the same blast on an adaptive mesh: 3 levels, Loehner tagging on
+                 density (refine 0.3, derefine 0.05).
 
 Every builder takes keyword overrides for the mesh size so tests can run the
 same physics on small meshes.
@@ -117,4 +119,20 @@ def blast_2d(n: int = 128, nb: int = 16, precision: str = "fp64", bc: str = "out
     d.set("blast", "explosion_pressure", 10.0)
     d.set("blast", "radius", 0.1)
     d.set("kamayan_b200", "precision", precision)
+    return d
+
+
+def blast_2d_amr(n: int = 128, nb: int = 16, precision: str = "fp64", numlevel: int = 3,
+                 refine_tol: float = 0.3, derefine_tol: float = 0.05, tlim: float = 0.2,
+                 derefine_count: int = 10, field: str = "dens") -> Deck:
+    """The AMR workload: ``blast_2d`` on an adaptive mesh with Loehner tagging on density."""
+    d = blast_2d(n=n, nb=nb, precision=precision, tlim=tlim)
+    d.set("parthenon/mesh", "refinement", "adaptive")
+    d.set("parthenon/mesh", "numlevel", numlevel)
+    d.set("parthenon/mesh", "derefine_count", derefine_count)
+    d.set("kamayan/refinement0", "field", field)
+    d.set("kamayan/refinement0", "method", "loehner")
+    d.set("kamayan/refinement0", "refine_tol", refine_tol)
+    d.set("kamayan/refinement0", "derefine_tol", derefine_tol)
+    d.set("kamayan/refinement0", "max_level", numlevel - 1)
     return d

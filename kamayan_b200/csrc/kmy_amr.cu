@@ -1,0 +1,737 @@
+// kmy_amr.cu -- adaptive mesh refinement: boundary exchange across levels,
+// flux correction at fine/coarse faces, Loehner tagging, and the remesh (tree
+// update on the host, data remap on the device).
+//
+// Semantics (Parthenon's block tree and exchange are un-vendored and restated;
+// the operators are kamayan's):
+//   RestrictAverage            refinement_operations.hpp:56-120
+//   ProlongateSharedGeneral    refinement_operations.hpp:123-264 (minmod)
+//   GradMinMod                 refinement_operations.hpp:44-50
+//   AMRLoehner::operator()     grid_refinement.cpp:30-152
+//   flux correction task       kamayan_driver.cpp:206-207
+//   tagging before exchange    kamayan_driver.cpp:178-181, :150-151
+//
+// The value of a cell at level L and global index G is the best
+// representation the mesh has there: the cell of the level-L leaf that holds
+// it, the volume-weighted restriction of the finer leaves covering it, or the
+// minmod prolongation from level L-1.  Ghost cells, cells remapped by a remesh
+// and the coarse stencils of a prolongation all take that value.  With 2:1
+// balance (corners included) the recursion stays within a few levels; it is
+// unrolled to a fixed depth so the stack size is known at compile time, and a
+// deeper request sets an error flag instead of recursing.
+//
+// The unit is compiled without FMA contraction, so each expression rounds as
+// written and tag decisions match a CPU evaluation of the same expressions.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <map>
+#include <vector>
+
+#include "../../include/kmy_hydro.h"
+#include "kmy_internal.hpp"
+
+namespace kmy {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxDepth = 12;               // unrolled depth of the level value
+constexpr long long kMaxTable = 1ll << 26;  // level-table entries over all levels
+
+unsigned nblk(long long n) { return unsigned((n + kThreads - 1) / kThreads); }
+
+__device__ __forceinline__ long long cidx(const MeshDesc &m, int k, int j, int i) {
+  return ((long long)k * m.np[1] + j) * m.np[0] + i;
+}
+__device__ __forceinline__ long long fidx(const MeshDesc &m, int k, int j, int i) {
+  return ((long long)k * m.nf[1] + j) * m.nf[0] + i;
+}
+
+// Physical boundary map of a global index on an N-cell axis.
+__device__ __forceinline__ int amr_map(int G, int N, int bc, bool &flip) {
+  if (G >= 0 && G < N) return G;
+  if (bc == BC_PERIODIC) return ((G % N) + N) % N;
+  if (bc == BC_OUTFLOW) return G < 0 ? 0 : N - 1;
+  flip = !flip;
+  return G < 0 ? -G - 1 : 2 * N - G - 1;
+}
+
+// Leaf id at block position bx of level L, -1 when finer leaves cover it,
+// -2 when a coarser leaf does (or L is outside the tables).
+__device__ __forceinline__ int table_at(const MeshDesc &m, int L, const int bx[3]) {
+  if (L < 0 || L >= m.nlev) return -2;
+  return m.tabs[m.tab_off[L] + ((long long)bx[2] * m.tab_dim[L][1] + bx[1]) * m.tab_dim[L][0] + bx[0]];
+}
+
+// One stored variable over [nb][P]: FP64, or FP32 with an optional low word.
+struct Field {
+  const void *p;
+  const float *lo;
+  int f32;
+};
+__device__ __forceinline__ double fetch(const Field &f, long long n) {
+  if (f.f32) {
+    double v = double(static_cast<const float *>(f.p)[n]);
+    if (f.lo) v += double(f.lo[n]);
+    return v;
+  }
+  return static_cast<const double *>(f.p)[n];
+}
+
+// RestrictAverage over the 2^d children, index (ok*4 + oj*2 + oi); the sums
+// keep the operator's pairing.
+__device__ __forceinline__ double restrict8(const double t[8], const double v[8]) {
+  const double tvol = ((v[0] + v[2]) + (v[1] + v[3])) + ((v[4] + v[6]) + (v[5] + v[7]));
+  return tvol > 0.0 ? (((t[0] + t[2]) + (t[1] + t[3])) + ((t[4] + t[6]) + (t[5] + t[7]))) / tvol : 0.0;
+}
+
+// GradMinMod with SIGN(x) = x < 0 ? -1 : 1
+__device__ __forceinline__ double grad_minmod(double fc, double fm, double fp, double dxm, double dxp) {
+  const double gxm = (fc - fm) / dxm;
+  const double gxp = (fp - fc) / dxp;
+  const double sm = gxm < 0 ? -1.0 : 1.0, sp = gxp < 0 ? -1.0 : 1.0;
+  const double agm = fabs(gxm), agp = fabs(gxp);
+  return 0.5 * (sm + sp) * ((agp < agm) ? agp : agm);
+}
+
+// Value of field f at level L, global cell G; flipdim is the vector component
+// the field carries (its sign flips across reflecting boundaries) or -1.
+template <int D>
+__device__ __noinline__ double level_value(const MeshDesc &m, int L, int G0, int G1, int G2, const Field &f,
+                                           int flipdim, int *err) {
+  const int G[3] = {G0, G1, G2};
+  int M[3] = {0, 0, 0};
+  bool flip[3] = {false, false, false};
+  for (int d = 0; d < m.ndim; d++) {
+    const int N = m.mesh_nx[d] << L;
+    M[d] = amr_map(G[d], N, m.bc[d][G[d] < 0 ? 0 : 1], flip[d]);
+  }
+  const double sgn = (flipdim >= 0 && flip[flipdim]) ? -1.0 : 1.0;
+  int bx[3];
+  for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
+  const int e = table_at(m, L, bx);
+  if (e >= 0)
+    return sgn * fetch(f, (long long)e * m.P + cidx(m, M[2] - bx[2] * m.nx[2] + m.g[2],
+                                                    M[1] - bx[1] * m.nx[1] + m.g[1],
+                                                    M[0] - bx[0] * m.nx[0] + m.g[0]));
+  if constexpr (D == 0) {
+    *err = 1;
+    return 0.0;
+  } else {
+    const int nd = m.ndim;
+    if (e == -1) {  // covered by finer leaves: restrict from level L+1
+      double t[8] = {0, 0, 0, 0, 0, 0, 0, 0}, v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      double vol = 1.0;
+      for (int d = 0; d < 3; d++) vol *= d < nd ? m.dx[d] / double(1 << (L + 1)) : m.dx[d];
+      for (int ok = 0; ok < 1 + (nd > 2); ok++)
+        for (int oj = 0; oj < 1 + (nd > 1); oj++)
+          for (int oi = 0; oi < 2; oi++) {
+            const int q = ok * 4 + oj * 2 + oi;
+            v[q] = vol;
+            t[q] = vol * level_value<D - 1>(m, L + 1, 2 * M[0] + oi, nd > 1 ? 2 * M[1] + oj : 0,
+                                            nd > 2 ? 2 * M[2] + ok : 0, f, flipdim, err);
+          }
+      return sgn * restrict8(t, v);
+    }
+    if (L == 0) {  // a level-0 position always has a leaf at or below it
+      *err = 2;
+      return 0.0;
+    }
+    // covered by a coarser leaf: prolongate from level L-1
+    int Mc[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+    for (int d = 0; d < nd; d++) {
+      Mc[d] = M[d] >> 1;
+      o[d] = M[d] & 1;
+    }
+    const double fc = level_value<D - 1>(m, L - 1, Mc[0], Mc[1], Mc[2], f, flipdim, err);
+    double gq[3] = {0, 0, 0}, dfm[3] = {0, 0, 0}, dfp[3] = {0, 0, 0};
+    for (int d = 0; d < nd; d++) {
+      const double dxc = m.dx[d] / double(1 << (L - 1)), dxf = m.dx[d] / double(1 << L);
+      const double x0 = m.xmin[d];
+      int Gm[3] = {Mc[0], Mc[1], Mc[2]}, Gp[3] = {Mc[0], Mc[1], Mc[2]};
+      Gm[d] -= 1;
+      Gp[d] += 1;
+      const double fm = level_value<D - 1>(m, L - 1, Gm[0], Gm[1], Gm[2], f, flipdim, err);
+      const double fp = level_value<D - 1>(m, L - 1, Gp[0], Gp[1], Gp[2], f, flipdim, err);
+      const double xm = x0 + (double(Mc[d] - 1) + 0.5) * dxc;
+      const double xc = x0 + (double(Mc[d]) + 0.5) * dxc;
+      const double xp = x0 + (double(Mc[d] + 1) + 0.5) * dxc;
+      const double dxm = xc - xm, dxp = xp - xc;
+      dfm[d] = xc - (x0 + (double(2 * Mc[d]) + 0.5) * dxf);
+      dfp[d] = (x0 + (double(2 * Mc[d] + 1) + 0.5) * dxf) - xc;
+      gq[d] = grad_minmod(fc, fm, fp, dxm, dxp);
+    }
+    const double g1 = gq[0], g2 = gq[1], g3 = gq[2];
+    const double d1m = dfm[0], d1p = dfp[0], d2m = dfm[1], d2p = dfp[1], d3m = dfm[2], d3p = dfp[2];
+    double val;
+    switch (o[0] + 2 * o[1] + 4 * o[2]) {
+      case 0: val = fc - (g1 * d1m + g2 * d2m + g3 * d3m); break;
+      case 1: val = fc + (g1 * d1p - g2 * d2m - g3 * d3m); break;
+      case 2: val = fc - (g1 * d1m - g2 * d2p + g3 * d3m); break;
+      case 3: val = fc + (g1 * d1p + g2 * d2p - g3 * d3m); break;
+      case 4: val = fc - (g1 * d1m + g2 * d2m - g3 * d3p); break;
+      case 5: val = fc + (g1 * d1p - g2 * d2m + g3 * d3p); break;
+      case 6: val = fc - (g1 * d1m - g2 * d2p - g3 * d3p); break;
+      default: val = fc + (g1 * d1p + g2 * d2p + g3 * d3p); break;
+    }
+    return sgn * val;
+  }
+}
+
+template <typename S>
+__device__ __forceinline__ void store_value(S *arr, float *lo, long long n, double v) {
+  if constexpr (sizeof(S) == 4) {
+    const float hi = float(v);
+    arr[n] = hi;
+    if (lo) lo[n] = float(v - double(hi));
+  } else {
+    arr[n] = v;
+  }
+}
+
+// Ghost cells of every block from the level value of the cell they cover.  A
+// ghost whose same-level position holds a leaf (the common case) copies it
+// directly; the rest restrict or prolongate.  Reads interior cells only.
+template <typename S>
+__global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, float *lo, S *prim, int ncc,
+                                  int *err) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)m.nb * m.P) return;
+  const int b = int(t / m.P);
+  long long r = t - (long long)b * m.P;
+  const int i = int(r % m.np[0]);
+  r /= m.np[0];
+  const int j = int(r % m.np[1]);
+  const int k = int(r / m.np[1]);
+  const int loc[3] = {i, j, k};
+  bool interior = true;
+  for (int d = 0; d < 3; d++)
+    if (loc[d] < m.g[d] || loc[d] >= m.g[d] + m.nx[d]) interior = false;
+  if (interior) return;
+  const int L = m.blev[b];
+  int G[3];
+  for (int d = 0; d < 3; d++) G[d] = m.bloc[3 * b + d] * m.nx[d] + (loc[d] - m.g[d]);
+  const long long NP = (long long)m.nb * m.P;
+  const long long dst = (long long)b * m.P + cidx(m, k, j, i);
+  constexpr bool F32 = sizeof(S) == 4;
+
+  int M[3] = {0, 0, 0}, bx[3];
+  bool flip[3] = {false, false, false};
+  for (int d = 0; d < m.ndim; d++) M[d] = amr_map(G[d], m.mesh_nx[d] << L, m.bc[d][G[d] < 0 ? 0 : 1], flip[d]);
+  for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
+  const int e = table_at(m, L, bx);
+  if (e >= 0) {
+    const long long s = (long long)e * m.P + cidx(m, M[2] - bx[2] * m.nx[2] + m.g[2],
+                                                  M[1] - bx[1] * m.nx[1] + m.g[1], M[0] - bx[0] * m.nx[0] + m.g[0]);
+    for (int v = 0; v < ncc; v++) {
+      S val = cc[v * NP + s];
+      if (v >= CMOM0 && v <= CMOM2 && flip[v - CMOM0]) val = -val;
+      cc[v * NP + dst] = val;
+    }
+    if constexpr (F32) {
+      if (lo) lo[dst] = lo[s];
+    }
+    for (int v = 0; v < NPRIM; v++) {
+      S val = prim[v * NP + s];
+      if (v <= PVEL2 && flip[v]) val = -val;
+      prim[v * NP + dst] = val;
+    }
+    return;
+  }
+  for (int v = 0; v < ncc; v++) {
+    const Field f{cc + v * NP, (F32 && v == CENER) ? lo : nullptr, F32};
+    const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : -1;
+    const double val = level_value<kMaxDepth>(m, L, G[0], G[1], G[2], f, fd, err);
+    store_value<S>(cc + v * NP, v == CENER ? lo : nullptr, dst, val);
+  }
+  for (int v = 0; v < NPRIM; v++) {
+    const Field f{prim + v * NP, nullptr, F32};
+    const double val = level_value<kMaxDepth>(m, L, G[0], G[1], G[2], f, v <= PVEL2 ? v : -1, err);
+    store_value<S>(prim + v * NP, nullptr, dst, val);
+  }
+}
+
+// Flux correction: a coarse block's boundary face whose neighbour across it
+// is finer takes the area-weighted restriction of the 2^(d-1) fine face
+// fluxes.  One thread per (block, direction, side, face); reads fine blocks'
+// boundary faces and writes coarse blocks' boundary faces only.
+template <typename S>
+__global__ void k_flux_correct(const __grid_constant__ MeshDesc m, S *flux, int ncc, int F) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)m.nb * 6 * F) return;
+  const int b = int(t / (6ll * F));
+  const int rr = int(t - (long long)b * 6 * F);
+  const int d = (rr / F) >> 1, s = (rr / F) & 1, a = rr % F;
+  if (d >= m.ndim) return;
+  const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+  const int a1 = a % m.nx[t1], a2 = a / m.nx[t1];
+  if (a2 >= m.nx[t2]) return;
+  const int L = m.blev[b];
+  const int *bl = m.bloc + 3 * b;
+  // the cell across the face, at level L
+  int Gn[3];
+  Gn[d] = bl[d] * m.nx[d] + (s ? m.nx[d] : -1);
+  Gn[t1] = bl[t1] * m.nx[t1] + a1;
+  Gn[t2] = bl[t2] * m.nx[t2] + a2;
+  const int N = m.mesh_nx[d] << L;
+  if ((Gn[d] < 0 || Gn[d] >= N) && m.bc[d][s] != BC_PERIODIC) return;
+  bool fl = false;
+  Gn[d] = amr_map(Gn[d], N, m.bc[d][s], fl);
+  int bxn[3];
+  for (int q = 0; q < 3; q++) bxn[q] = Gn[q] / m.nx[q];
+  if (table_at(m, L, bxn) != -1) return;  // not finer across this face
+  const long long NF = (long long)m.nb * m.Pf;
+  double vv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long src[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // flux index of the fine face, per slot
+  for (int o2 = 0; o2 < 1 + (t2 < m.ndim); o2++)
+    for (int o1 = 0; o1 < 1 + (t1 < m.ndim); o1++) {
+      int Gf[3];
+      const int Ff = 2 * (bl[d] * m.nx[d] + (s ? m.nx[d] : 0));
+      Gf[d] = s ? Ff : Ff - 1;
+      Gf[t1] = t1 < m.ndim ? 2 * (bl[t1] * m.nx[t1] + a1) + o1 : 0;
+      Gf[t2] = t2 < m.ndim ? 2 * (bl[t2] * m.nx[t2] + a2) + o2 : 0;
+      bool f2 = false;
+      Gf[d] = amr_map(Gf[d], m.mesh_nx[d] << (L + 1), m.bc[d][s], f2);
+      int bf[3], lf[3];
+      for (int q = 0; q < 3; q++) bf[q] = Gf[q] / m.nx[q];
+      const int e = table_at(m, L + 1, bf);
+      if (e < 0) return;  // not a leaf one level finer: the mesh is not 2:1 balanced
+      for (int q = 0; q < 3; q++) lf[q] = Gf[q] - bf[q] * m.nx[q] + m.g[q];
+      if (!s) lf[d] += 1;  // the fine cell's high face
+      int off[3] = {0, 0, 0};
+      off[t1] = o1;
+      off[t2] = o2;
+      const int slot = off[2] * 4 + off[1] * 2 + off[0];
+      vv[slot] = blk_area(m, e, d);
+      src[slot] = (long long)e * m.Pf + fidx(m, lf[2], lf[1], lf[0]);
+    }
+  int lc[3];
+  lc[d] = m.g[d] + (s ? m.nx[d] : 0);
+  lc[t1] = m.g[t1] + a1;
+  lc[t2] = m.g[t2] + a2;
+  const long long dst = (long long)b * m.Pf + fidx(m, lc[2], lc[1], lc[0]);
+  for (int v = 0; v < ncc; v++) {
+    const S *fv = flux + ((long long)d * ncc + v) * NF;
+    double tt[8];
+    for (int q = 0; q < 8; q++) tt[q] = vv[q] > 0.0 ? vv[q] * double(fv[src[q]]) : 0.0;
+    flux[((long long)d * ncc + v) * NF + dst] = S(restrict8(tt, vv));
+  }
+}
+
+// AMRLoehner on one field of a container: one CTA per block, one thread per
+// (k, j) row; the block's tag is the maximum of the row flags.
+__global__ void k_amr_tag(const __grid_constant__ MeshDesc m, Field f, double refine_tol, double derefine_tol,
+                          double filter, int max_level, int *tags) {
+  __shared__ int flag_sh;
+  const int b = blockIdx.x;
+  if (threadIdx.x == 0) flag_sh = -1;
+  __syncthreads();
+  const int nd = m.ndim;
+  const double dxq[3] = {blk_dx(m, b, 0), blk_dx(m, b, 1), blk_dx(m, b, 2)};
+  const long long base = (long long)b * m.P;
+  const long long st[3] = {1, m.np[0], (long long)m.np[0] * m.np[1]};
+  auto U = [&](long long n) { return fetch(f, base + n); };
+  // central first derivative along p at cell n
+  auto Dv = [&](int p, long long n) { return 0.5 * (U(n + st[p]) - U(n - st[p])) / dxq[p]; };
+  const int rows = m.nx[1] * m.nx[2];
+  int flag_row_max = -1;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    const int j = m.g[1] + r % m.nx[1], k = m.g[2] + r / m.nx[1];
+    double max_err_2 = 0.;
+    for (int i = m.g[0]; i < m.g[0] + m.nx[0]; i++) {
+      const long long n = cidx(m, k, j, i);
+      double numerator = 0.0, denominator = 1.e-12;
+      for (int q = 0; q < nd; q++) {
+        const long long sq = st[q];
+        for (int p = 0; p < nd; p++) {
+          const long long sp = st[p];
+          const double dpp = Dv(p, n + sq), dpm = Dv(p, n - sq);
+          const double num = 0.5 * (dpp - dpm) / dxq[q];
+          numerator += num * num;
+          const double denom =
+              0.5 * (fabs(dpp) + fabs(dpm)) / dxq[p] +
+              filter * (fabs(U(n + sq)) + fabs(U(n - sq)) + fabs(U(n - sp)) + fabs(U(n + sp))) / (dxq[q] * dxq[p]);
+          denominator += denom * denom;
+        }
+      }
+      if (denominator != 0.0) {
+        const double ratio = numerator / denominator;
+        max_err_2 = (max_err_2 < ratio) ? ratio : max_err_2;
+      }
+    }
+    const double max_err = sqrt(max_err_2);
+    int flag = 0;
+    if (max_err > refine_tol && m.blev[b] < max_level) flag = 1;
+    if (max_err < derefine_tol) flag = -1;
+    flag_row_max = max(flag_row_max, flag);
+  }
+  atomicMax(&flag_sh, flag_row_max);
+  __syncthreads();
+  if (threadIdx.x == 0) tags[b] = flag_sh;
+}
+
+// Remap after a remesh: every interior cell of the new leaves takes the level
+// value of the old mesh (copy, prolongation or restriction).
+template <typename S>
+__global__ void k_amr_remap(const __grid_constant__ MeshDesc mo, const S *occ, const float *olo, const S *oprim,
+                            int nnew, const int *nlev, const int *nloc, S *ncc_out, float *nlo, S *nprim, int ncc,
+                            int *err) {
+  const long long cells = (long long)mo.nx[0] * mo.nx[1] * mo.nx[2];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= cells * nnew) return;
+  const int q = int(t / cells);
+  long long r = t - (long long)q * cells;
+  const int i = mo.g[0] + int(r % mo.nx[0]);
+  r /= mo.nx[0];
+  const int j = mo.g[1] + int(r % mo.nx[1]);
+  const int k = mo.g[2] + int(r / mo.nx[1]);
+  const int G0 = nloc[3 * q] * mo.nx[0] + (i - mo.g[0]);
+  const int G1 = nloc[3 * q + 1] * mo.nx[1] + (j - mo.g[1]);
+  const int G2 = nloc[3 * q + 2] * mo.nx[2] + (k - mo.g[2]);
+  const int L = nlev[q];
+  constexpr bool F32 = sizeof(S) == 4;
+  const long long NPo = (long long)mo.nb * mo.P, NPn = (long long)nnew * mo.P;
+  const long long dst = (long long)q * mo.P + cidx(mo, k, j, i);
+  for (int v = 0; v < ncc; v++) {
+    const Field f{occ + v * NPo, (F32 && v == CENER) ? olo : nullptr, F32};
+    const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : -1, err);
+    store_value<S>(ncc_out + v * NPn, v == CENER ? nlo : nullptr, dst, val);
+  }
+  for (int v = 0; v < NPRIM; v++) {
+    const Field f{oprim + v * NPo, nullptr, F32};
+    const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, v <= PVEL2 ? v : -1, err);
+    store_value<S>(nprim + v * NPn, nullptr, dst, val);
+  }
+}
+
+// Morton key of a leaf's lower corner at the finest level, level in the low bits.
+uint64_t morton_key(int x0, int y0, int z0, int level, int maxl) {
+  const int sh = maxl - level;
+  const uint64_t x = uint64_t(x0) << sh, y = uint64_t(y0) << sh, z = uint64_t(z0) << sh;
+  uint64_t key = 0;
+  for (int bit = 0; bit < 20; bit++) {
+    key |= ((x >> bit) & 1ull) << (3 * bit);
+    key |= ((y >> bit) & 1ull) << (3 * bit + 1);
+    key |= ((z >> bit) & 1ull) << (3 * bit + 2);
+  }
+  return (key << 5) | uint64_t(level);
+}
+
+}  // namespace
+
+// Level tables and leaf arrays to the device; MeshDesc points at them.
+int amr_upload(kmy_ctx *c) {
+  AmrHost &a = c->amr;
+  MeshDesc &m = c->m;
+  const int nb = int(a.lev.size());
+  const int nlev = a.max_level + 1;
+  std::vector<int> tabs;
+  long long total = 0;
+  for (int L = 0; L < nlev; L++) {
+    m.tab_off[L] = int(total);
+    long long n = 1;
+    for (int d = 0; d < 3; d++) {
+      m.tab_dim[L][d] = d < m.ndim ? (m.nbx[d] << L) : 1;
+      n *= m.tab_dim[L][d];
+    }
+    total += n;
+    if (total > kMaxTable) {
+      c->err = "adaptive mesh: level tables exceed " + std::to_string(kMaxTable) + " entries";
+      return KMY_ERR_BAD_PARAM;
+    }
+  }
+  tabs.assign(size_t(total), -2);
+  for (int b = 0; b < nb; b++) {
+    const int Lb = a.lev[b];
+    for (int L = 0; L <= Lb; L++) {
+      int q[3];
+      for (int d = 0; d < 3; d++) q[d] = d < m.ndim ? (a.loc[3 * b + d] >> (Lb - L)) : 0;
+      const long long idx = m.tab_off[L] + ((long long)q[2] * m.tab_dim[L][1] + q[1]) * m.tab_dim[L][0] + q[0];
+      tabs[size_t(idx)] = L == Lb ? b : -1;
+    }
+  }
+  dfree(c, a.d_blev);
+  dfree(c, a.d_bloc);
+  dfree(c, a.d_tabs);
+  dfree(c, a.d_tags);
+  a.d_blev = a.d_bloc = a.d_tabs = a.d_tags = nullptr;
+  int rc = dalloc(c, reinterpret_cast<void **>(&a.d_blev), sizeof(int) * nb);
+  if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&a.d_bloc), sizeof(int) * 3 * nb);
+  if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&a.d_tabs), sizeof(int) * size_t(total));
+  if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&a.d_tags), sizeof(int) * nb);
+  if (rc) return rc;
+  rc = cuda_check(c, cudaMemcpyAsync(a.d_blev, a.lev.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->stream),
+                  "amr levels");
+  if (!rc)
+    rc = cuda_check(c, cudaMemcpyAsync(a.d_bloc, a.loc.data(), sizeof(int) * 3 * nb, cudaMemcpyHostToDevice,
+                                       c->stream), "amr locations");
+  if (!rc)
+    rc = cuda_check(c, cudaMemcpyAsync(a.d_tabs, tabs.data(), sizeof(int) * size_t(total), cudaMemcpyHostToDevice,
+                                       c->stream), "amr tables");
+  // pageable sources: wait so the host vectors may go
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "amr upload");
+  if (rc) return rc;
+  m.nb = nb;
+  m.blev = a.d_blev;
+  m.bloc = a.d_bloc;
+  m.tabs = a.d_tabs;
+  m.nlev = nlev;
+  return KMY_OK;
+}
+
+// Initial leaves: every block of the root grid at level 0, lexicographic.
+int amr_setup(kmy_ctx *c) {
+  AmrHost &a = c->amr;
+  const MeshDesc &m = c->m;
+  a.lev.assign(m.nb, 0);
+  a.loc.assign(size_t(3) * m.nb, 0);
+  a.cnt.assign(m.nb, 0);
+  for (int b = 0; b < m.nb; b++) {
+    a.loc[3 * b] = b % m.nbx[0];
+    a.loc[3 * b + 1] = (b / m.nbx[0]) % m.nbx[1];
+    a.loc[3 * b + 2] = b / (m.nbx[0] * m.nbx[1]);
+  }
+  int rc = dalloc(c, reinterpret_cast<void **>(&a.d_err), sizeof(int));
+  if (!rc) rc = amr_upload(c);
+  return rc;
+}
+
+int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct) {
+  const MeshDesc &m = c->m;
+  const long long n = (long long)m.nb * m.P;
+  if (c->esz == 8)
+    k_amr_fill_ghosts<double><<<nblk(n), kThreads, 0, c->stream>>>(m, (double *)ct.cc, nullptr, (double *)c->prim,
+                                                                   c->ncc, c->amr.d_err);
+  else
+    k_amr_fill_ghosts<float><<<nblk(n), kThreads, 0, c->stream>>>(m, (float *)ct.cc, (float *)ct.ener_lo,
+                                                                  (float *)c->prim, c->ncc, c->amr.d_err);
+  c->launches++;
+  return cuda_check(c, cudaGetLastError(), "amr fill_ghosts");
+}
+
+int launch_flux_correct(kmy_ctx *c) {
+  const MeshDesc &m = c->m;
+  if (!c->flux) return KMY_OK;
+  int F = 1;
+  for (int d = 0; d < m.ndim; d++) F = std::max(F, m.nx[(d + 1) % 3] * m.nx[(d + 2) % 3]);
+  const long long n = (long long)m.nb * 6 * F;
+  if (c->esz == 8)
+    k_flux_correct<double><<<nblk(n), kThreads, 0, c->stream>>>(m, (double *)c->flux, c->ncc, F);
+  else
+    k_flux_correct<float><<<nblk(n), kThreads, 0, c->stream>>>(m, (float *)c->flux, c->ncc, F);
+  c->launches++;
+  return cuda_check(c, cudaGetLastError(), "flux_correct");
+}
+
+int launch_amr_tag(kmy_ctx *c, Container &ct) {
+  const MeshDesc &m = c->m;
+  const AmrHost &a = c->amr;
+  const long long NP = (long long)m.nb * m.P;
+  Field f{nullptr, nullptr, c->esz == 4};
+  if (a.field == "pres") {
+    f.p = static_cast<const char *>(c->prim) + c->esz * NP * PPRES;
+  } else if (a.field == "ener") {
+    f.p = static_cast<const char *>(ct.cc) + c->esz * NP * CENER;
+    f.lo = static_cast<const float *>(ct.ener_lo);
+  } else {
+    f.p = static_cast<const char *>(ct.cc) + c->esz * NP * CDENS;
+  }
+  k_amr_tag<<<m.nb, kThreads, 0, c->stream>>>(m, f, a.refine_tol, a.derefine_tol, a.filter, a.max_level, a.d_tags);
+  c->launches++;
+  return cuda_check(c, cudaGetLastError(), "amr tag");
+}
+
+// Parthenon's tree update, restated: refine the leaves tagged for refinement
+// below max_level, restore 2:1 balance across faces, edges and corners by
+// refining coarser neighbours, then (allow_derefine) merge sibling groups
+// whose members were tagged for derefinement derefine_count times in a row
+// when the merged parent keeps the balance.  New leaves are ordered by the
+// Morton key of their lower corner and get their data from the old mesh.
+int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
+  AmrHost &a = c->amr;
+  MeshDesc &m = c->m;
+  const int nd = m.ndim;
+  const int nb = m.nb;
+  *changed_out = false;
+  std::vector<int> tags(nb);
+  int err = 0;
+  int rc = cuda_check(c, cudaMemcpyAsync(tags.data(), a.d_tags, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream),
+                      "amr tags");
+  if (!rc) rc = cuda_check(c, cudaMemcpyAsync(&err, a.d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "amr err");
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "amr tags sync");
+  if (rc) return rc;
+  if (err) {
+    c->err = "adaptive mesh: level value recursion exceeded its depth (mesh not 2:1 balanced)";
+    return KMY_ERR_STATE;
+  }
+  typedef std::array<int, 4> Key;  // level, location
+  std::map<Key, int> leaf;         // -> old leaf id, -1 for a new leaf
+  for (int b = 0; b < nb; b++) {
+    leaf[{a.lev[b], a.loc[3 * b], a.loc[3 * b + 1], a.loc[3 * b + 2]}] = b;
+    a.cnt[b] = tags[b] == -1 ? a.cnt[b] + 1 : 0;
+  }
+  bool changed = false;
+  auto child = [&](const Key &p, int o) {
+    return Key{p[0] + 1, 2 * p[1] + (o & 1), nd > 1 ? 2 * p[2] + ((o >> 1) & 1) : 0,
+               nd > 2 ? 2 * p[3] + ((o >> 2) & 1) : 0};
+  };
+  auto split = [&](const Key &k) {
+    leaf.erase(k);
+    for (int o = 0; o < (1 << nd); o++) leaf[child(k, o)] = -1;
+    changed = true;
+  };
+  // the leaf covering block position p of level L, if it is at level <= L
+  auto covering = [&](int L, int p0, int p1, int p2, Key &out) -> bool {
+    int p[3] = {p0, p1, p2};
+    for (int d = 0; d < nd; d++) {
+      const int NB = m.nbx[d] << L;
+      if (p[d] < 0 || p[d] >= NB) {
+        if (m.bc[d][p[d] < 0 ? 0 : 1] != BC_PERIODIC) return false;
+        p[d] = ((p[d] % NB) + NB) % NB;
+      }
+    }
+    for (int l = L; l >= 0; l--) {
+      const Key k = {l, p[0] >> (L - l), nd > 1 ? p[1] >> (L - l) : 0, nd > 2 ? p[2] >> (L - l) : 0};
+      if (leaf.count(k)) {
+        out = k;
+        return true;
+      }
+    }
+    return false;
+  };
+  for (int b = 0; b < nb; b++)
+    if (tags[b] == 1 && a.lev[b] < a.max_level) split({a.lev[b], a.loc[3 * b], a.loc[3 * b + 1], a.loc[3 * b + 2]});
+  for (bool again = true; again;) {  // 2:1 balance
+    again = false;
+    std::vector<Key> keys;
+    for (auto &kv : leaf) keys.push_back(kv.first);
+    for (const Key &k : keys) {
+      if (!leaf.count(k)) continue;
+      for (int dz = -(nd > 2); dz <= (nd > 2); dz++)
+        for (int dy = -(nd > 1); dy <= (nd > 1); dy++)
+          for (int dxo = -1; dxo <= 1; dxo++) {
+            if (!dxo && !dy && !dz) continue;
+            Key n;
+            if (!covering(k[0], k[1] + dxo, k[2] + dy, k[3] + dz, n)) continue;
+            if (n[0] < k[0] - 1) {
+              split(n);
+              again = true;
+            }
+          }
+    }
+  }
+  if (allow_derefine) {
+    std::map<Key, int> parents;
+    for (auto &kv : leaf) {
+      const Key &k = kv.first;
+      if (k[0] == 0 || kv.second < 0) continue;
+      if (a.cnt[kv.second] < a.derefine_count) continue;
+      parents[{k[0] - 1, k[1] >> 1, k[2] >> 1, k[3] >> 1}]++;
+    }
+    for (auto &pk : parents) {
+      if (pk.second != (1 << nd)) continue;
+      const Key &p = pk.first;
+      bool ok = true;
+      for (int dz = -(nd > 2); dz <= (nd > 2) && ok; dz++)
+        for (int dy = -(nd > 1); dy <= (nd > 1) && ok; dy++)
+          for (int dxo = -1; dxo <= 1 && ok; dxo++) {
+            if (!dxo && !dy && !dz) continue;
+            Key n;
+            if (covering(p[0], p[1] + dxo, p[2] + dy, p[3] + dz, n)) continue;
+            // finer there: each child one level below p must be a leaf
+            int q[3] = {p[1] + dxo, p[2] + dy, p[3] + dz};
+            for (int d = 0; d < nd; d++) {
+              const int NB = m.nbx[d] << p[0];
+              if (q[d] < 0 || q[d] >= NB) q[d] = ((q[d] % NB) + NB) % NB;
+            }
+            const Key qp = {p[0], q[0], q[1], q[2]};
+            for (int o = 0; o < (1 << nd) && ok; o++)
+              if (!leaf.count(child(qp, o))) ok = false;
+          }
+      if (!ok) continue;
+      for (int o = 0; o < (1 << nd); o++) leaf.erase(child(p, o));
+      leaf[p] = -1;
+      changed = true;
+    }
+  }
+  if (!changed) return KMY_OK;
+
+  std::vector<std::pair<uint64_t, Key>> order;
+  int maxl = 0;
+  for (auto &kv : leaf) maxl = std::max(maxl, kv.first[0]);
+  for (auto &kv : leaf) order.push_back({morton_key(kv.first[1], kv.first[2], kv.first[3], kv.first[0], maxl), kv.first});
+  std::sort(order.begin(), order.end());
+  const int nnew = int(order.size());
+  std::vector<int> nlev(nnew), nloc(size_t(3) * nnew), ncnt(nnew, 0);
+  for (int q = 0; q < nnew; q++) {
+    const Key &k = order[q].second;
+    nlev[q] = k[0];
+    for (int d = 0; d < 3; d++) nloc[3 * q + d] = k[1 + d];
+    const int old = leaf.find(k)->second;
+    if (old >= 0) ncnt[q] = a.cnt[old];
+  }
+
+  // remap base and the primitives through the old mesh's level values
+  const MeshDesc mo = m;
+  const size_t n_new = size_t(nnew) * m.P;
+  int *d_nlev = nullptr, *d_nloc = nullptr;
+  Container nb_ct;
+  void *nprim = nullptr;
+  rc = dalloc(c, reinterpret_cast<void **>(&d_nlev), sizeof(int) * nnew);
+  if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&d_nloc), sizeof(int) * 3 * nnew);
+  if (!rc) rc = dalloc(c, &nb_ct.cc, c->esz * c->ncc * n_new);
+  if (!rc && c->esz == 4) rc = dalloc(c, &nb_ct.ener_lo, 4 * n_new);
+  if (!rc) rc = dalloc(c, &nprim, c->esz * NPRIM * n_new);
+  if (!rc)
+    rc = cuda_check(c, cudaMemcpyAsync(d_nlev, nlev.data(), sizeof(int) * nnew, cudaMemcpyHostToDevice, c->stream),
+                    "remap levels");
+  if (!rc)
+    rc = cuda_check(c, cudaMemcpyAsync(d_nloc, nloc.data(), sizeof(int) * 3 * nnew, cudaMemcpyHostToDevice, c->stream),
+                    "remap locations");
+  if (rc) return rc;
+  Container &ob = c->md["base"];
+  const long long cells = (long long)m.nx[0] * m.nx[1] * m.nx[2] * nnew;
+  if (c->esz == 8)
+    k_amr_remap<double><<<nblk(cells), kThreads, 0, c->stream>>>(
+        mo, (const double *)ob.cc, nullptr, (const double *)c->prim, nnew, d_nlev, d_nloc, (double *)nb_ct.cc,
+        nullptr, (double *)nprim, c->ncc, a.d_err);
+  else
+    k_amr_remap<float><<<nblk(cells), kThreads, 0, c->stream>>>(
+        mo, (const float *)ob.cc, (const float *)ob.ener_lo, (const float *)c->prim, nnew, d_nlev, d_nloc,
+        (float *)nb_ct.cc, (float *)nb_ct.ener_lo, (float *)nprim, c->ncc, a.d_err);
+  c->launches++;
+  rc = cuda_check(c, cudaGetLastError(), "amr remap");
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "amr remap sync");
+  if (rc) return rc;
+
+  // release the old mesh's storage (stream ordered after the remap)
+  for (auto &kv : c->md) {
+    dfree(c, kv.second.cc);
+    dfree(c, kv.second.ener_lo);
+    dfree(c, kv.second.fc);
+    dfree(c, kv.second.emf);
+  }
+  c->md.clear();
+  dfree(c, c->prim);
+  dfree(c, c->flux);
+  c->flux = nullptr;
+  dfree(c, d_nlev);
+  dfree(c, d_nloc);
+  a.lev = nlev;
+  a.loc = nloc;
+  a.cnt = ncnt;
+  rc = amr_upload(c);
+  if (rc) return rc;
+  c->md["base"] = nb_ct;
+  c->prim = nprim;
+  const auto &nm = c->prm.stage_name;
+  for (size_t s = 1; s + 1 < nm.size() && !rc; s++)
+    if (!c->md.count(nm[s])) rc = make_container(c, nm[s]);
+  if (!rc) rc = launch_amr_fill_ghosts(c, c->md["base"]);
+  if (rc) return rc;
+  *changed_out = true;
+  return KMY_OK;
+}
+
+}  // namespace kmy

@@ -136,8 +136,26 @@ static int setup_params(kmy_ctx *c, const char *deck) {
 
   const std::string refine = p.str("parthenon/mesh/refinement", "none");
   if (!one_of(refine, {"none", "static", "adaptive"})) return bad("parthenon/mesh/refinement");
-  if (refine != "none" && p.integer("parthenon/mesh/numlevel", 1) > 1)
-    return bad("parthenon/mesh/refinement: multi-level meshes use the AMR entry points");
+  const int numlevel = p.integer("parthenon/mesh/numlevel", 1);
+  if (refine == "static" && numlevel > 1)
+    return bad("parthenon/mesh/refinement = static with numlevel > 1 is not supported");
+  // adaptive mesh: a <kamayan/refinement0> block with a field (grid.cpp:229-262)
+  AmrHost &amr = c->amr;
+  amr.on = refine == "adaptive" && numlevel > 1 && p.deck.count("kamayan/refinement0/field");
+  if (amr.on) {
+    if (numlevel > 8) return bad("parthenon/mesh/numlevel: at most 8 levels");
+    if (p.mhd) return bad("adaptive meshes are supported for hydro only");
+    amr.numlevel = numlevel;
+    amr.field = p.str("kamayan/refinement0/field", "dens");
+    if (!one_of(amr.field, {"dens", "pres", "ener"})) return bad("kamayan/refinement0/field: " + amr.field);
+    if (p.str("kamayan/refinement0/method", "loehner") != "loehner")
+      return bad("kamayan/refinement0/method: only loehner is implemented");
+    amr.refine_tol = p.real("kamayan/refinement0/refine_tol", 0.8);
+    amr.derefine_tol = p.real("kamayan/refinement0/derefine_tol", 0.2);
+    amr.filter = p.real("kamayan/refinement0/filter", 0.01);
+    amr.max_level = std::min(numlevel - 1, p.integer("kamayan/refinement0/max_level", numlevel - 1));
+    amr.derefine_count = p.integer("parthenon/mesh/derefine_count", 10);
+  }
 
   MeshDesc &m = c->m;
   const char *ax[3] = {"1", "2", "3"};
@@ -157,6 +175,8 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   const int ng = p.integer("parthenon/mesh/nghost", 4);
   const int need = ReconWidthRuntime(p.recon) + 1 + (p.mhd ? 1 : 0);
   if (ng < need) return bad("parthenon/mesh/nghost too small for the reconstruction");
+  // the refinement estimator takes second differences across the block edge
+  if (c->amr.on && ng < 2) return bad("parthenon/mesh/nghost: adaptive meshes need at least 2");
   m.nb = 1;
   for (int i = 0; i < 3; i++) {
     if (m.nx[i] <= 0 || m.mesh_nx[i] % m.nx[i] != 0)
@@ -195,6 +215,10 @@ int deck_footprint(const char *deck, Footprint *out, std::string *err) {
   if (rc) {
     if (err) *err = tmp.err;
     return rc;
+  }
+  if (tmp.amr.on) {
+    if (err) *err = "adaptive meshes are not batched: the block count changes between steps";
+    return KMY_ERR_BAD_PARAM;
   }
   const MeshDesc &m = tmp.m;
   const size_t n = size_t(m.nb) * m.P, nf = size_t(m.nb) * m.Pf;
@@ -240,7 +264,17 @@ int dalloc(kmy_ctx *c, void **p, size_t bytes) {
   return cuda_check(c, cudaMemsetAsync(*p, 0, bytes, c->stream), "memset");
 }
 
-static int make_container(kmy_ctx *c, const std::string &name) {
+void dfree(kmy_ctx *c, void *p) {
+  if (!p) return;
+  for (size_t i = 0; i < c->allocations.size(); i++)
+    if (c->allocations[i] == p) {
+      c->allocations.erase(c->allocations.begin() + long(i));
+      cudaFreeAsync(p, c->stream);
+      return;
+    }
+}
+
+int make_container(kmy_ctx *c, const std::string &name) {
   Container ct;
   const MeshDesc &m = c->m;
   const size_t n = size_t(m.nb) * m.P, nf = size_t(m.nb) * m.Pf;
@@ -391,6 +425,7 @@ int kmy_create(const char *deck, int device, kmy_ctx **out) {
   if (!rc && c->prm.mhd) rc = dalloc(c, reinterpret_cast<void **>(&c->divb), 8 * n);
   if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&c->clock), sizeof(DevClock));
   if (!rc) rc = dalloc(c, reinterpret_cast<void **>(&c->scratch), 8 * 64);
+  if (!rc && c->amr.on) rc = amr_setup(c);
   if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "create sync");
   if (rc) {
     std::fprintf(stderr, "kmy_create: %s\n", c->err.c_str());
@@ -530,13 +565,31 @@ int kmy_finalize_import(kmy_ctx *c) {
 int kmy_pgen(kmy_ctx *c, const char *problem) {
   if (!c || !problem) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
-  int rc = launch_pgen(c, problem);
+  auto generate = [&]() {
+    int r = launch_pgen(c, problem);
+    if (!r) r = launch_eos_init(c, c->md["base"]);
+    if (!r) r = launch_convert_to_conserved(c, c->md["base"]);
+    if (!r) r = launch_fill_ghosts(c, c->md["base"]);
+    return r;
+  };
+  int rc = KMY_OK;
+  if (c->amr.on) {
+    // initial refinement: generate, tag, refine (no derefinement) until the
+    // mesh stops changing, then generate on the final mesh
+    for (int it = 0; it < c->amr.numlevel && !rc; it++) {
+      bool changed = false;
+      rc = generate();
+      if (!rc) rc = launch_amr_tag(c, c->md["base"]);
+      if (!rc) rc = amr_remesh(c, false, &changed);
+      if (!changed) break;
+    }
+    if (rc) return rc;
+  }
+  rc = generate();
   if (rc) return rc;
+  if (c->amr.on) c->amr.cnt.assign(c->amr.cnt.size(), 0);
   Container &b = c->md["base"];
-  rc = launch_eos_init(c, b);
-  if (!rc) rc = launch_convert_to_conserved(c, b);
-  if (!rc) rc = launch_fill_ghosts(c, b);
-  if (!rc && c->prm.mhd) rc = launch_fill_derived(c, b);
+  if (c->prm.mhd) rc = launch_fill_derived(c, b);
   if (!rc) rc = launch_estimate_dt(c, b, true);
   if (!rc) rc = launch_dt_controller(c, 1);
   if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "pgen");
@@ -620,6 +673,7 @@ static int task_stage(kmy_ctx *c, int stage, double dt) {
     c->prims_valid = true;
   }
   int rc = launch_compute_fluxes(c, md0);
+  if (!rc && c->amr.on) rc = launch_flux_correct(c);
   if (!rc) rc = launch_compute_emf(c, md0);
   if (!rc) rc = launch_flux_divergence(c, md0, du);
   if (!rc) rc = launch_apply_dudt(c, base, md0, md1, du, c->prm.beta[stage - 1], dt,
@@ -628,8 +682,20 @@ static int task_stage(kmy_ctx *c, int stage, double dt) {
   if (!rc && stage == ns) {
     rc = launch_estimate_dt(c, base, true);
     if (!rc && c->prm.mhd) rc = launch_fill_derived(c, base);
+    // RefinementTagging runs before this stage's boundary exchange
+    if (!rc && c->amr.on) rc = launch_amr_tag(c, base);
   }
   if (!rc) rc = launch_fill_ghosts(c, md1);
+  return rc;
+}
+
+// After the stages of a step on an adaptive mesh: the tree update and remap,
+// and when the mesh changed the next dt also respects the new blocks' CFL
+// limit (the estimate accumulates into the step's minimum).
+static int amr_after_step(kmy_ctx *c) {
+  bool changed = false;
+  int rc = amr_remesh(c, true, &changed);
+  if (!rc && changed) rc = launch_estimate_dt(c, c->md["base"], false);
   return rc;
 }
 
@@ -672,14 +738,19 @@ int kmy_rk_stage(kmy_ctx *c, int stage, double dt) {
     c->err = "the fused stage covers hydro; use kmy_task_stage for constrained transport";
     return KMY_ERR_BAD_PARAM;
   }
+  if (c->amr.on) {
+    c->err = "the fused stage covers single-level meshes; use kmy_task_stage on an adaptive mesh";
+    return KMY_ERR_BAD_PARAM;
+  }
   return fused_stage(c, stage);
 }
 
 static int step_async(kmy_ctx *c) {
   const int ns = int(c->prm.beta.size());
   int rc = KMY_OK;
-  const bool fused = c->path == 0 && !c->prm.mhd;
+  const bool fused = c->path == 0 && !c->prm.mhd && !c->amr.on;
   for (int s = 1; s <= ns && !rc; s++) rc = fused ? fused_stage(c, s) : task_stage(c, s, -1.0);
+  if (!rc && c->amr.on) rc = amr_after_step(c);
   if (!rc) rc = launch_dt_controller(c, 0);
   return rc;
 }
@@ -709,7 +780,9 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
   int n = 0;
   DevClock h{};
   while (!rc) {
-    const int chunk = 8;
+    // an adaptive mesh reads its tags back every step anyway; stepping one at
+    // a time keeps it from running (and remeshing) past tlim
+    const int chunk = c->amr.on ? 1 : 8;
     for (int i = 0; i < chunk && !rc && (nlim < 0 || n < nlim); i++, n++) rc = step_async(c);
     if (rc) break;
     rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
@@ -729,7 +802,20 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
 int kmy_end_step(kmy_ctx *c) {
   if (!c) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
-  return launch_dt_controller(c, 0);
+  int rc = c->amr.on ? amr_after_step(c) : KMY_OK;
+  if (!rc) rc = launch_dt_controller(c, 0);
+  return rc;
+}
+
+int kmy_get_blocks(const kmy_ctx *c, int *levels, int *locations, int max_blocks, int *nblocks) {
+  if (!c) return KMY_ERR_BAD_PARAM;
+  const MeshDesc &m = c->m;
+  if (nblocks) *nblocks = m.nb;
+  for (int b = 0; b < m.nb && b < max_blocks; b++) {
+    if (levels) levels[b] = c->amr.on ? c->amr.lev[b] : 0;
+    for (int d = 0; d < 3 && locations; d++) locations[3 * b + d] = c->amr.on ? c->amr.loc[3 * b + d] : blk_loc(m, b, d);
+  }
+  return KMY_OK;
 }
 
 int kmy_get_time(const kmy_ctx *c, double *time, double *dt, double *dt_est, int *ncycle) {

@@ -33,7 +33,39 @@ struct MeshDesc {
   // cartesian geometry (Parthenon UniformCartesian products)
   double area[3];  // dy*dz, dx*dz, dx*dy
   double vol;      // dx*dy*dz
+  // adaptive mesh: per-block level and logical location, and per level a
+  // table of (leaf id | -1 covered by finer | -2 covered by coarser) over the
+  // level's block positions.  All null / zero on a single-level mesh, where
+  // block b sits at lexicographic location b at level 0.
+  const int *blev;
+  const int *bloc;
+  const int *tabs;
+  int nlev;
+  int tab_off[8];
+  int tab_dim[8][3];
 };
+
+__host__ __device__ __forceinline__ int blk_level(const MeshDesc &m, int b) { return m.blev ? m.blev[b] : 0; }
+__host__ __device__ __forceinline__ int blk_loc(const MeshDesc &m, int b, int d) {
+  if (m.bloc) return m.bloc[3 * b + d];
+  if (d == 0) return b % m.nbx[0];
+  if (d == 1) return (b / m.nbx[0]) % m.nbx[1];
+  return b / (m.nbx[0] * m.nbx[1]);
+}
+// cell size of block b (only active dimensions refine)
+__host__ __device__ __forceinline__ double blk_dx(const MeshDesc &m, int b, int d) {
+  return d < m.ndim ? m.dx[d] / double(1 << blk_level(m, b)) : m.dx[d];
+}
+__host__ __device__ __forceinline__ double blk_area(const MeshDesc &m, int b, int d) {
+  if (!m.blev) return m.area[d];
+  if (d == 0) return blk_dx(m, b, 1) * blk_dx(m, b, 2);
+  if (d == 1) return blk_dx(m, b, 0) * blk_dx(m, b, 2);
+  return blk_dx(m, b, 0) * blk_dx(m, b, 1);
+}
+__host__ __device__ __forceinline__ double blk_vol(const MeshDesc &m, int b) {
+  if (!m.blev) return m.vol;
+  return blk_dx(m, b, 0) * blk_dx(m, b, 1) * blk_dx(m, b, 2);
+}
 
 // Device-resident simulation clock.  The dt controller runs on the device so
 // that a whole step (all stages + controller) needs no host round trip.
@@ -98,6 +130,19 @@ struct Container {
   void *emf = nullptr;    // [3][nb][Pf] edge EMFs (CT only)
 };
 
+// Host side of an adaptive mesh: the leaf list and the refinement parameters.
+struct AmrHost {
+  bool on = false;
+  int numlevel = 1, max_level = 0, derefine_count = 10;
+  std::string field = "dens";
+  double refine_tol = 0.8, derefine_tol = 0.2, filter = 0.01;
+  std::vector<int> lev;  // per leaf
+  std::vector<int> loc;  // 3 per leaf
+  std::vector<int> cnt;  // consecutive derefine tags per leaf
+  int *d_blev = nullptr, *d_bloc = nullptr, *d_tabs = nullptr, *d_tags = nullptr;
+  int *d_err = nullptr;  // set by a level-value recursion that ran out of depth
+};
+
 }  // namespace kmy
 
 struct kmy_ctx {
@@ -117,6 +162,7 @@ struct kmy_ctx {
   double *scratch = nullptr;       // reduction scratch (device)
   bool prims_valid = false;  // stored prims match "base" (after pgen/import/tasks)
   int path = 0;              // 0 fused, 1 tasks
+  kmy::AmrHost amr;          // adaptive mesh (task path only)
   int64_t launches = 0;
   std::string err;
   std::vector<void *> allocations;
@@ -150,6 +196,17 @@ int launch_pgen(kmy_ctx *c, const std::string &problem);
 int cuda_check(kmy_ctx *c, cudaError_t e, const char *what);
 // Zeroed device allocation from the stream-ordered pool, freed with the context.
 int dalloc(kmy_ctx *c, void **p, size_t bytes);
+// Return one allocation of the context to the pool before the context ends.
+void dfree(kmy_ctx *c, void *p);
+int make_container(kmy_ctx *c, const std::string &name);
+
+// ---- adaptive mesh (kmy_amr.cu) ----
+int amr_setup(kmy_ctx *c);
+int amr_upload(kmy_ctx *c);
+int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct);
+int launch_flux_correct(kmy_ctx *c);
+int launch_amr_tag(kmy_ctx *c, Container &ct);
+int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed);
 
 // Device footprint and kernel class of a deck (kmy_api.cu), for admission.
 struct Footprint {

@@ -37,11 +37,11 @@ __global__ void k_pgen_cells(MeshDesc m, PgenParams pp, S *cc, S *prim) {
   r /= m.nx[0];
   const int j = int(r % m.nx[1]);
   const int k = int(r / m.nx[1]);
-  const int lx0 = b % m.nbx[0], lx1 = (b / m.nbx[0]) % m.nbx[1], lx2 = b / (m.nbx[0] * m.nbx[1]);
+  const int lx0 = blk_loc(m, b, 0), lx1 = blk_loc(m, b, 1), lx2 = blk_loc(m, b, 2);
   const long long gi = (long long)lx0 * m.nx[0] + i, gj = (long long)lx1 * m.nx[1] + j,
                   gk = (long long)lx2 * m.nx[2] + k;
-  const double x = m.xmin[0] + (double(gi) + 0.5) * m.dx[0];
-  const double y = m.xmin[1] + (double(gj) + 0.5) * m.dx[1];
+  const double x = m.xmin[0] + (double(gi) + 0.5) * blk_dx(m, b, 0);
+  const double y = m.xmin[1] + (double(gj) + 0.5) * blk_dx(m, b, 1);
   double dens = 1.0, v0 = 0.0, v1 = 0.0, v2 = 0.0, pres = 1.0;
   const double gamma = pp.gamma;
   if (pp.problem == P_VORTEX && pp.mhd) {

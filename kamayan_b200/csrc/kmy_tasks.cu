@@ -151,6 +151,7 @@ __global__ void k_fill_ghost_faces(MeshDesc m, S *fc, int e) {
 }
 
 int launch_fill_ghosts(kmy_ctx *c, Container &ct) {
+  if (c->amr.on) return launch_amr_fill_ghosts(c, ct);
   const MeshDesc &m = c->m;
   const long long n = (long long)m.nb * m.P;
   if (c->esz == 8)
@@ -363,11 +364,11 @@ __global__ void k_flux_divergence(MeshDesc m, const S *flux, S *du, int ncc) {
     S d = S(0);
     for (int dir = 0; dir < m.ndim; dir++) {
       const int kp = k + (dir == 2), jp = j + (dir == 1), ip = i + (dir == 0);
-      const S A = S(m.area[dir]);
+      const S A = S(blk_area(m, b, dir));
       const S *F = flux + ((long long)dir * ncc + v) * NF + bo;
       d -= (A * F[fidx(m, kp, jp, ip)] - A * F[fidx(m, k, j, i)]);
     }
-    du[v * NP + (long long)b * m.P + cidx(m, k, j, i)] = d / S(m.vol);
+    du[v * NP + (long long)b * m.P + cidx(m, k, j, i)] = d / S(blk_vol(m, b));
   }
 }
 
@@ -649,7 +650,7 @@ __global__ void k_estimate_dt(MeshDesc m, const S *cc, const S *prim, DevClock *
       for (int d = 0; d < 3; d++) V[RMAGC0 + d] = cc[(CMAGC0 + d) * NP + n];
     for (int dir = 0; dir < m.ndim; dir++) {
       const S cf = FastSpeed<MHD>(dir, V);
-      const double x = double(S(m.dx[dir]) / (fabs(V[RVEL0 + dir]) + cf));
+      const double x = double(S(blk_dx(m, b, dir)) / (fabs(V[RVEL0 + dir]) + cf));
       dtl = (x < dtl || x != x) ? x : dtl;
     }
   }
@@ -892,7 +893,7 @@ __global__ void k_cons_sums(MeshDesc m, const S *cc, const float *lo, int ncc, d
       const int j = m.g[1] + int(r % m.nx[1]);
       const int k = m.g[2] + int(r / m.nx[1]);
       const long long n = (long long)b * m.P + cidx(m, k, j, i);
-      const double x = (v == CENER ? load_ener(cc, lo, NP, n) : double(cc[v * NP + n])) * m.vol;
+      const double x = (v == CENER ? load_ener(cc, lo, NP, n) : double(cc[v * NP + n])) * blk_vol(m, b);
       two_sum(s, cm, x);
     }
     ss[threadIdx.x] = s;
@@ -964,8 +965,8 @@ __global__ void k_vortex_err(MeshDesc m, const S *cc, const S *prim, int var, in
     const int j = int(r % m.nx[1]);
     const int k = int(r / m.nx[1]);
     const long long n = (long long)b * m.P + cidx(m, k + m.g[2], j + m.g[1], i + m.g[0]);
-    const double x = m.xmin[0] + (double(block_loc(m, b, 0) * m.nx[0] + i) + 0.5) * m.dx[0];
-    const double y = m.xmin[1] + (double(block_loc(m, b, 1) * m.nx[1] + j) + 0.5) * m.dx[1];
+    const double x = m.xmin[0] + (double(blk_loc(m, b, 0) * m.nx[0] + i) + 0.5) * blk_dx(m, b, 0);
+    const double y = m.xmin[1] + (double(blk_loc(m, b, 1) * m.nx[1] + j) + 0.5) * blk_dx(m, b, 1);
     const double r2 = x * x + y * y;
     const double dv = strength * exp(0.5 * (1.0 - r2)) / (2.0 * M_PI);
     const double T = pressure / density -
@@ -995,7 +996,7 @@ __global__ void k_vortex_err(MeshDesc m, const S *cc, const S *prim, int var, in
       exact = presx;
       have = double(prim[PPRES * NP + n]);
     }
-    s += fabs(exact - have) * m.vol;
+    s += fabs(exact - have) * blk_vol(m, b);
   }
   ss[threadIdx.x] = s;
   __syncthreads();

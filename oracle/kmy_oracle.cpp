@@ -33,6 +33,7 @@
 // dt controller and singularity::IdealGas::FillEos.  Each such function says
 // so in its comment.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -429,18 +430,30 @@ struct Sim {
   // ---- indexing
   long cidx(int k, int j, int i) const { return (long(k) * np[1] + j) * np[0] + i; }
   long fidx(int k, int j, int i) const { return (long(k) * nf[1] + j) * nf[0] + i; }
-  int lx(int b, int d) const {
-    if (d == 0) return b % nbx[0];
-    if (d == 1) return (b / nbx[0]) % nbx[1];
-    return b / (nbx[0] * nbx[1]);
-  }
+  // Leaf blocks: level and logical location at that level.  A single-level
+  // mesh has every block at level 0 in lexicographic order; an adaptive mesh
+  // keeps its leaves in Morton order of their lower corners.
+  std::vector<int> blev;
+  std::vector<std::array<int, 3>> bloc;
+  std::vector<int> deref_count;  // consecutive derefine tags per leaf
+  std::vector<int> tags;         // last Loehner tag per leaf (-1, 0, 1)
+  bool amr = false;
+  int numlevel = 1;
+  int derefine_count = 10;
+  std::string ref_field = "dens";
+  Real refine_tol = 0.8, derefine_tol = 0.2, ref_filter = 0.01;
+  int max_level = 0;
+
+  int lx(int b, int d) const { return bloc[b][d]; }
+  // cell size of block b along d (only active dimensions refine)
+  Real dxb(int b, int d) const { return d < ndim ? dx[d] / Real(1 << blev[b]) : dx[d]; }
   // Uniform-mesh coordinate generator (Parthenon UniformCartesian, unpinned):
-  // dx = (xmax-xmin)/mesh_nx; block origin = xmin + lx*nx*dx.
+  // dx = (xmax-xmin)/mesh_nx / 2^level; block origin = xmin + lx*nx*dx.
   Real xface(int b, int d, int idx) const {
-    return xmin[d] + Real(lx(b, d) * nx[d] + (idx - g[d])) * dx[d];
+    return xmin[d] + Real(lx(b, d) * nx[d] + (idx - g[d])) * dxb(b, d);
   }
   Real xcen(int b, int d, int idx) const {
-    return xmin[d] + (Real(lx(b, d) * nx[d] + (idx - g[d])) + 0.5) * dx[d];
+    return xmin[d] + (Real(lx(b, d) * nx[d] + (idx - g[d])) + 0.5) * dxb(b, d);
   }
   // Parthenon UniformCartesian area/volume products (unpinned restatement)
   Real FaceArea(int d) const {
@@ -450,6 +463,12 @@ struct Sim {
   }
   Real CellVolume() const { return dx[0] * dx[1] * dx[2]; }
   Real EdgeLength(int d) const { return dx[d]; }
+  Real FaceAreaB(int b, int d) const {
+    if (d == 0) return dxb(b, 1) * dxb(b, 2);
+    if (d == 1) return dxb(b, 0) * dxb(b, 2);
+    return dxb(b, 0) * dxb(b, 1);
+  }
+  Real CellVolumeB(int b) const { return dxb(b, 0) * dxb(b, 1) * dxb(b, 2); }
 
   Container &C(const std::string &name) {
     auto it = md.find(name);
@@ -474,6 +493,17 @@ struct Sim {
   Real *pr(int v, int b) { return prim.data() + (size_t(v) * nb + b) * P; }
 
   bool setup(const char *deck_text);
+  // ---- adaptive mesh
+  std::vector<std::vector<int>> ltab;        // per level: leaf id, -1 finer, -2 coarser
+  std::vector<std::array<int, 3>> ltab_dim;  // blocks per dim at each level
+  void build_tables();
+  int table_at(int L, const int bx[3]) const;
+  Real V(int L, const int G[3], const Real *arr, int flipdim) const;
+  void fill_ghosts_amr(const std::string &name);
+  void flux_correct(const std::string &md0);
+  void tag_blocks(const std::string &name);
+  bool remesh(bool allow_derefine);
+  void resize_state(int new_nb);
   void fill_ghosts(const std::string &name);
   void calc_fluxes(const std::string &md0);
   void calc_emf(const std::string &md0);
@@ -489,6 +519,7 @@ struct Sim {
   void step(Real dt);
   void set_global_dt();
   int pgen(const std::string &problem);
+  int pgen_cells(const std::string &problem);
   Real vortex_error(int var, int comp);
 };
 
@@ -527,6 +558,29 @@ bool Sim::setup(const char *deck_text) {
     dx[i] = (xmax[i] - xmin[i]) / Real(mesh_nx[i]);
   }
   P = long(np[0]) * np[1] * np[2];
+  blev.assign(nb, 0);
+  bloc.resize(nb);
+  for (int b = 0; b < nb; b++)
+    bloc[b] = {b % nbx[0], (b / nbx[0]) % nbx[1], b / (nbx[0] * nbx[1])};
+  deref_count.assign(nb, 0);
+  tags.assign(nb, 0);
+  // adaptive mesh: <parthenon/mesh> refinement = adaptive with numlevel > 1 and
+  // a <kamayan/refinement0> block (grid.cpp:229-262)
+  numlevel = d.integer("parthenon/mesh/numlevel", 1);
+  amr = d.str("parthenon/mesh/refinement", "none") == "adaptive" && numlevel > 1 &&
+        d.has("kamayan/refinement0/field");
+  if (amr) {
+    ref_field = d.str("kamayan/refinement0/field", "dens");
+    refine_tol = d.real("kamayan/refinement0/refine_tol", 0.8);
+    derefine_tol = d.real("kamayan/refinement0/derefine_tol", 0.2);
+    ref_filter = d.real("kamayan/refinement0/filter", 0.01);
+    max_level = std::min(numlevel - 1, d.integer("kamayan/refinement0/max_level", numlevel - 1));
+    derefine_count = d.integer("parthenon/mesh/derefine_count", 10);
+    if (ph.mhd) {
+      error = "adaptive meshes are restated for hydro only";
+      return false;
+    }
+  }
   Pf = long(nf[0]) * nf[1] * nf[2];
 
   const std::string rc = d.str("hydro/reconstruction", "fog");
@@ -591,6 +645,7 @@ static inline int map_index(int G, int N, int bc, bool &flip) {
 }
 
 void Sim::fill_ghosts(const std::string &name) {
+  if (amr) return fill_ghosts_amr(name);
   Container &c = C(name);
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nb; b++) {
@@ -668,6 +723,471 @@ void Sim::fill_ghosts(const std::string &name) {
 }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Adaptive mesh (Parthenon's block tree and boundary exchange across levels,
+// un-vendored, restated; the refinement operators are kamayan's
+// refinement_operations.hpp:52-264 and the Loehner estimator is
+// grid_refinement.cpp:30-152).
+//
+// The value of a cell at level L and global index G is the best
+// representation available there: the cell of the leaf at level L that holds
+// it, the volume-weighted restriction of the finer leaves that cover it, or
+// the minmod prolongation from level L-1.  Ghost cells, remapped cells after a
+// remesh and the coarse stencils of a prolongation all use it.  With 2:1 level
+// balance (corners included) the recursion stays within one level of the
+// caller in either direction, apart from a restriction of a restriction.
+
+void Sim::build_tables() {
+  int maxl = 0;
+  for (int b = 0; b < nb; b++) maxl = std::max(maxl, blev[b]);
+  const int nlev = std::max(maxl, amr ? max_level : 0) + 1;
+  ltab.assign(nlev, {});
+  ltab_dim.assign(nlev, {1, 1, 1});
+  for (int L = 0; L < nlev; L++) {
+    size_t n = 1;
+    for (int d = 0; d < 3; d++) {
+      ltab_dim[L][d] = d < ndim ? (nbx[d] << L) : 1;
+      n *= size_t(ltab_dim[L][d]);
+    }
+    ltab[L].assign(n, -2);
+  }
+  for (int b = 0; b < nb; b++) {
+    const int Lb = blev[b];
+    for (int L = 0; L <= Lb; L++) {
+      int q[3];
+      for (int d = 0; d < 3; d++) q[d] = d < ndim ? (bloc[b][d] >> (Lb - L)) : 0;
+      const size_t idx = (size_t(q[2]) * ltab_dim[L][1] + q[1]) * ltab_dim[L][0] + q[0];
+      ltab[L][idx] = L == Lb ? b : -1;
+    }
+  }
+}
+
+int Sim::table_at(int L, const int bx[3]) const {
+  if (L < 0 || L >= int(ltab.size())) return -2;
+  return ltab[L][(size_t(bx[2]) * ltab_dim[L][1] + bx[1]) * ltab_dim[L][0] + bx[0]];
+}
+
+// RestrictAverage (refinement_operations.hpp:56-120) over the 2^d children;
+// cartesian volumes are equal, the sums keep the reference's grouping.
+static inline Real restrict_sum(const Real t[2][2][2], const Real v[2][2][2]) {
+  const Real tvol = ((v[0][0][0] + v[0][1][0]) + (v[0][0][1] + v[0][1][1])) +
+                    ((v[1][0][0] + v[1][1][0]) + (v[1][0][1] + v[1][1][1]));
+  return tvol > 0.0 ? (((t[0][0][0] + t[0][1][0]) + (t[0][0][1] + t[0][1][1])) +
+                       ((t[1][0][0] + t[1][1][0]) + (t[1][0][1] + t[1][1][1]))) /
+                          tvol
+                    : 0.0;
+}
+
+// util::GradMinMod (refinement_operations.hpp:44-50), SIGN(x) = x < 0 ? -1 : 1
+static inline Real grad_minmod(Real fc, Real fm, Real fp, Real dxm, Real dxp) {
+  const Real gxm = (fc - fm) / dxm;
+  const Real gxp = (fp - fc) / dxp;
+  const Real sm = gxm < 0 ? -1.0 : 1.0, sp = gxp < 0 ? -1.0 : 1.0;
+  return 0.5 * (sm + sp) * std::min(std::fabs(gxm), std::fabs(gxp));
+}
+
+Real Sim::V(int L, const int G[3], const Real *arr, int flipdim) const {
+  int M[3] = {0, 0, 0};
+  bool flip[3] = {false, false, false};
+  for (int d = 0; d < ndim; d++) {
+    const int N = mesh_nx[d] << L;
+    M[d] = map_index(G[d], N, bc[d][G[d] < 0 ? 0 : 1], flip[d]);
+  }
+  const Real sgn = (flipdim >= 0 && flip[flipdim]) ? -1.0 : 1.0;
+  int bx[3];
+  for (int d = 0; d < 3; d++) bx[d] = M[d] / nx[d];
+  const int e = table_at(L, bx);
+  if (e >= 0) {
+    return sgn * arr[size_t(e) * P + cidx(M[2] - bx[2] * nx[2] + g[2], M[1] - bx[1] * nx[1] + g[1],
+                                          M[0] - bx[0] * nx[0] + g[0])];
+  }
+  if (e == -1) {  // covered by finer leaves: restrict from level L+1
+    Real t[2][2][2] = {}, v[2][2][2] = {};
+    Real vol = 1.0;
+    for (int d = 0; d < 3; d++) vol *= d < ndim ? dx[d] / Real(1 << (L + 1)) : dx[d];
+    for (int ok = 0; ok < 1 + (ndim > 2); ok++)
+      for (int oj = 0; oj < 1 + (ndim > 1); oj++)
+        for (int oi = 0; oi < 2; oi++) {
+          const int Gc[3] = {2 * M[0] + oi, ndim > 1 ? 2 * M[1] + oj : 0, ndim > 2 ? 2 * M[2] + ok : 0};
+          v[ok][oj][oi] = vol;
+          t[ok][oj][oi] = vol * V(L + 1, Gc, arr, flipdim);
+        }
+    return sgn * restrict_sum(t, v);
+  }
+  // covered by a coarser leaf: prolongate from level L-1
+  // (ProlongateSharedGeneral<minmod>, refinement_operations.hpp:123-264)
+  int Mc[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+  for (int d = 0; d < ndim; d++) {
+    Mc[d] = M[d] >> 1;
+    o[d] = M[d] & 1;
+  }
+  const Real fc = V(L - 1, Mc, arr, flipdim);
+  Real gq[3] = {0, 0, 0}, dfm[3] = {0, 0, 0}, dfp[3] = {0, 0, 0};
+  for (int d = 0; d < ndim; d++) {
+    const Real dxc = dx[d] / Real(1 << (L - 1)), dxf = dx[d] / Real(1 << L);
+    auto xc_of = [&](int i) { return xmin[d] + (Real(i) + 0.5) * dxc; };
+    auto xf_of = [&](int i) { return xmin[d] + (Real(i) + 0.5) * dxf; };
+    int Gm[3] = {Mc[0], Mc[1], Mc[2]}, Gp[3] = {Mc[0], Mc[1], Mc[2]};
+    Gm[d] -= 1;
+    Gp[d] += 1;
+    const Real fm = V(L - 1, Gm, arr, flipdim), fp = V(L - 1, Gp, arr, flipdim);
+    const Real xm = xc_of(Mc[d] - 1), xc = xc_of(Mc[d]), xp = xc_of(Mc[d] + 1);
+    const Real dxm = xc - xm, dxp = xp - xc;
+    dfm[d] = xc - xf_of(2 * Mc[d]);
+    dfp[d] = xf_of(2 * Mc[d] + 1) - xc;
+    gq[d] = grad_minmod(fc, fm, fp, dxm, dxp);
+  }
+  const Real g1 = gq[0], g2 = gq[1], g3 = gq[2];
+  const Real d1m = dfm[0], d1p = dfp[0], d2m = dfm[1], d2p = dfp[1], d3m = dfm[2], d3p = dfp[2];
+  Real val;
+  const int code = o[0] + 2 * o[1] + 4 * o[2];
+  switch (code) {
+    case 0: val = fc - (g1 * d1m + g2 * d2m + g3 * d3m); break;
+    case 1: val = fc + (g1 * d1p - g2 * d2m - g3 * d3m); break;
+    case 2: val = fc - (g1 * d1m - g2 * d2p + g3 * d3m); break;
+    case 3: val = fc + (g1 * d1p + g2 * d2p - g3 * d3m); break;
+    case 4: val = fc - (g1 * d1m + g2 * d2m - g3 * d3p); break;
+    case 5: val = fc + (g1 * d1p - g2 * d2m + g3 * d3p); break;
+    case 6: val = fc - (g1 * d1m - g2 * d2p - g3 * d3p); break;
+    default: val = fc + (g1 * d1p + g2 * d2p + g3 * d3p); break;
+  }
+  return sgn * val;
+}
+
+void Sim::fill_ghosts_amr(const std::string &name) {
+  Container &c = C(name);
+  build_tables();
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < nb; b++) {
+    const int L = blev[b];
+    for (int k = 0; k < np[2]; k++)
+      for (int j = 0; j < np[1]; j++)
+        for (int i = 0; i < np[0]; i++) {
+          const int loc[3] = {i, j, k};
+          bool interior = true;
+          for (int d = 0; d < 3; d++)
+            if (loc[d] < g[d] || loc[d] >= g[d] + nx[d]) interior = false;
+          if (interior) continue;
+          const int G[3] = {bloc[b][0] * nx[0] + (i - g[0]), bloc[b][1] * nx[1] + (j - g[1]),
+                            bloc[b][2] * nx[2] + (k - g[2])};
+          const long n = cidx(k, j, i);
+          for (int v = 0; v < ncc; v++) {
+            const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : -1;
+            cc(c, v, b)[n] = V(L, G, cc(c, v, 0), fd);
+          }
+          for (int v = 0; v < NPRIM; v++) pr(v, b)[n] = V(L, G, pr(v, 0), v <= PVEL2 ? v : -1);
+        }
+  }
+}
+
+// Flux correction at fine/coarse faces (Parthenon AddFluxCorrectionTasks,
+// kamayan_driver.cpp:206-207): a coarse face flux is replaced by the
+// area-weighted restriction (RestrictAverage on face elements) of the fine
+// fluxes that share the face.
+void Sim::flux_correct(const std::string &md0name) {
+  Container &c = C(md0name);
+  build_tables();
+  for (int b = 0; b < nb; b++) {
+    const int L = blev[b];
+    for (int d = 0; d < ndim; d++)
+      for (int s = 0; s < 2; s++) {
+        const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+        for (int a2 = 0; a2 < nx[t2]; a2++)
+          for (int a1 = 0; a1 < nx[t1]; a1++) {
+            // the coarse cell across the face, at level L
+            int Gn[3];
+            Gn[d] = bloc[b][d] * nx[d] + (s ? nx[d] : -1);
+            Gn[t1] = bloc[b][t1] * nx[t1] + a1;
+            Gn[t2] = bloc[b][t2] * nx[t2] + a2;
+            const int N = mesh_nx[d] << L;
+            if ((Gn[d] < 0 || Gn[d] >= N) && bc[d][s] != PERIODIC) continue;
+            int Mn[3] = {Gn[0], Gn[1], Gn[2]};
+            bool fl_ = false;
+            Mn[d] = map_index(Gn[d], N, bc[d][s], fl_);
+            int bxn[3];
+            for (int q = 0; q < 3; q++) bxn[q] = Mn[q] / nx[q];
+            if (table_at(L, bxn) != -1) continue;  // not finer across this face
+            // the fine faces: level L+1, fine cell on the far side of the face
+            Real t[2][2][2][8] = {}, vv[2][2][2] = {};
+            for (int o2 = 0; o2 < 1 + (t2 < ndim); o2++)
+              for (int o1 = 0; o1 < 1 + (t1 < ndim); o1++) {
+                int Gf[3];
+                const int Ff = 2 * (bloc[b][d] * nx[d] + (s ? nx[d] : 0));
+                Gf[d] = s ? Ff : Ff - 1;
+                Gf[t1] = t1 < ndim ? 2 * (bloc[b][t1] * nx[t1] + a1) + o1 : 0;
+                Gf[t2] = t2 < ndim ? 2 * (bloc[b][t2] * nx[t2] + a2) + o2 : 0;
+                const int Nf = mesh_nx[d] << (L + 1);
+                bool f2 = false;
+                Gf[d] = map_index(Gf[d], Nf, bc[d][s], f2);
+                int bf[3];
+                for (int q = 0; q < 3; q++) bf[q] = Gf[q] / nx[q];
+                const int e = table_at(L + 1, bf);
+                int lf[3];
+                for (int q = 0; q < 3; q++) lf[q] = Gf[q] - bf[q] * nx[q] + g[q];
+                if (!s) lf[d] += 1;  // the fine cell's high face
+                const Real area = FaceAreaB(e, d);
+                // reference index order [ok][oj][oi] over the transverse offsets
+                int oi = 0, oj = 0, ok = 0;
+                int off[3] = {0, 0, 0};
+                off[t1] = o1;
+                off[t2] = o2;
+                oi = off[0];
+                oj = off[1];
+                ok = off[2];
+                vv[ok][oj][oi] = area;
+                for (int v = 0; v < ncc; v++)
+                  t[ok][oj][oi][v] = area * fl(c, d, v, e)[fidx(lf[2], lf[1], lf[0])];
+              }
+            int lc[3] = {g[0], g[1], g[2]};
+            lc[d] = g[d] + (s ? nx[d] : 0);
+            lc[t1] = g[t1] + a1;
+            lc[t2] = g[t2] + a2;
+            for (int v = 0; v < ncc; v++) {
+              Real tv[2][2][2];
+              for (int x = 0; x < 2; x++)
+                for (int y = 0; y < 2; y++)
+                  for (int z = 0; z < 2; z++) tv[x][y][z] = t[x][y][z][v];
+              fl(c, d, v, b)[fidx(lc[2], lc[1], lc[0])] = restrict_sum(tv, vv);
+            }
+          }
+      }
+  }
+}
+
+// AMRLoehner::operator() (grid_refinement.cpp:30-152) on one field of `name`.
+void Sim::tag_blocks(const std::string &name) {
+  Container &c = C(name);
+  const Real *arr = nullptr;
+  if (ref_field == "dens") arr = cc(c, CDENS, 0);
+  else if (ref_field == "pres") arr = pr(PPRES, 0);
+  else if (ref_field == "ener") arr = cc(c, CENER, 0);
+  else arr = cc(c, CDENS, 0);
+  tags.assign(nb, 0);
+  const int k2d = ndim > 1 ? 1 : 0, k3d = ndim > 2 ? 1 : 0;
+  for (int b = 0; b < nb; b++) {
+    const Real *u = arr + size_t(b) * P;
+    std::vector<Real> der(size_t(3) * P, 0.0);
+    auto D = [&](int p, int k, int j, int i) -> Real & { return der[size_t(p) * P + cidx(k, j, i)]; };
+    const Real dxq[3] = {dxb(b, 0), dxb(b, 1), dxb(b, 2)};
+    for (int k = g[2] - k3d; k <= g[2] + nx[2] - 1 + k3d; k++)
+      for (int j = g[1] - k2d; j <= g[1] + nx[1] - 1 + k2d; j++)
+        for (int i = g[0] - 1; i <= g[0] + nx[0]; i++) {
+          D(0, k, j, i) = 0.5 * (u[cidx(k, j, i + 1)] - u[cidx(k, j, i - 1)]) / dxq[0];
+          if (ndim > 1) D(1, k, j, i) = 0.5 * (u[cidx(k, j + 1, i)] - u[cidx(k, j - 1, i)]) / dxq[1];
+          if (ndim > 2) D(2, k, j, i) = 0.5 * (u[cidx(k + 1, j, i)] - u[cidx(k - 1, j, i)]) / dxq[2];
+        }
+    int flag_block = -1;
+    for (int k = g[2]; k < g[2] + nx[2]; k++)
+      for (int j = g[1]; j < g[1] + nx[1]; j++) {
+        Real max_err_2 = 0.;
+        for (int i = g[0]; i < g[0] + nx[0]; i++) {
+          Real numerator = 0.0, denominator = 1.e-12;
+          for (int q = 0; q < ndim; q++) {
+            const int kq = q == 2, jq = q == 1, iq = q == 0;
+            for (int p = 0; p < ndim; p++) {
+              const int kp = p == 2, jp = p == 1, ip = p == 0;
+              const Real num = 0.5 * (D(p, k + kq, j + jq, i + iq) - D(p, k - kq, j - jq, i - iq)) / dxq[q];
+              numerator += num * num;
+              const Real denom =
+                  0.5 * (std::fabs(D(p, k + kq, j + jq, i + iq)) + std::fabs(D(p, k - kq, j - jq, i - iq))) /
+                      dxq[p] +
+                  ref_filter *
+                      (std::fabs(u[cidx(k + kq, j + jq, i + iq)]) + std::fabs(u[cidx(k - kq, j - jq, i - iq)]) +
+                       std::fabs(u[cidx(k - kp, j - jp, i - ip)]) + std::fabs(u[cidx(k + kp, j + jp, i + ip)])) /
+                      (dxq[q] * dxq[p]);
+              denominator += denom * denom;
+            }
+          }
+          max_err_2 = denominator == 0.0 ? max_err_2 : kmax(max_err_2, numerator / denominator);
+        }
+        const Real max_err = std::sqrt(max_err_2);
+        int flag = 0;
+        if (max_err > refine_tol && blev[b] < max_level) flag = 1;
+        if (max_err < derefine_tol) flag = -1;
+        flag_block = std::max(flag_block, flag);
+      }
+    tags[b] = flag_block;
+  }
+}
+
+void Sim::resize_state(int new_nb) {
+  nb = new_nb;
+  for (auto &kv : md) {
+    Container &c = kv.second;
+    c.cc.assign(size_t(ncc) * nb * P, 0.0);
+    c.flux.assign(size_t(3) * ncc * nb * Pf, 0.0);
+  }
+  prim.assign(size_t(NPRIM) * nb * P, 0.0);
+}
+
+// Morton key of a leaf's lower corner at the finest level (block ordering).
+static uint64_t morton_key(const std::array<int, 3> &loc, int level, int maxl) {
+  const int sh = maxl - level;
+  uint64_t x = uint64_t(loc[0]) << sh, y = uint64_t(loc[1]) << sh, z = uint64_t(loc[2]) << sh;
+  uint64_t key = 0;
+  for (int bit = 0; bit < 20; bit++) {
+    key |= ((x >> bit) & 1ull) << (3 * bit);
+    key |= ((y >> bit) & 1ull) << (3 * bit + 1);
+    key |= ((z >> bit) & 1ull) << (3 * bit + 2);
+  }
+  return (key << 5) | uint64_t(level);
+}
+
+// Parthenon's tree update (Mesh::UpdateMeshBlockTree), restated: refine the
+// leaves tagged for refinement below max_level, restore 2:1 balance across
+// faces, edges and corners by refining coarser neighbours, then merge sibling
+// groups whose members have all been tagged for derefinement derefine_count
+// times in a row when the merged parent keeps the balance.  New leaves get
+// their data from the old mesh through V (copy, prolongation or restriction).
+bool Sim::remesh(bool allow_derefine) {
+  typedef std::array<int, 4> Key;  // level, loc
+  std::map<Key, int> leaf;         // key -> old leaf id (or -1 for new)
+  for (int b = 0; b < nb; b++) {
+    leaf[{blev[b], bloc[b][0], bloc[b][1], bloc[b][2]}] = b;
+    deref_count[b] = tags[b] == -1 ? deref_count[b] + 1 : 0;
+  }
+  bool changed = false;
+  auto split = [&](const Key &k) {
+    leaf.erase(k);
+    for (int o = 0; o < (1 << ndim); o++) {
+      Key ch = {k[0] + 1, 2 * k[1] + (o & 1), ndim > 1 ? 2 * k[2] + ((o >> 1) & 1) : 0,
+                ndim > 2 ? 2 * k[3] + ((o >> 2) & 1) : 0};
+      leaf[ch] = -1;
+    }
+    changed = true;
+  };
+  // leaf covering block position p at level L (or level -1 if finer leaves cover it)
+  auto covering = [&](int L, int p0, int p1, int p2, Key &out) -> bool {
+    int p[3] = {p0, p1, p2};
+    for (int d = 0; d < ndim; d++) {
+      const int NB = nbx[d] << L;
+      if (p[d] < 0 || p[d] >= NB) {
+        if (bc[d][p[d] < 0 ? 0 : 1] != PERIODIC) return false;
+        p[d] = ((p[d] % NB) + NB) % NB;
+      }
+    }
+    for (int l = L; l >= 0; l--) {
+      Key k = {l, p[0] >> (L - l), ndim > 1 ? p[1] >> (L - l) : 0, ndim > 2 ? p[2] >> (L - l) : 0};
+      if (leaf.count(k)) {
+        out = k;
+        return true;
+      }
+    }
+    return false;
+  };
+  for (int b = 0; b < nb; b++)
+    if (tags[b] == 1 && blev[b] < max_level) split({blev[b], bloc[b][0], bloc[b][1], bloc[b][2]});
+  // 2:1 balance
+  for (bool again = true; again;) {
+    again = false;
+    std::vector<Key> keys;
+    for (auto &kv : leaf) keys.push_back(kv.first);
+    for (const Key &k : keys) {
+      if (!leaf.count(k)) continue;
+      for (int dz = -(ndim > 2); dz <= (ndim > 2); dz++)
+        for (int dy = -(ndim > 1); dy <= (ndim > 1); dy++)
+          for (int dxo = -1; dxo <= 1; dxo++) {
+            if (!dxo && !dy && !dz) continue;
+            Key n;
+            if (!covering(k[0], k[1] + dxo, k[2] + dy, k[3] + dz, n)) continue;
+            if (n[0] < k[0] - 1) {
+              split(n);
+              again = true;
+            }
+          }
+    }
+  }
+  if (allow_derefine) {
+    // candidate parents: all children leaves, none refined this cycle, tagged long enough
+    std::map<Key, int> parents;
+    for (auto &kv : leaf) {
+      const Key &k = kv.first;
+      if (k[0] == 0 || kv.second < 0) continue;
+      if (deref_count[kv.second] < derefine_count) continue;
+      Key p = {k[0] - 1, k[1] >> 1, k[2] >> 1, k[3] >> 1};
+      parents[p]++;
+    }
+    for (auto &pk : parents) {
+      if (pk.second != (1 << ndim)) continue;
+      const Key &p = pk.first;
+      bool ok = true;
+      for (int dz = -(ndim > 2); dz <= (ndim > 2) && ok; dz++)
+        for (int dy = -(ndim > 1); dy <= (ndim > 1) && ok; dy++)
+          for (int dxo = -1; dxo <= 1 && ok; dxo++) {
+            if (!dxo && !dy && !dz) continue;
+            Key n;
+            if (covering(p[0], p[1] + dxo, p[2] + dy, p[3] + dz, n)) continue;  // leaf at <= p level
+            // the region is finer: every child at p's level + 1 must be a leaf
+            int q[3] = {p[1] + dxo, p[2] + dy, p[3] + dz};
+            for (int d = 0; d < ndim; d++) {
+              const int NB = nbx[d] << p[0];
+              if (q[d] < 0 || q[d] >= NB) q[d] = ((q[d] % NB) + NB) % NB;
+            }
+            for (int o = 0; o < (1 << ndim) && ok; o++) {
+              Key ch = {p[0] + 1, 2 * q[0] + (o & 1), ndim > 1 ? 2 * q[1] + ((o >> 1) & 1) : 0,
+                        ndim > 2 ? 2 * q[2] + ((o >> 2) & 1) : 0};
+              if (!leaf.count(ch)) ok = false;
+            }
+          }
+      if (!ok) continue;
+      for (int o = 0; o < (1 << ndim); o++)
+        leaf.erase({p[0] + 1, 2 * p[1] + (o & 1), ndim > 1 ? 2 * p[2] + ((o >> 1) & 1) : 0,
+                    ndim > 2 ? 2 * p[3] + ((o >> 2) & 1) : 0});
+      leaf[p] = -1;
+      changed = true;
+    }
+  }
+  if (!changed) return false;
+  // new leaf list in Morton order
+  std::vector<std::pair<uint64_t, Key>> order;
+  int maxl = 0;
+  for (auto &kv : leaf) maxl = std::max(maxl, kv.first[0]);
+  for (auto &kv : leaf)
+    order.push_back({morton_key({kv.first[1], kv.first[2], kv.first[3]}, kv.first[0], maxl), kv.first});
+  std::sort(order.begin(), order.end());
+  // remap base + primitives through V of the old mesh
+  build_tables();
+  Container &base = C("base");
+  std::vector<Real> old_cc = base.cc, old_prim = prim;
+  const int old_nb = nb;
+  const std::vector<int> old_cnt = deref_count;
+  const int nnew = int(order.size());
+  std::vector<int> nlev(nnew), ncnt(nnew, 0);
+  std::vector<std::array<int, 3>> nloc(nnew);
+  for (int q = 0; q < nnew; q++) {
+    const Key &k = order[q].second;
+    nlev[q] = k[0];
+    nloc[q] = {k[1], k[2], k[3]};
+    auto it = leaf.find(k);
+    if (it->second >= 0) ncnt[q] = old_cnt[it->second];
+  }
+  std::vector<Real> new_cc(size_t(ncc) * nnew * P, 0.0), new_prim(size_t(NPRIM) * nnew * P, 0.0);
+#pragma omp parallel for schedule(dynamic)
+  for (int q = 0; q < nnew; q++)
+    for (int k = g[2]; k < g[2] + nx[2]; k++)
+      for (int j = g[1]; j < g[1] + nx[1]; j++)
+        for (int i = g[0]; i < g[0] + nx[0]; i++) {
+          const int G[3] = {nloc[q][0] * nx[0] + (i - g[0]), nloc[q][1] * nx[1] + (j - g[1]),
+                            nloc[q][2] * nx[2] + (k - g[2])};
+          const long n = cidx(k, j, i);
+          for (int v = 0; v < ncc; v++)
+            new_cc[(size_t(v) * nnew + q) * P + n] =
+                V(nlev[q], G, old_cc.data() + size_t(v) * old_nb * P, v >= CMOM0 && v <= CMOM2 ? v - CMOM0 : -1);
+          for (int v = 0; v < NPRIM; v++)
+            new_prim[(size_t(v) * nnew + q) * P + n] =
+                V(nlev[q], G, old_prim.data() + size_t(v) * old_nb * P, v <= PVEL2 ? v : -1);
+        }
+  resize_state(nnew);
+  base.cc = std::move(new_cc);
+  prim = std::move(new_prim);
+  blev = nlev;
+  bloc = nloc;
+  deref_count = ncnt;
+  tags.assign(nb, 0);
+  fill_ghosts("base");
+  return true;
+}
+
 // hydro_add_flux_tasks.cpp:36-264 (CalculateFluxesNested, the default
 // "scratchpad" strategy).  The "scratchvar" strategy (:266-385) evaluates the
 // same per-face expressions, so both give identical bits.
@@ -808,17 +1328,17 @@ void Sim::calc_emf(const std::string &md0name) {
 void Sim::fluxes_to_dudt(const std::string &md0name, const std::string &dudtname) {
   Container &c = C(md0name);
   Container &du = C(dudtname);
-  const Real vol = CellVolume();
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nb; b++)
     for (int k = g[2]; k < g[2] + nx[2]; k++)
       for (int j = g[1]; j < g[1] + nx[1]; j++)
         for (int i = g[0]; i < g[0] + nx[0]; i++)
           for (int v = 0; v < ncc; v++) {
+            const Real vol = CellVolumeB(b);
             Real d = 0.;
             for (int dir = 0; dir < ndim; dir++) {
               const int kp = k + (dir == 2), jp = j + (dir == 1), ip = i + (dir == 0);
-              const Real A = FaceArea(dir);
+              const Real A = FaceAreaB(b, dir);
               d -= (A * fl(c, dir, v, b)[fidx(kp, jp, ip)] - A * fl(c, dir, v, b)[fidx(k, j, i)]);
             }
             cc(du, v, b)[cidx(k, j, i)] = d / vol;
@@ -995,7 +1515,7 @@ Real Sim::estimate_dt(const std::string &name) {
             for (int d = 0; d < 3; d++) V[RMAGC0 + d] = cc(c, CMAGC0 + d, b)[n];
           for (int dir = 0; dir < ndim; dir++) {
             const Real cfast = FastSpeed(ph, dir, V);
-            dt_min = kmin(dt_min, dx[dir] / (std::fabs(V[RVEL0 + dir]) + cfast));
+            dt_min = kmin(dt_min, dxb(b, dir) / (std::fabs(V[RVEL0 + dir]) + cfast));
           }
         }
   return dt_min * cfl_nd;
@@ -1030,6 +1550,7 @@ void Sim::rk_stage(int stage, Real dt_) {
   const std::string &md1 = stage_name[stage];
   const Real b = beta[stage - 1];
   calc_fluxes(md0);
+  if (amr) flux_correct(md0);
   calc_emf(md0);
   fluxes_to_dudt(md0, "dUdt");
   apply_dudt(base, md0, md1, "dUdt", b, dt_);
@@ -1037,6 +1558,9 @@ void Sim::rk_stage(int stage, Real dt_) {
   if (stage == nstages) {
     dt_est = estimate_dt(base);
     fill_derived(base);
+    // RefinementTagging runs before this stage's boundary exchange
+    // (kamayan_driver.cpp:178-181 then :150-151)
+    if (amr) tag_blocks(base);
   }
   fill_ghosts(md1);
 }
@@ -1071,7 +1595,7 @@ static inline Real kh_uniform(uint64_t seed, uint64_t gidx, int comp) {
   return Real(h >> 11) * 0x1.0p-53;  // [0, 1)
 }
 
-int Sim::pgen(const std::string &problem) {
+int Sim::pgen_cells(const std::string &problem) {
   Container &c = C("base");
   const Real gm1 = gamma - 1.0;
   (void)gm1;
@@ -1197,6 +1721,23 @@ int Sim::pgen(const std::string &problem) {
   eos_init("base");
   convert_to_conserved("base");
   fill_ghosts("base");
+  return 0;
+}
+
+// Problem set-up.  On an adaptive mesh the problem generator, tagging and
+// refinement repeat (refinement only) until the mesh stops changing, as in
+// Parthenon's initial refinement; the generator then runs on the final mesh.
+int Sim::pgen(const std::string &problem) {
+  if (amr) {
+    for (int it = 0; it < numlevel; it++) {
+      if (pgen_cells(problem)) return -1;
+      tag_blocks("base");
+      if (!remesh(false)) break;
+    }
+  }
+  if (pgen_cells(problem)) return -1;
+  deref_count.assign(nb, 0);
+  tags.assign(nb, 0);
   // initial time step (Parthenon driver initialisation)
   dt_est = estimate_dt("base");
   if (ph.mhd) fill_derived("base");
@@ -1255,7 +1796,7 @@ Real Sim::vortex_error(int var, int comp) {
             exact = presx;
             have = pr(PPRES, b)[n];
           }
-          err += std::fabs(exact - have) * CellVolume();
+          err += std::fabs(exact - have) * CellVolumeB(b);
         }
   return err / ((xmax[0] - xmin[0]) * (xmax[1] - xmin[1]));
 }
@@ -1360,8 +1901,22 @@ Real kmyo_step(void *h) {
   s->step(dt);
   s->time += dt;
   s->ncycle += 1;
+  if (s->amr && s->remesh(true)) {
+    // new (finer) blocks: the next dt also respects their CFL limit
+    s->dt_est = kmyo::kmin(s->dt_est, s->estimate_dt("base"));
+  }
   s->set_global_dt();
   return dt;
+}
+
+// Leaf list: level and logical location of each block (in block order).
+int kmyo_blocks(void *h, int *levels, int *locs, int max) {
+  Sim *s = static_cast<Sim *>(h);
+  for (int b = 0; b < s->nb && b < max; b++) {
+    levels[b] = s->blev[b];
+    for (int d = 0; d < 3; d++) locs[3 * b + d] = s->bloc[b][d];
+  }
+  return s->nb;
 }
 
 // Driver loop to tlim / nlim (Parthenon EvolutionDriver semantics, restated).

@@ -63,6 +63,8 @@ def lib():
         L.kmyo_reconstruct.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]
         L.kmyo_eos.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
         L.kmyo_riemann.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.kmyo_blocks.argtypes = [ctypes.c_void_p, ip, ip, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -114,13 +116,30 @@ class OracleSim:
             lib().kmyo_destroy(self._h)
             self._h = None
 
+    def refresh(self) -> None:
+        """Re-read the mesh description (the block count changes on an adaptive mesh)."""
+        buf = (ctypes.c_long * 32)()
+        n = lib().kmyo_info(self._h, buf)
+        self.info = dict(zip(self.INFO, buf[:n]))
+
+    def blocks(self):
+        """(levels, locations) of the leaf blocks in block order."""
+        self.refresh()
+        nb = self.info["nb"]
+        lev = (ctypes.c_int * nb)()
+        loc = (ctypes.c_int * (3 * nb))()
+        lib().kmyo_blocks(self._h, lev, loc, nb)
+        return np.array(lev[:]), np.array(loc[:]).reshape(nb, 3)
+
     @property
     def cell_shape(self):
+        self.refresh()
         i = self.info
         return (i["nb"], i["np3"], i["np2"], i["np1"])
 
     @property
     def face_shape(self):
+        self.refresh()
         i = self.info
         return (i["nb"], i["nf3"], i["nf2"], i["nf1"])
 
