@@ -52,6 +52,8 @@ def args():
     ap.add_argument("--serve", type=int, default=120,
                     help="requests in the serving-stream measurement (0: skip; 2000 = full stream)")
     ap.add_argument("--serve-steps", type=int, default=100)
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the vortex / Orszag-Tang / adaptive-blast measurements")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
                     help="time one precision only (profiling captures); prints its own line")
     return ap.parse_args()
@@ -285,9 +287,10 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(sample_n: int, min_seconds: float, max_steps: int, steps: int = 1):
-    cmd = [sys.executable, "-m", "oracle.cpu_bench", "--workload", "kh_3d", "--n", str(sample_n),
-           "--nb", "32", "--steps", str(steps), "--warmup", "1", "--min-seconds", str(min_seconds),
+def cpu_baseline(sample_n: int, min_seconds: float, max_steps: int, steps: int = 1,
+                 workload: str = "kh_3d", nb: int = 32, warmup: int = 1):
+    cmd = [sys.executable, "-m", "oracle.cpu_bench", "--workload", workload, "--n", str(sample_n),
+           "--nb", str(nb), "--steps", str(steps), "--warmup", str(warmup), "--min-seconds", str(min_seconds),
            "--max-steps", str(max_steps)]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
     if r.returncode != 0:
@@ -317,6 +320,79 @@ def serving_block(a, device: int) -> dict:
         "sequential_per_solve": seq,
         "batched_over_sequential": sat["cell_updates_per_s"] / seq["cell_updates_per_s"],
     }
+
+
+def _evolve_timed(s, stream, tlim=None, nsteps=None):
+    """Step to tlim (or nsteps) with kmy_step; device time between two events on the
+    solver's stream, and the interior cells advanced (block counts change under AMR)."""
+    import torch
+
+    cells_per_block = 1
+    for x in s.info.nx:
+        cells_per_block *= x
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    updates, steps, nbs = 0, 0, []
+    t0.record(stream)
+    while True:
+        if nsteps is not None and steps >= nsteps:
+            break
+        if tlim is not None and s.time["time"] >= tlim * (1 - 1e-14):
+            break
+        nb = s.nblocks
+        s.step()
+        updates += nb * cells_per_block
+        nbs.append(nb)
+        steps += 1
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1), updates, steps, nbs
+
+
+def workloads_block(a, device: int, stream) -> dict:
+    """The other configurations of the path, each timed through kmy_step on one GPU:
+    2D vortex to t=10 (FP64, fused), 3D Orszag-Tang with constrained transport
+    (FP32 bulk, per-task kernels), and the 2D blast on an adaptive mesh to t=0.2."""
+    import kamayan_b200
+    from kamayan_b200 import configs
+
+    out = {}
+
+    def solver(deck, problem, path):
+        s = kamayan_b200.Solver(deck, device=device)
+        s.set_stream(stream.cuda_stream)
+        s.set_path(path)
+        s.pgen(problem)
+        return s
+
+    # c1: vortex 128^2, 4 blocks of 64^2, PLM(MC)+HLL, RK2, to t = 10
+    s = solver(configs.vortex_2d(), "isentropic_vortex", "fused")
+    ms, upd, steps, _ = _evolve_timed(s, stream, tlim=10.0)
+    out["vortex_2d_fp64"] = {"cell_updates_per_s": upd / (ms / 1e3), "steps": steps, "seconds": ms / 1e3,
+                             "l1_density_vs_exact": s.vortex_error("dens"),
+                             "config": "128^2 in 4x64^2, g=2, PLM(MC)+HLL, RK2, CFL 0.8, t=10"}
+    s.close()
+    # c3: Orszag-Tang 192^3, 216 blocks of 32^3, CT, PPM+HLL, RK2, FP32 bulk
+    n3 = min(a.n, 192)
+    s = solver(configs.ot_3d(n=n3, nb=32, precision="fp32"), "orszag_tang", "tasks")
+    _evolve_timed(s, stream, nsteps=2)
+    ms, upd, steps, _ = _evolve_timed(s, stream, nsteps=max(3, a.steps // 4))
+    divb = s.export("divb")
+    out["orszag_tang_3d_ct_fp32"] = {
+        "cell_updates_per_s": upd / (ms / 1e3), "steps": steps, "ms_per_step": ms / steps,
+        "max_abs_divb": float(abs(s.interior(divb)).max()),
+        "config": f"{n3}^3 in 32^3 blocks, g=4, CT, PPM(MC)+HLL, RK2, CFL 0.3, per-task kernels"}
+    s.close()
+    # c4: blast on an adaptive mesh, 128^2 base in 16^2 blocks, 3 levels, Loehner on density
+    s = solver(configs.blast_2d_amr(), "blast", "tasks")
+    ms, upd, steps, nbs = _evolve_timed(s, stream, tlim=0.2)
+    out["blast_2d_amr_fp64"] = {
+        "cell_updates_per_s": upd / (ms / 1e3), "steps": steps, "seconds": ms / 1e3,
+        "blocks_min_max": [min(nbs), max(nbs)], "blocks_final": s.nblocks,
+        "config": "128^2 base in 16^2 blocks, 3 levels, Loehner dens 0.3/0.05, PLM(MC)+HLLC, RK2, t=0.2"}
+    s.close()
+    return out
 
 
 def main_reference(a):
@@ -431,6 +507,17 @@ def main():
         "l1_density_fp32_vs_fp64": l1,
         "sim_time_fp32_fp64": [t32, t64],
     }
+    if not a.no_workloads:
+        line["workloads"] = wl = workloads_block(a, device, stream)
+        if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+            # the oracle on bounded samples of the same workloads (all host threads)
+            for key, args_ in (("vortex_2d_fp64", dict(workload="vortex_2d", sample_n=128, nb=64, steps=200)),
+                               ("orszag_tang_3d_ct_fp32", dict(workload="ot_3d", sample_n=64, nb=32, steps=1)),
+                               ("blast_2d_amr_fp64", dict(workload="blast_2d_amr", sample_n=128, nb=16,
+                                                          steps=100, warmup=0))):
+                cb = cpu_baseline(min_seconds=0.0, max_steps=args_["steps"], **args_)
+                wl[key]["cpu_sample"] = {"value": cb.get("value"), "cores": cb.get("threads"),
+                                         "sample": cb.get("sample"), "kind": "port"}
     if a.serve > 0:
         line["serving"] = serving_block(a, device)
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
