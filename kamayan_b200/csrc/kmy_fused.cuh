@@ -44,9 +44,27 @@ struct FusedShape {
       cmax(faces(0), cmax(NDIM > 1 ? faces(1) : 0, NDIM > 2 ? faces(2) : 0));
   static constexpr int NR = 7;
   static constexpr int NC = 5;
+  // local coordinates per axis the brick's stencils touch
+  static constexpr int TAB = cmax(B[0], cmax(B[1], B[2])) + 2 * H;
+  // cells reconstructed per direction in the two-sided sweep: -1 .. B along d
+  static constexpr int rcells(int d) { return (B[d] + 2) * (NCELL / B[d]); }
+  static constexpr int RC_MAX = cmax(rcells(0), cmax(NDIM > 1 ? rcells(1) : 0, NDIM > 2 ? rcells(2) : 0));
+  // The FP32 stage reconstructs each cell once (both faces, shared smoothness
+  // indicators) into shared memory and solves the Riemann problems from
+  // there; the FP64 stage reconstructs per face in registers, which keeps
+  // its shared memory at two CTAs per SM.
+  template <typename S>
+  static constexpr bool two_sided() {
+    return sizeof(S) == 4;
+  }
   template <typename S>
   static constexpr size_t smem_bytes() {
-    return sizeof(S) * (size_t(NR) * REG_MAX + size_t(NC) * FACE_MAX);
+    if constexpr (two_sided<S>()) {
+      // primitive tile (face fluxes reuse it) + both reconstructed states
+      return sizeof(S) * (size_t(NR) * REG_MAX + size_t(2 * NR) * RC_MAX);
+    } else {
+      return sizeof(S) * (size_t(NR) * REG_MAX + size_t(NC) * FACE_MAX);
+    }
   }
 };
 
@@ -86,26 +104,46 @@ __device__ __forceinline__ int fz_map(int G, int N, int bc, bool &flip) {
   return M < 0 ? 0 : (M >= N ? N - 1 : M);
 }
 
-// Load the primitive state of block-interior cell (l0,l1,l2) of block at
-// logical location lx (coordinates may lie up to H cells outside the block).
-template <typename S>
-__device__ __forceinline__ void fz_load_prim(const FusedArgs<S> &a, const int lx[3], int l0, int l1,
-                                             int l2, S *V) {
+// Per-brick address tables.  The element offset of a mesh cell separates by
+// axis: n = sum_d (owner_block_d * blocks_below_d * P + local_d * stride_d).
+// For each axis and each local coordinate the brick can touch (o - H ..
+// o + B + H - 1) the table holds that axis's share of n and whether the
+// boundary map mirrored it (reflect), so staging a cell costs three shared
+// loads instead of a boundary map and an integer division per axis.
+template <int NDIM, int RECON>
+struct FzTables {
+  static constexpr int TAB = FusedShape<NDIM, RECON>::TAB;
+  long long off[3][TAB];
+  unsigned char flip[3][TAB];
+};
+
+template <typename S, int NDIM, int RECON>
+__device__ __forceinline__ void fz_fill_tables(const FusedArgs<S> &a, const int lx[3], const int o[3],
+                                               FzTables<NDIM, RECON> &t) {
+  using Sh = FusedShape<NDIM, RECON>;
+  constexpr int H = Sh::H;
   const MeshDesc &m = a.m;
-  const int l[3] = {l0, l1, l2};
-  int sb = 0, mult = 1, loc[3];
-  bool flip[3] = {false, false, false};
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const int G = lx[d] * m.nx[d] + l[d];
-    const int M = fz_map(G, m.mesh_nx[d], m.bc[d][G < 0 ? 0 : 1], flip[d]);
+  const int n0 = Sh::B[0] + 2 * H, n1 = Sh::B[1] + 2 * H, n2 = Sh::B[2] + 2 * H;
+  for (int q = threadIdx.x; q < n0 + n1 + n2; q += Sh::NT) {
+    const int d = q < n0 ? 0 : (q < n0 + n1 ? 1 : 2);
+    const int i = q - (d == 0 ? 0 : d == 1 ? n0 : n0 + n1);
+    const int l = o[d] + i - H;
+    bool f = false;
+    const int G = lx[d] * m.nx[d] + l;
+    const int M = fz_map(G, m.mesh_nx[d], m.bc[d][G < 0 ? 0 : 1], f);
     const int ob = M / m.nx[d];
-    sb += ob * mult;
-    mult *= m.nbx[d];
-    loc[d] = M - ob * m.nx[d] + m.g[d];
+    const long long below = d == 0 ? 1 : d == 1 ? m.nbx[0] : (long long)m.nbx[0] * m.nbx[1];
+    const long long stride = d == 0 ? 1 : d == 1 ? m.np[0] : (long long)m.np[0] * m.np[1];
+    t.off[d][i] = ob * below * m.P + (long long)(M - ob * m.nx[d] + m.g[d]) * stride;
+    t.flip[d][i] = f;
   }
+}
+
+// Primitive state of the mesh cell at element offset n (flips: mirrored axes).
+template <typename S>
+__device__ __forceinline__ void fz_load_prim(const FusedArgs<S> &a, long long n, const bool flip[3], S *V) {
+  const MeshDesc &m = a.m;
   const long long NP = (long long)m.nb * m.P;
-  const long long n = (long long)sb * m.P + ((long long)loc[2] * m.np[1] + loc[1]) * m.np[0] + loc[0];
   const S dens = a.u0[n];
   if (a.stored) {
     V[RDENS] = dens;
@@ -130,30 +168,75 @@ __device__ __forceinline__ void fz_load_prim(const FusedArgs<S> &a, const int lx
   }
 }
 
+// 1. Primitives of the brick extended by H cells along DIR, into sp.
+template <typename S, int NDIM, int RECON, int DIR>
+__device__ __forceinline__ void fz_stage_prims(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &t, S *sp) {
+  using Sh = FusedShape<NDIM, RECON>;
+  constexpr int H = Sh::H;
+  constexpr int E0 = Sh::B[0] + (DIR == 0 ? 2 * H : 0);
+  constexpr int E1 = Sh::B[1] + (DIR == 1 ? 2 * H : 0);
+  constexpr int E2 = Sh::B[2] + (DIR == 2 ? 2 * H : 0);
+  constexpr int NREG = E0 * E1 * E2;
+  constexpr int RM = Sh::REG_MAX;
+  for (int q = threadIdx.x; q < NREG; q += Sh::NT) {
+    // table index: region coordinate along DIR, brick coordinate + H across
+    const int t0 = q % E0 + (DIR == 0 ? 0 : H);
+    const int t1 = (q / E0) % E1 + (DIR == 1 ? 0 : H);
+    const int t2 = q / (E0 * E1) + (DIR == 2 ? 0 : H);
+    const bool flip[3] = {t.flip[0][t0] != 0, t.flip[1][t1] != 0, t.flip[2][t2] != 0};
+    S V[7];
+    fz_load_prim<S>(a, t.off[0][t0] + t.off[1][t1] + t.off[2][t2], flip, V);
+#pragma unroll
+    for (int r = 0; r < 7; r++) sp[r * RM + q] = V[r];
+  }
+}
+
+// Last step of a direction: the divergence contribution of the DIR faces in sf
+// to the owned cells' accumulators.
+template <typename S, int NDIM, int RECON, int DIR>
+__device__ __forceinline__ void fz_accumulate(const FusedArgs<S> &a, const S *sf,
+                                              S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
+  using Sh = FusedShape<NDIM, RECON>;
+  constexpr int B0 = Sh::B[0], B1 = Sh::B[1];
+  constexpr int FM = Sh::template two_sided<S>() ? Sh::NR * Sh::REG_MAX / Sh::NC : Sh::FACE_MAX;
+  const S A = S(a.m.area[DIR]);
+#pragma unroll
+  for (int s = 0; s < Sh::CPT; s++) {
+    const int c = threadIdx.x + s * Sh::NT;
+    if (c < Sh::NCELL) {
+      const int x = c % B0, y = (c / B0) % B1, z = c / (B0 * B1);
+      int lo, hi;
+      if (DIR == 0) {
+        lo = x + (B0 + 1) * (y + B1 * z);
+        hi = lo + 1;
+      } else if (DIR == 1) {
+        lo = x + B0 * (y + (B1 + 1) * z);
+        hi = lo + B0;
+      } else {
+        lo = x + B0 * (y + B1 * z);
+        hi = lo + B0 * B1;
+      }
+#pragma unroll
+      for (int v = 0; v < 5; v++) du[s][v] -= (A * sf[v * FM + hi] - A * sf[v * FM + lo]);
+    }
+  }
+}
+
+// One direction, per-face reconstruction (FP64): both one-sided
+// reconstructions of every face are evaluated in registers from the staged
+// primitives, then the Riemann flux goes to sf.
 template <typename S, int NDIM, int RECON, int RIEMANN, int DIR>
-__device__ __forceinline__ void fz_direction(const FusedArgs<S> &a, const int lx[3], const int o[3],
+__device__ __forceinline__ void fz_direction(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &tb,
                                              S *sp, S *sf, S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
   using Sh = FusedShape<NDIM, RECON>;
   constexpr int H = Sh::H, W = Sh::W;
   constexpr int B0 = Sh::B[0], B1 = Sh::B[1], B2 = Sh::B[2];
   constexpr int E0 = B0 + (DIR == 0 ? 2 * H : 0);
   constexpr int E1 = B1 + (DIR == 1 ? 2 * H : 0);
-  constexpr int E2 = B2 + (DIR == 2 ? 2 * H : 0);
-  constexpr int NREG = E0 * E1 * E2;
   constexpr int RM = Sh::REG_MAX, FM = Sh::FACE_MAX;
   const int tid = threadIdx.x;
 
-  // 1. stage primitives of the direction-extended brick
-  for (int q = tid; q < NREG; q += Sh::NT) {
-    const int x = q % E0, y = (q / E0) % E1, z = q / (E0 * E1);
-    const int l0 = o[0] + x - (DIR == 0 ? H : 0);
-    const int l1 = o[1] + y - (DIR == 1 ? H : 0);
-    const int l2 = o[2] + z - (DIR == 2 ? H : 0);
-    S V[7];
-    fz_load_prim<S>(a, lx, l0, l1, l2, V);
-#pragma unroll
-    for (int r = 0; r < 7; r++) sp[r * RM + q] = V[r];
-  }
+  fz_stage_prims<S, NDIM, RECON, DIR>(a, tb, sp);
   __syncthreads();
 
   // 2. face fluxes of this direction
@@ -188,28 +271,76 @@ __device__ __forceinline__ void fz_direction(const FusedArgs<S> &a, const int lx
   }
   __syncthreads();
 
-  // 3. divergence contribution of this direction for the owned cells
-  const S A = S(a.m.area[DIR]);
+  fz_accumulate<S, NDIM, RECON, DIR>(a, sf, du);
+  __syncthreads();
+}
+
+// One direction, two-sided reconstruction (FP32): every cell from -1 to B
+// along DIR is reconstructed once per primitive (both face values share the
+// smoothness indicators and weights), one (primitive, cell) pair per thread
+// so the CTA's threads stay busy; the Riemann solver then reads the two
+// states of each face from shared memory.  Face fluxes reuse the primitive
+// tile's storage.
+template <typename S, int NDIM, int RECON, int RIEMANN, int DIR>
+__device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &tb,
+                                              S *sp, S *rm, S *rp, S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
+  using Sh = FusedShape<NDIM, RECON>;
+  constexpr int H = Sh::H, W = Sh::W;
+  constexpr int B0 = Sh::B[0], B1 = Sh::B[1], B2 = Sh::B[2];
+  constexpr int E0 = B0 + (DIR == 0 ? 2 * H : 0);
+  constexpr int E1 = B1 + (DIR == 1 ? 2 * H : 0);
+  constexpr int RM = Sh::REG_MAX, RC = Sh::RC_MAX;
+  constexpr int FM = Sh::NR * Sh::REG_MAX / Sh::NC;  // face-flux stride inside the primitive tile
+  static_assert(Sh::FACE_MAX <= FM, "face fluxes must fit in the primitive tile");
+  constexpr int ST = DIR == 0 ? 1 : DIR == 1 ? E0 : E0 * E1;  // region stride along DIR
+  // reconstruction grid: B+2 cells along DIR (positions -1 .. B), the brick across
+  constexpr int R0 = B0 + (DIR == 0 ? 2 : 0), R1 = B1 + (DIR == 1 ? 2 : 0), R2 = B2 + (DIR == 2 ? 2 : 0);
+  constexpr int NRC = R0 * R1 * R2;
+  constexpr int RST = DIR == 0 ? 1 : DIR == 1 ? R0 : R0 * R1;  // reconstruction-grid stride along DIR
+  const int tid = threadIdx.x;
+
+  fz_stage_prims<S, NDIM, RECON, DIR>(a, tb, sp);
+  __syncthreads();
+
+  // 2. both face values of every (primitive, cell)
+  for (int it = tid; it < Sh::NR * NRC; it += Sh::NT) {
+    const int r = it / NRC, q = it - r * NRC;
+    const int x = q % R0, y = (q / R0) % R1, z = q / (R0 * R1);
+    // region coordinate: position p = x - 1 along DIR sits at p + H
+    const int ex = x + (DIR == 0 ? H - 1 : 0), ey = y + (DIR == 1 ? H - 1 : 0), ez = z + (DIR == 2 ? H - 1 : 0);
+    const S *c = sp + r * RM + ex + E0 * (ey + E1 * ez);
+    S s[5];
 #pragma unroll
-  for (int s = 0; s < Sh::CPT; s++) {
-    const int c = tid + s * Sh::NT;
-    if (c < Sh::NCELL) {
-      const int x = c % B0, y = (c / B0) % B1, z = c / (B0 * B1);
-      int lo, hi;
-      if (DIR == 0) {
-        lo = x + (B0 + 1) * (y + B1 * z);
-        hi = lo + 1;
-      } else if (DIR == 1) {
-        lo = x + B0 * (y + (B1 + 1) * z);
-        hi = lo + B0;
-      } else {
-        lo = x + B0 * (y + B1 * z);
-        hi = lo + B0 * B1;
-      }
-#pragma unroll
-      for (int v = 0; v < 5; v++) du[s][v] -= (A * sf[v * FM + hi] - A * sf[v * FM + lo]);
-    }
+    for (int k = 0; k < 5; k++) s[k] = (k - 2 >= -W && k - 2 <= W) ? c[(k - 2) * ST] : S(0);
+    S vm, vp;
+    Reconstruct<RECON, S>(a.limiter, s, vm, vp);
+    rm[r * RC + q] = vm;
+    rp[r * RC + q] = vp;
   }
+  __syncthreads();
+
+  // 3. Riemann flux at every DIR face of the brick; the face at position f
+  // joins reconstruction cells f (its low cell, position f-1) and f+1
+  constexpr int NFACE = (DIR == 0 ? B0 + 1 : B0) * (DIR == 1 ? B1 + 1 : B1) * (DIR == 2 ? B2 + 1 : B2);
+  constexpr int F0 = DIR == 0 ? B0 + 1 : B0, F1 = DIR == 1 ? B1 + 1 : B1;
+  S *sf = sp;
+  for (int it = tid; it < NFACE; it += Sh::NT) {
+    const int x = it % F0, y = (it / F0) % F1, z = it / (F0 * F1);
+    const int lq = x + R0 * (y + R1 * z);
+    S vL[7], vR[7];
+#pragma unroll
+    for (int r = 0; r < 7; r++) {
+      vL[r] = rp[r * RC + lq];
+      vR[r] = rm[r * RC + lq + RST];
+    }
+    S F[5];
+    RiemannFlux<RIEMANN, false, DIR, S>(vL, vR, F);
+#pragma unroll
+    for (int v = 0; v < 5; v++) sf[v * FM + it] = F[v];
+  }
+  __syncthreads();
+
+  fz_accumulate<S, NDIM, RECON, DIR>(a, sf, du);
   __syncthreads();
 }
 
@@ -233,9 +364,20 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
 #pragma unroll
     for (int v = 0; v < 5; v++) du[s][v] = S(0);
 
-  fz_direction<S, NDIM, RECON, RIEMANN, 0>(a, lx, o, sp, sf, du);
-  if constexpr (NDIM > 1) fz_direction<S, NDIM, RECON, RIEMANN, 1>(a, lx, o, sp, sf, du);
-  if constexpr (NDIM > 2) fz_direction<S, NDIM, RECON, RIEMANN, 2>(a, lx, o, sp, sf, du);
+  __shared__ FzTables<NDIM, RECON> tb;
+  fz_fill_tables<S, NDIM, RECON>(a, lx, o, tb);
+  __syncthreads();
+  if constexpr (Sh::template two_sided<S>()) {
+    S *rm = sp + Sh::NR * Sh::REG_MAX;
+    S *rp = rm + Sh::NR * Sh::RC_MAX;
+    fz_direction2<S, NDIM, RECON, RIEMANN, 0>(a, tb, sp, rm, rp, du);
+    if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1>(a, tb, sp, rm, rp, du);
+    if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2>(a, tb, sp, rm, rp, du);
+  } else {
+    fz_direction<S, NDIM, RECON, RIEMANN, 0>(a, tb, sp, sf, du);
+    if constexpr (NDIM > 1) fz_direction<S, NDIM, RECON, RIEMANN, 1>(a, tb, sp, sf, du);
+    if constexpr (NDIM > 2) fz_direction<S, NDIM, RECON, RIEMANN, 2>(a, tb, sp, sf, du);
+  }
 
   // epilogue: low-storage update of the owned interior cells
   const long long NP = (long long)m.nb * m.P;
