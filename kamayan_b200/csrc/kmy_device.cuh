@@ -133,6 +133,36 @@ __device__ __forceinline__ void Reconstruct(int limiter, const R (&s)[5], R &vM,
   }
 }
 
+// Both face values for the FP32 fused stage.  WENO-Z folds the 1/6 of the
+// three candidate stencils into the normalisation (one multiply per face
+// value instead of six); the weights and smoothness indicators are the
+// reference's.  Other reconstructions are Reconstruct itself.
+template <int RECON, typename R>
+__device__ __forceinline__ void ReconstructBoth(int limiter, const R (&s)[5], R &vM, R &vP) {
+  if constexpr (RECON == WENOZ) {
+    const R s0 = s[2];
+    const R ep0 = -s[4] + R(5) * s[3] + R(2) * s0;
+    const R ep1 = R(2) * s[3] + R(5) * s0 - s[1];
+    const R ep2 = R(11) * s0 - R(7) * s[1] + R(2) * s[0];
+    const R em0 = -s[0] + R(5) * s[1] + R(2) * s0;
+    const R em1 = R(2) * s[1] + R(5) * s0 - s[3];
+    const R em2 = R(11) * s0 - R(7) * s[3] + R(2) * s[4];
+    const R c1312 = R(13.) / R(12.);
+    const R b0 = c1312 * sq(s[0] - R(2) * s[1] + s0) + R(0.25) * sq(s[0] - R(4) * s[1] + R(3) * s0);
+    const R b1 = c1312 * sq(s[1] - R(2) * s0 + s[3]) + R(0.25) * sq(s[1] - s[3]);
+    const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
+    const R tau = fabs(b2 - b0);
+    const R q0 = weno_q(tau, b0);
+    const R q1 = weno_q(tau, b1);
+    const R q2 = weno_q(tau, b2);
+    const R t0 = R(3) * q0, t1 = R(6) * q1, t2 = R(3) * q2;
+    vM = (t0 * em0 + t1 * em1 + q2 * em2) / (R(6) * (t0 + t1 + q2));
+    vP = (t2 * ep0 + t1 * ep1 + q0 * ep2) / (R(6) * (t2 + t1 + q0));
+  } else {
+    Reconstruct<RECON, R>(limiter, s, vM, vP);
+  }
+}
+
 // Value at the plus face only (for the cell left of a face).
 template <int RECON, typename R>
 __device__ __forceinline__ R ReconstructPlus(int limiter, const R (&s)[5]) {

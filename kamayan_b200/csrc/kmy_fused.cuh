@@ -313,7 +313,7 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
 #pragma unroll
     for (int k = 0; k < 5; k++) s[k] = (k - 2 >= -W && k - 2 <= W) ? c[(k - 2) * ST] : S(0);
     S vm, vp;
-    Reconstruct<RECON, S>(a.limiter, s, vm, vp);
+    ReconstructBoth<RECON, S>(a.limiter, s, vm, vp);
     rm[r * RC + q] = vm;
     rp[r * RC + q] = vp;
   }
@@ -445,7 +445,7 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
 
 // One stage of one mesh: one CTA per brick.
 template <typename S, int NDIM, int RECON, int RIEMANN>
-__global__ void __launch_bounds__(256) k_fused_stage(FusedArgs<S> a) {
+__global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT) k_fused_stage(FusedArgs<S> a) {
   if (a.clock->done) return;
   const int nbrick = a.nbr[0] * a.nbr[1] * a.nbr[2];
   const int b = blockIdx.x / nbrick;
@@ -499,7 +499,7 @@ __device__ __forceinline__ void batch_args(const SolveDesc<S> &q, int stage, Fus
 }
 
 template <typename S, int NDIM, int RECON, int RIEMANN>
-__global__ void __launch_bounds__(256) k_fused_batch(const SolveDesc<S> *__restrict__ d,
+__global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT) k_fused_batch(const SolveDesc<S> *__restrict__ d,
                                                      const long long *__restrict__ prefix,
                                                      const int *nsolves_dev, int stage) {
   __shared__ FusedArgs<S> sa;
