@@ -49,22 +49,25 @@ struct FusedShape {
   // cells reconstructed per direction in the two-sided sweep: -1 .. B along d
   static constexpr int rcells(int d) { return (B[d] + 2) * (NCELL / B[d]); }
   static constexpr int RC_MAX = cmax(rcells(0), cmax(NDIM > 1 ? rcells(1) : 0, NDIM > 2 ? rcells(2) : 0));
-  // The FP32 stage reconstructs each cell once (both faces, shared smoothness
-  // indicators) into shared memory and solves the Riemann problems from
-  // there; the FP64 stage reconstructs per face in registers, which keeps
-  // its shared memory at two CTAs per SM.
+  // Each cell is reconstructed once (both faces, shared smoothness
+  // indicators) into shared memory and the Riemann problems read from there.
+  // In 3D FP64 the transverse plane goes through in two chunks, which keeps
+  // the reconstruction buffers small enough for two CTAs per SM.
   template <typename S>
-  static constexpr bool two_sided() {
-    return sizeof(S) == 4;
+  static constexpr int nchunk() {
+    return (sizeof(S) == 8 && NDIM == 3) ? 2 : 1;
+  }
+  // Face fluxes reuse the primitive tile with one chunk; with several they
+  // need their own buffer (the tile is still being read).
+  template <typename S>
+  static constexpr int face_stride() {
+    return nchunk<S>() == 1 ? NR * REG_MAX / NC : FACE_MAX;
   }
   template <typename S>
   static constexpr size_t smem_bytes() {
-    if constexpr (two_sided<S>()) {
-      // primitive tile (face fluxes reuse it) + both reconstructed states
-      return sizeof(S) * (size_t(NR) * REG_MAX + size_t(2 * NR) * RC_MAX);
-    } else {
-      return sizeof(S) * (size_t(NR) * REG_MAX + size_t(NC) * FACE_MAX);
-    }
+    const size_t rec = size_t(2 * NR) * (RC_MAX / nchunk<S>());
+    const size_t flux = nchunk<S>() == 1 ? 0 : size_t(NC) * FACE_MAX;
+    return sizeof(S) * (size_t(NR) * REG_MAX + rec + flux);
   }
 };
 
@@ -198,7 +201,7 @@ __device__ __forceinline__ void fz_accumulate(const FusedArgs<S> &a, const S *sf
                                               S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
   using Sh = FusedShape<NDIM, RECON>;
   constexpr int B0 = Sh::B[0], B1 = Sh::B[1];
-  constexpr int FM = Sh::template two_sided<S>() ? Sh::NR * Sh::REG_MAX / Sh::NC : Sh::FACE_MAX;
+  constexpr int FM = Sh::template face_stride<S>();
   const S A = S(a.m.area[DIR]);
 #pragma unroll
   for (int s = 0; s < Sh::CPT; s++) {
@@ -222,123 +225,91 @@ __device__ __forceinline__ void fz_accumulate(const FusedArgs<S> &a, const S *sf
   }
 }
 
-// One direction, per-face reconstruction (FP64): both one-sided
-// reconstructions of every face are evaluated in registers from the staged
-// primitives, then the Riemann flux goes to sf.
-template <typename S, int NDIM, int RECON, int RIEMANN, int DIR>
-__device__ __forceinline__ void fz_direction(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &tb,
-                                             S *sp, S *sf, S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
-  using Sh = FusedShape<NDIM, RECON>;
-  constexpr int H = Sh::H, W = Sh::W;
-  constexpr int B0 = Sh::B[0], B1 = Sh::B[1], B2 = Sh::B[2];
-  constexpr int E0 = B0 + (DIR == 0 ? 2 * H : 0);
-  constexpr int E1 = B1 + (DIR == 1 ? 2 * H : 0);
-  constexpr int RM = Sh::REG_MAX, FM = Sh::FACE_MAX;
-  const int tid = threadIdx.x;
-
-  fz_stage_prims<S, NDIM, RECON, DIR>(a, tb, sp);
-  __syncthreads();
-
-  // 2. face fluxes of this direction
-  constexpr int NFACE = (DIR == 0 ? B0 + 1 : B0) * (DIR == 1 ? B1 + 1 : B1) * (DIR == 2 ? B2 + 1 : B2);
-  constexpr int F0 = DIR == 0 ? B0 + 1 : B0, F1 = DIR == 1 ? B1 + 1 : B1;
-  constexpr int ST = DIR == 0 ? 1 : DIR == 1 ? E0 : E0 * E1;  // region stride along DIR
-  for (int it = tid; it < NFACE; it += Sh::NT) {
-    const int x = it % F0, y = (it / F0) % F1, z = it / (F0 * F1);
-    // region coordinate of the face's high cell
-    const int hx = x + (DIR == 0 ? H : 0), hy = y + (DIR == 1 ? H : 0), hz = z + (DIR == 2 ? H : 0);
-    const int hq = hx + E0 * (hy + E1 * hz);
-    S vL[7], vR[7];
-#pragma unroll
-    for (int r = 0; r < 7; r++) {
-      S line[2 * W + 2];
-#pragma unroll
-      for (int q = 0; q < 2 * W + 2; q++) line[q] = sp[r * RM + hq + (q - 1 - W) * ST];
-      S sl[5], sr[5];
-#pragma unroll
-      for (int q = 0; q < 5; q++) {
-        const int ol = q - 2 + W, orr = q - 1 + W;
-        sl[q] = (ol >= 0 && ol < 2 * W + 2) ? line[ol] : S(0);
-        sr[q] = (orr >= 0 && orr < 2 * W + 2) ? line[orr] : S(0);
-      }
-      vL[r] = ReconstructPlus<RECON, S>(a.limiter, sl);
-      vR[r] = ReconstructMinus<RECON, S>(a.limiter, sr);
-    }
-    S F[5];
-    RiemannFlux<RIEMANN, false, DIR, S>(vL, vR, F);
-#pragma unroll
-    for (int v = 0; v < 5; v++) sf[v * FM + it] = F[v];
-  }
-  __syncthreads();
-
-  fz_accumulate<S, NDIM, RECON, DIR>(a, sf, du);
-  __syncthreads();
-}
-
-// One direction, two-sided reconstruction (FP32): every cell from -1 to B
-// along DIR is reconstructed once per primitive (both face values share the
-// smoothness indicators and weights), one (primitive, cell) pair per thread
-// so the CTA's threads stay busy; the Riemann solver then reads the two
-// states of each face from shared memory.  Face fluxes reuse the primitive
-// tile's storage.
+// One direction, two-sided reconstruction: every cell from -1 to B along DIR
+// is reconstructed once per primitive (both face values share the smoothness
+// indicators and weights), one (primitive, cell) pair per thread so the
+// CTA's threads stay busy; the Riemann solver then reads the two states of
+// each face from shared memory.  The FP64 stage works through the
+// transverse plane in NCH chunks so its reconstruction buffers stay small
+// enough for two CTAs per SM; in FP32 one chunk covers the plane and the
+// face fluxes reuse the primitive tile's storage.
 template <typename S, int NDIM, int RECON, int RIEMANN, int DIR>
 __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &tb,
-                                              S *sp, S *rm, S *rp, S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
+                                              S *sp, S *rm, S *rp, S *sf,
+                                              S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
   using Sh = FusedShape<NDIM, RECON>;
   constexpr int H = Sh::H, W = Sh::W;
   constexpr int B0 = Sh::B[0], B1 = Sh::B[1], B2 = Sh::B[2];
   constexpr int E0 = B0 + (DIR == 0 ? 2 * H : 0);
   constexpr int E1 = B1 + (DIR == 1 ? 2 * H : 0);
-  constexpr int RM = Sh::REG_MAX, RC = Sh::RC_MAX;
-  constexpr int FM = Sh::NR * Sh::REG_MAX / Sh::NC;  // face-flux stride inside the primitive tile
-  static_assert(Sh::FACE_MAX <= FM, "face fluxes must fit in the primitive tile");
+  constexpr int RM = Sh::REG_MAX;
+  constexpr int NCH = Sh::template nchunk<S>();
+  constexpr int RC = Sh::RC_MAX / NCH;
+  constexpr int FM = Sh::template face_stride<S>();
   constexpr int ST = DIR == 0 ? 1 : DIR == 1 ? E0 : E0 * E1;  // region stride along DIR
-  // reconstruction grid: B+2 cells along DIR (positions -1 .. B), the brick across
-  constexpr int R0 = B0 + (DIR == 0 ? 2 : 0), R1 = B1 + (DIR == 1 ? 2 : 0), R2 = B2 + (DIR == 2 ? 2 : 0);
-  constexpr int NRC = R0 * R1 * R2;
-  constexpr int RST = DIR == 0 ? 1 : DIR == 1 ? R0 : R0 * R1;  // reconstruction-grid stride along DIR
+  // the transverse axis split into chunks
+  constexpr int CA = DIR == 2 ? 1 : 2;
+  // reconstruction grid of one chunk: B+2 cells along DIR (positions -1 .. B)
+  constexpr int C0 = B0 + (DIR == 0 ? 2 : 0);
+  constexpr int C1 = (B1 + (DIR == 1 ? 2 : 0)) / (CA == 1 ? NCH : 1);
+  constexpr int C2 = (B2 + (DIR == 2 ? 2 : 0)) / (CA == 2 ? NCH : 1);
+  constexpr int NRC = C0 * C1 * C2;
+  static_assert(NRC <= RC, "chunk exceeds the reconstruction buffers");
+  static_assert(NCH == 1 || ((CA == 1 ? B1 : B2) % NCH == 0 && DIR != CA), "chunks must split a transverse axis");
+  constexpr int RST = DIR == 0 ? 1 : DIR == 1 ? C0 : C0 * C1;  // chunk-grid stride along DIR
+  // faces: B+1 along DIR; of one chunk and of the whole brick
+  constexpr int F0 = DIR == 0 ? B0 + 1 : B0, F1 = DIR == 1 ? B1 + 1 : B1;
+  constexpr int G0 = F0, G1 = CA == 1 ? F1 / NCH : F1;
+  constexpr int G2 = (DIR == 2 ? B2 + 1 : B2) / (CA == 2 ? NCH : 1);
+  constexpr int NFC = G0 * G1 * G2;
   const int tid = threadIdx.x;
 
   fz_stage_prims<S, NDIM, RECON, DIR>(a, tb, sp);
   __syncthreads();
 
-  // 2. both face values of every (primitive, cell)
-  for (int it = tid; it < Sh::NR * NRC; it += Sh::NT) {
-    const int r = it / NRC, q = it - r * NRC;
-    const int x = q % R0, y = (q / R0) % R1, z = q / (R0 * R1);
-    // region coordinate: position p = x - 1 along DIR sits at p + H
-    const int ex = x + (DIR == 0 ? H - 1 : 0), ey = y + (DIR == 1 ? H - 1 : 0), ez = z + (DIR == 2 ? H - 1 : 0);
-    const S *c = sp + r * RM + ex + E0 * (ey + E1 * ez);
-    S s[5];
+#pragma unroll 1
+  for (int ch = 0; ch < NCH; ch++) {
+    const int c1 = CA == 1 ? ch * C1 : 0, c2 = CA == 2 ? ch * C2 : 0;
+    // 2. both face values of every (primitive, cell) of the chunk
+    for (int it = tid; it < Sh::NR * NRC; it += Sh::NT) {
+      const int r = it / NRC, q = it - r * NRC;
+      const int x = q % C0, y = (q / C0) % C1 + c1, z = q / (C0 * C1) + c2;
+      // region coordinate: position p = x - 1 along DIR sits at p + H
+      const int ex = x + (DIR == 0 ? H - 1 : 0), ey = y + (DIR == 1 ? H - 1 : 0), ez = z + (DIR == 2 ? H - 1 : 0);
+      const S *c = sp + r * RM + ex + E0 * (ey + E1 * ez);
+      S s[5];
 #pragma unroll
-    for (int k = 0; k < 5; k++) s[k] = (k - 2 >= -W && k - 2 <= W) ? c[(k - 2) * ST] : S(0);
-    S vm, vp;
-    ReconstructBoth<RECON, S>(a.limiter, s, vm, vp);
-    rm[r * RC + q] = vm;
-    rp[r * RC + q] = vp;
-  }
-  __syncthreads();
-
-  // 3. Riemann flux at every DIR face of the brick; the face at position f
-  // joins reconstruction cells f (its low cell, position f-1) and f+1
-  constexpr int NFACE = (DIR == 0 ? B0 + 1 : B0) * (DIR == 1 ? B1 + 1 : B1) * (DIR == 2 ? B2 + 1 : B2);
-  constexpr int F0 = DIR == 0 ? B0 + 1 : B0, F1 = DIR == 1 ? B1 + 1 : B1;
-  S *sf = sp;
-  for (int it = tid; it < NFACE; it += Sh::NT) {
-    const int x = it % F0, y = (it / F0) % F1, z = it / (F0 * F1);
-    const int lq = x + R0 * (y + R1 * z);
-    S vL[7], vR[7];
-#pragma unroll
-    for (int r = 0; r < 7; r++) {
-      vL[r] = rp[r * RC + lq];
-      vR[r] = rm[r * RC + lq + RST];
+      for (int k = 0; k < 5; k++) s[k] = (k - 2 >= -W && k - 2 <= W) ? c[(k - 2) * ST] : S(0);
+      S vm, vp;
+      if constexpr (sizeof(S) == 4) {
+        ReconstructBoth<RECON, S>(a.limiter, s, vm, vp);
+      } else {
+        Reconstruct<RECON, S>(a.limiter, s, vm, vp);
+      }
+      rm[r * RC + q] = vm;
+      rp[r * RC + q] = vp;
     }
-    S F[5];
-    RiemannFlux<RIEMANN, false, DIR, S>(vL, vR, F);
+    __syncthreads();
+
+    // 3. Riemann flux at the chunk's DIR faces; the face at position f joins
+    // reconstruction cells f (its low cell, position f-1) and f+1
+    for (int it = tid; it < NFC; it += Sh::NT) {
+      const int x = it % G0, y = (it / G0) % G1, z = it / (G0 * G1);
+      const int lq = x + C0 * (y + C1 * z);
+      S vL[7], vR[7];
 #pragma unroll
-    for (int v = 0; v < 5; v++) sf[v * FM + it] = F[v];
+      for (int r = 0; r < 7; r++) {
+        vL[r] = rp[r * RC + lq];
+        vR[r] = rm[r * RC + lq + RST];
+      }
+      S F[5];
+      RiemannFlux<RIEMANN, false, DIR, S>(vL, vR, F);
+      const int gf = x + F0 * ((y + c1) + F1 * (z + c2));
+#pragma unroll
+      for (int v = 0; v < 5; v++) sf[v * FM + gf] = F[v];
+    }
+    __syncthreads();
   }
-  __syncthreads();
 
   fz_accumulate<S, NDIM, RECON, DIR>(a, sf, du);
   __syncthreads();
@@ -351,7 +322,6 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
   using Sh = FusedShape<NDIM, RECON>;
   extern __shared__ __align__(16) unsigned char kmy_smem[];
   S *sp = reinterpret_cast<S *>(kmy_smem);
-  S *sf = sp + Sh::NR * Sh::REG_MAX;
 
   const MeshDesc &m = a.m;
   const int o[3] = {(br % a.nbr[0]) * Sh::B[0], ((br / a.nbr[0]) % a.nbr[1]) * Sh::B[1],
@@ -367,17 +337,13 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
   __shared__ FzTables<NDIM, RECON> tb;
   fz_fill_tables<S, NDIM, RECON>(a, lx, o, tb);
   __syncthreads();
-  if constexpr (Sh::template two_sided<S>()) {
-    S *rm = sp + Sh::NR * Sh::REG_MAX;
-    S *rp = rm + Sh::NR * Sh::RC_MAX;
-    fz_direction2<S, NDIM, RECON, RIEMANN, 0>(a, tb, sp, rm, rp, du);
-    if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1>(a, tb, sp, rm, rp, du);
-    if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2>(a, tb, sp, rm, rp, du);
-  } else {
-    fz_direction<S, NDIM, RECON, RIEMANN, 0>(a, tb, sp, sf, du);
-    if constexpr (NDIM > 1) fz_direction<S, NDIM, RECON, RIEMANN, 1>(a, tb, sp, sf, du);
-    if constexpr (NDIM > 2) fz_direction<S, NDIM, RECON, RIEMANN, 2>(a, tb, sp, sf, du);
-  }
+  constexpr int NCH = Sh::template nchunk<S>();
+  S *rm = sp + Sh::NR * Sh::REG_MAX;
+  S *rp = rm + Sh::NR * (Sh::RC_MAX / NCH);
+  S *sf = NCH == 1 ? sp : rp + Sh::NR * (Sh::RC_MAX / NCH);
+  fz_direction2<S, NDIM, RECON, RIEMANN, 0>(a, tb, sp, rm, rp, sf, du);
+  if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1>(a, tb, sp, rm, rp, sf, du);
+  if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2>(a, tb, sp, rm, rp, sf, du);
 
   // epilogue: low-storage update of the owned interior cells
   const long long NP = (long long)m.nb * m.P;
