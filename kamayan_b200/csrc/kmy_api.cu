@@ -139,7 +139,7 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   const int numlevel = p.integer("parthenon/mesh/numlevel", 1);
   if (refine == "static" && numlevel > 1)
     return bad("parthenon/mesh/refinement = static with numlevel > 1 is not supported");
-  // adaptive mesh: a <kamayan/refinement0> block with a field (grid.cpp:229-262)
+  // adaptive mesh: a <kamayan/refinement0> block with a field (grid.cpp:43-48, :90-124)
   AmrHost &amr = c->amr;
   amr.on = refine == "adaptive" && numlevel > 1 && p.deck.count("kamayan/refinement0/field");
   if (amr.on) {
@@ -705,23 +705,32 @@ int kmy_task_stage(kmy_ctx *c, int stage, double dt) {
   return task_stage(c, stage, dt);
 }
 
+// A fused stage stages the primitives of its input from c->prim when they
+// are current (after set-up, an import, the task path or a previous fused
+// stage) and writes those of its output to c->prim_alt; the buffers swap.
 static int fused_stage(kmy_ctx *c, int stage) {
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());
-  const bool stored = stage == 1 && c->prims_valid;
+  // FP32 stages keep their output's primitives (kmy_fused.cu)
+  const bool keep = c->esz == 4;
+  const bool stored = c->prims_valid || c->prims_interior;
+  if (keep && !c->prim_alt && dalloc(c, &c->prim_alt, c->esz * NPRIM * size_t(c->m.nb) * c->m.P))
+    return KMY_ERR_OOM;
+  int rc;
   if (ns == 1) {
     // rk1 updates base in place (stage names base -> base).  The fused stage
     // reads neighbouring bricks' halos while it writes, so it writes a scratch
     // container and the two swap roles afterwards.
     if (!c->md.count("1") && make_container(c, "1")) return KMY_ERR_OOM;
     Container &base = c->md["base"], &out = c->md["1"];
-    int rc = launch_fused_stage(c, base, base, out, c->prm.beta[0], stored, true);
+    rc = launch_fused_stage(c, base, base, out, c->prm.beta[0], stored, true);
     if (!rc) std::swap(c->md["base"], c->md["1"]);
-    c->prims_valid = false;
-    return rc;
+  } else {
+    Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
+    rc = launch_fused_stage(c, base, md0, md1, c->prm.beta[stage - 1], stored, stage == ns);
   }
-  Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
-  int rc = launch_fused_stage(c, base, md0, md1, c->prm.beta[stage - 1], stored, stage == ns);
+  if (!rc && keep) std::swap(c->prim, c->prim_alt);
+  c->prims_interior = !rc && keep;
   c->prims_valid = false;
   return rc;
 }
@@ -745,10 +754,14 @@ int kmy_rk_stage(kmy_ctx *c, int stage, double dt) {
   return fused_stage(c, stage);
 }
 
+// Whole steps go through the fused stage unless the path was set to tasks,
+// the mesh carries CT, or the mesh is adaptive.
+static bool steps_fused(const kmy_ctx *c) { return c->path == 0 && !c->prm.mhd && !c->amr.on; }
+
 static int step_async(kmy_ctx *c) {
   const int ns = int(c->prm.beta.size());
   int rc = KMY_OK;
-  const bool fused = c->path == 0 && !c->prm.mhd && !c->amr.on;
+  const bool fused = steps_fused(c);
   for (int s = 1; s <= ns && !rc; s++) rc = fused ? fused_stage(c, s) : task_stage(c, s, -1.0);
   if (!rc && c->amr.on) rc = amr_after_step(c);
   if (!rc) rc = launch_dt_controller(c, 0);
@@ -780,9 +793,11 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
   int n = 0;
   DevClock h{};
   while (!rc) {
-    // an adaptive mesh reads its tags back every step anyway; stepping one at
-    // a time keeps it from running (and remeshing) past tlim
-    const int chunk = c->amr.on ? 1 : 8;
+    // Fused steps queue ahead in chunks: a step queued after the clock
+    // reached tlim leaves the state unchanged.  The per-task kernels (CT,
+    // adaptive meshes, the tasks path) do not check the clock, so they step
+    // one at a time; an adaptive mesh reads its tags back every step anyway.
+    const int chunk = steps_fused(c) ? 8 : 1;
     for (int i = 0; i < chunk && !rc && (nlim < 0 || n < nlim); i++, n++) rc = step_async(c);
     if (rc) break;
     rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");

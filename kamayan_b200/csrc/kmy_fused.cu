@@ -25,6 +25,10 @@ static FusedArgs<S> fused_args(kmy_ctx *c, Container &base, Container &md0, Cont
   a.u1 = static_cast<S *>(md1.cc);
   a.u1lo = static_cast<float *>(md1.ener_lo);
   a.prim = static_cast<const S *>(c->prim);
+  // FP32 keeps the primitives of each stage's output for the next stage (its
+  // staging then skips the FP64 energy recovery); in FP64 the extra stores
+  // cost more than the conversions they save, so every stage converts.
+  a.prim_out = sizeof(S) == 4 ? static_cast<S *>(c->prim_alt) : nullptr;
   a.stored = stored ? 1 : 0;
   a.last = last ? 1 : 0;
   a.beta = beta;

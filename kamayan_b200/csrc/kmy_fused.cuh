@@ -83,6 +83,7 @@ struct FusedArgs {
   S *u1;
   float *u1lo;
   const S *prim;
+  S *prim_out;  // primitives of u1's interior cells for the next stage (null: not kept)
   int stored;
   int last;
   double beta;
@@ -380,17 +381,27 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
       un[v] = x0 + bt * S(dt) * dudt;
       a.u1[v * NP + n] = un[v];
     }
-    if (a.last) {
+    if (a.last || a.prim_out) {
       double e = double(un[CENER]);
       if constexpr (sizeof(S) == 4) e += double(a.u1lo[n]);
       S V[7];
       Cons2PrimEos<false, S>(a.eos, un[CDENS], un[CMOM0], un[CMOM1], un[CMOM2], e, nullptr, V);
+      if (a.prim_out) {
+        // the next stage stages these instead of converting its input again
 #pragma unroll
-      for (int dir = 0; dir < NDIM; dir++) {
-        const S cf = FastSpeed<false>(dir, V);
-        double xv = double(S(m.dx[dir]) / (fabs(V[RVEL0 + dir]) + cf));
-        if (xv != xv) xv = 0.0;
-        dtl = xv < dtl ? xv : dtl;
+        for (int d = 0; d < 3; d++) a.prim_out[(PVEL0 + d) * NP + n] = V[RVEL0 + d];
+        a.prim_out[PPRES * NP + n] = V[RPRES];
+        a.prim_out[PBMOD * NP + n] = V[RBMOD];
+        a.prim_out[PEINT * NP + n] = V[REINT];
+      }
+      if (a.last) {
+#pragma unroll
+        for (int dir = 0; dir < NDIM; dir++) {
+          const S cf = FastSpeed<false>(dir, V);
+          double xv = double(S(m.dx[dir]) / (fabs(V[RVEL0 + dir]) + cf));
+          if (xv != xv) xv = 0.0;
+          dtl = xv < dtl ? xv : dtl;
+        }
       }
     }
   }
@@ -409,12 +420,48 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
   }
 }
 
+// A stage after the run reached tlim (queued ahead of the host's check)
+// leaves the state as it is: u1 and the output primitives become copies of
+// the input, so the host's container and buffer swaps stay consistent.
+template <typename S, int NDIM, int RECON>
+__device__ __forceinline__ void fused_passthrough(const FusedArgs<S> &a, int b, int br) {
+  using Sh = FusedShape<NDIM, RECON>;
+  const MeshDesc &m = a.m;
+  const long long NP = (long long)m.nb * m.P;
+  const int o[3] = {(br % a.nbr[0]) * Sh::B[0], ((br / a.nbr[0]) % a.nbr[1]) * Sh::B[1],
+                    (br / (a.nbr[0] * a.nbr[1])) * Sh::B[2]};
+  for (int c = threadIdx.x; c < Sh::NCELL; c += Sh::NT) {
+    const int l0 = o[0] + c % Sh::B[0], l1 = o[1] + (c / Sh::B[0]) % Sh::B[1], l2 = o[2] + c / (Sh::B[0] * Sh::B[1]);
+    if (l0 >= m.nx[0] || l1 >= m.nx[1] || l2 >= m.nx[2]) continue;
+    const long long n = (long long)b * m.P +
+                        ((long long)(l2 + m.g[2]) * m.np[1] + (l1 + m.g[1])) * m.np[0] + (l0 + m.g[0]);
+    if (a.u1 != a.u0) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) a.u1[v * NP + n] = a.u0[v * NP + n];
+      if constexpr (sizeof(S) == 4) a.u1lo[n] = a.u0lo[n];
+    }
+    if (a.prim_out) {
+      const bool keep[3] = {false, false, false};
+      S V[7];
+      fz_load_prim<S>(a, n, keep, V);
+#pragma unroll
+      for (int d = 0; d < 3; d++) a.prim_out[(PVEL0 + d) * NP + n] = V[RVEL0 + d];
+      a.prim_out[PPRES * NP + n] = V[RPRES];
+      a.prim_out[PBMOD * NP + n] = V[RBMOD];
+      a.prim_out[PEINT * NP + n] = V[REINT];
+    }
+  }
+}
+
 // One stage of one mesh: one CTA per brick.
 template <typename S, int NDIM, int RECON, int RIEMANN>
 __global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT) k_fused_stage(FusedArgs<S> a) {
-  if (a.clock->done) return;
   const int nbrick = a.nbr[0] * a.nbr[1] * a.nbr[2];
   const int b = blockIdx.x / nbrick;
+  if (a.clock->done) {
+    fused_passthrough<S, NDIM, RECON>(a, b, blockIdx.x - b * nbrick);
+    return;
+  }
   fused_brick<S, NDIM, RECON, RIEMANN>(a, b, blockIdx.x - b * nbrick, a.clock->dt);
 }
 
@@ -455,6 +502,7 @@ __device__ __forceinline__ void batch_args(const SolveDesc<S> &q, int stage, Fus
   a.u1 = q.cont[i1];
   a.u1lo = q.lo[i1];
   a.prim = q.prim;
+  a.prim_out = nullptr;
   a.stored = stage == 1 ? q.stored : 0;
   a.last = stage == q.nstages;
   a.beta = q.beta[stage - 1];

@@ -156,6 +156,10 @@ struct kmy_ctx {
   size_t esz = 8;  // bytes per stored real
   std::map<std::string, kmy::Container> md;
   void *prim = nullptr;   // [NPRIM][nb][P] shared primitives (S)
+  // Fused path: the stage reads the primitives of its input from `prim` and
+  // writes those of its output to `prim_alt`; the two swap after the stage.
+  void *prim_alt = nullptr;
+  bool prims_interior = false;  // `prim` holds the interior primitives of "base" (ghosts stale)
   void *flux = nullptr;   // [3][ncc][nb][Pf] face fluxes (S), shared by all containers
   double *divb = nullptr; // [nb][P]
   kmy::DevClock *clock = nullptr;  // device

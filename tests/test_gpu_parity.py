@@ -126,3 +126,25 @@ def test_estimate_dt_and_sums(kmy_lib, oracle_mod):
                                     ("ener", 0)]):
         ref = float(np.sum(o.interior(o.get(name, c)).astype(np.longdouble) * vol))
         assert sums[v] == pytest.approx(ref, rel=1e-14, abs=1e-16)
+
+
+@pytest.mark.parametrize("integ", ["rk1", "rk2", "rk3"])
+@pytest.mark.parametrize("path", ["fused", "tasks"])
+def test_evolve_past_tlim_keeps_state(kmy_lib, integ, path):
+    # kmy_evolve queues fused steps in chunks, so steps can be queued after the
+    # clock reaches tlim; the state must be the same as stepping one at a time,
+    # and a later evolve must continue from it
+    from kamayan_b200 import Solver
+
+    deck = configs.vortex_2d(n=64, nb=32, integrator=integ)
+    a, b = Solver(deck.text()), Solver(deck.text())
+    for s in (a, b):
+        s.set_path(path)
+        s.pgen("isentropic_vortex")
+    for tlim in (0.05, 0.11):
+        a.evolve(tlim)
+        while b.time["time"] < tlim:
+            b.evolve(tlim, nlim=1)
+        assert a.time["time"] == b.time["time"] and a.time["time"] >= tlim
+        for var, c in (("dens", 0), ("momentum", 0), ("ener", 0)):
+            assert np.array_equal(a.export(var, c), b.export(var, c)), (tlim, var)
