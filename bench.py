@@ -12,8 +12,9 @@ batched into one launch per stage, timed with CUDA events on the solver's
 stream.  Beside it: the FP64 fused path, the FP64 per-task path (the
 reference task list, one kernel per task) and the FP32-vs-FP64 density L1.
 ``e2e``: the same metric through the C ABI with host buffers: import of the
-initial state from pinned host memory, K x kmy_step (each returns dt to the
-host), export of the final conserved state.
+initial conserved state from pinned host memory (finalize derives the
+primitives), K x kmy_step (each returns dt to the host), export of the final
+conserved state.
 
 ``--impl reference`` times the reference's CPU path (the C++ restatement in
 oracle/, all host threads) on a bounded sample of the same workload.
@@ -229,10 +230,9 @@ def e2e_solve(a, device: int, stream, K: int):
     import kamayan_b200
 
     src = make_solver(a, "fp64", device, stream)
-    names_in = [("dens", 0), ("momentum", 0), ("momentum", 1), ("momentum", 2), ("ener", 0),
-                ("velocity", 0), ("velocity", 1), ("velocity", 2), ("pres", 0), ("bulk modulus", 0),
-                ("eint", 0), ("temp", 0)]
-    names_out = names_in[:5]
+    # the conserved state in; finalize derives the primitives on the device
+    names_in = [("dens", 0), ("momentum", 0), ("momentum", 1), ("momentum", 2), ("ener", 0)]
+    names_out = names_in
     n = 1
     for x in src.cell_shape:
         n *= x
@@ -494,7 +494,8 @@ def main():
         "dtype": "f32", "data": "synthetic", "config": workload_config(a, ws),
         "e2e": {"value": ws * cells * K / (e2e_ms / 1e3), "unit": METRIC,
                 "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
-                "what": "kmy_import_var (pinned host) + finalize + K x kmy_step + kmy_export_var, FP32"},
+                "what": "kmy_import_var of the conserved state (pinned host) + finalize + K x kmy_step + "
+                        "kmy_export_var of the conserved state, FP32"},
         "gpu_launches": r32["launches"],
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
                      "frac": ach32 / peak, "traffic": traffic, "peak_kind": peak_kind,

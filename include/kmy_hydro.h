@@ -92,7 +92,9 @@ int kmy_import_var(kmy_ctx *ctx, const char *container, const char *var, int com
 int kmy_export_var(kmy_ctx *ctx, const char *container, const char *var, int comp,
                    double *host, size_t n);
 /* Mark imported state complete: prims of "base" are taken as given (as after
- * the reference's MeshPostInitialization), ghosts are filled, dt is estimated.
+ * the reference's MeshPostInitialization) or, when no primitive variable was
+ * imported since the last finalize, derived from the conserved state
+ * (PreparePrimitive); ghosts are filled, dt is estimated.
  * Replaces: the driver initialisation path (EstimateTimestep after pgen). */
 int kmy_finalize_import(kmy_ctx *ctx);
 

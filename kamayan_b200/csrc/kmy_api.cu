@@ -498,6 +498,9 @@ int kmy_import_var(kmy_ctx *c, const char *container, const char *var, int comp,
     c->err = "size mismatch: expected " + std::to_string(r.n);
     return KMY_ERR_BAD_PARAM;
   }
+  const std::string vn(var);
+  if (vn == "velocity" || vn == "pres" || vn == "bulk modulus" || vn == "eint" || vn == "temp")
+    c->prims_imported = true;
   if (r.is_double || c->esz == 8) {
     rc = cuda_check(c, cudaMemcpyAsync(r.p, host, n * 8, cudaMemcpyHostToDevice, c->stream), "import copy");
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "import sync");
@@ -553,7 +556,11 @@ int kmy_finalize_import(kmy_ctx *c) {
   if (!c) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
   Container &b = c->md["base"];
-  int rc = launch_fill_ghosts(c, b);
+  int rc = KMY_OK;
+  // primitives that were not imported come from the conserved state
+  if (!c->prims_imported) rc = launch_prepare_primitive(c, b);
+  c->prims_imported = false;
+  if (!rc) rc = launch_fill_ghosts(c, b);
   if (!rc && c->prm.mhd) rc = launch_fill_derived(c, b);
   if (!rc) rc = launch_estimate_dt(c, b, true);
   if (!rc) rc = launch_dt_controller(c, 1);

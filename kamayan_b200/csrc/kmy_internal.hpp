@@ -160,6 +160,7 @@ struct kmy_ctx {
   // writes those of its output to `prim_alt`; the two swap after the stage.
   void *prim_alt = nullptr;
   bool prims_interior = false;  // `prim` holds the interior primitives of "base" (ghosts stale)
+  bool prims_imported = false;  // a primitive was imported since the last finalize
   void *flux = nullptr;   // [3][ncc][nb][Pf] face fluxes (S), shared by all containers
   double *divb = nullptr; // [nb][P]
   kmy::DevClock *clock = nullptr;  // device

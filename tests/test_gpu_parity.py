@@ -148,3 +148,24 @@ def test_evolve_past_tlim_keeps_state(kmy_lib, integ, path):
         assert a.time["time"] == b.time["time"] and a.time["time"] >= tlim
         for var, c in (("dens", 0), ("momentum", 0), ("ener", 0)):
             assert np.array_equal(a.export(var, c), b.export(var, c)), (tlim, var)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_import_conserved_only(kmy_lib, precision):
+    # finalize derives the primitives when only the conserved state was imported
+    from kamayan_b200 import Solver
+
+    deck = configs.kh_3d(n=32, nb=16, precision=precision)
+    a = Solver(deck.text())
+    a.pgen("kelvin_helmholtz")
+    b = Solver(deck.text())
+    for var, c in (("dens", 0), ("momentum", 0), ("momentum", 1), ("momentum", 2), ("ener", 0)):
+        b.import_(var, a.export(var, c), c)
+    b.finalize_import()
+    tol = 1e-13 if precision == "fp64" else 1e-6
+    for var, c in (("pres", 0), ("velocity", 1), ("eint", 0)):
+        assert rel_l1(b.interior(b.export(var, c)), a.interior(a.export(var, c))) <= tol, var
+    for s in (a, b):
+        s.step()
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    assert rel_l1(b.interior(b.export("dens")), a.interior(a.export("dens"))) <= tol
