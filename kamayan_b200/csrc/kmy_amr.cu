@@ -320,9 +320,10 @@ __global__ void k_flux_correct(const __grid_constant__ MeshDesc m, S *flux, int 
 }
 
 // AMRLoehner on one field of a container: one CTA per block, one thread per
-// (k, j) row; the block's tag is the maximum of the row flags.
+// (k, j) row; the block's flag is the maximum of the row flags.  With
+// several criteria the tag is the maximum over them (combine: max into tags).
 __global__ void k_amr_tag(const __grid_constant__ MeshDesc m, Field f, double refine_tol, double derefine_tol,
-                          double filter, int max_level, int *tags) {
+                          double filter, int max_level, int combine, int *tags) {
   __shared__ int flag_sh;
   const int b = blockIdx.x;
   if (threadIdx.x == 0) flag_sh = -1;
@@ -368,7 +369,7 @@ __global__ void k_amr_tag(const __grid_constant__ MeshDesc m, Field f, double re
   }
   atomicMax(&flag_sh, flag_row_max);
   __syncthreads();
-  if (threadIdx.x == 0) tags[b] = flag_sh;
+  if (threadIdx.x == 0) tags[b] = combine ? max(tags[b], flag_sh) : flag_sh;
 }
 
 // Remap after a remesh: every interior cell of the new leaves takes the level
@@ -528,17 +529,21 @@ int launch_amr_tag(kmy_ctx *c, Container &ct) {
   const MeshDesc &m = c->m;
   const AmrHost &a = c->amr;
   const long long NP = (long long)m.nb * m.P;
-  Field f{nullptr, nullptr, c->esz == 4};
-  if (a.field == "pres") {
-    f.p = static_cast<const char *>(c->prim) + c->esz * NP * PPRES;
-  } else if (a.field == "ener") {
-    f.p = static_cast<const char *>(ct.cc) + c->esz * NP * CENER;
-    f.lo = static_cast<const float *>(ct.ener_lo);
-  } else {
-    f.p = static_cast<const char *>(ct.cc) + c->esz * NP * CDENS;
+  for (size_t i = 0; i < a.crits.size(); i++) {
+    const AmrCriterion &cr = a.crits[i];
+    Field f{nullptr, nullptr, c->esz == 4};
+    if (cr.field == "pres") {
+      f.p = static_cast<const char *>(c->prim) + c->esz * NP * PPRES;
+    } else if (cr.field == "ener") {
+      f.p = static_cast<const char *>(ct.cc) + c->esz * NP * CENER;
+      f.lo = static_cast<const float *>(ct.ener_lo);
+    } else {
+      f.p = static_cast<const char *>(ct.cc) + c->esz * NP * CDENS;
+    }
+    k_amr_tag<<<m.nb, kThreads, 0, c->stream>>>(m, f, cr.refine_tol, cr.derefine_tol, cr.filter, cr.max_level,
+                                                 i > 0, a.d_tags);
+    c->launches++;
   }
-  k_amr_tag<<<m.nb, kThreads, 0, c->stream>>>(m, f, a.refine_tol, a.derefine_tol, a.filter, a.max_level, a.d_tags);
-  c->launches++;
   return cuda_check(c, cudaGetLastError(), "amr tag");
 }
 

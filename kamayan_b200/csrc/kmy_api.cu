@@ -139,21 +139,34 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   const int numlevel = p.integer("parthenon/mesh/numlevel", 1);
   if (refine == "static" && numlevel > 1)
     return bad("parthenon/mesh/refinement = static with numlevel > 1 is not supported");
-  // adaptive mesh: a <kamayan/refinement0> block with a field (grid.cpp:43-48, :90-124)
+  // adaptive mesh: one criterion per <kamayan/refinementN> block, N = 0, 1, ...
+  // while the blocks exist; a block without a field adds none
+  // (grid.cpp:43-48, :90-124, :127-141)
   AmrHost &amr = c->amr;
-  amr.on = refine == "adaptive" && numlevel > 1 && p.deck.count("kamayan/refinement0/field");
+  amr.crits.clear();
+  if (refine == "adaptive") {
+    for (int n = 0;; n++) {
+      const std::string b = "kamayan/refinement" + std::to_string(n) + "/";
+      auto it = p.deck.lower_bound(b);
+      if (it == p.deck.end() || it->first.compare(0, b.size(), b) != 0) break;
+      if (!p.deck.count(b + "field")) continue;
+      AmrCriterion cr;
+      cr.field = p.str(b + "field", "dens");
+      if (!one_of(cr.field, {"dens", "pres", "ener"})) return bad(b + "field: " + cr.field);
+      if (p.str(b + "method", "loehner") != "loehner") return bad(b + "method: only loehner is implemented");
+      cr.refine_tol = p.real(b + "refine_tol", 0.8);
+      cr.derefine_tol = p.real(b + "derefine_tol", 0.2);
+      cr.filter = p.real(b + "filter", 0.01);
+      cr.max_level = std::min(numlevel - 1, p.integer(b + "max_level", numlevel - 1));
+      amr.crits.push_back(cr);
+    }
+  }
+  amr.on = numlevel > 1 && !amr.crits.empty();
   if (amr.on) {
     if (numlevel > 8) return bad("parthenon/mesh/numlevel: at most 8 levels");
     if (p.mhd) return bad("adaptive meshes are supported for hydro only");
     amr.numlevel = numlevel;
-    amr.field = p.str("kamayan/refinement0/field", "dens");
-    if (!one_of(amr.field, {"dens", "pres", "ener"})) return bad("kamayan/refinement0/field: " + amr.field);
-    if (p.str("kamayan/refinement0/method", "loehner") != "loehner")
-      return bad("kamayan/refinement0/method: only loehner is implemented");
-    amr.refine_tol = p.real("kamayan/refinement0/refine_tol", 0.8);
-    amr.derefine_tol = p.real("kamayan/refinement0/derefine_tol", 0.2);
-    amr.filter = p.real("kamayan/refinement0/filter", 0.01);
-    amr.max_level = std::min(numlevel - 1, p.integer("kamayan/refinement0/max_level", numlevel - 1));
+    amr.max_level = numlevel - 1;
     amr.derefine_count = p.integer("parthenon/mesh/derefine_count", 10);
   }
 

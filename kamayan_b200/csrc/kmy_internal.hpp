@@ -131,11 +131,15 @@ struct Container {
 };
 
 // Host side of an adaptive mesh: the leaf list and the refinement parameters.
-struct AmrHost {
-  bool on = false;
-  int numlevel = 1, max_level = 0, derefine_count = 10;
+struct AmrCriterion {
   std::string field = "dens";
   double refine_tol = 0.8, derefine_tol = 0.2, filter = 0.01;
+  int max_level = 0;
+};
+struct AmrHost {
+  bool on = false;
+  int numlevel = 1, max_level = 0, derefine_count = 10;  // max_level = numlevel - 1
+  std::vector<AmrCriterion> crits;  // one per <kamayan/refinementN> block with a field
   std::vector<int> lev;  // per leaf
   std::vector<int> loc;  // 3 per leaf
   std::vector<int> cnt;  // consecutive derefine tags per leaf

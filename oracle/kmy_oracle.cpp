@@ -440,9 +440,14 @@ struct Sim {
   bool amr = false;
   int numlevel = 1;
   int derefine_count = 10;
-  std::string ref_field = "dens";
-  Real refine_tol = 0.8, derefine_tol = 0.2, ref_filter = 0.01;
-  int max_level = 0;
+  // one Loehner criterion per <kamayan/refinementN> block (grid.cpp:90-124)
+  struct RefCrit {
+    std::string field;
+    Real refine_tol, derefine_tol, filter;
+    int max_level;
+  };
+  std::vector<RefCrit> crits;
+  int max_level = 0;  // numlevel - 1
 
   int lx(int b, int d) const { return bloc[b][d]; }
   // cell size of block b along d (only active dimensions refine)
@@ -567,14 +572,24 @@ bool Sim::setup(const char *deck_text) {
   // adaptive mesh: <parthenon/mesh> refinement = adaptive with numlevel > 1 and
   // a <kamayan/refinement0> block (grid.cpp:229-262)
   numlevel = d.integer("parthenon/mesh/numlevel", 1);
-  amr = d.str("parthenon/mesh/refinement", "none") == "adaptive" && numlevel > 1 &&
-        d.has("kamayan/refinement0/field");
+  crits.clear();
+  if (d.str("parthenon/mesh/refinement", "none") == "adaptive") {
+    // blocks refinement0, refinement1, ... while they exist; a block without a
+    // field adds no criterion
+    for (int n = 0;; n++) {
+      const std::string b = "kamayan/refinement" + std::to_string(n) + "/";
+      bool exists = false;
+      for (auto &kv : d.kv)
+        if (kv.first.compare(0, b.size(), b) == 0) exists = true;
+      if (!exists) break;
+      if (!d.has(b + "field")) continue;
+      crits.push_back({d.str(b + "field", "dens"), d.real(b + "refine_tol", 0.8), d.real(b + "derefine_tol", 0.2),
+                       d.real(b + "filter", 0.01), d.integer(b + "max_level", numlevel - 1)});
+    }
+  }
+  amr = numlevel > 1 && !crits.empty();
   if (amr) {
-    ref_field = d.str("kamayan/refinement0/field", "dens");
-    refine_tol = d.real("kamayan/refinement0/refine_tol", 0.8);
-    derefine_tol = d.real("kamayan/refinement0/derefine_tol", 0.2);
-    ref_filter = d.real("kamayan/refinement0/filter", 0.01);
-    max_level = std::min(numlevel - 1, d.integer("kamayan/refinement0/max_level", numlevel - 1));
+    max_level = numlevel - 1;
     derefine_count = d.integer("parthenon/mesh/derefine_count", 10);
     if (ph.mhd) {
       error = "adaptive meshes are restated for hydro only";
@@ -954,59 +969,63 @@ void Sim::flux_correct(const std::string &md0name) {
   }
 }
 
-// AMRLoehner::operator() (grid_refinement.cpp:30-152) on one field of `name`.
+// AMRLoehner::operator() (grid_refinement.cpp:30-152) for every criterion on
+// its field of `name`; a block's tag is the largest over the criteria.
 void Sim::tag_blocks(const std::string &name) {
   Container &c = C(name);
-  const Real *arr = nullptr;
-  if (ref_field == "dens") arr = cc(c, CDENS, 0);
-  else if (ref_field == "pres") arr = pr(PPRES, 0);
-  else if (ref_field == "ener") arr = cc(c, CENER, 0);
-  else arr = cc(c, CDENS, 0);
-  tags.assign(nb, 0);
-  const int k2d = ndim > 1 ? 1 : 0, k3d = ndim > 2 ? 1 : 0;
-  for (int b = 0; b < nb; b++) {
-    const Real *u = arr + size_t(b) * P;
-    std::vector<Real> der(size_t(3) * P, 0.0);
-    auto D = [&](int p, int k, int j, int i) -> Real & { return der[size_t(p) * P + cidx(k, j, i)]; };
-    const Real dxq[3] = {dxb(b, 0), dxb(b, 1), dxb(b, 2)};
-    for (int k = g[2] - k3d; k <= g[2] + nx[2] - 1 + k3d; k++)
-      for (int j = g[1] - k2d; j <= g[1] + nx[1] - 1 + k2d; j++)
-        for (int i = g[0] - 1; i <= g[0] + nx[0]; i++) {
-          D(0, k, j, i) = 0.5 * (u[cidx(k, j, i + 1)] - u[cidx(k, j, i - 1)]) / dxq[0];
-          if (ndim > 1) D(1, k, j, i) = 0.5 * (u[cidx(k, j + 1, i)] - u[cidx(k, j - 1, i)]) / dxq[1];
-          if (ndim > 2) D(2, k, j, i) = 0.5 * (u[cidx(k + 1, j, i)] - u[cidx(k - 1, j, i)]) / dxq[2];
-        }
-    int flag_block = -1;
-    for (int k = g[2]; k < g[2] + nx[2]; k++)
-      for (int j = g[1]; j < g[1] + nx[1]; j++) {
-        Real max_err_2 = 0.;
-        for (int i = g[0]; i < g[0] + nx[0]; i++) {
-          Real numerator = 0.0, denominator = 1.e-12;
-          for (int q = 0; q < ndim; q++) {
-            const int kq = q == 2, jq = q == 1, iq = q == 0;
-            for (int p = 0; p < ndim; p++) {
-              const int kp = p == 2, jp = p == 1, ip = p == 0;
-              const Real num = 0.5 * (D(p, k + kq, j + jq, i + iq) - D(p, k - kq, j - jq, i - iq)) / dxq[q];
-              numerator += num * num;
-              const Real denom =
-                  0.5 * (std::fabs(D(p, k + kq, j + jq, i + iq)) + std::fabs(D(p, k - kq, j - jq, i - iq))) /
-                      dxq[p] +
-                  ref_filter *
-                      (std::fabs(u[cidx(k + kq, j + jq, i + iq)]) + std::fabs(u[cidx(k - kq, j - jq, i - iq)]) +
-                       std::fabs(u[cidx(k - kp, j - jp, i - ip)]) + std::fabs(u[cidx(k + kp, j + jp, i + ip)])) /
-                      (dxq[q] * dxq[p]);
-              denominator += denom * denom;
-            }
+  tags.assign(nb, -1);
+  for (const RefCrit &cr : crits) {
+    const Real *arr = nullptr;
+    if (cr.field == "pres") arr = pr(PPRES, 0);
+    else if (cr.field == "ener") arr = cc(c, CENER, 0);
+    else arr = cc(c, CDENS, 0);
+    const Real refine_tol = cr.refine_tol, derefine_tol = cr.derefine_tol, ref_filter = cr.filter;
+    const int crit_max_level = std::min(cr.max_level, max_level);
+    const int k2d = ndim > 1 ? 1 : 0, k3d = ndim > 2 ? 1 : 0;
+    for (int b = 0; b < nb; b++) {
+      const Real *u = arr + size_t(b) * P;
+      std::vector<Real> der(size_t(3) * P, 0.0);
+      auto D = [&](int p, int k, int j, int i) -> Real & { return der[size_t(p) * P + cidx(k, j, i)]; };
+      const Real dxq[3] = {dxb(b, 0), dxb(b, 1), dxb(b, 2)};
+      for (int k = g[2] - k3d; k <= g[2] + nx[2] - 1 + k3d; k++)
+        for (int j = g[1] - k2d; j <= g[1] + nx[1] - 1 + k2d; j++)
+          for (int i = g[0] - 1; i <= g[0] + nx[0]; i++) {
+            D(0, k, j, i) = 0.5 * (u[cidx(k, j, i + 1)] - u[cidx(k, j, i - 1)]) / dxq[0];
+            if (ndim > 1) D(1, k, j, i) = 0.5 * (u[cidx(k, j + 1, i)] - u[cidx(k, j - 1, i)]) / dxq[1];
+            if (ndim > 2) D(2, k, j, i) = 0.5 * (u[cidx(k + 1, j, i)] - u[cidx(k - 1, j, i)]) / dxq[2];
           }
-          max_err_2 = denominator == 0.0 ? max_err_2 : kmax(max_err_2, numerator / denominator);
+      int flag_block = -1;
+      for (int k = g[2]; k < g[2] + nx[2]; k++)
+        for (int j = g[1]; j < g[1] + nx[1]; j++) {
+          Real max_err_2 = 0.;
+          for (int i = g[0]; i < g[0] + nx[0]; i++) {
+            Real numerator = 0.0, denominator = 1.e-12;
+            for (int q = 0; q < ndim; q++) {
+              const int kq = q == 2, jq = q == 1, iq = q == 0;
+              for (int p = 0; p < ndim; p++) {
+                const int kp = p == 2, jp = p == 1, ip = p == 0;
+                const Real num = 0.5 * (D(p, k + kq, j + jq, i + iq) - D(p, k - kq, j - jq, i - iq)) / dxq[q];
+                numerator += num * num;
+                const Real denom =
+                    0.5 * (std::fabs(D(p, k + kq, j + jq, i + iq)) + std::fabs(D(p, k - kq, j - jq, i - iq))) /
+                        dxq[p] +
+                    ref_filter *
+                        (std::fabs(u[cidx(k + kq, j + jq, i + iq)]) + std::fabs(u[cidx(k - kq, j - jq, i - iq)]) +
+                         std::fabs(u[cidx(k - kp, j - jp, i - ip)]) + std::fabs(u[cidx(k + kp, j + jp, i + ip)])) /
+                        (dxq[q] * dxq[p]);
+                denominator += denom * denom;
+              }
+            }
+            max_err_2 = denominator == 0.0 ? max_err_2 : kmax(max_err_2, numerator / denominator);
+          }
+          const Real max_err = std::sqrt(max_err_2);
+          int flag = 0;
+          if (max_err > refine_tol && blev[b] < crit_max_level) flag = 1;
+          if (max_err < derefine_tol) flag = -1;
+          flag_block = std::max(flag_block, flag);
         }
-        const Real max_err = std::sqrt(max_err_2);
-        int flag = 0;
-        if (max_err > refine_tol && blev[b] < max_level) flag = 1;
-        if (max_err < derefine_tol) flag = -1;
-        flag_block = std::max(flag_block, flag);
-      }
-    tags[b] = flag_block;
+      tags[b] = std::max(tags[b], flag_block);
+    }
   }
 }
 

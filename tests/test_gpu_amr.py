@@ -156,3 +156,22 @@ def test_server_refuses_adaptive_deck(kmy_lib):
             srv.submit(configs.blast_2d_amr(n=64, nb=8), "blast", 4)
     finally:
         srv.close()
+
+
+def test_two_criteria_take_the_larger_tag(kmy_lib, oracle_mod):
+    # <kamayan/refinement0> on density and <kamayan/refinement1> on pressure:
+    # a block's tag is the larger of the two criteria's
+    deck = configs.blast_2d_amr(n=64, nb=8, derefine_count=2)
+    deck.set("kamayan/refinement1", "field", "pres")
+    deck.set("kamayan/refinement1", "refine_tol", 0.5)
+    deck.set("kamayan/refinement1", "derefine_tol", 0.1)
+    deck.set("kamayan/refinement1", "max_level", 1)
+    o, s = _pair(deck)
+    _same_blocks(o, s)
+    for _ in range(30):
+        s.set_dt(o.time["dt"])
+        o.step()
+        s.step()
+        _same_blocks(o, s)
+    res = compare(o, s)
+    assert all(v <= TOL_NSTEP for v in res.values()), res
