@@ -504,6 +504,9 @@ struct Sim {
   void build_tables();
   int table_at(int L, const int bx[3]) const;
   Real V(int L, const int G[3], const Real *arr, int flipdim) const;
+  Real FV(const Real *fcb, int e, int L, const int G[3]) const;
+  Real toth_roe(const Real *fcb, int e, int L, const int M[3]) const;
+  void emf_correct(const std::string &md0);
   void fill_ghosts_amr(const std::string &name);
   void flux_correct(const std::string &md0);
   void tag_blocks(const std::string &name);
@@ -591,10 +594,6 @@ bool Sim::setup(const char *deck_text) {
   if (amr) {
     max_level = numlevel - 1;
     derefine_count = d.integer("parthenon/mesh/derefine_count", 10);
-    if (ph.mhd) {
-      error = "adaptive meshes are restated for hydro only";
-      return false;
-    }
   }
   Pf = long(nf[0]) * nf[1] * nf[2];
 
@@ -869,6 +868,147 @@ Real Sim::V(int L, const int G[3], const Real *arr, int flipdim) const {
   return sgn * val;
 }
 
+// Face-field value of component e at level L and global face index G (face
+// index along e, cell indices across), on the face arrays fcb = [3][nb][Pf].
+// Same preference as V: a face owned by a level-L leaf (its low face, else the
+// high face of the leaf below it along e), the area-weighted restriction of
+// the finer leaves' faces on the same plane (RestrictAverage on faces), or a
+// prolongation from level L-1: faces on a coarse face plane by minmod in the
+// plane (ProlongateSharedMinMod, refinement_operations.hpp:123-264), faces
+// inside a coarse cell by Toth & Roe (ProlongateInternalTothAndRoe,
+// refinement_operations.hpp:270-398).  Along e out-of-range faces clamp to the
+// boundary face (or wrap when periodic); across e the cell map applies.  No
+// sign flips on face values, as in the single-level face fill.
+Real Sim::FV(const Real *fcb, int e, int L, const int G[3]) const {
+  int M[3] = {0, 0, 0};
+  for (int d = 0; d < ndim; d++) {
+    const int N = mesh_nx[d] << L;
+    if (d == e) {
+      if (G[d] >= 0 && G[d] <= N) M[d] = G[d];
+      else if (bc[d][G[d] < 0 ? 0 : 1] == PERIODIC) M[d] = ((G[d] % N) + N) % N;
+      else M[d] = G[d] < 0 ? 0 : N;
+    } else {
+      bool f = false;
+      M[d] = map_index(G[d], N, bc[d][G[d] < 0 ? 0 : 1], f);
+    }
+  }
+  const bool act = e < ndim;
+  int bx[3];
+  for (int d = 0; d < 3; d++) bx[d] = M[d] / nx[d];
+  const int NBe = act ? (nbx[e] << L) : 1;
+  int ehi = -3, elo = -3;
+  if (bx[e] < NBe) ehi = table_at(L, bx);
+  int bl[3] = {bx[0], bx[1], bx[2]};
+  if (act && M[e] % nx[e] == 0 && M[e] > 0) {
+    bl[e] -= 1;
+    elo = table_at(L, bl);
+  }
+  auto at = [&](int leaf, const int q[3], int le) {
+    int l[3];
+    for (int d = 0; d < 3; d++) l[d] = M[d] - q[d] * nx[d] + g[d];
+    l[e] = le;
+    return fcb[(size_t(e) * nb + leaf) * Pf + fidx(l[2], l[1], l[0])];
+  };
+  if (ehi >= 0) return at(ehi, bx, M[e] - bx[e] * nx[e] + g[e]);
+  if (elo >= 0) return at(elo, bl, nx[e] + g[e]);
+  if (ehi == -1 || elo == -1) {  // finer leaves: restrict the fine faces on this plane
+    Real t[2][2][2] = {}, v[2][2][2] = {};
+    Real area = 1.0;
+    for (int d = 0; d < 3; d++)
+      if (d != e) area *= d < ndim ? dx[d] / Real(1 << (L + 1)) : dx[d];
+    const bool in0 = e != 0, in1 = e != 1 && ndim > 1, in2 = e != 2 && ndim > 2;
+    for (int ok = 0; ok < 1 + in2; ok++)
+      for (int oj = 0; oj < 1 + in1; oj++)
+        for (int oi = 0; oi < 1 + in0; oi++) {
+          const int Gf[3] = {2 * M[0] + oi, ndim > 1 ? 2 * M[1] + oj : 0, ndim > 2 ? 2 * M[2] + ok : 0};
+          v[ok][oj][oi] = area;
+          t[ok][oj][oi] = area * FV(fcb, e, L + 1, Gf);
+        }
+    return restrict_sum(t, v);
+  }
+  if (L == 0) return 0.0;  // unreachable on a balanced tree
+  if (!act || M[e] % 2 == 0) {
+    // shared face: minmod prolongation in the plane of the coarse face
+    int Mc[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+    for (int d = 0; d < ndim; d++) {
+      Mc[d] = d == e ? M[d] / 2 : M[d] >> 1;
+      o[d] = d == e ? 0 : M[d] & 1;
+    }
+    const Real fc = FV(fcb, e, L - 1, Mc);
+    Real gq[3] = {0, 0, 0}, dfm[3] = {0, 0, 0}, dfp[3] = {0, 0, 0};
+    for (int d = 0; d < ndim; d++) {
+      if (d == e) continue;
+      const Real dxc = dx[d] / Real(1 << (L - 1)), dxf = dx[d] / Real(1 << L);
+      auto xc_of = [&](int i) { return xmin[d] + (Real(i) + 0.5) * dxc; };
+      auto xf_of = [&](int i) { return xmin[d] + (Real(i) + 0.5) * dxf; };
+      int Gm[3] = {Mc[0], Mc[1], Mc[2]}, Gp[3] = {Mc[0], Mc[1], Mc[2]};
+      Gm[d] -= 1;
+      Gp[d] += 1;
+      const Real fm = FV(fcb, e, L - 1, Gm), fp = FV(fcb, e, L - 1, Gp);
+      const Real xm = xc_of(Mc[d] - 1), xc = xc_of(Mc[d]), xp = xc_of(Mc[d] + 1);
+      dfm[d] = xc - xf_of(2 * Mc[d]);
+      dfp[d] = xf_of(2 * Mc[d] + 1) - xc;
+      gq[d] = grad_minmod(fc, fm, fp, xc - xm, xp - xc);
+    }
+    const Real g1 = gq[0], g2 = gq[1], g3 = gq[2];
+    const Real d1m = dfm[0], d1p = dfp[0], d2m = dfm[1], d2p = dfp[1], d3m = dfm[2], d3p = dfp[2];
+    switch (o[0] + 2 * o[1] + 4 * o[2]) {
+      case 0: return fc - (g1 * d1m + g2 * d2m + g3 * d3m);
+      case 1: return fc + (g1 * d1p - g2 * d2m - g3 * d3m);
+      case 2: return fc - (g1 * d1m - g2 * d2p + g3 * d3m);
+      case 3: return fc + (g1 * d1p + g2 * d2p - g3 * d3m);
+      case 4: return fc - (g1 * d1m + g2 * d2m - g3 * d3p);
+      case 5: return fc + (g1 * d1p - g2 * d2m + g3 * d3p);
+      case 6: return fc - (g1 * d1m - g2 * d2p - g3 * d3p);
+      default: return fc + (g1 * d1p + g2 * d2p + g3 * d3p);
+    }
+  }
+  return toth_roe(fcb, e, L, M);
+}
+
+// ProlongateInternalTothAndRoe (refinement_operations.hpp:270-398) for the
+// internal face M (odd along e) of a coarse cell, from the level-L faces on
+// the coarse cell's boundary.  Axes: a0 = e, a1 = e+1, a2 = e+2 (cyclic);
+// offsets oi along a0, oj along a1, ok along a2, collapsed in inactive
+// dimensions as the operator's guards do.  In a collapsed axis the operator
+// writes the same face for both offsets and the second write (offset 1) stays.
+Real Sim::toth_roe(const Real *fcb, int e, int L, const int M[3]) const {
+  const int a0 = e, a1 = (e + 1) % 3, a2 = (e + 2) % 3;
+  int f0[3] = {0, 0, 0}, act[3];
+  for (int d = 0; d < 3; d++) {
+    act[d] = d < ndim ? 1 : 0;
+    f0[d] = d < ndim ? 2 * (M[d] >> 1) : 0;
+  }
+  auto fine = [&](int eidx, int ok, int oj, int oi) {
+    const int comp = (e + eidx) % 3;
+    int P[3] = {f0[0], f0[1], f0[2]};
+    P[a0] += oi * act[a0];
+    P[a1] += oj * act[a1];
+    P[a2] += ok * act[a2];
+    return FV(fcb, comp, L, P);
+  };
+  auto sg = [](int off) { return off == 0 ? -1.0 : 1.0; };
+  Real Uxx = 0.0, Vxyz = 0.0, Wxyz = 0.0;
+  for (int v : {0, 1})
+    for (int u : {0, 2})
+      for (int t : {0, 1}) {
+        const Real fine2 = fine(1, v, u, t);
+        const Real fine3 = fine(2, u, v, t);
+        Uxx += sg(t) * sg(u) * (fine2 + fine3);
+        Vxyz += sg(t) * sg(u) * sg(v) * fine2;
+        Wxyz += sg(t) * sg(u) * sg(v) * fine3;
+      }
+  Uxx *= 0.125;
+  Real cdx[3];
+  for (int d = 0; d < 3; d++) cdx[d] = d < ndim ? dx[d] / Real(1 << (L - 1)) : dx[d];
+  const Real dx2 = cdx[0] * cdx[0], dy2 = cdx[1] * cdx[1], dz2 = cdx[2] * cdx[2];
+  Vxyz *= 0.125 * dz2 / (dx2 + dz2);
+  Wxyz *= 0.125 * dy2 / (dx2 + dy2);
+  const int ok = act[a2] ? M[a2] - f0[a2] : 1;
+  const int oj = act[a1] ? M[a1] - f0[a1] : 1;
+  return 0.5 * (fine(0, ok, oj, 0) + fine(0, ok, oj, 2)) + Uxx + sg(ok) * Vxyz + sg(oj) * Wxyz;
+}
+
 void Sim::fill_ghosts_amr(const std::string &name) {
   Container &c = C(name);
   build_tables();
@@ -887,13 +1027,121 @@ void Sim::fill_ghosts_amr(const std::string &name) {
                             bloc[b][2] * nx[2] + (k - g[2])};
           const long n = cidx(k, j, i);
           for (int v = 0; v < ncc; v++) {
-            const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : -1;
+            const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1);
             cc(c, v, b)[n] = V(L, G, cc(c, v, 0), fd);
           }
           for (int v = 0; v < NPRIM; v++) pr(v, b)[n] = V(L, G, pr(v, 0), v <= PVEL2 ? v : -1);
         }
+    if (!ph.mhd) continue;
+    // ghost faces of the active components (the block's own faces, boundary
+    // faces included, are left alone)
+    for (int e = 0; e < ndim; e++)
+      for (int k = 0; k < np[2] + (e == 2); k++)
+        for (int j = 0; j < np[1] + (e == 1); j++)
+          for (int i = 0; i < np[0] + (e == 0); i++) {
+            const int loc[3] = {i, j, k};
+            bool interior = true;
+            for (int d = 0; d < 3; d++) {
+              const int hi = g[d] + nx[d] - 1 + (d == e ? 1 : 0);
+              if (loc[d] < g[d] || loc[d] > hi) interior = false;
+            }
+            if (interior) continue;
+            const int G[3] = {bloc[b][0] * nx[0] + (i - g[0]), bloc[b][1] * nx[1] + (j - g[1]),
+                              bloc[b][2] * nx[2] + (k - g[2])};
+            fc(c, e, b)[fidx(k, j, i)] = FV(c.fc.data(), e, L, G);
+          }
   }
 }
+
+// Edge-EMF correction at fine/coarse boundaries (the face-field part of
+// Parthenon's flux correction, kamayan_driver.cpp:198-207).  An edge on a
+// coarse block's boundary where any of the cells around it (four in 3D, the
+// four quadrants of a corner in 2D) is covered by finer leaves takes the
+// length-weighted restriction (RestrictAverage on edges) of the collinear fine
+// EMFs.  They are read from the fine leaf holding the first such cell (order
+// (-,-), (+,-), (-,+), (+,+) over the edge's two transverse axes).  Every coarse
+// block that holds the edge computes the same value, so coarse neighbours keep
+// identical copies of their shared faces.
+void Sim::emf_correct(const std::string &md0name) {
+  if (!ph.mhd || ndim < 2) return;
+  Container &c = C(md0name);
+  build_tables();
+  const Real *eo = c.emf.data();
+  std::vector<Real> out(c.emf);  // corrections read the EMFs as computed
+  for (int b = 0; b < nb; b++) {
+    const int L = blev[b];
+    for (int t = 0; t < 3; t++) {
+      if (ndim == 2 && t != 2) continue;  // 2D has z-edges only
+      const int p = (t + 1) % 3, q = (t + 2) % 3;
+      for (int at = 0; at < nx[t]; at++)
+        for (int aq = 0; aq <= nx[q]; aq++)
+          for (int ap = 0; ap <= nx[p]; ap++) {
+            if (ap != 0 && ap != nx[p] && aq != 0 && aq != nx[q]) continue;  // not on the boundary
+            const int Ep = bloc[b][p] * nx[p] + ap, Eq = bloc[b][q] * nx[q] + aq;
+            const int Et = bloc[b][t] * nx[t] + at;
+            Real val = 0.0;
+            bool found = false;
+            for (int s = 0; s < 4 && !found; s++) {
+              const int dp = s & 1, dq = s >> 1;  // 0: the cell below the edge, 1: above
+              int Gc[3];
+              Gc[p] = Ep - 1 + dp;
+              Gc[q] = Eq - 1 + dq;
+              Gc[t] = Et;
+              bool skip = false;
+              for (int d : {p, q}) {
+                const int N = mesh_nx[d] << L;
+                if (Gc[d] < 0 || Gc[d] >= N) {
+                  if (bc[d][Gc[d] < 0 ? 0 : 1] != PERIODIC) skip = true;
+                  else Gc[d] = ((Gc[d] % N) + N) % N;
+                }
+              }
+              if (skip) continue;
+              int bxc[3];
+              for (int d = 0; d < 3; d++) bxc[d] = Gc[d] / nx[d];
+              if (table_at(L, bxc) != -1) continue;
+              // the fine cell of that coarse cell next to the edge
+              int Fc[3];
+              Fc[p] = 2 * Gc[p] + (dp ? 0 : 1);
+              Fc[q] = 2 * Gc[q] + (dq ? 0 : 1);
+              Fc[t] = t < ndim ? 2 * Et : 0;
+              Real tt[2][2][2] = {}, vv[2][2][2] = {};
+              bool ok = true;
+              for (int o = 0; o < 1 + (t < ndim); o++) {
+                int Ff[3] = {Fc[0], Fc[1], Fc[2]};
+                Ff[t] += o;
+                int bf[3];
+                for (int d = 0; d < 3; d++) bf[d] = Ff[d] / nx[d];
+                const int fe = table_at(L + 1, bf);
+                if (fe < 0) {
+                  ok = false;
+                  break;
+                }
+                int lf[3];
+                for (int d = 0; d < 3; d++) lf[d] = Ff[d] - bf[d] * nx[d] + g[d];
+                if (!dp) lf[p] += 1;  // the edge is the fine cell's high face along p
+                if (!dq) lf[q] += 1;
+                int off[3] = {0, 0, 0};
+                off[t] = o;
+                const Real len = dxb(fe, t);
+                vv[off[2]][off[1]][off[0]] = len;
+                tt[off[2]][off[1]][off[0]] = len * eo[(size_t(t) * nb + fe) * Pf + fidx(lf[2], lf[1], lf[0])];
+              }
+              if (!ok) continue;
+              val = restrict_sum(tt, vv);
+              found = true;
+            }
+            if (!found) continue;
+            int le[3];
+            le[p] = g[p] + ap;
+            le[q] = g[q] + aq;
+            le[t] = g[t] + at;
+            out[(size_t(t) * nb + b) * Pf + fidx(le[2], le[1], le[0])] = val;
+          }
+    }
+  }
+  c.emf = std::move(out);
+}
+
 
 // Flux correction at fine/coarse faces (Parthenon AddFluxCorrectionTasks,
 // kamayan_driver.cpp:206-207): a coarse face flux is replaced by the
@@ -1035,8 +1283,13 @@ void Sim::resize_state(int new_nb) {
     Container &c = kv.second;
     c.cc.assign(size_t(ncc) * nb * P, 0.0);
     c.flux.assign(size_t(3) * ncc * nb * Pf, 0.0);
+    if (ph.mhd) {
+      c.fc.assign(size_t(3) * nb * Pf, 0.0);
+      c.emf.assign(size_t(3) * nb * Pf, 0.0);
+    }
   }
   prim.assign(size_t(NPRIM) * nb * P, 0.0);
+  if (ph.mhd) divb.assign(size_t(nb) * P, 0.0);
 }
 
 // Morton key of a leaf's lower corner at the finest level (block ordering).
@@ -1191,14 +1444,33 @@ bool Sim::remesh(bool allow_derefine) {
           const long n = cidx(k, j, i);
           for (int v = 0; v < ncc; v++)
             new_cc[(size_t(v) * nnew + q) * P + n] =
-                V(nlev[q], G, old_cc.data() + size_t(v) * old_nb * P, v >= CMOM0 && v <= CMOM2 ? v - CMOM0 : -1);
+                V(nlev[q], G, old_cc.data() + size_t(v) * old_nb * P,
+                  v >= CMOM0 && v <= CMOM2 ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1));
           for (int v = 0; v < NPRIM; v++)
             new_prim[(size_t(v) * nnew + q) * P + n] =
                 V(nlev[q], G, old_prim.data() + size_t(v) * old_nb * P, v <= PVEL2 ? v : -1);
         }
+  // face fields: every face of the new leaf (boundary faces included) from
+  // the old mesh (copy, restriction, or shared + Toth-Roe prolongation)
+  std::vector<Real> new_fc;
+  if (ph.mhd) {
+    new_fc.assign(size_t(3) * nnew * Pf, 0.0);
+    const Real *ofc = base.fc.data();
+#pragma omp parallel for schedule(dynamic)
+    for (int q = 0; q < nnew; q++)
+      for (int e = 0; e < 3; e++)
+        for (int k = g[2]; k < g[2] + nx[2] + (e == 2 && ndim > 2); k++)
+          for (int j = g[1]; j < g[1] + nx[1] + (e == 1 && ndim > 1); j++)
+            for (int i = g[0]; i < g[0] + nx[0] + (e == 0); i++) {
+              const int G[3] = {nloc[q][0] * nx[0] + (i - g[0]), nloc[q][1] * nx[1] + (j - g[1]),
+                                nloc[q][2] * nx[2] + (k - g[2])};
+              new_fc[(size_t(e) * nnew + q) * Pf + fidx(k, j, i)] = FV(ofc, e, nlev[q], G);
+            }
+  }
   resize_state(nnew);
   base.cc = std::move(new_cc);
   prim = std::move(new_prim);
+  if (ph.mhd) base.fc = std::move(new_fc);
   blev = nlev;
   bloc = nloc;
   deref_count = ncnt;
@@ -1389,11 +1661,11 @@ void Sim::fluxes_to_dudt(const std::string &md0name, const std::string &dudtname
               int ijk[3] = {i, j, k};
               ijk[axis] += 1;
               const Real sign = ((axis + 1) % 3 == edge) ? 1.0 : -1.0;
-              const Real L = EdgeLength(edge);
+              const Real L = dxb(b, edge);
               out += sign * (L * em(c, edge, b)[fidx(k, j, i)] -
                              L * em(c, edge, b)[fidx(ijk[2], ijk[1], ijk[0])]);
             }
-            out *= 1. / (FaceArea(face) + 1.e-36);
+            out *= 1. / (FaceAreaB(b, face) + 1.e-36);
           }
   }
 }
@@ -1427,22 +1699,22 @@ void Sim::apply_dudt(const std::string &basen, const std::string &md0n,
 
 // CT face -> cell average of primconsflux.cpp:40-67 / :102-129
 static inline void face_average(Sim &s, Container &c, int b, int k, int j, int i) {
-  const Real vol = s.CellVolume();
+  const Real vol = s.CellVolumeB(b);
   if (s.ndim > 1) {
     s.cc(c, CMAGC0, b)[s.cidx(k, j, i)] =
-        0.5 * s.dx[0] *
-        (s.FaceArea(0) * s.fc(c, 0, b)[s.fidx(k, j, i + 1)] +
-         s.FaceArea(0) * s.fc(c, 0, b)[s.fidx(k, j, i)]) / vol;
+        0.5 * s.dxb(b, 0) *
+        (s.FaceAreaB(b, 0) * s.fc(c, 0, b)[s.fidx(k, j, i + 1)] +
+         s.FaceAreaB(b, 0) * s.fc(c, 0, b)[s.fidx(k, j, i)]) / vol;
     s.cc(c, CMAGC0 + 1, b)[s.cidx(k, j, i)] =
-        0.5 * s.dx[1] *
-        (s.FaceArea(1) * s.fc(c, 1, b)[s.fidx(k, j + 1, i)] +
-         s.FaceArea(1) * s.fc(c, 1, b)[s.fidx(k, j, i)]) / vol;
+        0.5 * s.dxb(b, 1) *
+        (s.FaceAreaB(b, 1) * s.fc(c, 1, b)[s.fidx(k, j + 1, i)] +
+         s.FaceAreaB(b, 1) * s.fc(c, 1, b)[s.fidx(k, j, i)]) / vol;
   }
   if (s.ndim > 2) {
     s.cc(c, CMAGC0 + 2, b)[s.cidx(k, j, i)] =
-        0.5 * s.dx[2] *
-        (s.FaceArea(2) * s.fc(c, 2, b)[s.fidx(k + 1, j, i)] +
-         s.FaceArea(2) * s.fc(c, 2, b)[s.fidx(k, j, i)]) / vol;
+        0.5 * s.dxb(b, 2) *
+        (s.FaceAreaB(b, 2) * s.fc(c, 2, b)[s.fidx(k + 1, j, i)] +
+         s.FaceAreaB(b, 2) * s.fc(c, 2, b)[s.fidx(k, j, i)]) / vol;
   }
 }
 
@@ -1544,17 +1816,17 @@ Real Sim::estimate_dt(const std::string &name) {
 void Sim::fill_derived(const std::string &name) {
   if (!ph.mhd) return;
   Container &c = C(name);
-  const Real vol = CellVolume();
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nb; b++)
     for (int k = g[2]; k < g[2] + nx[2]; k++)
       for (int j = g[1]; j < g[1] + nx[1]; j++)
         for (int i = g[0]; i < g[0] + nx[0]; i++) {
+          const Real vol = CellVolumeB(b);
           Real d = 0.;
           for (int dir = 0; dir < ndim; dir++) {
             const int kp = k + (dir == 2), jp = j + (dir == 1), ip = i + (dir == 0);
-            d += FaceArea(dir) * fc(c, dir, b)[fidx(kp, jp, ip)] -
-                 FaceArea(dir) * fc(c, dir, b)[fidx(k, j, i)];
+            d += FaceAreaB(b, dir) * fc(c, dir, b)[fidx(kp, jp, ip)] -
+                 FaceAreaB(b, dir) * fc(c, dir, b)[fidx(k, j, i)];
           }
           divb[size_t(b) * P + cidx(k, j, i)] = d / vol;
         }
@@ -1571,6 +1843,7 @@ void Sim::rk_stage(int stage, Real dt_) {
   calc_fluxes(md0);
   if (amr) flux_correct(md0);
   calc_emf(md0);
+  if (amr) emf_correct(md0);
   fluxes_to_dudt(md0, "dUdt");
   apply_dudt(base, md0, md1, "dUdt", b, dt_);
   prepare_primitive(md1);
@@ -1731,9 +2004,10 @@ int Sim::pgen_cells(const std::string &problem) {
         for (int j = g[1]; j < g[1] + nx[1] + 1; j++)
           for (int i = g[0]; i < g[0] + nx[0] + 1; i++) {
             const Real xf = xface(b, 0, i), yc = xcen(b, 1, j);
-            fc(c, 0, b)[fidx(k, j, i)] = 1. / dx[1] * (Az(xf, yc + 0.5 * dx[1]) - Az(xf, yc - 0.5 * dx[1]));
+            const Real dxx = dxb(b, 0), dyy = dxb(b, 1);
+            fc(c, 0, b)[fidx(k, j, i)] = 1. / dyy * (Az(xf, yc + 0.5 * dyy) - Az(xf, yc - 0.5 * dyy));
             const Real xc = xcen(b, 0, i), yf = xface(b, 1, j);
-            fc(c, 1, b)[fidx(k, j, i)] = -1. / dx[0] * (Az(xc + 0.5 * dx[0], yf) - Az(xc - 0.5 * dx[0], yf));
+            fc(c, 1, b)[fidx(k, j, i)] = -1. / dxx * (Az(xc + 0.5 * dxx, yf) - Az(xc - 0.5 * dxx, yf));
             if (ndim > 2) fc(c, 2, b)[fidx(k, j, i)] = 0.0;
           }
   }
@@ -1926,6 +2200,12 @@ Real kmyo_step(void *h) {
   }
   s->set_global_dt();
   return dt;
+}
+
+// The tree update alone (tags from the last stage); 1 when the mesh changed.
+int kmyo_remesh(void *h, int allow_derefine) {
+  Sim *s = static_cast<Sim *>(h);
+  return s->amr && s->remesh(allow_derefine != 0) ? 1 : 0;
 }
 
 // Leaf list: level and logical location of each block (in block order).
