@@ -136,3 +136,17 @@ def blast_2d_amr(n: int = 128, nb: int = 16, precision: str = "fp64", numlevel: 
     d.set("kamayan/refinement0", "derefine_tol", derefine_tol)
     d.set("kamayan/refinement0", "max_level", numlevel - 1)
     return d
+
+
+def mhd_vortex_2d_amr(n: int = 64, nb: int = 8, numlevel: int = 2, refine_tol: float = 0.02,
+                      field: str = "pres", derefine_count: int = 2, precision: str = "fp64") -> Deck:
+    """The CT vortex on an adaptive mesh: Loehner tagging on pressure refines the
+    vortex core, and the core's motion refines and derefines blocks as it goes."""
+    d = mhd_vortex_2d(n=n, nb=nb, precision=precision)
+    d.set("parthenon/mesh", "refinement", "adaptive")
+    d.set("parthenon/mesh", "numlevel", numlevel)
+    d.set("parthenon/mesh", "derefine_count", derefine_count)
+    d.set("kamayan/refinement0", "field", field)
+    d.set("kamayan/refinement0", "refine_tol", refine_tol)
+    d.set("kamayan/refinement0", "derefine_tol", refine_tol / 4)
+    return d

@@ -179,6 +179,209 @@ __device__ __noinline__ double level_value(const MeshDesc &m, int L, int G0, int
   }
 }
 
+// Face arrays [3][nb][Pf] of one container.
+struct FaceField {
+  const void *p;
+  long long NF;  // nb * Pf
+  int f32;
+};
+__device__ __forceinline__ double ffetch(const FaceField &f, int e, long long n) {
+  const long long i = e * f.NF + n;
+  return f.f32 ? double(static_cast<const float *>(f.p)[i]) : static_cast<const double *>(f.p)[i];
+}
+
+// Global index along axis d of a face of component e at level L: along e
+// out-of-range faces clamp to the boundary face (or wrap when periodic),
+// across e the cell map applies; 0 in inactive dimensions.
+__device__ __forceinline__ int face_axis_map(const MeshDesc &m, int d, int e, int L, int Gd) {
+  if (d >= m.ndim) return 0;
+  const int N = m.mesh_nx[d] << L;
+  if (d == e) {
+    if (Gd >= 0 && Gd <= N) return Gd;
+    if (m.bc[d][Gd < 0 ? 0 : 1] == BC_PERIODIC) return ((Gd % N) + N) % N;
+    return Gd < 0 ? 0 : N;
+  }
+  bool fl = false;
+  return amr_map(Gd, N, m.bc[d][Gd < 0 ? 0 : 1], fl);
+}
+
+// Small fixed-size vectors held in registers (selects instead of indexed
+// local arrays) for the face recursion.
+struct I3 {
+  int v0, v1, v2;
+  __device__ __forceinline__ int operator[](int d) const { return d == 0 ? v0 : d == 1 ? v1 : v2; }
+  __device__ __forceinline__ void set(int d, int x) {
+    if (d == 0) v0 = x;
+    else if (d == 1) v1 = x;
+    else v2 = x;
+  }
+};
+struct R3 {
+  double v0, v1, v2;
+  __device__ __forceinline__ double operator[](int d) const { return d == 0 ? v0 : d == 1 ? v1 : v2; }
+  __device__ __forceinline__ void set(int d, double x) {
+    if (d == 0) v0 = x;
+    else if (d == 1) v1 = x;
+    else v2 = x;
+  }
+};
+
+// Every face_value evaluation a thread may make before it gives up (the
+// error flag is set and 0 returned), so a malformed tree cannot make a launch
+// run away.
+constexpr int kFaceBudget = 1 << 16;
+
+// Value of face component e at level L, global face index G (face index along
+// e, cell indices across).  Preference as for cells: the face of a level-L
+// leaf (its low face, else the high face of the leaf below it along e), the
+// area-weighted restriction of the finer leaves' faces on the same plane, or
+// a prolongation from level L-1: faces on a coarse face plane by minmod in
+// the plane (ProlongateSharedMinMod), faces inside a coarse cell by Toth & Roe
+// (ProlongateInternalTothAndRoe, refinement_operations.hpp:270-398).
+template <int D>
+__device__ __noinline__ double face_value(const MeshDesc &m, int e, int L, int G0, int G1, int G2,
+                                          const FaceField &f, int *err, int *calls) {
+  if (++*calls > kFaceBudget) {
+    *err = 3;
+    return 0.0;
+  }
+  const I3 M{face_axis_map(m, 0, e, L, G0), face_axis_map(m, 1, e, L, G1), face_axis_map(m, 2, e, L, G2)};
+  const bool act = e < m.ndim;
+  const I3 bx{M.v0 / m.nx[0], M.v1 / m.nx[1], M.v2 / m.nx[2]};
+  I3 bl = bx;
+  const int NBe = act ? (m.nbx[e] << L) : 1;
+  int ehi = -3, elo = -3;
+  if (bx[e] < NBe) {
+    const int q3[3] = {bx.v0, bx.v1, bx.v2};
+    ehi = table_at(m, L, q3);
+  }
+  if (act && M[e] % m.nx[e] == 0 && M[e] > 0) {
+    bl.set(e, bx[e] - 1);
+    const int q3[3] = {bl.v0, bl.v1, bl.v2};
+    elo = table_at(m, L, q3);
+  }
+  if (ehi >= 0 || elo >= 0) {
+    const I3 q = ehi >= 0 ? bx : bl;
+    int l0 = M.v0 - q.v0 * m.nx[0] + m.g[0], l1 = M.v1 - q.v1 * m.nx[1] + m.g[1], l2 = M.v2 - q.v2 * m.nx[2] + m.g[2];
+    if (ehi < 0) {
+      const int le = m.nx[e] + m.g[e];
+      if (e == 0) l0 = le;
+      else if (e == 1) l1 = le;
+      else l2 = le;
+    }
+    return ffetch(f, e, (long long)(ehi >= 0 ? ehi : elo) * m.Pf + fidx(m, l2, l1, l0));
+  }
+  if constexpr (D == 0) {
+    *err = 1;
+    return 0.0;
+  } else {
+    const int nd = m.ndim;
+    if (ehi == -1 || elo == -1) {  // finer leaves: restrict the fine faces on this plane
+      double area = 1.0;
+      for (int d = 0; d < 3; d++)
+        if (d != e) area *= d < nd ? m.dx[d] / double(1 << (L + 1)) : m.dx[d];
+      const int in0 = e != 0, in1 = e != 1 && nd > 1, in2 = e != 2 && nd > 2;
+      // slots (ok*4 + oj*2 + oi); at most two offsets vary for a face
+      double t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0;
+      double w0 = 0, w1 = 0, w2 = 0, w3 = 0, w4 = 0, w5 = 0, w6 = 0, w7 = 0;
+      for (int ok = 0; ok < 1 + in2; ok++)
+        for (int oj = 0; oj < 1 + in1; oj++)
+          for (int oi = 0; oi < 1 + in0; oi++) {
+            const double val = area * face_value<D - 1>(m, e, L + 1, 2 * M.v0 + oi, nd > 1 ? 2 * M.v1 + oj : 0,
+                                                        nd > 2 ? 2 * M.v2 + ok : 0, f, err, calls);
+            switch (ok * 4 + oj * 2 + oi) {
+              case 0: t0 = val; w0 = area; break;
+              case 1: t1 = val; w1 = area; break;
+              case 2: t2 = val; w2 = area; break;
+              case 3: t3 = val; w3 = area; break;
+              case 4: t4 = val; w4 = area; break;
+              case 5: t5 = val; w5 = area; break;
+              case 6: t6 = val; w6 = area; break;
+              default: t7 = val; w7 = area; break;
+            }
+          }
+      const double tvol = ((w0 + w2) + (w1 + w3)) + ((w4 + w6) + (w5 + w7));
+      return tvol > 0.0 ? (((t0 + t2) + (t1 + t3)) + ((t4 + t6) + (t5 + t7))) / tvol : 0.0;
+    }
+    if (L == 0) {
+      *err = 2;
+      return 0.0;
+    }
+    if (!act || M[e] % 2 == 0) {  // shared face: minmod in the coarse face's plane
+      I3 Mc{0, 0, 0}, o{0, 0, 0};
+      for (int d = 0; d < nd; d++) {
+        Mc.set(d, d == e ? M[d] / 2 : M[d] >> 1);
+        o.set(d, d == e ? 0 : M[d] & 1);
+      }
+      const double fc = face_value<D - 1>(m, e, L - 1, Mc.v0, Mc.v1, Mc.v2, f, err, calls);
+      R3 gq{0, 0, 0}, dfm{0, 0, 0}, dfp{0, 0, 0};
+      for (int d = 0; d < nd; d++) {
+        if (d == e) continue;
+        const double dxc = m.dx[d] / double(1 << (L - 1)), dxf = m.dx[d] / double(1 << L);
+        const double x0 = m.xmin[d];
+        I3 Gm = Mc, Gp = Mc;
+        Gm.set(d, Mc[d] - 1);
+        Gp.set(d, Mc[d] + 1);
+        const double fm = face_value<D - 1>(m, e, L - 1, Gm.v0, Gm.v1, Gm.v2, f, err, calls);
+        const double fp = face_value<D - 1>(m, e, L - 1, Gp.v0, Gp.v1, Gp.v2, f, err, calls);
+        const double xm = x0 + (double(Mc[d] - 1) + 0.5) * dxc;
+        const double xc = x0 + (double(Mc[d]) + 0.5) * dxc;
+        const double xp = x0 + (double(Mc[d] + 1) + 0.5) * dxc;
+        dfm.set(d, xc - (x0 + (double(2 * Mc[d]) + 0.5) * dxf));
+        dfp.set(d, (x0 + (double(2 * Mc[d] + 1) + 0.5) * dxf) - xc);
+        gq.set(d, grad_minmod(fc, fm, fp, xc - xm, xp - xc));
+      }
+      const double g1 = gq.v0, g2 = gq.v1, g3 = gq.v2;
+      const double d1m = dfm.v0, d1p = dfp.v0, d2m = dfm.v1, d2p = dfp.v1, d3m = dfm.v2, d3p = dfp.v2;
+      switch (o.v0 + 2 * o.v1 + 4 * o.v2) {
+        case 0: return fc - (g1 * d1m + g2 * d2m + g3 * d3m);
+        case 1: return fc + (g1 * d1p - g2 * d2m - g3 * d3m);
+        case 2: return fc - (g1 * d1m - g2 * d2p + g3 * d3m);
+        case 3: return fc + (g1 * d1p + g2 * d2p - g3 * d3m);
+        case 4: return fc - (g1 * d1m + g2 * d2m - g3 * d3p);
+        case 5: return fc + (g1 * d1p - g2 * d2m + g3 * d3p);
+        case 6: return fc - (g1 * d1m - g2 * d2p - g3 * d3p);
+        default: return fc + (g1 * d1p + g2 * d2p + g3 * d3p);
+      }
+    }
+    // internal face (odd along e): Toth & Roe from the level-L faces on the
+    // coarse cell's boundary; offsets oi along a0 = e, oj along a1, ok along
+    // a2, collapsed in inactive dimensions (where the operator's second write,
+    // offset 1, is the one that stays)
+    const int a0 = e, a1 = (e + 1) % 3, a2 = (e + 2) % 3;
+    const I3 f0{nd > 0 ? 2 * (M.v0 >> 1) : 0, nd > 1 ? 2 * (M.v1 >> 1) : 0, nd > 2 ? 2 * (M.v2 >> 1) : 0};
+    const I3 act3{nd > 0 ? 1 : 0, nd > 1 ? 1 : 0, nd > 2 ? 1 : 0};
+    auto fine = [&](int eidx, int ok, int oj, int oi) {
+      I3 P = f0;
+      P.set(a0, P[a0] + oi * act3[a0]);
+      P.set(a1, P[a1] + oj * act3[a1]);
+      P.set(a2, P[a2] + ok * act3[a2]);
+      return face_value<D - 1>(m, (e + eidx) % 3, L, P.v0, P.v1, P.v2, f, err, calls);
+    };
+    auto sg = [](int off) { return off == 0 ? -1.0 : 1.0; };
+    double Uxx = 0.0, Vxyz = 0.0, Wxyz = 0.0;
+    for (int vv = 0; vv < 2; vv++)
+      for (int u = 0; u <= 2; u += 2)
+        for (int t = 0; t < 2; t++) {
+          const double fine2 = fine(1, vv, u, t);
+          const double fine3 = fine(2, u, vv, t);
+          Uxx += sg(t) * sg(u) * (fine2 + fine3);
+          Vxyz += sg(t) * sg(u) * sg(vv) * fine2;
+          Wxyz += sg(t) * sg(u) * sg(vv) * fine3;
+        }
+    Uxx *= 0.125;
+    const double c0 = nd > 0 ? m.dx[0] / double(1 << (L - 1)) : m.dx[0];
+    const double c1 = nd > 1 ? m.dx[1] / double(1 << (L - 1)) : m.dx[1];
+    const double c2 = nd > 2 ? m.dx[2] / double(1 << (L - 1)) : m.dx[2];
+    const double dx2 = c0 * c0, dy2 = c1 * c1, dz2 = c2 * c2;
+    Vxyz *= 0.125 * dz2 / (dx2 + dz2);
+    Wxyz *= 0.125 * dy2 / (dx2 + dy2);
+    const int ok = act3[a2] ? M[a2] - f0[a2] : 1;
+    const int oj = act3[a1] ? M[a1] - f0[a1] : 1;
+    return 0.5 * (fine(0, ok, oj, 0) + fine(0, ok, oj, 2)) + Uxx + sg(ok) * Vxyz + sg(oj) * Wxyz;
+  }
+}
+
 template <typename S>
 __device__ __forceinline__ void store_value(S *arr, float *lo, long long n, double v) {
   if constexpr (sizeof(S) == 4) {
@@ -227,6 +430,7 @@ __global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, flo
     for (int v = 0; v < ncc; v++) {
       S val = cc[v * NP + s];
       if (v >= CMOM0 && v <= CMOM2 && flip[v - CMOM0]) val = -val;
+      if (v >= CMAGC0 && flip[v - CMAGC0]) val = -val;
       cc[v * NP + dst] = val;
     }
     if constexpr (F32) {
@@ -241,7 +445,7 @@ __global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, flo
   }
   for (int v = 0; v < ncc; v++) {
     const Field f{cc + v * NP, (F32 && v == CENER) ? lo : nullptr, F32};
-    const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : -1;
+    const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1);
     const double val = level_value<kMaxDepth>(m, L, G[0], G[1], G[2], f, fd, err);
     store_value<S>(cc + v * NP, v == CENER ? lo : nullptr, dst, val);
   }
@@ -396,7 +600,8 @@ __global__ void k_amr_remap(const __grid_constant__ MeshDesc mo, const S *occ, c
   const long long dst = (long long)q * mo.P + cidx(mo, k, j, i);
   for (int v = 0; v < ncc; v++) {
     const Field f{occ + v * NPo, (F32 && v == CENER) ? olo : nullptr, F32};
-    const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : -1, err);
+    const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1);
+    const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, fd, err);
     store_value<S>(ncc_out + v * NPn, v == CENER ? nlo : nullptr, dst, val);
   }
   for (int v = 0; v < NPRIM; v++) {
@@ -404,6 +609,143 @@ __global__ void k_amr_remap(const __grid_constant__ MeshDesc mo, const S *occ, c
     const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, v <= PVEL2 ? v : -1, err);
     store_value<S>(nprim + v * NPn, nullptr, dst, val);
   }
+}
+
+// Ghost faces of component e (active components only): the face value of
+// the position they cover.  The block's own faces, boundary faces included,
+// are left alone; the kernel reads only faces that leaves own.
+template <typename S>
+__global__ void k_amr_fill_ghost_faces(const __grid_constant__ MeshDesc m, S *fc, int e, int *err) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)m.nb * m.Pf) return;
+  const int b = int(t / m.Pf);
+  long long r = t - (long long)b * m.Pf;
+  const int i = int(r % m.nf[0]);
+  r /= m.nf[0];
+  const int j = int(r % m.nf[1]);
+  const int k = int(r / m.nf[1]);
+  const int loc[3] = {i, j, k};
+  for (int d = 0; d < 3; d++)
+    if (loc[d] >= m.np[d] + (d == e ? 1 : 0)) return;  // outside this component's extent
+  bool interior = true;
+  for (int d = 0; d < 3; d++) {
+    const int hi = m.g[d] + m.nx[d] - 1 + (d == e ? 1 : 0);
+    if (loc[d] < m.g[d] || loc[d] > hi) interior = false;
+  }
+  if (interior) return;
+  int G[3];
+  for (int d = 0; d < 3; d++) G[d] = m.bloc[3 * b + d] * m.nx[d] + (loc[d] - m.g[d]);
+  const FaceField f{fc, (long long)m.nb * m.Pf, sizeof(S) == 4};
+  int calls = 0;
+  const double v = face_value<kMaxDepth>(m, e, m.blev[b], G[0], G[1], G[2], f, err, &calls);
+  fc[e * f.NF + (long long)b * m.Pf + fidx(m, k, j, i)] = S(v);
+}
+
+// Edge-EMF correction at fine/coarse boundaries (the face-field part of the
+// flux correction, kamayan_driver.cpp:198-207).  An edge on a block's boundary
+// where any of the cells around it (four in 3D, the four quadrants of a
+// corner in 2D) is covered by finer leaves takes the length-weighted
+// restriction of the collinear fine EMFs, read from the fine leaf holding the
+// first such cell (order (-,-), (+,-), (-,+), (+,+) over the edge's two
+// transverse axes).  Every block holding the edge computes the same value, so
+// same-level neighbours keep identical copies of their shared faces.  Reads
+// the EMFs as computed (eo), writes the corrected ones (emf).
+template <typename S>
+__global__ void k_emf_correct(const __grid_constant__ MeshDesc m, const S *eo, S *emf, int E) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (tid >= (long long)m.nb * 3 * E) return;
+  const int b = int(tid / (3ll * E));
+  const int rr = int(tid - (long long)b * 3 * E);
+  const int t = rr / E, idx = rr % E;
+  if (m.ndim == 2 && t != 2) return;  // 2D has z-edges only
+  const int p = (t + 1) % 3, q = (t + 2) % 3;
+  const int np_ = m.nx[p] + 1, nq_ = m.nx[q] + 1;
+  const int ap = idx % np_, aq = (idx / np_) % nq_, at = idx / (np_ * nq_);
+  if (at >= m.nx[t]) return;
+  if (ap != 0 && ap != m.nx[p] && aq != 0 && aq != m.nx[q]) return;  // not on the block boundary
+  const int L = m.blev[b];
+  const int *bl = m.bloc + 3 * b;
+  const int Ep = bl[p] * m.nx[p] + ap, Eq = bl[q] * m.nx[q] + aq, Et = bl[t] * m.nx[t] + at;
+  const long long NF = (long long)m.nb * m.Pf;
+  for (int s = 0; s < 4; s++) {
+    const int dp = s & 1, dq = s >> 1;
+    int Gc[3];
+    Gc[p] = Ep - 1 + dp;
+    Gc[q] = Eq - 1 + dq;
+    Gc[t] = Et;
+    bool skip = false;
+    for (int w = 0; w < 2; w++) {
+      const int d = w ? q : p;
+      const int N = m.mesh_nx[d] << L;
+      if (Gc[d] < 0 || Gc[d] >= N) {
+        if (m.bc[d][Gc[d] < 0 ? 0 : 1] != BC_PERIODIC) skip = true;
+        else Gc[d] = ((Gc[d] % N) + N) % N;
+      }
+    }
+    if (skip) continue;
+    int bxc[3];
+    for (int d = 0; d < 3; d++) bxc[d] = Gc[d] / m.nx[d];
+    if (table_at(m, L, bxc) != -1) continue;
+    int Fc[3];
+    Fc[p] = 2 * Gc[p] + (dp ? 0 : 1);
+    Fc[q] = 2 * Gc[q] + (dq ? 0 : 1);
+    Fc[t] = t < m.ndim ? 2 * Et : 0;
+    double tt[8] = {0, 0, 0, 0, 0, 0, 0, 0}, vv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool ok = true;
+    for (int o = 0; o < 1 + (t < m.ndim); o++) {
+      int Ff[3] = {Fc[0], Fc[1], Fc[2]};
+      Ff[t] += o;
+      int bf[3];
+      for (int d = 0; d < 3; d++) bf[d] = Ff[d] / m.nx[d];
+      const int fe = table_at(m, L + 1, bf);
+      if (fe < 0) {
+        ok = false;
+        break;
+      }
+      int lf[3];
+      for (int d = 0; d < 3; d++) lf[d] = Ff[d] - bf[d] * m.nx[d] + m.g[d];
+      if (!dp) lf[p] += 1;
+      if (!dq) lf[q] += 1;
+      const int slot = t == 0 ? o : t == 1 ? 2 * o : 4 * o;
+      const double len = blk_dx(m, fe, t);
+      vv[slot] = len;
+      tt[slot] = len * double(eo[t * NF + (long long)fe * m.Pf + fidx(m, lf[2], lf[1], lf[0])]);
+    }
+    if (!ok) continue;
+    int le[3];
+    le[p] = m.g[p] + ap;
+    le[q] = m.g[q] + aq;
+    le[t] = m.g[t] + at;
+    emf[t * NF + (long long)b * m.Pf + fidx(m, le[2], le[1], le[0])] = S(restrict8(tt, vv));
+    return;
+  }
+}
+
+// Faces of the new leaves after a remesh, every component, boundary faces
+// included: the face value of the old mesh.
+template <typename S>
+__global__ void k_amr_remap_faces(const __grid_constant__ MeshDesc mo, const S *ofc, int nnew, const int *nlev,
+                                  const int *nloc, S *nfc, int *err) {
+  const long long per = (long long)(mo.nx[0] + 1) * (mo.nx[1] + 1) * (mo.nx[2] + 1);
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= per * 3 * nnew) return;
+  const int q = int(t / (per * 3));
+  long long r = t - (long long)q * per * 3;
+  const int e = int(r / per);
+  r -= (long long)e * per;
+  const int i = int(r % (mo.nx[0] + 1));
+  r /= (mo.nx[0] + 1);
+  const int j = int(r % (mo.nx[1] + 1));
+  const int k = int(r / (mo.nx[1] + 1));
+  // own faces: nx + 1 along e when e is active, nx across
+  const int ext[3] = {mo.nx[0] + (e == 0 ? 1 : 0), mo.nx[1] + (e == 1 && mo.ndim > 1 ? 1 : 0),
+                      mo.nx[2] + (e == 2 && mo.ndim > 2 ? 1 : 0)};
+  if (i >= ext[0] || j >= ext[1] || k >= ext[2]) return;
+  const int G0 = nloc[3 * q] * mo.nx[0] + i, G1 = nloc[3 * q + 1] * mo.nx[1] + j, G2 = nloc[3 * q + 2] * mo.nx[2] + k;
+  const FaceField f{ofc, (long long)mo.nb * mo.Pf, sizeof(S) == 4};
+  int calls = 0;
+  const double v = face_value<kMaxDepth>(mo, e, nlev[q], G0, G1, G2, f, err, &calls);
+  nfc[e * (long long)nnew * mo.Pf + (long long)q * mo.Pf + fidx(mo, k + mo.g[2], j + mo.g[1], i + mo.g[0])] = S(v);
 }
 
 // Morton key of a leaf's lower corner at the finest level, level in the low bits.
@@ -508,8 +850,46 @@ int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct) {
     k_amr_fill_ghosts<float><<<nblk(n), kThreads, 0, c->stream>>>(m, (float *)ct.cc, (float *)ct.ener_lo,
                                                                   (float *)c->prim, c->ncc, c->amr.d_err);
   c->launches++;
+  if (c->prm.mhd) {
+    const long long nf = (long long)m.nb * m.Pf;
+    for (int e = 0; e < m.ndim; e++) {
+      if (c->esz == 8)
+        k_amr_fill_ghost_faces<double><<<nblk(nf), kThreads, 0, c->stream>>>(m, (double *)ct.fc, e, c->amr.d_err);
+      else
+        k_amr_fill_ghost_faces<float><<<nblk(nf), kThreads, 0, c->stream>>>(m, (float *)ct.fc, e, c->amr.d_err);
+      c->launches++;
+    }
+  }
   return cuda_check(c, cudaGetLastError(), "amr fill_ghosts");
 }
+
+int launch_emf_correct(kmy_ctx *c, Container &md0) {
+  const MeshDesc &m = c->m;
+  AmrHost &a = c->amr;
+  if (!c->prm.mhd || m.ndim < 2 || !md0.emf) return KMY_OK;
+  const size_t bytes = c->esz * 3 * size_t(m.nb) * m.Pf;
+  if (a.emf_tmp_bytes != bytes) {
+    dfree(c, a.d_emf_tmp);
+    a.d_emf_tmp = nullptr;
+    a.emf_tmp_bytes = 0;
+    const int rc = dalloc(c, &a.d_emf_tmp, bytes);
+    if (rc) return rc;
+    a.emf_tmp_bytes = bytes;
+  }
+  int rc = cuda_check(c, cudaMemcpyAsync(a.d_emf_tmp, md0.emf, bytes, cudaMemcpyDeviceToDevice, c->stream),
+                      "emf copy");
+  if (rc) return rc;
+  int E = 1;
+  for (int t = 0; t < 3; t++) E = std::max(E, (m.nx[(t + 1) % 3] + 1) * (m.nx[(t + 2) % 3] + 1) * m.nx[t]);
+  const long long n = (long long)m.nb * 3 * E;
+  if (c->esz == 8)
+    k_emf_correct<double><<<nblk(n), kThreads, 0, c->stream>>>(m, (const double *)a.d_emf_tmp, (double *)md0.emf, E);
+  else
+    k_emf_correct<float><<<nblk(n), kThreads, 0, c->stream>>>(m, (const float *)a.d_emf_tmp, (float *)md0.emf, E);
+  c->launches++;
+  return cuda_check(c, cudaGetLastError(), "emf_correct");
+}
+
 
 int launch_flux_correct(kmy_ctx *c) {
   const MeshDesc &m = c->m;
@@ -567,7 +947,7 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
   if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "amr tags sync");
   if (rc) return rc;
   if (err) {
-    c->err = "adaptive mesh: level value recursion exceeded its depth (mesh not 2:1 balanced)";
+    c->err = "adaptive mesh: a level-value evaluation exceeded its depth or call budget (mesh not 2:1 balanced)";
     return KMY_ERR_STATE;
   }
   typedef std::array<int, 4> Key;  // level, location
@@ -688,6 +1068,9 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
   if (!rc) rc = dalloc(c, &nb_ct.cc, c->esz * c->ncc * n_new);
   if (!rc && c->esz == 4) rc = dalloc(c, &nb_ct.ener_lo, 4 * n_new);
   if (!rc) rc = dalloc(c, &nprim, c->esz * NPRIM * n_new);
+  const size_t nf_new = size_t(nnew) * m.Pf;
+  if (!rc && c->prm.mhd) rc = dalloc(c, &nb_ct.fc, c->esz * 3 * nf_new);
+  if (!rc && c->prm.mhd) rc = dalloc(c, &nb_ct.emf, c->esz * 3 * nf_new);
   if (!rc)
     rc = cuda_check(c, cudaMemcpyAsync(d_nlev, nlev.data(), sizeof(int) * nnew, cudaMemcpyHostToDevice, c->stream),
                     "remap levels");
@@ -706,6 +1089,16 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
         mo, (const float *)ob.cc, (const float *)ob.ener_lo, (const float *)c->prim, nnew, d_nlev, d_nloc,
         (float *)nb_ct.cc, (float *)nb_ct.ener_lo, (float *)nprim, c->ncc, a.d_err);
   c->launches++;
+  if (c->prm.mhd) {
+    const long long faces = (long long)(m.nx[0] + 1) * (m.nx[1] + 1) * (m.nx[2] + 1) * 3 * nnew;
+    if (c->esz == 8)
+      k_amr_remap_faces<double><<<nblk(faces), kThreads, 0, c->stream>>>(mo, (const double *)ob.fc, nnew, d_nlev,
+                                                                         d_nloc, (double *)nb_ct.fc, a.d_err);
+    else
+      k_amr_remap_faces<float><<<nblk(faces), kThreads, 0, c->stream>>>(mo, (const float *)ob.fc, nnew, d_nlev,
+                                                                        d_nloc, (float *)nb_ct.fc, a.d_err);
+    c->launches++;
+  }
   rc = cuda_check(c, cudaGetLastError(), "amr remap");
   if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "amr remap sync");
   if (rc) return rc;
@@ -721,6 +1114,13 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
   dfree(c, c->prim);
   dfree(c, c->flux);
   c->flux = nullptr;
+  if (c->prm.mhd) {
+    // div B at the new block count (recomputed on the next last stage)
+    dfree(c, c->divb);
+    c->divb = nullptr;
+    rc = dalloc(c, reinterpret_cast<void **>(&c->divb), 8 * n_new);
+    if (rc) return rc;
+  }
   dfree(c, d_nlev);
   dfree(c, d_nloc);
   a.lev = nlev;

@@ -164,7 +164,6 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   amr.on = numlevel > 1 && !amr.crits.empty();
   if (amr.on) {
     if (numlevel > 8) return bad("parthenon/mesh/numlevel: at most 8 levels");
-    if (p.mhd) return bad("adaptive meshes are supported for hydro only");
     amr.numlevel = numlevel;
     amr.max_level = numlevel - 1;
     amr.derefine_count = p.integer("parthenon/mesh/derefine_count", 10);
@@ -695,6 +694,7 @@ static int task_stage(kmy_ctx *c, int stage, double dt) {
   int rc = launch_compute_fluxes(c, md0);
   if (!rc && c->amr.on) rc = launch_flux_correct(c);
   if (!rc) rc = launch_compute_emf(c, md0);
+  if (!rc && c->amr.on) rc = launch_emf_correct(c, md0);
   if (!rc) rc = launch_flux_divergence(c, md0, du);
   if (!rc) rc = launch_apply_dudt(c, base, md0, md1, du, c->prm.beta[stage - 1], dt,
                                   dt < 0 ? &c->clock->dt : nullptr);

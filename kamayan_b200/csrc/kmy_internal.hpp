@@ -145,6 +145,8 @@ struct AmrHost {
   std::vector<int> cnt;  // consecutive derefine tags per leaf
   int *d_blev = nullptr, *d_bloc = nullptr, *d_tabs = nullptr, *d_tags = nullptr;
   int *d_err = nullptr;  // set by a level-value recursion that ran out of depth
+  void *d_emf_tmp = nullptr;  // EMFs as computed, read by the edge correction
+  size_t emf_tmp_bytes = 0;
 };
 
 }  // namespace kmy
@@ -214,6 +216,7 @@ int amr_setup(kmy_ctx *c);
 int amr_upload(kmy_ctx *c);
 int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct);
 int launch_flux_correct(kmy_ctx *c);
+int launch_emf_correct(kmy_ctx *c, Container &md0);
 int launch_amr_tag(kmy_ctx *c, Container &ct);
 int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed);
 

@@ -112,10 +112,11 @@ __global__ void k_pgen_faces(MeshDesc m, PgenParams pp, S *fc) {
   r /= n0;
   const int j = int(r % n1);
   const int k = int(r / n1);
-  const int lx0 = b % m.nbx[0], lx1 = (b / m.nbx[0]) % m.nbx[1];
-  const double xf = m.xmin[0] + double(lx0 * m.nx[0] + i) * m.dx[0];
-  const double yf = m.xmin[1] + double(lx1 * m.nx[1] + j) * m.dx[1];
-  const double xc = xf + 0.5 * m.dx[0], yc = yf + 0.5 * m.dx[1];
+  const int lx0 = blk_loc(m, b, 0), lx1 = blk_loc(m, b, 1);
+  const double dx0 = blk_dx(m, b, 0), dx1 = blk_dx(m, b, 1);
+  const double xf = m.xmin[0] + double(lx0 * m.nx[0] + i) * dx0;
+  const double yf = m.xmin[1] + double(lx1 * m.nx[1] + j) * dx1;
+  const double xc = xf + 0.5 * dx0, yc = yf + 0.5 * dx1;
   const double B0 = 1.0 / sqrt(4.0 * M_PI);
   auto Az = [&](double X, double Y) {
     if (pp.problem == P_VORTEX)  // isentropic_vortex.hpp:140-144
@@ -126,8 +127,8 @@ __global__ void k_pgen_faces(MeshDesc m, PgenParams pp, S *fc) {
   const long long NF = (long long)m.nb * m.Pf;
   const long long o = (long long)b * m.Pf +
                       ((long long)(k + m.g[2]) * m.nf[1] + (j + m.g[1])) * m.nf[0] + (i + m.g[0]);
-  fc[o] = S(1. / m.dx[1] * (Az(xf, yc + 0.5 * m.dx[1]) - Az(xf, yc - 0.5 * m.dx[1])));
-  fc[NF + o] = S(-1. / m.dx[0] * (Az(xc + 0.5 * m.dx[0], yf) - Az(xc - 0.5 * m.dx[0], yf)));
+  fc[o] = S(1. / dx1 * (Az(xf, yc + 0.5 * dx1) - Az(xf, yc - 0.5 * dx1)));
+  fc[NF + o] = S(-1. / dx0 * (Az(xc + 0.5 * dx0, yf) - Az(xc - 0.5 * dx0, yf)));
   if (m.ndim > 2) fc[2 * NF + o] = S(0);
 }
 

@@ -397,11 +397,11 @@ __global__ void k_flux_stokes(MeshDesc m, const S *emf, S *dufc, int face, int n
     int ijk[3] = {i, j, k};
     ijk[axis] += 1;
     const S sign = ((axis + 1) % 3 == edge) ? S(1.0) : S(-1.0);
-    const S L = S(m.dx[edge]);
+    const S L = S(blk_dx(m, b, edge));
     const S *E = emf + edge * NF + bo;
     out += sign * (L * E[fidx(m, k, j, i)] - L * E[fidx(m, ijk[2], ijk[1], ijk[0])]);
   }
-  out *= S(1.) / (S(m.area[face]) + S(1.e-36));
+  out *= S(1.) / (S(blk_area(m, b, face)) + S(1.e-36));
   dufc[face * NF + bo + fidx(m, k, j, i)] = out;
 }
 
@@ -532,17 +532,17 @@ template <typename S>
 __device__ __forceinline__ void face_average(const MeshDesc &m, const S *fc, int b, int k, int j,
                                              int i, S *B) {
   const long long NF = (long long)m.nb * m.Pf, bo = (long long)b * m.Pf;
-  const S vol = S(m.vol);
+  const S vol = S(blk_vol(m, b));
+  const S a0 = S(blk_area(m, b, 0)), a1 = S(blk_area(m, b, 1)), a2 = S(blk_area(m, b, 2));
   if (m.ndim > 1) {
-    B[0] = S(0.5) * S(m.dx[0]) *
-           (S(m.area[0]) * fc[bo + fidx(m, k, j, i + 1)] + S(m.area[0]) * fc[bo + fidx(m, k, j, i)]) / vol;
-    B[1] = S(0.5) * S(m.dx[1]) *
-           (S(m.area[1]) * fc[NF + bo + fidx(m, k, j + 1, i)] + S(m.area[1]) * fc[NF + bo + fidx(m, k, j, i)]) / vol;
+    B[0] = S(0.5) * S(blk_dx(m, b, 0)) *
+           (a0 * fc[bo + fidx(m, k, j, i + 1)] + a0 * fc[bo + fidx(m, k, j, i)]) / vol;
+    B[1] = S(0.5) * S(blk_dx(m, b, 1)) *
+           (a1 * fc[NF + bo + fidx(m, k, j + 1, i)] + a1 * fc[NF + bo + fidx(m, k, j, i)]) / vol;
   }
   if (m.ndim > 2) {
-    B[2] = S(0.5) * S(m.dx[2]) *
-           (S(m.area[2]) * fc[2 * NF + bo + fidx(m, k + 1, j, i)] +
-            S(m.area[2]) * fc[2 * NF + bo + fidx(m, k, j, i)]) / vol;
+    B[2] = S(0.5) * S(blk_dx(m, b, 2)) *
+           (a2 * fc[2 * NF + bo + fidx(m, k + 1, j, i)] + a2 * fc[2 * NF + bo + fidx(m, k, j, i)]) / vol;
   }
 }
 
@@ -746,10 +746,10 @@ __global__ void k_divb(MeshDesc m, const S *fc, double *divb) {
   double d = 0.;
   for (int dir = 0; dir < m.ndim; dir++) {
     const int kp = k + (dir == 2), jp = j + (dir == 1), ip = i + (dir == 0);
-    d += m.area[dir] * double(fc[dir * NF + bo + fidx(m, kp, jp, ip)]) -
-         m.area[dir] * double(fc[dir * NF + bo + fidx(m, k, j, i)]);
+    d += blk_area(m, b, dir) * double(fc[dir * NF + bo + fidx(m, kp, jp, ip)]) -
+         blk_area(m, b, dir) * double(fc[dir * NF + bo + fidx(m, k, j, i)]);
   }
-  divb[(long long)b * m.P + cidx(m, k, j, i)] = d / m.vol;
+  divb[(long long)b * m.P + cidx(m, k, j, i)] = d / blk_vol(m, b);
 }
 
 int launch_fill_derived(kmy_ctx *c, Container &md) {

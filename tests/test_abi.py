@@ -71,13 +71,10 @@ def test_null_arguments(kmy_lib):
     ("kamayan/refinement0", "method", "derivative_order_1"),
     ("kamayan/refinement0", "field", "velocity"),
     ("parthenon/mesh", "numlevel", "9"),
-    ("physics", "MHD", "ct"),
     ("parthenon/mesh", "refinement", "static"),
 ])
 def test_bad_adaptive_parameters_rejected(kmy_lib, block, key, value):
     d = configs.blast_2d_amr(n=64, nb=8)
     d.set(block, key, value)
-    if (block, key) == ("physics", "MHD"):
-        d.set("parthenon/mesh", "nghost", 4)
     assert _create(d.text()) == 1
 
