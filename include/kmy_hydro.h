@@ -56,13 +56,14 @@ typedef struct {
  * <material/single> (gamma, Abar, eos_type), <eos> (mode_init), plus
  * <kamayan_b200> (precision = fp64|fp32).  Unknown option values fail with
  * KMY_ERR_BAD_PARAM.
- * Adaptive meshes (hydro): <parthenon/mesh> refinement = adaptive, numlevel
- * (<= 8), derefine_count, and a <kamayan/refinement0> block with field
- * (dens|pres|ener), method = loehner, refine_tol, derefine_tol, filter,
- * max_level (src/grid/grid.cpp:43-48, :90-124; src/grid/grid_refinement.cpp:15-30).
- * Blocks then carry a level and a logical location (kmy_get_blocks) and the
- * block count changes as the mesh adapts; the step runs the per-task kernels
- * with flux correction, Loehner tagging and a remesh after each step.
+ * Adaptive meshes (hydro and CT): <parthenon/mesh> refinement = adaptive, numlevel
+ * (<= 8), derefine_count, and <kamayan/refinement0>, <kamayan/refinement1>, ...
+ * blocks, each with field (dens|pres|ener), method = loehner, refine_tol,
+ * derefine_tol, filter, max_level (src/grid/grid.cpp:43-48, :90-124;
+ * src/grid/grid_refinement.cpp:15-30).  Blocks then carry a level and a logical
+ * location (kmy_get_blocks) and the block count changes as the mesh adapts; the
+ * step runs the per-task kernels with flux (and, with CT, EMF) correction,
+ * Loehner tagging and a remesh after each step.
  * Replaces: InitEnv/InitPackages parameter setup (src/kamayan/kamayan.cpp:20-138),
  * hydro::SetupParams (src/physics/hydro/hydro.cpp:51-92),
  * grid::SetupParams (src/grid/grid.cpp:169-262),
