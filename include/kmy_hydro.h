@@ -153,6 +153,19 @@ int kmy_get_time(const kmy_ctx *ctx, double *time, double *dt, double *dt_est, i
  * Replaces: Parthenon MeshBlock::loc / LogicalLocation of each block of the
  * MeshData (used by the refinement tasks, src/grid/grid_refinement.cpp:30-152). */
 int kmy_get_blocks(const kmy_ctx *ctx, int *levels, int *locations, int max_blocks, int *nblocks);
+
+/* ---- restart files ----------------------------------------------------------
+ * kmy_save_restart writes the context's state to `path`: the deck, the "base"
+ * container as stored, the shared primitives, the face field and div B with
+ * CT, the device clock and time limits, and the leaf list of an adaptive
+ * mesh.  kmy_load_restart creates a new context on `device` from such a file;
+ * it continues exactly as the saved context would have (same bits).  Files
+ * are for the same build of the library (native byte order, raw arrays).
+ * Replaces: Parthenon restart outputs (<parthenon/output*> file_type = rst,
+ * src/problems/isentropic_vortex.in:40-43, variables flagged Metadata::Restart
+ * in src/kamayan/fields.hpp:160-161) and the driver's restart path (-r). */
+int kmy_save_restart(kmy_ctx *ctx, const char *path);
+int kmy_load_restart(const char *path, int device, kmy_ctx **out);
 /* Override the dt used by the next kmy_step (e.g. to replay a reference run). */
 int kmy_set_dt(kmy_ctx *ctx, double dt);
 /* Select the stepping path used by kmy_step/kmy_evolve: 0 = fused, 1 = tasks. */

@@ -34,7 +34,7 @@ EXPORTS = (
     "kmy_compute_fluxes", "kmy_compute_emf", "kmy_flux_divergence", "kmy_apply_dudt",
     "kmy_prepare_primitive", "kmy_fill_ghosts", "kmy_estimate_dt", "kmy_fill_derived",
     "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_end_step", "kmy_get_time",
-    "kmy_get_blocks", "kmy_set_dt",
+    "kmy_get_blocks", "kmy_set_dt", "kmy_save_restart", "kmy_load_restart",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
     "kmy_conserved_sums_noalloc",
     "kmy_server_create", "kmy_server_destroy", "kmy_server_last_error", "kmy_server_submit",
@@ -96,6 +96,8 @@ def lib() -> ctypes.CDLL:
         L.kmy_end_step.argtypes = [vp]
         L.kmy_get_time.argtypes = [vp, _dp, _dp, _dp, ctypes.POINTER(i)]
         L.kmy_get_blocks.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i), i, ctypes.POINTER(i)]
+        L.kmy_save_restart.argtypes = [vp, cp]
+        L.kmy_load_restart.argtypes = [cp, i, ctypes.POINTER(vp)]
         L.kmy_set_dt.argtypes = [vp, d]
         L.kmy_set_path.argtypes = [vp, i]
         L.kmy_vortex_error.argtypes = [vp, i, i, _dp]
@@ -125,12 +127,15 @@ def _ptr(a: np.ndarray):
 class Solver:
     """One mesh with its device-resident stage containers (one ``kmy_ctx``)."""
 
-    def __init__(self, deck: str | Deck, device: int = 0):
-        text = deck.text() if isinstance(deck, Deck) else deck
-        h = ctypes.c_void_p()
-        rc = lib().kmy_create(text.encode(), device, ctypes.byref(h))
-        if rc:
-            raise KmyError(rc, "kmy_create rejected the deck (see stderr)")
+    def __init__(self, deck: str | Deck | None, device: int = 0, _handle=None):
+        if _handle is not None:
+            h = _handle
+        else:
+            text = deck.text() if isinstance(deck, Deck) else deck
+            h = ctypes.c_void_p()
+            rc = lib().kmy_create(text.encode(), device, ctypes.byref(h))
+            if rc:
+                raise KmyError(rc, "kmy_create rejected the deck (see stderr)")
         self._h = h
         self._info = Info()
         self.ndim = self.info.ndim
@@ -155,6 +160,19 @@ class Solver:
     def face_shape(self) -> tuple:
         i = self.info
         return (i.nblocks, i.nfaces_pad[2], i.nfaces_pad[1], i.nfaces_pad[0])
+
+    def save_restart(self, path: str) -> None:
+        """Write the state needed to resume this solve (kmy_save_restart)."""
+        self._check(lib().kmy_save_restart(self._h, str(path).encode()))
+
+    @classmethod
+    def from_restart(cls, path: str, device: int = 0) -> "Solver":
+        """A new solver that resumes from a restart file (kmy_load_restart)."""
+        h = ctypes.c_void_p()
+        rc = lib().kmy_load_restart(str(path).encode(), device, ctypes.byref(h))
+        if rc:
+            raise KmyError(rc, f"kmy_load_restart failed for {path} (see stderr)")
+        return cls(None, device, _handle=h)
 
     def blocks(self) -> tuple[np.ndarray, np.ndarray]:
         """Leaf blocks in block order: levels (nb,) and logical locations (nb, 3)."""

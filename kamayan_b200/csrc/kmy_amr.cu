@@ -1140,3 +1140,32 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
 }
 
 }  // namespace kmy
+
+namespace kmy {
+
+int amr_adopt_leaves(kmy_ctx *c) {
+  for (auto &kv : c->md) {
+    dfree(c, kv.second.cc);
+    dfree(c, kv.second.ener_lo);
+    dfree(c, kv.second.fc);
+    dfree(c, kv.second.emf);
+  }
+  c->md.clear();
+  dfree(c, c->prim);
+  c->prim = nullptr;
+  dfree(c, c->flux);
+  c->flux = nullptr;
+  dfree(c, c->divb);
+  c->divb = nullptr;
+  int rc = amr_upload(c);
+  if (rc) return rc;
+  const size_t n = size_t(c->m.nb) * c->m.P;
+  const auto &nm = c->prm.stage_name;
+  for (size_t s = 0; s + 1 < nm.size() && !rc; s++)
+    if (!c->md.count(nm[s])) rc = make_container(c, nm[s]);
+  if (!rc) rc = dalloc(c, &c->prim, c->esz * NPRIM * n);
+  if (!rc && c->prm.mhd) rc = dalloc(c, reinterpret_cast<void **>(&c->divb), 8 * n);
+  return rc;
+}
+
+}  // namespace kmy

@@ -415,6 +415,7 @@ int kmy_create(const char *deck, int device, kmy_ctx **out) {
   *out = nullptr;
   auto *c = new kmy_ctx();
   c->device = device;
+  c->deck_text = deck ? deck : "";
   int rc = setup_params(c, deck);
   if (rc) {
     std::fprintf(stderr, "kmy_create: %s\n", c->err.c_str());

@@ -176,6 +176,7 @@ struct kmy_ctx {
   kmy::AmrHost amr;          // adaptive mesh (task path only)
   int64_t launches = 0;
   std::string err;
+  std::string deck_text;  // the deck the context was created from (restart files carry it)
   std::vector<void *> allocations;
 };
 
@@ -219,6 +220,9 @@ int launch_flux_correct(kmy_ctx *c);
 int launch_emf_correct(kmy_ctx *c, Container &md0);
 int launch_amr_tag(kmy_ctx *c, Container &ct);
 int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed);
+// Storage for the leaf list already in c->amr (lev, loc, cnt): level tables,
+// every stage container, the primitives and div B at the new block count.
+int amr_adopt_leaves(kmy_ctx *c);
 
 // Device footprint and kernel class of a deck (kmy_api.cu), for admission.
 struct Footprint {
