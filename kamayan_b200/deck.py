@@ -56,6 +56,29 @@ class Deck:
             self.set(b, key, v.strip())
         return self
 
+    def __setitem__(self, block: str, values) -> None:
+        """``deck["hydro"] = {"reconstruction": "wenoz"}``: set several keys of a
+        block at once, the way the reference's KamayanParams does
+        (python/kamayan/code_units/parameters.py, ``__setitem__``)."""
+        for k, v in values.items():
+            self.set(block, k, v)
+
+    def __getitem__(self, block: str) -> dict:
+        return dict(self.blocks.get(block, {}))
+
+    def write(self, path, problem_id: str | None = None) -> None:
+        """Write the deck as an input file.  With ``problem_id`` the file opens
+        with a ``<parthenon/job>`` block naming it, as the reference's
+        KamayanManager.write_input does (python/kamayan/kamayan_manager.py:123-156)."""
+        d = self.copy()
+        if problem_id is not None:
+            rest = OrderedDict((b, kv) for b, kv in d.blocks.items() if b != "parthenon/job")
+            job = OrderedDict(d.blocks.get("parthenon/job", {}))
+            job["problem_id"] = str(problem_id)
+            d.blocks = OrderedDict([("parthenon/job", job)] + list(rest.items()))
+        with open(path, "w") as f:
+            f.write(d.text())
+
     def copy(self) -> "Deck":
         return Deck({b: dict(kv) for b, kv in self.blocks.items()})
 

@@ -42,3 +42,19 @@ def test_workload_decks():
     assert v.get("parthenon/meshblock", "nx1") == "64" and v.get("parthenon/mesh", "nghost") == "2"
     ot = configs.ot_3d()
     assert ot.get("physics", "MHD") == "ct" and ot.get("parthenon/mesh", "nghost") == "4"
+
+
+def test_block_assignment_and_input_file(tmp_path):
+    # the reference's params["block"] = {...} form and its write_input layout
+    d = Deck()
+    d["hydro"] = {"reconstruction": "wenoz", "cfl": 0.4}
+    d["parthenon/mesh"] = {"nx1": 64}
+    assert d["hydro"] == {"reconstruction": "wenoz", "cfl": "0.4"}
+    f = tmp_path / "run.in"
+    d.write(f, problem_id="vortex")
+    text = f.read_text()
+    assert text.splitlines()[0] == "<parthenon/job>"
+    assert "problem_id = vortex" in text
+    back = Deck.parse(text)
+    assert back.get("hydro", "reconstruction") == "wenoz"
+    assert back.get("parthenon/mesh", "nx1") == "64"
