@@ -163,6 +163,79 @@ __device__ __forceinline__ void ReconstructBoth(int limiter, const R (&s)[5], R 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32.  sm_100 issues one add, multiply or fma instruction for both
+// lanes of a float2, so the FP32 fused stage reconstructs two cells per
+// thread.  Reciprocals stay per lane (rcp.approx on the XU pipe).
+__device__ __forceinline__ float2 p2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float2 prcp(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
+
+// WENO-Z weight factor on two lanes: 1 + min((tau/(eps+beta))^2, 1e30).
+// Capping the square at 1e30 is the FP32 cap of the ratio at 1e15 (weno_q),
+// and tau's sign drops out of the square, so tau may be b2 - b0 unsigned.
+__device__ __forceinline__ float2 weno_q2(float2 tau, float2 beta) {
+  const float2 r = pmul(tau, prcp(padd(p2(1.e-36f), beta)));
+  float2 r2 = pmul(r, r);
+  r2.x = fminf(r2.x, 1.0e30f);
+  r2.y = fminf(r2.y, 1.0e30f);
+  return padd(p2(1.f), r2);
+}
+
+// WENO-Z at both faces of two cells (reconstruction.hpp:104-142): the
+// reference's candidate stencils, smoothness indicators and weights, with
+// the 1/6 of the candidates folded into their coefficients and the
+// normalisation done by one reciprocal per face value.
+__device__ __forceinline__ void WenoZBoth2(const float2 (&s)[5], float2 &vM, float2 &vP) {
+  const float2 a = s[0], b = s[1], c = s[2], d = s[3], e = s[4];
+  const float2 c2 = pmul(p2(2.f / 6.f), c), c5 = pmul(p2(5.f / 6.f), c), c11 = pmul(p2(11.f / 6.f), c);
+  const float2 ep0 = pfma(p2(-1.f / 6.f), e, pfma(p2(5.f / 6.f), d, c2));
+  const float2 em0 = pfma(p2(-1.f / 6.f), a, pfma(p2(5.f / 6.f), b, c2));
+  const float2 ep1 = pfma(p2(2.f / 6.f), d, pfma(p2(-1.f / 6.f), b, c5));
+  const float2 em1 = pfma(p2(2.f / 6.f), b, pfma(p2(-1.f / 6.f), d, c5));
+  const float2 ep2 = pfma(p2(-7.f / 6.f), b, pfma(p2(2.f / 6.f), a, c11));
+  const float2 em2 = pfma(p2(-7.f / 6.f), d, pfma(p2(2.f / 6.f), e, c11));
+  const float2 k1 = p2(13.f / 12.f), k2 = p2(0.25f);
+  const float2 c3 = pmul(p2(3.f), c);
+  const float2 u0 = pfma(p2(-2.f), b, padd(a, c)), v0 = pfma(p2(-4.f), b, padd(a, c3));
+  const float2 u1 = pfma(p2(-2.f), c, padd(b, d)), v1 = pfma(p2(-1.f), d, b);
+  const float2 u2 = pfma(p2(-2.f), d, padd(c, e)), v2 = pfma(p2(-4.f), d, padd(e, c3));
+  const float2 b0 = pfma(pmul(k1, u0), u0, pmul(pmul(k2, v0), v0));
+  const float2 b1 = pfma(pmul(k1, u1), u1, pmul(pmul(k2, v1), v1));
+  const float2 b2 = pfma(pmul(k1, u2), u2, pmul(pmul(k2, v2), v2));
+  const float2 tau = pfma(p2(-1.f), b0, b2);
+  const float2 q0 = weno_q2(tau, b0), q1 = weno_q2(tau, b1), q2 = weno_q2(tau, b2);
+  const float2 t0 = pmul(p2(3.f), q0), t1 = pmul(p2(6.f), q1), t2 = pmul(p2(3.f), q2);
+  // minus face: w = (3 q0, 6 q1, q2); plus face: w = (3 q2, 6 q1, q0)
+  vM = pmul(pfma(t0, em0, pfma(t1, em1, pmul(q2, em2))), prcp(padd(t0, padd(t1, q2))));
+  vP = pmul(pfma(t2, ep0, pfma(t1, ep1, pmul(q0, ep2))), prcp(padd(t2, padd(t1, q0))));
+}
+
+// Both face values of two cells: packed WENO-Z, else the scalar
+// reconstruction once per lane (bit-identical to Reconstruct).
+template <int RECON>
+__device__ __forceinline__ void ReconstructBoth2(int limiter, const float2 (&s)[5], float2 &vM, float2 &vP) {
+  if constexpr (RECON == WENOZ) {
+    WenoZBoth2(s, vM, vP);
+  } else {
+    float lo[5], hi[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      lo[k] = s[k].x;
+      hi[k] = s[k].y;
+    }
+    Reconstruct<RECON, float>(limiter, lo, vM.x, vP.x);
+    Reconstruct<RECON, float>(limiter, hi, vM.y, vP.y);
+  }
+}
+
 // Value at the plus face only (for the cell left of a face).
 template <int RECON, typename R>
 __device__ __forceinline__ R ReconstructPlus(int limiter, const R (&s)[5]) {
@@ -369,6 +442,77 @@ __device__ __forceinline__ void RiemannFlux(const R *vL, const R *vR, R *flux) {
 #pragma unroll
     for (int v = 0; v < NC; v++)
       flux[v] = biasR * (FL[v] + sL * (UsL[v] - UL[v])) + biasL * (FR[v] + sR * (UsR[v] - UR[v]));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The hydro Riemann fluxes above on two faces at once (packed FP32, the FP32
+// fused stage).  Same formulas as RiemannFlux<RIEMANN, false, DIR1>: HLL
+// (riemann_solver.hpp:20-57) and HLLC with both star states blended by the
+// sign of u* (:59-149); divisions are per-lane approximate reciprocals.
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return pfma(p2(-1.f), b, a); }
+
+template <int DIR1>
+__device__ __forceinline__ void Prim2ConsFlux2(const float2 *V, float2 *U, float2 *F) {
+  const float2 rho = V[RDENS], un = V[RVEL0 + DIR1];
+  const float2 vv = pfma(V[RVEL0 + 2], V[RVEL0 + 2], pfma(V[RVEL0 + 1], V[RVEL0 + 1], pmul(V[RVEL0], V[RVEL0])));
+  U[CDENS] = rho;
+  F[CDENS] = pmul(rho, un);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    U[CMOM0 + d] = pmul(rho, V[RVEL0 + d]);
+    F[CMOM0 + d] = pmul(F[CDENS], V[RVEL0 + d]);
+  }
+  U[CENER] = padd(pmul(V[REINT], rho), pmul(pmul(p2(0.5f), rho), vv));
+  F[CMOM0 + DIR1] = padd(F[CMOM0 + DIR1], V[RPRES]);
+  F[CENER] = pmul(padd(U[CENER], V[RPRES]), un);
+}
+
+template <int RIEMANN, int DIR1>
+__device__ __forceinline__ void RiemannFlux2(const float2 *vL, const float2 *vR, float2 *flux) {
+  constexpr int DIR2 = (DIR1 + 1) % 3;
+  constexpr int DIR3 = (DIR1 + 2) % 3;
+  const float tiny = FLT_MIN;
+  const float2 uL = vL[RVEL0 + DIR1], uR = vR[RVEL0 + DIR1];
+  const float2 a2L = pmul(vL[RBMOD], prcp(vL[RDENS])), a2R = pmul(vR[RBMOD], prcp(vR[RDENS]));
+  const float2 cfL = make_float2(sqrtf(a2L.x), sqrtf(a2L.y)), cfR = make_float2(sqrtf(a2R.x), sqrtf(a2R.y));
+  const float2 mL = psub(uL, cfL), mR = psub(uR, cfR), pL = padd(uL, cfL), pR = padd(uR, cfR);
+  const float2 sL = make_float2(kmin(-tiny, kmin(mL.x, mR.x)), kmin(-tiny, kmin(mL.y, mR.y)));
+  const float2 sR = make_float2(kmax(tiny, kmax(pL.x, pR.x)), kmax(tiny, kmax(pL.y, pR.y)));
+  float2 UL[5], UR[5], FL[5], FR[5];
+  Prim2ConsFlux2<DIR1>(vL, UL, FL);
+  Prim2ConsFlux2<DIR1>(vR, UR, FR);
+  if constexpr (RIEMANN == HLL) {
+    const float2 sRmsLi = prcp(psub(sR, sL)), sRsL = pmul(sR, sL);
+#pragma unroll
+    for (int v = 0; v < 5; v++)
+      flux[v] = pmul(sRmsLi, pfma(sRsL, psub(UR[v], UL[v]), psub(pmul(sR, FL[v]), pmul(sL, FR[v]))));
+  } else {
+    const float2 dL = psub(sL, uL), dR = psub(sR, uR);
+    const float2 rdL = pmul(vL[RDENS], dL), rdR = pmul(vR[RDENS], dR);
+    float2 ustar = psub(pfma(UL[CMOM0 + DIR1], dL, psub(vR[RPRES], vL[RPRES])), pmul(UR[CMOM0 + DIR1], dR));
+    ustar = pmul(ustar, prcp(psub(rdL, rdR)));
+    const float2 pstar = pmul(p2(0.5f), padd(padd(vL[RPRES], vR[RPRES]),
+                                             pfma(rdL, psub(ustar, uL), pmul(rdR, psub(ustar, uR)))));
+    const float2 pu = pmul(pstar, ustar);
+    auto hllc_state = [&](float2 S, const float2 *U, float2 Pu, float2 *Us) {
+      const float2 susi = prcp(padd(psub(S, ustar), p2(tiny)));
+      Us[CDENS] = pmul(susi, psub(pmul(S, U[CDENS]), U[CMOM0 + DIR1]));
+      Us[CMOM0 + DIR1] = pmul(Us[CDENS], ustar);
+      const float2 ratio = pmul(Us[CDENS], prcp(U[CDENS]));
+      Us[CMOM0 + DIR2] = pmul(U[CMOM0 + DIR2], ratio);
+      Us[CMOM0 + DIR3] = pmul(U[CMOM0 + DIR3], ratio);
+      Us[CENER] = pfma(U[CENER], ratio, pmul(susi, psub(pu, Pu)));
+    };
+    float2 UsL[5], UsR[5];
+    hllc_state(sL, UL, pmul(vL[RPRES], uL), UsL);
+    hllc_state(sR, UR, pmul(vR[RPRES], uR), UsR);
+    const float2 sg = make_float2(copysignf(1.f, ustar.x), copysignf(1.f, ustar.y));
+    const float2 biasL = make_float2(-kmin(-tiny, sg.x), -kmin(-tiny, sg.y));
+    const float2 biasR = make_float2(kmax(tiny, sg.x), kmax(tiny, sg.y));
+#pragma unroll
+    for (int v = 0; v < 5; v++)
+      flux[v] = pfma(biasR, pfma(sL, psub(UsL[v], UL[v]), FL[v]), pmul(biasL, pfma(sR, psub(UsR[v], UR[v]), FR[v])));
   }
 }
 

@@ -272,42 +272,100 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
   for (int ch = 0; ch < NCH; ch++) {
     const int c1 = CA == 1 ? ch * C1 : 0, c2 = CA == 2 ? ch * C2 : 0;
     // 2. both face values of every (primitive, cell) of the chunk
-    for (int it = tid; it < Sh::NR * NRC; it += Sh::NT) {
-      const int r = it / NRC, q = it - r * NRC;
-      const int x = q % C0, y = (q / C0) % C1 + c1, z = q / (C0 * C1) + c2;
-      // region coordinate: position p = x - 1 along DIR sits at p + H
-      const int ex = x + (DIR == 0 ? H - 1 : 0), ey = y + (DIR == 1 ? H - 1 : 0), ez = z + (DIR == 2 ? H - 1 : 0);
-      const S *c = sp + r * RM + ex + E0 * (ey + E1 * ez);
-      S s[5];
+    if constexpr (sizeof(S) == 4) {
+      // FP32: two cells per thread in packed arithmetic, (r, q) and
+      // (r, q + NRC/2).  The grid is halved along its slowest axis of extent
+      // > 1, so the partner's region cell lies a constant PO further.
+      constexpr int PA = C2 > 1 ? 2 : (C1 > 1 ? 1 : 0);
+      static_assert((PA == 2 ? C2 : PA == 1 ? C1 : C0) % 2 == 0, "paired axis must have an even extent");
+      constexpr int HALF = NRC / 2;
+      constexpr int PO = PA == 2 ? (C2 / 2) * E0 * E1 : PA == 1 ? (C1 / 2) * E0 : C0 / 2;
+      for (int it = tid; it < Sh::NR * HALF; it += Sh::NT) {
+        const int r = it / HALF, q = it - r * HALF;
+        const int x = q % C0, y = (q / C0) % C1 + c1, z = q / (C0 * C1) + c2;
+        const int ex = x + (DIR == 0 ? H - 1 : 0), ey = y + (DIR == 1 ? H - 1 : 0), ez = z + (DIR == 2 ? H - 1 : 0);
+        const S *c = sp + r * RM + ex + E0 * (ey + E1 * ez);
+        float2 s[5];
 #pragma unroll
-      for (int k = 0; k < 5; k++) s[k] = (k - 2 >= -W && k - 2 <= W) ? c[(k - 2) * ST] : S(0);
-      S vm, vp;
-      if constexpr (sizeof(S) == 4) {
-        ReconstructBoth<RECON, S>(a.limiter, s, vm, vp);
-      } else {
-        Reconstruct<RECON, S>(a.limiter, s, vm, vp);
+        for (int k = 0; k < 5; k++)
+          s[k] = (k - 2 >= -W && k - 2 <= W) ? make_float2(c[(k - 2) * ST], c[(k - 2) * ST + PO]) : p2(0.f);
+        float2 vm, vp;
+        ReconstructBoth2<RECON>(a.limiter, s, vm, vp);
+        rm[r * RC + q] = vm.x;
+        rm[r * RC + q + HALF] = vm.y;
+        rp[r * RC + q] = vp.x;
+        rp[r * RC + q + HALF] = vp.y;
       }
-      rm[r * RC + q] = vm;
-      rp[r * RC + q] = vp;
+    } else {
+      for (int it = tid; it < Sh::NR * NRC; it += Sh::NT) {
+        const int r = it / NRC, q = it - r * NRC;
+        const int x = q % C0, y = (q / C0) % C1 + c1, z = q / (C0 * C1) + c2;
+        // region coordinate: position p = x - 1 along DIR sits at p + H
+        const int ex = x + (DIR == 0 ? H - 1 : 0), ey = y + (DIR == 1 ? H - 1 : 0), ez = z + (DIR == 2 ? H - 1 : 0);
+        const S *c = sp + r * RM + ex + E0 * (ey + E1 * ez);
+        S s[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) s[k] = (k - 2 >= -W && k - 2 <= W) ? c[(k - 2) * ST] : S(0);
+        S vm, vp;
+        if constexpr (sizeof(S) == 4) {
+          ReconstructBoth<RECON, S>(a.limiter, s, vm, vp);
+        } else {
+          Reconstruct<RECON, S>(a.limiter, s, vm, vp);
+        }
+        rm[r * RC + q] = vm;
+        rp[r * RC + q] = vp;
+      }
     }
     __syncthreads();
 
     // 3. Riemann flux at the chunk's DIR faces; the face at position f joins
     // reconstruction cells f (its low cell, position f-1) and f+1
-    for (int it = tid; it < NFC; it += Sh::NT) {
-      const int x = it % G0, y = (it / G0) % G1, z = it / (G0 * G1);
-      const int lq = x + C0 * (y + C1 * z);
-      S vL[7], vR[7];
+    // FP32 pairs faces across the slowest transverse axis of even extent
+    // (none in 1D); the partner lies LQO further in the reconstruction grid
+    // and GFO further in the face grid.
+    constexpr int QA = sizeof(S) != 4 ? -1
+                       : (G2 > 1 && G2 % 2 == 0) ? 2
+                       : (G1 > 1 && G1 % 2 == 0) ? 1
+                       : (G0 % 2 == 0 && DIR != 0) ? 0 : -1;
+    if constexpr (QA >= 0) {
+      static_assert(QA != DIR && NCH == 1, "faces pair across a transverse axis of one chunk");
+      constexpr int H0 = QA == 0 ? G0 / 2 : G0, H1 = QA == 1 ? G1 / 2 : G1, H2 = QA == 2 ? G2 / 2 : G2;
+      constexpr int LQO = QA == 0 ? G0 / 2 : QA == 1 ? (G1 / 2) * C0 : (G2 / 2) * C0 * C1;
+      constexpr int GFO = QA == 0 ? G0 / 2 : QA == 1 ? (G1 / 2) * F0 : (G2 / 2) * F0 * F1;
+      for (int it = tid; it < H0 * H1 * H2; it += Sh::NT) {
+        const int x = it % H0, y = (it / H0) % H1, z = it / (H0 * H1);
+        const int lq = x + C0 * (y + C1 * z);
+        float2 vL[7], vR[7];
 #pragma unroll
-      for (int r = 0; r < 7; r++) {
-        vL[r] = rp[r * RC + lq];
-        vR[r] = rm[r * RC + lq + RST];
+        for (int r = 0; r < 7; r++) {
+          vL[r] = make_float2(rp[r * RC + lq], rp[r * RC + lq + LQO]);
+          vR[r] = make_float2(rm[r * RC + lq + RST], rm[r * RC + lq + RST + LQO]);
+        }
+        float2 F[5];
+        RiemannFlux2<RIEMANN, DIR>(vL, vR, F);
+        const int gf = x + F0 * (y + F1 * z);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          sf[v * FM + gf] = F[v].x;
+          sf[v * FM + gf + GFO] = F[v].y;
+        }
       }
-      S F[5];
-      RiemannFlux<RIEMANN, false, DIR, S>(vL, vR, F);
-      const int gf = x + F0 * ((y + c1) + F1 * (z + c2));
+    } else {
+      for (int it = tid; it < NFC; it += Sh::NT) {
+        const int x = it % G0, y = (it / G0) % G1, z = it / (G0 * G1);
+        const int lq = x + C0 * (y + C1 * z);
+        S vL[7], vR[7];
 #pragma unroll
-      for (int v = 0; v < 5; v++) sf[v * FM + gf] = F[v];
+        for (int r = 0; r < 7; r++) {
+          vL[r] = rp[r * RC + lq];
+          vR[r] = rm[r * RC + lq + RST];
+        }
+        S F[5];
+        RiemannFlux<RIEMANN, false, DIR, S>(vL, vR, F);
+        const int gf = x + F0 * ((y + c1) + F1 * (z + c2));
+#pragma unroll
+        for (int v = 0; v < 5; v++) sf[v * FM + gf] = F[v];
+      }
     }
     __syncthreads();
   }
