@@ -182,16 +182,69 @@ __device__ __forceinline__ void fz_stage_prims(const FusedArgs<S> &a, const FzTa
   constexpr int E2 = Sh::B[2] + (DIR == 2 ? 2 * H : 0);
   constexpr int NREG = E0 * E1 * E2;
   constexpr int RM = Sh::REG_MAX;
-  for (int q = threadIdx.x; q < NREG; q += Sh::NT) {
-    // table index: region coordinate along DIR, brick coordinate + H across
-    const int t0 = q % E0 + (DIR == 0 ? 0 : H);
-    const int t1 = (q / E0) % E1 + (DIR == 1 ? 0 : H);
-    const int t2 = q / (E0 * E1) + (DIR == 2 ? 0 : H);
-    const bool flip[3] = {t.flip[0][t0] != 0, t.flip[1][t1] != 0, t.flip[2][t2] != 0};
-    S V[7];
-    fz_load_prim<S>(a, t.off[0][t0] + t.off[1][t1] + t.off[2][t2], flip, V);
+  // every load of the thread's cells first, then the stores: the loads of
+  // all its cells are in flight together
+  constexpr int NIT = (NREG + Sh::NT - 1) / Sh::NT;
+  S V[NIT][7];
 #pragma unroll
-    for (int r = 0; r < 7; r++) sp[r * RM + q] = V[r];
+  for (int k = 0; k < NIT; k++) {
+    const int q = threadIdx.x + k * Sh::NT;
+    if (q < NREG) {
+      // table index: region coordinate along DIR, brick coordinate + H across
+      const int t0 = q % E0 + (DIR == 0 ? 0 : H);
+      const int t1 = (q / E0) % E1 + (DIR == 1 ? 0 : H);
+      const int t2 = q / (E0 * E1) + (DIR == 2 ? 0 : H);
+      const bool flip[3] = {t.flip[0][t0] != 0, t.flip[1][t1] != 0, t.flip[2][t2] != 0};
+      fz_load_prim<S>(a, t.off[0][t0] + t.off[1][t1] + t.off[2][t2], flip, V[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NIT; k++) {
+    const int q = threadIdx.x + k * Sh::NT;
+    if (q < NREG) {
+#pragma unroll
+      for (int r = 0; r < 7; r++) sp[r * RM + q] = V[k][r];
+    }
+  }
+}
+
+// Element offset of the brick's owned cell c, or -1 past the block's edge
+// (partial bricks).
+template <typename S, int NDIM, int RECON>
+__device__ __forceinline__ long long fz_owned(const FusedArgs<S> &a, int b, const int o[3], int c) {
+  using Sh = FusedShape<NDIM, RECON>;
+  const MeshDesc &m = a.m;
+  if (c >= Sh::NCELL) return -1;
+  const int l0 = o[0] + c % Sh::B[0], l1 = o[1] + (c / Sh::B[0]) % Sh::B[1], l2 = o[2] + c / (Sh::B[0] * Sh::B[1]);
+  if (l0 >= m.nx[0] || l1 >= m.nx[1] || l2 >= m.nx[2]) return -1;
+  return (long long)b * m.P + ((long long)(l2 + m.g[2]) * m.np[1] + (l1 + m.g[1])) * m.np[0] + (l0 + m.g[0]);
+}
+
+// Ask L2 for the epilogue's inputs (U_base, and U_stage's momentum and
+// energy, which the stored-primitive staging does not read) at the start of
+// the stage, so the epilogue's loads do not wait on HBM.  One prefetch per
+// 128-byte line of each owned row; rows past the block's edge are skipped.
+template <typename S, int NDIM, int RECON>
+__device__ __forceinline__ void fz_prefetch_epilogue(const FusedArgs<S> &a, int b, const int o[3]) {
+  using Sh = FusedShape<NDIM, RECON>;
+  constexpr int LINE = 128 / sizeof(S);                      // elements per line
+  constexpr int NLR = (Sh::B[0] + LINE - 1) / LINE + 1;     // lines a row can touch
+  constexpr int NROW = Sh::NCELL / Sh::B[0];
+  constexpr int NARR = sizeof(S) == 4 ? 12 : 10;
+  const MeshDesc &m = a.m;
+  const long long NP = (long long)m.nb * m.P;
+  const int len = min(Sh::B[0], m.nx[0] - o[0]);
+  for (int q = threadIdx.x; q < NARR * NROW * NLR; q += Sh::NT) {
+    const int k = q % NLR, row = (q / NLR) % NROW, arr = q / (NLR * NROW);
+    const int l1 = o[1] + row % Sh::B[1], l2 = o[2] + row / Sh::B[1];
+    if (l1 >= m.nx[1] || l2 >= m.nx[2] || len <= 0) continue;
+    const long long n0 = (long long)b * m.P + ((long long)(l2 + m.g[2]) * m.np[1] + (l1 + m.g[1])) * m.np[0] + (o[0] + m.g[0]);
+    const int e = min(k * LINE, len - 1);  // last prefetch covers the row's end
+    const void *p;
+    if (arr < 5) p = a.ub + arr * NP + n0 + e;
+    else if (arr < 10) p = a.u0 + (arr - 5) * NP + n0 + e;
+    else p = (arr == 10 ? a.ublo : a.u0lo) + n0 + e;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
   }
 }
 
@@ -280,6 +333,7 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
       static_assert((PA == 2 ? C2 : PA == 1 ? C1 : C0) % 2 == 0, "paired axis must have an even extent");
       constexpr int HALF = NRC / 2;
       constexpr int PO = PA == 2 ? (C2 / 2) * E0 * E1 : PA == 1 ? (C1 / 2) * E0 : C0 / 2;
+#pragma unroll 2
       for (int it = tid; it < Sh::NR * HALF; it += Sh::NT) {
         const int r = it / HALF, q = it - r * HALF;
         const int x = q % C0, y = (q / C0) % C1 + c1, z = q / (C0 * C1) + c2;
@@ -328,7 +382,7 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
                        : (G1 > 1 && G1 % 2 == 0) ? 1
                        : (G0 % 2 == 0 && DIR != 0) ? 0 : -1;
     if constexpr (QA >= 0) {
-      static_assert(QA != DIR && NCH == 1, "faces pair across a transverse axis of one chunk");
+      static_assert(QA != DIR, "faces pair across a transverse axis");
       constexpr int H0 = QA == 0 ? G0 / 2 : G0, H1 = QA == 1 ? G1 / 2 : G1, H2 = QA == 2 ? G2 / 2 : G2;
       constexpr int LQO = QA == 0 ? G0 / 2 : QA == 1 ? (G1 / 2) * C0 : (G2 / 2) * C0 * C1;
       constexpr int GFO = QA == 0 ? G0 / 2 : QA == 1 ? (G1 / 2) * F0 : (G2 / 2) * F0 * F1;
@@ -343,7 +397,7 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
         }
         float2 F[5];
         RiemannFlux2<RIEMANN, DIR>(vL, vR, F);
-        const int gf = x + F0 * (y + F1 * z);
+        const int gf = x + F0 * ((y + c1) + F1 * (z + c2));
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           sf[v * FM + gf] = F[v].x;
@@ -393,6 +447,7 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
 #pragma unroll
     for (int v = 0; v < 5; v++) du[s][v] = S(0);
 
+  fz_prefetch_epilogue<S, NDIM, RECON>(a, b, o);
   __shared__ FzTables<NDIM, RECON> tb;
   fz_fill_tables<S, NDIM, RECON>(a, lx, o, tb);
   __syncthreads();
@@ -404,44 +459,59 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
   if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1>(a, tb, sp, rm, rp, sf, du);
   if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2>(a, tb, sp, rm, rp, sf, du);
 
-  // epilogue: low-storage update of the owned interior cells
+  // epilogue: low-storage update of the owned interior cells.  The inputs
+  // of all the thread's cells are loaded first so their loads overlap.
   const long long NP = (long long)m.nb * m.P;
   const S vol = S(m.vol);
   const S bt = S(a.beta);
   double dtl = INFINITY;
+  long long nc[Sh::CPT];
+  S xb[Sh::CPT][5], x0[Sh::CPT][5];
+  float xblo[Sh::CPT], x0lo[Sh::CPT];
 #pragma unroll
   for (int s = 0; s < Sh::CPT; s++) {
-    const int c = threadIdx.x + s * Sh::NT;
-    if (c >= Sh::NCELL) continue;
-    const int x = c % Sh::B[0], y = (c / Sh::B[0]) % Sh::B[1], z = c / (Sh::B[0] * Sh::B[1]);
-    const int l0 = o[0] + x, l1 = o[1] + y, l2 = o[2] + z;
-    if (l0 >= m.nx[0] || l1 >= m.nx[1] || l2 >= m.nx[2]) continue;
-    const long long n = (long long)b * m.P +
-                        ((long long)(l2 + m.g[2]) * m.np[1] + (l1 + m.g[1])) * m.np[0] + (l0 + m.g[0]);
+    nc[s] = fz_owned<S, NDIM, RECON>(a, b, o, threadIdx.x + s * Sh::NT);
+    if (nc[s] < 0) continue;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      xb[s][v] = a.ub[v * NP + nc[s]];
+      x0[s][v] = a.u0[v * NP + nc[s]];
+    }
+    if constexpr (sizeof(S) == 4) {
+      xblo[s] = a.ublo[nc[s]];
+      x0lo[s] = a.u0lo[nc[s]];
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < Sh::CPT; s++) {
+    const long long n = nc[s];
+    if (n < 0) continue;
     S un[5];
+    float unlo = 0.f;
 #pragma unroll
     for (int v = 0; v < 5; v++) {
       const S dudt = du[s][v] / vol;
       if (sizeof(S) == 4 && v == CENER) {
-        double eb = double(a.ub[CENER * NP + n]), e0 = double(a.u0[CENER * NP + n]);
+        double eb = double(xb[s][CENER]), e0 = double(x0[s][CENER]);
         if constexpr (sizeof(S) == 4) {
-          eb += double(a.ublo[n]);
-          e0 += double(a.u0lo[n]);
+          eb += double(xblo[s]);
+          e0 += double(x0lo[s]);
         }
         const double e1 = (a.beta * eb + (1.0 - a.beta) * e0) + a.beta * dt * double(dudt);
         const float hi = float(e1);
+        unlo = float(e1 - double(hi));
         a.u1[CENER * NP + n] = S(hi);
-        if constexpr (sizeof(S) == 4) a.u1lo[n] = float(e1 - double(hi));
+        if constexpr (sizeof(S) == 4) a.u1lo[n] = unlo;
         un[v] = S(hi);
         continue;
       }
-      const S x0 = bt * a.ub[v * NP + n] + (S(1.0) - bt) * a.u0[v * NP + n];
-      un[v] = x0 + bt * S(dt) * dudt;
+      const S y0 = bt * xb[s][v] + (S(1.0) - bt) * x0[s][v];
+      un[v] = y0 + bt * S(dt) * dudt;
       a.u1[v * NP + n] = un[v];
     }
     if (a.last || a.prim_out) {
       double e = double(un[CENER]);
-      if constexpr (sizeof(S) == 4) e += double(a.u1lo[n]);
+      if constexpr (sizeof(S) == 4) e += double(unlo);
       S V[7];
       Cons2PrimEos<false, S>(a.eos, un[CDENS], un[CMOM0], un[CMOM1], un[CMOM2], e, nullptr, V);
       if (a.prim_out) {
