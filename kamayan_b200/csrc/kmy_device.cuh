@@ -133,33 +133,37 @@ __device__ __forceinline__ void Reconstruct(int limiter, const R (&s)[5], R &vM,
   }
 }
 
-// Both face values for the FP32 fused stage.  WENO-Z folds the 1/6 of the
-// three candidate stencils into the normalisation (one multiply per face
-// value instead of six); the weights and smoothness indicators are the
-// reference's.  Other reconstructions are Reconstruct itself.
-template <int RECON, typename R>
-__device__ __forceinline__ void ReconstructBoth(int limiter, const R (&s)[5], R &vM, R &vP) {
-  if constexpr (RECON == WENOZ) {
-    const R s0 = s[2];
-    const R ep0 = -s[4] + R(5) * s[3] + R(2) * s0;
-    const R ep1 = R(2) * s[3] + R(5) * s0 - s[1];
-    const R ep2 = R(11) * s0 - R(7) * s[1] + R(2) * s[0];
-    const R em0 = -s[0] + R(5) * s[1] + R(2) * s0;
-    const R em1 = R(2) * s[1] + R(5) * s0 - s[3];
-    const R em2 = R(11) * s0 - R(7) * s[3] + R(2) * s[4];
-    const R c1312 = R(13.) / R(12.);
-    const R b0 = c1312 * sq(s[0] - R(2) * s[1] + s0) + R(0.25) * sq(s[0] - R(4) * s[1] + R(3) * s0);
-    const R b1 = c1312 * sq(s[1] - R(2) * s0 + s[3]) + R(0.25) * sq(s[1] - s[3]);
-    const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
-    const R tau = fabs(b2 - b0);
-    const R q0 = weno_q(tau, b0);
-    const R q1 = weno_q(tau, b1);
-    const R q2 = weno_q(tau, b2);
-    const R t0 = R(3) * q0, t1 = R(6) * q1, t2 = R(3) * q2;
-    vM = (t0 * em0 + t1 * em1 + q2 * em2) / (R(6) * (t0 + t1 + q2));
-    vP = (t2 * ep0 + t1 * ep1 + q0 * ep2) / (R(6) * (t2 + t1 + q0));
-  } else {
-    Reconstruct<RECON, R>(limiter, s, vM, vP);
+// WENO-Z at both faces with two divisions instead of five (FP64 fused
+// stage).  The reference's weights w_k = d_k (1 + tau^2 / A_k), with
+// A_k = (eps + beta_k)^2, are scaled by A_0 A_1 A_2, which the normalisation
+// cancels: W_k = d_k (A_k + tau^2) prod_{j != k} A_j.  Same value as
+// Reconstruct up to rounding; with eps = 1e-36 the scaled weights stay
+// within [1e-216, 1e+216] for smoothness indicators up to 1e+36.
+template <typename R>
+__device__ __forceinline__ void WenoZBothTwoDiv(const R (&s)[5], R &vM, R &vP) {
+  const R s0 = s[2];
+  const R sixth = R(1.) / R(6.);
+  const R ep0 = sixth * (-s[4] + R(5) * s[3] + R(2) * s0);
+  const R ep1 = sixth * (R(2) * s[3] + R(5) * s0 - s[1]);
+  const R ep2 = sixth * (R(11) * s0 - R(7) * s[1] + R(2) * s[0]);
+  const R em0 = sixth * (-s[0] + R(5) * s[1] + R(2) * s0);
+  const R em1 = sixth * (R(2) * s[1] + R(5) * s0 - s[3]);
+  const R em2 = sixth * (R(11) * s0 - R(7) * s[3] + R(2) * s[4]);
+  const R c1312 = R(13.) / R(12.);
+  const R b0 = c1312 * sq(s[0] - R(2) * s[1] + s0) + R(0.25) * sq(s[0] - R(4) * s[1] + R(3) * s0);
+  const R b1 = c1312 * sq(s[1] - R(2) * s0 + s[3]) + R(0.25) * sq(s[1] - s[3]);
+  const R b2 = c1312 * sq(s0 - R(2) * s[3] + s[4]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s0);
+  const R t2 = sq(b2 - b0);
+  const R A0 = sq(R(1.e-36) + b0), A1 = sq(R(1.e-36) + b1), A2 = sq(R(1.e-36) + b2);
+  const R N0 = A0 + t2, N1 = A1 + t2, N2 = A2 + t2;
+  const R P01 = A0 * A1, P02 = A0 * A2, P12 = A1 * A2;
+  {  // minus face: d = (3, 6, 1) on (beta0, beta1, beta2)
+    const R w0 = R(3) * N0 * P12, w1 = R(6) * N1 * P02, w2 = N2 * P01;
+    vM = (w0 * em0 + w1 * em1 + w2 * em2) / (w0 + w1 + w2);
+  }
+  {  // plus face: d = (3, 6, 1) on (beta2, beta1, beta0)
+    const R w0 = R(3) * N2 * P01, w1 = R(6) * N1 * P02, w2 = N0 * P12;
+    vP = (w0 * ep0 + w1 * ep1 + w2 * ep2) / (w0 + w1 + w2);
   }
 }
 

@@ -361,8 +361,8 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
 #pragma unroll
         for (int k = 0; k < 5; k++) s[k] = (k - 2 >= -W && k - 2 <= W) ? c[(k - 2) * ST] : S(0);
         S vm, vp;
-        if constexpr (sizeof(S) == 4) {
-          ReconstructBoth<RECON, S>(a.limiter, s, vm, vp);
+        if constexpr (RECON == WENOZ) {
+          WenoZBothTwoDiv<S>(s, vm, vp);
         } else {
           Reconstruct<RECON, S>(a.limiter, s, vm, vp);
         }
