@@ -222,29 +222,37 @@ __device__ __forceinline__ long long fz_owned(const FusedArgs<S> &a, int b, cons
 
 // Ask L2 for the epilogue's inputs (U_base, and U_stage's momentum and
 // energy, which the stored-primitive staging does not read) at the start of
-// the stage, so the epilogue's loads do not wait on HBM.  One prefetch per
-// 128-byte line of each owned row; rows past the block's edge are skipped.
+// the stage, so the epilogue's loads do not wait on HBM.  One bulk prefetch
+// per array and brick plane covers the plane's owned rows (the span from its
+// first owned cell to its last, rounded out to 16 bytes; the rounding stays
+// inside the block's ghost-padded storage).
 template <typename S, int NDIM, int RECON>
 __device__ __forceinline__ void fz_prefetch_epilogue(const FusedArgs<S> &a, int b, const int o[3]) {
   using Sh = FusedShape<NDIM, RECON>;
-  constexpr int LINE = 128 / sizeof(S);                      // elements per line
-  constexpr int NLR = (Sh::B[0] + LINE - 1) / LINE + 1;     // lines a row can touch
-  constexpr int NROW = Sh::NCELL / Sh::B[0];
   constexpr int NARR = sizeof(S) == 4 ? 12 : 10;
   const MeshDesc &m = a.m;
   const long long NP = (long long)m.nb * m.P;
-  const int len = min(Sh::B[0], m.nx[0] - o[0]);
-  for (int q = threadIdx.x; q < NARR * NROW * NLR; q += Sh::NT) {
-    const int k = q % NLR, row = (q / NLR) % NROW, arr = q / (NLR * NROW);
-    const int l1 = o[1] + row % Sh::B[1], l2 = o[2] + row / Sh::B[1];
-    if (l1 >= m.nx[1] || l2 >= m.nx[2] || len <= 0) continue;
-    const long long n0 = (long long)b * m.P + ((long long)(l2 + m.g[2]) * m.np[1] + (l1 + m.g[1])) * m.np[0] + (o[0] + m.g[0]);
-    const int e = min(k * LINE, len - 1);  // last prefetch covers the row's end
-    const void *p;
-    if (arr < 5) p = a.ub + arr * NP + n0 + e;
-    else if (arr < 10) p = a.u0 + (arr - 5) * NP + n0 + e;
-    else p = (arr == 10 ? a.ublo : a.u0lo) + n0 + e;
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  constexpr int B0 = Sh::B[0], B1 = Sh::B[1], B2 = Sh::B[2];
+  const int len0 = min(B0, m.nx[0] - o[0]), len1 = min(B1, m.nx[1] - o[1]);
+  for (int q = threadIdx.x; q < NARR * B2; q += Sh::NT) {
+    const int arr = q / B2, l2 = o[2] + q % B2;
+    if (l2 >= m.nx[2] || len0 <= 0 || len1 <= 0) continue;
+    const long long n0 =
+        (long long)b * m.P + ((long long)(l2 + m.g[2]) * m.np[1] + (o[1] + m.g[1])) * m.np[0] + (o[0] + m.g[0]);
+    const long long n1 = n0 + (long long)(len1 - 1) * m.np[0] + len0;  // one past the plane's last owned cell
+    uintptr_t lo, hi;
+    if (arr < 10) {
+      const S *base = arr < 5 ? a.ub + arr * NP : a.u0 + (arr - 5) * NP;
+      lo = uintptr_t(base + n0);
+      hi = uintptr_t(base + n1);
+    } else {
+      const float *base = arr == 10 ? a.ublo : a.u0lo;
+      lo = uintptr_t(base + n0);
+      hi = uintptr_t(base + n1);
+    }
+    lo &= ~uintptr_t(15);
+    hi = (hi + 15) & ~uintptr_t(15);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(unsigned(hi - lo)) : "memory");
   }
 }
 
@@ -289,7 +297,7 @@ __device__ __forceinline__ void fz_accumulate(const FusedArgs<S> &a, const S *sf
 // face fluxes reuse the primitive tile's storage.
 template <typename S, int NDIM, int RECON, int RIEMANN, int DIR>
 __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &tb,
-                                              S *sp, S *rm, S *rp, S *sf,
+                                              unsigned short *rofs, S *sp, S *rm, S *rp, S *sf,
                                               S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
   using Sh = FusedShape<NDIM, RECON>;
   constexpr int H = Sh::H, W = Sh::W;
@@ -318,6 +326,23 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
   constexpr int NFC = G0 * G1 * G2;
   const int tid = threadIdx.x;
 
+  // FP32 reconstructs two cells per thread in packed arithmetic, (r, q) and
+  // (r, q + NRC/2).  The grid is halved along its slowest axis of extent > 1,
+  // so the partner's region cell lies a constant PO further.  rofs holds the
+  // region offset of each cell q of the first half.
+  constexpr int PA = C2 > 1 ? 2 : (C1 > 1 ? 1 : 0);
+  constexpr int HALF = NRC / 2;
+  constexpr int PO = PA == 2 ? (C2 / 2) * E0 * E1 : PA == 1 ? (C1 / 2) * E0 : C0 / 2;
+  if constexpr (sizeof(S) == 4) {
+    static_assert(NCH == 1 && (PA == 2 ? C2 : PA == 1 ? C1 : C0) % 2 == 0, "pairs split one even axis of one chunk");
+    static_assert(Sh::REG_MAX < 65536, "region offsets are 16-bit");
+    for (int q = tid; q < HALF; q += Sh::NT) {
+      const int x = q % C0, y = (q / C0) % C1, z = q / (C0 * C1);
+      // region coordinate: position p = x - 1 along DIR sits at p + H
+      const int ex = x + (DIR == 0 ? H - 1 : 0), ey = y + (DIR == 1 ? H - 1 : 0), ez = z + (DIR == 2 ? H - 1 : 0);
+      rofs[q] = (unsigned short)(ex + E0 * (ey + E1 * ez));
+    }
+  }
   fz_stage_prims<S, NDIM, RECON, DIR>(a, tb, sp);
   __syncthreads();
 
@@ -326,19 +351,11 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
     const int c1 = CA == 1 ? ch * C1 : 0, c2 = CA == 2 ? ch * C2 : 0;
     // 2. both face values of every (primitive, cell) of the chunk
     if constexpr (sizeof(S) == 4) {
-      // FP32: two cells per thread in packed arithmetic, (r, q) and
-      // (r, q + NRC/2).  The grid is halved along its slowest axis of extent
-      // > 1, so the partner's region cell lies a constant PO further.
-      constexpr int PA = C2 > 1 ? 2 : (C1 > 1 ? 1 : 0);
-      static_assert((PA == 2 ? C2 : PA == 1 ? C1 : C0) % 2 == 0, "paired axis must have an even extent");
-      constexpr int HALF = NRC / 2;
-      constexpr int PO = PA == 2 ? (C2 / 2) * E0 * E1 : PA == 1 ? (C1 / 2) * E0 : C0 / 2;
+      // item it = r * HALF + q, stepping by NT without divisions
+      int r = tid / HALF, q = tid - (tid / HALF) * HALF;
 #pragma unroll 2
-      for (int it = tid; it < Sh::NR * HALF; it += Sh::NT) {
-        const int r = it / HALF, q = it - r * HALF;
-        const int x = q % C0, y = (q / C0) % C1 + c1, z = q / (C0 * C1) + c2;
-        const int ex = x + (DIR == 0 ? H - 1 : 0), ey = y + (DIR == 1 ? H - 1 : 0), ez = z + (DIR == 2 ? H - 1 : 0);
-        const S *c = sp + r * RM + ex + E0 * (ey + E1 * ez);
+      for (; r < Sh::NR;) {
+        const S *c = sp + r * RM + rofs[q];
         float2 s[5];
 #pragma unroll
         for (int k = 0; k < 5; k++)
@@ -349,6 +366,12 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
         rm[r * RC + q + HALF] = vm.y;
         rp[r * RC + q] = vp.x;
         rp[r * RC + q + HALF] = vp.y;
+        q += Sh::NT % HALF;
+        r += Sh::NT / HALF;
+        if (q >= HALF) {
+          q -= HALF;
+          r++;
+        }
       }
     } else {
       for (int it = tid; it < Sh::NR * NRC; it += Sh::NT) {
@@ -455,9 +478,10 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
   S *rm = sp + Sh::NR * Sh::REG_MAX;
   S *rp = rm + Sh::NR * (Sh::RC_MAX / NCH);
   S *sf = NCH == 1 ? sp : rp + Sh::NR * (Sh::RC_MAX / NCH);
-  fz_direction2<S, NDIM, RECON, RIEMANN, 0>(a, tb, sp, rm, rp, sf, du);
-  if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1>(a, tb, sp, rm, rp, sf, du);
-  if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2>(a, tb, sp, rm, rp, sf, du);
+  __shared__ unsigned short rofs[sizeof(S) == 4 ? Sh::RC_MAX / 2 : 1];
+  fz_direction2<S, NDIM, RECON, RIEMANN, 0>(a, tb, rofs, sp, rm, rp, sf, du);
+  if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1>(a, tb, rofs, sp, rm, rp, sf, du);
+  if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2>(a, tb, rofs, sp, rm, rp, sf, du);
 
   // epilogue: low-storage update of the owned interior cells.  The inputs
   // of all the thread's cells are loaded first so their loads overlap.
