@@ -173,7 +173,7 @@ __device__ __forceinline__ void fz_load_prim(const FusedArgs<S> &a, long long n,
 }
 
 // 1. Primitives of the brick extended by H cells along DIR, into sp.
-template <typename S, int NDIM, int RECON, int DIR>
+template <typename S, int NDIM, int RECON, int DIR, bool OVERLAP>
 __device__ __forceinline__ void fz_stage_prims(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &t, S *sp) {
   using Sh = FusedShape<NDIM, RECON>;
   constexpr int H = Sh::H;
@@ -182,28 +182,59 @@ __device__ __forceinline__ void fz_stage_prims(const FusedArgs<S> &a, const FzTa
   constexpr int E2 = Sh::B[2] + (DIR == 2 ? 2 * H : 0);
   constexpr int NREG = E0 * E1 * E2;
   constexpr int RM = Sh::REG_MAX;
-  // every load of the thread's cells first, then the stores: the loads of
-  // all its cells are in flight together
+  // Stored primitives with OVERLAP: every load of the thread's cells first,
+  // then the stores, so the loads of all its cells are in flight together.
+  // Otherwise one cell at a time: the conversion path (several FP64
+  // equation-of-state evaluations at once would cost more registers than the
+  // overlap saves) and the batched kernel, whose per-solve arguments already
+  // hold many registers.
   constexpr int NIT = (NREG + Sh::NT - 1) / Sh::NT;
-  S V[NIT][7];
+  auto cell = [&](int q, bool flip[3]) -> long long {
+    // table index: region coordinate along DIR, brick coordinate + H across
+    const int t0 = q % E0 + (DIR == 0 ? 0 : H);
+    const int t1 = (q / E0) % E1 + (DIR == 1 ? 0 : H);
+    const int t2 = q / (E0 * E1) + (DIR == 2 ? 0 : H);
+    flip[0] = t.flip[0][t0] != 0;
+    flip[1] = t.flip[1][t1] != 0;
+    flip[2] = t.flip[2][t2] != 0;
+    return t.off[0][t0] + t.off[1][t1] + t.off[2][t2];
+  };
+  if (OVERLAP && a.stored) {
+    const long long NP = (long long)a.m.nb * a.m.P;
+    S V[NIT][7];
 #pragma unroll
-  for (int k = 0; k < NIT; k++) {
-    const int q = threadIdx.x + k * Sh::NT;
-    if (q < NREG) {
-      // table index: region coordinate along DIR, brick coordinate + H across
-      const int t0 = q % E0 + (DIR == 0 ? 0 : H);
-      const int t1 = (q / E0) % E1 + (DIR == 1 ? 0 : H);
-      const int t2 = q / (E0 * E1) + (DIR == 2 ? 0 : H);
-      const bool flip[3] = {t.flip[0][t0] != 0, t.flip[1][t1] != 0, t.flip[2][t2] != 0};
-      fz_load_prim<S>(a, t.off[0][t0] + t.off[1][t1] + t.off[2][t2], flip, V[k]);
+    for (int k = 0; k < NIT; k++) {
+      const int q = threadIdx.x + k * Sh::NT;
+      if (q < NREG) {
+        bool flip[3];
+        const long long n = cell(q, flip);
+        V[k][RDENS] = a.u0[n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const S v = a.prim[(PVEL0 + d) * NP + n];
+          V[k][RVEL0 + d] = flip[d] ? -v : v;
+        }
+        V[k][RPRES] = a.prim[PPRES * NP + n];
+        V[k][RBMOD] = a.prim[PBMOD * NP + n];
+        V[k][REINT] = a.prim[PEINT * NP + n];
+      }
     }
-  }
 #pragma unroll
-  for (int k = 0; k < NIT; k++) {
-    const int q = threadIdx.x + k * Sh::NT;
-    if (q < NREG) {
+    for (int k = 0; k < NIT; k++) {
+      const int q = threadIdx.x + k * Sh::NT;
+      if (q < NREG) {
 #pragma unroll
-      for (int r = 0; r < 7; r++) sp[r * RM + q] = V[k][r];
+        for (int r = 0; r < 7; r++) sp[r * RM + q] = V[k][r];
+      }
+    }
+  } else {
+    for (int q = threadIdx.x; q < NREG; q += Sh::NT) {
+      bool flip[3];
+      const long long n = cell(q, flip);
+      S V[7];
+      fz_load_prim<S>(a, n, flip, V);
+#pragma unroll
+      for (int r = 0; r < 7; r++) sp[r * RM + q] = V[r];
     }
   }
 }
@@ -295,7 +326,7 @@ __device__ __forceinline__ void fz_accumulate(const FusedArgs<S> &a, const S *sf
 // transverse plane in NCH chunks so its reconstruction buffers stay small
 // enough for two CTAs per SM; in FP32 one chunk covers the plane and the
 // face fluxes reuse the primitive tile's storage.
-template <typename S, int NDIM, int RECON, int RIEMANN, int DIR>
+template <typename S, int NDIM, int RECON, int RIEMANN, int DIR, bool OVERLAP>
 __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &tb,
                                               unsigned short *rofs, S *sp, S *rm, S *rp, S *sf,
                                               S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
@@ -343,7 +374,7 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
       rofs[q] = (unsigned short)(ex + E0 * (ey + E1 * ez));
     }
   }
-  fz_stage_prims<S, NDIM, RECON, DIR>(a, tb, sp);
+  fz_stage_prims<S, NDIM, RECON, DIR, OVERLAP>(a, tb, sp);
   __syncthreads();
 
 #pragma unroll 1
@@ -453,7 +484,7 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
 
 // Brick br of block b for one stage: the whole per-CTA body.  Every thread of
 // the CTA calls it (it synchronises internally).
-template <typename S, int NDIM, int RECON, int RIEMANN>
+template <typename S, int NDIM, int RECON, int RIEMANN, bool OVERLAP>
 __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br, double dt) {
   using Sh = FusedShape<NDIM, RECON>;
   extern __shared__ __align__(16) unsigned char kmy_smem[];
@@ -479,36 +510,49 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
   S *rp = rm + Sh::NR * (Sh::RC_MAX / NCH);
   S *sf = NCH == 1 ? sp : rp + Sh::NR * (Sh::RC_MAX / NCH);
   __shared__ unsigned short rofs[sizeof(S) == 4 ? Sh::RC_MAX / 2 : 1];
-  fz_direction2<S, NDIM, RECON, RIEMANN, 0>(a, tb, rofs, sp, rm, rp, sf, du);
-  if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1>(a, tb, rofs, sp, rm, rp, sf, du);
-  if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2>(a, tb, rofs, sp, rm, rp, sf, du);
+  fz_direction2<S, NDIM, RECON, RIEMANN, 0, OVERLAP>(a, tb, rofs, sp, rm, rp, sf, du);
+  if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1, OVERLAP>(a, tb, rofs, sp, rm, rp, sf, du);
+  if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2, OVERLAP>(a, tb, rofs, sp, rm, rp, sf, du);
 
-  // epilogue: low-storage update of the owned interior cells.  The inputs
-  // of all the thread's cells are loaded first so their loads overlap.
+  // epilogue: low-storage update of the owned interior cells.  With OVERLAP
+  // the inputs of all the thread's cells are loaded first so their loads
+  // overlap; the batched kernel loads cell by cell.
   const long long NP = (long long)m.nb * m.P;
   const S vol = S(m.vol);
   const S bt = S(a.beta);
   double dtl = INFINITY;
-  long long nc[Sh::CPT];
-  S xb[Sh::CPT][5], x0[Sh::CPT][5];
-  float xblo[Sh::CPT], x0lo[Sh::CPT];
-#pragma unroll
-  for (int s = 0; s < Sh::CPT; s++) {
-    nc[s] = fz_owned<S, NDIM, RECON>(a, b, o, threadIdx.x + s * Sh::NT);
-    if (nc[s] < 0) continue;
+  struct In {
+    long long n;
+    S b[5], z[5];
+    float blo, zlo;
+  };
+  auto load = [&](int s, In &in) {
+    in.n = fz_owned<S, NDIM, RECON>(a, b, o, threadIdx.x + s * Sh::NT);
+    if (in.n < 0) return;
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-      xb[s][v] = a.ub[v * NP + nc[s]];
-      x0[s][v] = a.u0[v * NP + nc[s]];
+      in.b[v] = a.ub[v * NP + in.n];
+      in.z[v] = a.u0[v * NP + in.n];
     }
     if constexpr (sizeof(S) == 4) {
-      xblo[s] = a.ublo[nc[s]];
-      x0lo[s] = a.u0lo[nc[s]];
+      in.blo = a.ublo[in.n];
+      in.zlo = a.u0lo[in.n];
     }
+  };
+  In pre[OVERLAP ? Sh::CPT : 1];
+  if constexpr (OVERLAP) {
+#pragma unroll
+    for (int s = 0; s < Sh::CPT; s++) load(s, pre[s]);
   }
 #pragma unroll
   for (int s = 0; s < Sh::CPT; s++) {
-    const long long n = nc[s];
+    In cur;
+    if constexpr (OVERLAP) {
+      cur = pre[s];
+    } else {
+      load(s, cur);
+    }
+    const long long n = cur.n;
     if (n < 0) continue;
     S un[5];
     float unlo = 0.f;
@@ -516,10 +560,10 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
     for (int v = 0; v < 5; v++) {
       const S dudt = du[s][v] / vol;
       if (sizeof(S) == 4 && v == CENER) {
-        double eb = double(xb[s][CENER]), e0 = double(x0[s][CENER]);
+        double eb = double(cur.b[CENER]), e0 = double(cur.z[CENER]);
         if constexpr (sizeof(S) == 4) {
-          eb += double(xblo[s]);
-          e0 += double(x0lo[s]);
+          eb += double(cur.blo);
+          e0 += double(cur.zlo);
         }
         const double e1 = (a.beta * eb + (1.0 - a.beta) * e0) + a.beta * dt * double(dudt);
         const float hi = float(e1);
@@ -529,7 +573,7 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
         un[v] = S(hi);
         continue;
       }
-      const S y0 = bt * xb[s][v] + (S(1.0) - bt) * x0[s][v];
+      const S y0 = bt * cur.b[v] + (S(1.0) - bt) * cur.z[v];
       un[v] = y0 + bt * S(dt) * dudt;
       a.u1[v * NP + n] = un[v];
     }
@@ -614,7 +658,7 @@ __global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT) k_fused_stage(Fus
     fused_passthrough<S, NDIM, RECON>(a, b, blockIdx.x - b * nbrick);
     return;
   }
-  fused_brick<S, NDIM, RECON, RIEMANN>(a, b, blockIdx.x - b * nbrick, a.clock->dt);
+  fused_brick<S, NDIM, RECON, RIEMANN, true>(a, b, blockIdx.x - b * nbrick, a.clock->dt);
 }
 
 // ---------------------------------------------------------------------------
@@ -665,7 +709,7 @@ __device__ __forceinline__ void batch_args(const SolveDesc<S> &q, int stage, Fus
 }
 
 template <typename S, int NDIM, int RECON, int RIEMANN>
-__global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT) k_fused_batch(const SolveDesc<S> *__restrict__ d,
+__global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT, sizeof(S) == 4 ? 3 : 2) k_fused_batch(const SolveDesc<S> *__restrict__ d,
                                                      const long long *__restrict__ prefix,
                                                      const int *nsolves_dev, int stage) {
   __shared__ FusedArgs<S> sa;
@@ -694,7 +738,7 @@ __global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT) k_fused_batch(con
       const long long wl = w - s_base;
       const int nbrick = sa.nbr[0] * sa.nbr[1] * sa.nbr[2];
       const int b = int(wl / nbrick);
-      fused_brick<S, NDIM, RECON, RIEMANN>(sa, b, int(wl - (long long)b * nbrick), s_dt);
+      fused_brick<S, NDIM, RECON, RIEMANN, false>(sa, b, int(wl - (long long)b * nbrick), s_dt);
     }
     __syncthreads();
   }
