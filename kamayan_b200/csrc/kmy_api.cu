@@ -729,7 +729,37 @@ int kmy_task_stage(kmy_ctx *c, int stage, double dt) {
 // A fused stage stages the primitives of its input from c->prim when they
 // are current (after set-up, an import, the task path or a previous fused
 // stage) and writes those of its output to c->prim_alt; the buffers swap.
+// Constrained transport: the fused stage updates the cells and writes the
+// transverse field fluxes; the edge EMFs, the face update and the
+// primitives (which need the new cell-centred field) follow as separate
+// kernels, in the order of the task list (hydro_add_flux_tasks.cpp,
+// grid.cpp:353-381, primconsflux.cpp:82-142).
+static int fused_stage_ct(kmy_ctx *c, int stage) {
+  const auto &nm = c->prm.stage_name;
+  const int ns = int(c->prm.beta.size());
+  Container *dup = find_container(c, "dUdt");
+  if (!dup) return KMY_ERR_OOM;
+  Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
+  const bool stored = c->prims_valid || c->prims_interior;
+  const double beta = c->prm.beta[stage - 1];
+  int rc = launch_fused_stage(c, base, md0, md1, beta, stored, false);
+  if (!rc) rc = launch_flux_halo(c);
+  if (!rc) rc = launch_compute_emf(c, md0);
+  if (!rc) rc = launch_flux_stokes(c, md0, *dup);
+  if (!rc) rc = launch_apply_faces(c, base, md0, md1, *dup, beta, -1.0, &c->clock->dt);
+  if (!rc) rc = launch_prepare_primitive(c, md1);
+  if (!rc && stage == ns) {
+    rc = launch_estimate_dt(c, base, true);
+    if (!rc) rc = launch_fill_derived(c, base);
+  }
+  // interior primitives of md1 are current (ghost zones are not)
+  c->prims_interior = !rc;
+  c->prims_valid = false;
+  return rc;
+}
+
 static int fused_stage(kmy_ctx *c, int stage) {
+  if (c->prm.mhd) return fused_stage_ct(c, stage);
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());
   // FP32 stages keep their output's primitives (kmy_fused.cu)
@@ -776,8 +806,11 @@ int kmy_rk_stage(kmy_ctx *c, int stage, double dt) {
 }
 
 // Whole steps go through the fused stage unless the path was set to tasks,
-// the mesh carries CT, or the mesh is adaptive.
-static bool steps_fused(const kmy_ctx *c) { return c->path == 0 && !c->prm.mhd && !c->amr.on; }
+// the mesh is adaptive, or it carries CT in a configuration the fused stage
+// does not cover.
+static bool steps_fused(const kmy_ctx *c) {
+  return c->path == 0 && !c->amr.on && (!c->prm.mhd || !fused_ct_unsupported(c));
+}
 
 static int step_async(kmy_ctx *c) {
   const int ns = int(c->prm.beta.size());
@@ -814,11 +847,13 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
   int n = 0;
   DevClock h{};
   while (!rc) {
-    // Fused steps queue ahead in chunks: a step queued after the clock
-    // reached tlim leaves the state unchanged.  The per-task kernels (CT,
-    // adaptive meshes, the tasks path) do not check the clock, so they step
-    // one at a time; an adaptive mesh reads its tags back every step anyway.
-    const int chunk = steps_fused(c) ? 8 : 1;
+    // Fused hydro steps queue ahead in chunks: a step queued after the clock
+    // reached tlim leaves the state unchanged.  The per-task kernels
+    // (adaptive meshes, the tasks path, and the face update and primitives
+    // of a constrained-transport stage) do not check the clock, so those
+    // step one at a time; an adaptive mesh reads its tags back every step
+    // anyway.
+    const int chunk = steps_fused(c) && !c->prm.mhd ? 8 : 1;
     for (int i = 0; i < chunk && !rc && (nlim < 0 || n < nlim); i++, n++) rc = step_async(c);
     if (rc) break;
     rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");

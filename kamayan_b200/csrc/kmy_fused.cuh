@@ -26,7 +26,7 @@
 
 namespace kmy {
 
-template <int NDIM, int RECON>
+template <int NDIM, int RECON, bool MHD = false>
 struct FusedShape {
   static constexpr int W = ReconWidth<RECON>::value;
   static constexpr int H = W + 1;
@@ -42,8 +42,14 @@ struct FusedShape {
       cmax(region(0), cmax(NDIM > 1 ? region(1) : 0, NDIM > 2 ? region(2) : 0));
   static constexpr int FACE_MAX =
       cmax(faces(0), cmax(NDIM > 1 ? faces(1) : 0, NDIM > 2 ? faces(2) : 0));
-  static constexpr int NR = 7;
-  static constexpr int NC = 5;
+  // reconstructed variables: the hydro seven, plus the cell-centred field
+  // with MHD (hydro_types.hpp:61-77 order)
+  static constexpr int NR = MHD ? 10 : 7;
+  // conserved components the stage updates from its fluxes: the hydro five,
+  // plus B_z in 2D MHD (B_x, B_y and in 3D all of B come from the faces)
+  static constexpr int NC = (MHD && NDIM == 2) ? 6 : 5;
+  // conserved index of update slot v
+  static constexpr int cons(int v) { return v < 5 ? v : CMAGC0 + 2; }
   // local coordinates per axis the brick's stencils touch
   static constexpr int TAB = cmax(B[0], cmax(B[1], B[2])) + 2 * H;
   // cells reconstructed per direction in the two-sided sweep: -1 .. B along d
@@ -89,6 +95,8 @@ struct FusedArgs {
   double beta;
   DevClock *clock;
   int nbr[3];
+  const S *fc0;  // MHD: face field of the stage input (the Riemann problems' normal B)
+  S *flux;       // MHD: face fluxes for the edge EMFs, layout [dir][8][nb * Pf]
 };
 
 // Global index -> interior index under the physical boundary of that side.
@@ -144,11 +152,18 @@ __device__ __forceinline__ void fz_fill_tables(const FusedArgs<S> &a, const int 
 }
 
 // Primitive state of the mesh cell at element offset n (flips: mirrored axes).
-template <typename S>
+template <typename S, bool MHD = false>
 __device__ __forceinline__ void fz_load_prim(const FusedArgs<S> &a, long long n, const bool flip[3], S *V) {
   const MeshDesc &m = a.m;
   const long long NP = (long long)m.nb * m.P;
   const S dens = a.u0[n];
+  // MHD: the cell-centred field (the face averages the previous stage left in
+  // the conserved container); reflecting boundaries are not run with MHD
+  S B[3] = {S(0), S(0), S(0)};
+  if constexpr (MHD) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) B[d] = a.u0[(CMAGC0 + d) * NP + n];
+  }
   if (a.stored) {
     V[RDENS] = dens;
 #pragma unroll
@@ -159,6 +174,10 @@ __device__ __forceinline__ void fz_load_prim(const FusedArgs<S> &a, long long n,
     V[RPRES] = a.prim[PPRES * NP + n];
     V[RBMOD] = a.prim[PBMOD * NP + n];
     V[REINT] = a.prim[PEINT * NP + n];
+    if constexpr (MHD) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) V[RMAGC0 + d] = B[d];
+    }
   } else {
     S mo[3];
 #pragma unroll
@@ -168,14 +187,14 @@ __device__ __forceinline__ void fz_load_prim(const FusedArgs<S> &a, long long n,
     }
     double e = double(a.u0[CENER * NP + n]);
     if constexpr (sizeof(S) == 4) e += double(a.u0lo[n]);
-    Cons2PrimEos<false, S>(a.eos, dens, mo[0], mo[1], mo[2], e, nullptr, V);
+    Cons2PrimEos<MHD, S>(a.eos, dens, mo[0], mo[1], mo[2], e, B, V);
   }
 }
 
 // 1. Primitives of the brick extended by H cells along DIR, into sp.
-template <typename S, int NDIM, int RECON, int DIR, bool OVERLAP>
+template <typename S, int NDIM, int RECON, int DIR, bool OVERLAP, bool MHD>
 __device__ __forceinline__ void fz_stage_prims(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &t, S *sp) {
-  using Sh = FusedShape<NDIM, RECON>;
+  using Sh = FusedShape<NDIM, RECON, MHD>;
   constexpr int H = Sh::H;
   constexpr int E0 = Sh::B[0] + (DIR == 0 ? 2 * H : 0);
   constexpr int E1 = Sh::B[1] + (DIR == 1 ? 2 * H : 0);
@@ -199,7 +218,7 @@ __device__ __forceinline__ void fz_stage_prims(const FusedArgs<S> &a, const FzTa
     flip[2] = t.flip[2][t2] != 0;
     return t.off[0][t0] + t.off[1][t1] + t.off[2][t2];
   };
-  if (OVERLAP && a.stored) {
+  if (OVERLAP && !MHD && a.stored) {
     const long long NP = (long long)a.m.nb * a.m.P;
     S V[NIT][7];
 #pragma unroll
@@ -231,10 +250,10 @@ __device__ __forceinline__ void fz_stage_prims(const FusedArgs<S> &a, const FzTa
     for (int q = threadIdx.x; q < NREG; q += Sh::NT) {
       bool flip[3];
       const long long n = cell(q, flip);
-      S V[7];
-      fz_load_prim<S>(a, n, flip, V);
+      S V[Sh::NR];
+      fz_load_prim<S, MHD>(a, n, flip, V);
 #pragma unroll
-      for (int r = 0; r < 7; r++) sp[r * RM + q] = V[r];
+      for (int r = 0; r < Sh::NR; r++) sp[r * RM + q] = V[r];
     }
   }
 }
@@ -257,10 +276,11 @@ __device__ __forceinline__ long long fz_owned(const FusedArgs<S> &a, int b, cons
 // per array and brick plane covers the plane's owned rows (the span from its
 // first owned cell to its last, rounded out to 16 bytes; the rounding stays
 // inside the block's ghost-padded storage).
-template <typename S, int NDIM, int RECON>
+template <typename S, int NDIM, int RECON, bool MHD>
 __device__ __forceinline__ void fz_prefetch_epilogue(const FusedArgs<S> &a, int b, const int o[3]) {
-  using Sh = FusedShape<NDIM, RECON>;
-  constexpr int NARR = sizeof(S) == 4 ? 12 : 10;
+  using Sh = FusedShape<NDIM, RECON, MHD>;
+  constexpr int NV = Sh::NC;
+  constexpr int NARR = 2 * NV + (sizeof(S) == 4 ? 2 : 0);
   const MeshDesc &m = a.m;
   const long long NP = (long long)m.nb * m.P;
   constexpr int B0 = Sh::B[0], B1 = Sh::B[1], B2 = Sh::B[2];
@@ -272,12 +292,12 @@ __device__ __forceinline__ void fz_prefetch_epilogue(const FusedArgs<S> &a, int 
         (long long)b * m.P + ((long long)(l2 + m.g[2]) * m.np[1] + (o[1] + m.g[1])) * m.np[0] + (o[0] + m.g[0]);
     const long long n1 = n0 + (long long)(len1 - 1) * m.np[0] + len0;  // one past the plane's last owned cell
     uintptr_t lo, hi;
-    if (arr < 10) {
-      const S *base = arr < 5 ? a.ub + arr * NP : a.u0 + (arr - 5) * NP;
+    if (arr < 2 * NV) {
+      const S *base = arr < NV ? a.ub + Sh::cons(arr) * NP : a.u0 + Sh::cons(arr - NV) * NP;
       lo = uintptr_t(base + n0);
       hi = uintptr_t(base + n1);
     } else {
-      const float *base = arr == 10 ? a.ublo : a.u0lo;
+      const float *base = arr == 2 * NV ? a.ublo : a.u0lo;
       lo = uintptr_t(base + n0);
       hi = uintptr_t(base + n1);
     }
@@ -289,10 +309,10 @@ __device__ __forceinline__ void fz_prefetch_epilogue(const FusedArgs<S> &a, int 
 
 // Last step of a direction: the divergence contribution of the DIR faces in sf
 // to the owned cells' accumulators.
-template <typename S, int NDIM, int RECON, int DIR>
+template <typename S, int NDIM, int RECON, int DIR, bool MHD>
 __device__ __forceinline__ void fz_accumulate(const FusedArgs<S> &a, const S *sf,
-                                              S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
-  using Sh = FusedShape<NDIM, RECON>;
+                                              S (&du)[FusedShape<NDIM, RECON, MHD>::CPT][FusedShape<NDIM, RECON, MHD>::NC]) {
+  using Sh = FusedShape<NDIM, RECON, MHD>;
   constexpr int B0 = Sh::B[0], B1 = Sh::B[1];
   constexpr int FM = Sh::template face_stride<S>();
   const S A = S(a.m.area[DIR]);
@@ -313,7 +333,7 @@ __device__ __forceinline__ void fz_accumulate(const FusedArgs<S> &a, const S *sf
         hi = lo + B0 * B1;
       }
 #pragma unroll
-      for (int v = 0; v < 5; v++) du[s][v] -= (A * sf[v * FM + hi] - A * sf[v * FM + lo]);
+      for (int v = 0; v < Sh::NC; v++) du[s][v] -= (A * sf[v * FM + hi] - A * sf[v * FM + lo]);
     }
   }
 }
@@ -326,11 +346,11 @@ __device__ __forceinline__ void fz_accumulate(const FusedArgs<S> &a, const S *sf
 // transverse plane in NCH chunks so its reconstruction buffers stay small
 // enough for two CTAs per SM; in FP32 one chunk covers the plane and the
 // face fluxes reuse the primitive tile's storage.
-template <typename S, int NDIM, int RECON, int RIEMANN, int DIR, bool OVERLAP>
-__device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &tb,
-                                              unsigned short *rofs, S *sp, S *rm, S *rp, S *sf,
-                                              S (&du)[FusedShape<NDIM, RECON>::CPT][5]) {
-  using Sh = FusedShape<NDIM, RECON>;
+template <typename S, int NDIM, int RECON, int RIEMANN, int DIR, bool OVERLAP, bool MHD>
+__device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTables<NDIM, RECON> &tb, int b,
+                                              const int o[3], unsigned short *rofs, S *sp, S *rm, S *rp, S *sf,
+                                              S (&du)[FusedShape<NDIM, RECON, MHD>::CPT][FusedShape<NDIM, RECON, MHD>::NC]) {
+  using Sh = FusedShape<NDIM, RECON, MHD>;
   constexpr int H = Sh::H, W = Sh::W;
   constexpr int B0 = Sh::B[0], B1 = Sh::B[1], B2 = Sh::B[2];
   constexpr int E0 = B0 + (DIR == 0 ? 2 * H : 0);
@@ -374,7 +394,7 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
       rofs[q] = (unsigned short)(ex + E0 * (ey + E1 * ez));
     }
   }
-  fz_stage_prims<S, NDIM, RECON, DIR, OVERLAP>(a, tb, sp);
+  fz_stage_prims<S, NDIM, RECON, DIR, OVERLAP, MHD>(a, tb, sp);
   __syncthreads();
 
 #pragma unroll 1
@@ -431,7 +451,7 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
     // FP32 pairs faces across the slowest transverse axis of even extent
     // (none in 1D); the partner lies LQO further in the reconstruction grid
     // and GFO further in the face grid.
-    constexpr int QA = sizeof(S) != 4 ? -1
+    constexpr int QA = (sizeof(S) != 4 || MHD) ? -1
                        : (G2 > 1 && G2 % 2 == 0) ? 2
                        : (G1 > 1 && G1 % 2 == 0) ? 1
                        : (G0 % 2 == 0 && DIR != 0) ? 0 : -1;
@@ -462,31 +482,65 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
       for (int it = tid; it < NFC; it += Sh::NT) {
         const int x = it % G0, y = (it / G0) % G1, z = it / (G0 * G1);
         const int lq = x + C0 * (y + C1 * z);
-        S vL[7], vR[7];
+        S vL[Sh::NR], vR[Sh::NR];
 #pragma unroll
-        for (int r = 0; r < 7; r++) {
+        for (int r = 0; r < Sh::NR; r++) {
           vL[r] = rp[r * RC + lq];
           vR[r] = rm[r * RC + lq + RST];
         }
-        S F[5];
-        RiemannFlux<RIEMANN, false, DIR, S>(vL, vR, F);
+        // MHD: block-local cell coordinates of the face (the face between
+        // cells L-1 and L along DIR) and its offset in the face arrays
+        const int L0 = o[0] + x, L1 = o[1] + y + c1, L2 = o[2] + z + c2;
+        long long fo = 0;
+        bool own = false;
+        if constexpr (MHD) {
+          const MeshDesc &m = a.m;
+          const int Ld = DIR == 0 ? L0 : DIR == 1 ? L1 : L2;
+          const int f = Ld - o[DIR];
+          constexpr int BD = DIR == 0 ? B0 : DIR == 1 ? B1 : B2;
+          own = Ld <= m.nx[DIR] && (f < BD || Ld == m.nx[DIR]);
+#pragma unroll
+          for (int t = 0; t < 3; t++)
+            if (t != DIR) own = own && (t == 0 ? L0 : t == 1 ? L1 : L2) < m.nx[t];
+          // clamped into the block for faces of partial bricks, which no
+          // owned cell uses
+          const int c0 = min(L0, m.nx[0] - (DIR == 0 ? 0 : 1)), c1_ = min(L1, m.nx[1] - (DIR == 1 ? 0 : 1)),
+                    c2_ = min(L2, m.nx[2] - (DIR == 2 ? 0 : 1));
+          fo = (long long)b * m.Pf + ((long long)(c2_ + m.g[2]) * m.nf[1] + (c1_ + m.g[1])) * m.nf[0] + (c0 + m.g[0]);
+          // CT: the normal component is the face field (hydro_add_flux_tasks.cpp:343-346)
+          const S bn = a.fc0[(long long)DIR * m.nb * m.Pf + fo];
+          vL[RMAGC0 + DIR] = bn;
+          vR[RMAGC0 + DIR] = bn;
+        }
+        S F[MHD ? 8 : 5];
+        RiemannFlux<RIEMANN, MHD, DIR, S>(vL, vR, F);
         const int gf = x + F0 * ((y + c1) + F1 * (z + c2));
 #pragma unroll
-        for (int v = 0; v < 5; v++) sf[v * FM + gf] = F[v];
+        for (int v = 0; v < Sh::NC; v++) sf[v * FM + gf] = F[Sh::cons(v)];
+        if constexpr (MHD) {
+          // the transverse field fluxes the edge EMFs read
+          if (own) {
+            const long long NF = (long long)a.m.nb * a.m.Pf;
+#pragma unroll
+            for (int t = 0; t < NDIM; t++)
+              if (t != DIR) a.flux[((long long)DIR * 8 + CMAGC0 + t) * NF + fo] = F[CMAGC0 + t];
+          }
+        }
       }
     }
     __syncthreads();
   }
 
-  fz_accumulate<S, NDIM, RECON, DIR>(a, sf, du);
+  fz_accumulate<S, NDIM, RECON, DIR, MHD>(a, sf, du);
   __syncthreads();
 }
 
 // Brick br of block b for one stage: the whole per-CTA body.  Every thread of
 // the CTA calls it (it synchronises internally).
-template <typename S, int NDIM, int RECON, int RIEMANN, bool OVERLAP>
+template <typename S, int NDIM, int RECON, int RIEMANN, bool OVERLAP, bool MHD = false>
 __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br, double dt) {
-  using Sh = FusedShape<NDIM, RECON>;
+  using Sh = FusedShape<NDIM, RECON, MHD>;
+  constexpr int NV = Sh::NC;
   extern __shared__ __align__(16) unsigned char kmy_smem[];
   S *sp = reinterpret_cast<S *>(kmy_smem);
 
@@ -495,13 +549,13 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
                     (br / (a.nbr[0] * a.nbr[1])) * Sh::B[2]};
   const int lx[3] = {b % m.nbx[0], (b / m.nbx[0]) % m.nbx[1], b / (m.nbx[0] * m.nbx[1])};
 
-  S du[Sh::CPT][5];
+  S du[Sh::CPT][NV];
 #pragma unroll
   for (int s = 0; s < Sh::CPT; s++)
 #pragma unroll
-    for (int v = 0; v < 5; v++) du[s][v] = S(0);
+    for (int v = 0; v < NV; v++) du[s][v] = S(0);
 
-  fz_prefetch_epilogue<S, NDIM, RECON>(a, b, o);
+  fz_prefetch_epilogue<S, NDIM, RECON, MHD>(a, b, o);
   __shared__ FzTables<NDIM, RECON> tb;
   fz_fill_tables<S, NDIM, RECON>(a, lx, o, tb);
   __syncthreads();
@@ -510,9 +564,9 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
   S *rp = rm + Sh::NR * (Sh::RC_MAX / NCH);
   S *sf = NCH == 1 ? sp : rp + Sh::NR * (Sh::RC_MAX / NCH);
   __shared__ unsigned short rofs[sizeof(S) == 4 ? Sh::RC_MAX / 2 : 1];
-  fz_direction2<S, NDIM, RECON, RIEMANN, 0, OVERLAP>(a, tb, rofs, sp, rm, rp, sf, du);
-  if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1, OVERLAP>(a, tb, rofs, sp, rm, rp, sf, du);
-  if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2, OVERLAP>(a, tb, rofs, sp, rm, rp, sf, du);
+  fz_direction2<S, NDIM, RECON, RIEMANN, 0, OVERLAP, MHD>(a, tb, b, o, rofs, sp, rm, rp, sf, du);
+  if constexpr (NDIM > 1) fz_direction2<S, NDIM, RECON, RIEMANN, 1, OVERLAP, MHD>(a, tb, b, o, rofs, sp, rm, rp, sf, du);
+  if constexpr (NDIM > 2) fz_direction2<S, NDIM, RECON, RIEMANN, 2, OVERLAP, MHD>(a, tb, b, o, rofs, sp, rm, rp, sf, du);
 
   // epilogue: low-storage update of the owned interior cells.  With OVERLAP
   // the inputs of all the thread's cells are loaded first so their loads
@@ -523,16 +577,16 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
   double dtl = INFINITY;
   struct In {
     long long n;
-    S b[5], z[5];
+    S b[NV], z[NV];
     float blo, zlo;
   };
   auto load = [&](int s, In &in) {
     in.n = fz_owned<S, NDIM, RECON>(a, b, o, threadIdx.x + s * Sh::NT);
     if (in.n < 0) return;
 #pragma unroll
-    for (int v = 0; v < 5; v++) {
-      in.b[v] = a.ub[v * NP + in.n];
-      in.z[v] = a.u0[v * NP + in.n];
+    for (int v = 0; v < NV; v++) {
+      in.b[v] = a.ub[Sh::cons(v) * NP + in.n];
+      in.z[v] = a.u0[Sh::cons(v) * NP + in.n];
     }
     if constexpr (sizeof(S) == 4) {
       in.blo = a.ublo[in.n];
@@ -554,10 +608,10 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
     }
     const long long n = cur.n;
     if (n < 0) continue;
-    S un[5];
+    S un[NV];
     float unlo = 0.f;
 #pragma unroll
-    for (int v = 0; v < 5; v++) {
+    for (int v = 0; v < NV; v++) {
       const S dudt = du[s][v] / vol;
       if (sizeof(S) == 4 && v == CENER) {
         double eb = double(cur.b[CENER]), e0 = double(cur.z[CENER]);
@@ -575,9 +629,10 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
       }
       const S y0 = bt * cur.b[v] + (S(1.0) - bt) * cur.z[v];
       un[v] = y0 + bt * S(dt) * dudt;
-      a.u1[v * NP + n] = un[v];
+      a.u1[Sh::cons(v) * NP + n] = un[v];
     }
-    if (a.last || a.prim_out) {
+    // MHD: the primitives and the time step wait for the face update
+    if (!MHD && (a.last || a.prim_out)) {
       double e = double(un[CENER]);
       if constexpr (sizeof(S) == 4) e += double(unlo);
       S V[7];
@@ -619,9 +674,10 @@ __device__ __forceinline__ void fused_brick(const FusedArgs<S> &a, int b, int br
 // A stage after the run reached tlim (queued ahead of the host's check)
 // leaves the state as it is: u1 and the output primitives become copies of
 // the input, so the host's container and buffer swaps stay consistent.
-template <typename S, int NDIM, int RECON>
+template <typename S, int NDIM, int RECON, bool MHD>
 __device__ __forceinline__ void fused_passthrough(const FusedArgs<S> &a, int b, int br) {
   using Sh = FusedShape<NDIM, RECON>;
+  constexpr int NCC = MHD ? 8 : 5;
   const MeshDesc &m = a.m;
   const long long NP = (long long)m.nb * m.P;
   const int o[3] = {(br % a.nbr[0]) * Sh::B[0], ((br / a.nbr[0]) % a.nbr[1]) * Sh::B[1],
@@ -633,7 +689,7 @@ __device__ __forceinline__ void fused_passthrough(const FusedArgs<S> &a, int b, 
                         ((long long)(l2 + m.g[2]) * m.np[1] + (l1 + m.g[1])) * m.np[0] + (l0 + m.g[0]);
     if (a.u1 != a.u0) {
 #pragma unroll
-      for (int v = 0; v < 5; v++) a.u1[v * NP + n] = a.u0[v * NP + n];
+      for (int v = 0; v < NCC; v++) a.u1[v * NP + n] = a.u0[v * NP + n];
       if constexpr (sizeof(S) == 4) a.u1lo[n] = a.u0lo[n];
     }
     if (a.prim_out) {
@@ -650,15 +706,15 @@ __device__ __forceinline__ void fused_passthrough(const FusedArgs<S> &a, int b, 
 }
 
 // One stage of one mesh: one CTA per brick.
-template <typename S, int NDIM, int RECON, int RIEMANN>
-__global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT) k_fused_stage(FusedArgs<S> a) {
+template <typename S, int NDIM, int RECON, int RIEMANN, bool MHD>
+__global__ void __launch_bounds__(FusedShape<NDIM, RECON, MHD>::NT) k_fused_stage(FusedArgs<S> a) {
   const int nbrick = a.nbr[0] * a.nbr[1] * a.nbr[2];
   const int b = blockIdx.x / nbrick;
   if (a.clock->done) {
-    fused_passthrough<S, NDIM, RECON>(a, b, blockIdx.x - b * nbrick);
+    fused_passthrough<S, NDIM, RECON, MHD>(a, b, blockIdx.x - b * nbrick);
     return;
   }
-  fused_brick<S, NDIM, RECON, RIEMANN, true>(a, b, blockIdx.x - b * nbrick, a.clock->dt);
+  fused_brick<S, NDIM, RECON, RIEMANN, true, MHD>(a, b, blockIdx.x - b * nbrick, a.clock->dt);
 }
 
 // ---------------------------------------------------------------------------
@@ -706,6 +762,8 @@ __device__ __forceinline__ void batch_args(const SolveDesc<S> &q, int stage, Fus
   a.nbr[0] = q.nbr[0];
   a.nbr[1] = q.nbr[1];
   a.nbr[2] = q.nbr[2];
+  a.fc0 = nullptr;
+  a.flux = nullptr;
 }
 
 template <typename S, int NDIM, int RECON, int RIEMANN>
@@ -744,14 +802,14 @@ __global__ void __launch_bounds__(FusedShape<NDIM, RECON>::NT, sizeof(S) == 4 ? 
   }
 }
 
-template <typename S, int NDIM, int RECON, int RIEMANN>
+template <typename S, int NDIM, int RECON, int RIEMANN, bool MHD>
 int fused_launch(kmy_ctx *c, FusedArgs<S> a) {
-  using Sh = FusedShape<NDIM, RECON>;
+  using Sh = FusedShape<NDIM, RECON, MHD>;
   const MeshDesc &m = c->m;
   for (int d = 0; d < 3; d++) a.nbr[d] = (m.nx[d] + Sh::B[d] - 1) / Sh::B[d];
   const long long grid = (long long)a.nbr[0] * a.nbr[1] * a.nbr[2] * m.nb;
   const size_t smem = Sh::template smem_bytes<S>();
-  auto kern = k_fused_stage<S, NDIM, RECON, RIEMANN>;
+  auto kern = k_fused_stage<S, NDIM, RECON, RIEMANN, MHD>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return cuda_check(c, e, "fused smem attribute");
   kern<<<unsigned(grid), Sh::NT, smem, c->stream>>>(a);
@@ -759,18 +817,22 @@ int fused_launch(kmy_ctx *c, FusedArgs<S> a) {
   return cuda_check(c, cudaGetLastError(), "fused stage");
 }
 
+// Hydro in 1D-3D; MHD (constrained transport) in 2D and 3D.
 template <typename S>
 int fused_dispatch(kmy_ctx *c, FusedArgs<S> a) {
   const int nd = c->m.ndim, rec = c->prm.recon, rie = c->prm.riemann;
-#define KMY_FZ(ND, RC)                                               \
-  if (nd == ND && rec == RC) {                                       \
-    return rie == HLL ? fused_launch<S, ND, RC, HLL>(c, a)           \
-                      : fused_launch<S, ND, RC, HLLC>(c, a);         \
+  const bool mhd = c->prm.mhd;
+#define KMY_FZ(ND, RC, M)                                            \
+  if (nd == ND && rec == RC && mhd == M) {                           \
+    return rie == HLL ? fused_launch<S, ND, RC, HLL, M>(c, a)        \
+                      : fused_launch<S, ND, RC, HLLC, M>(c, a);      \
   }
-#define KMY_FZ_ND(ND) KMY_FZ(ND, FOG) KMY_FZ(ND, PLM) KMY_FZ(ND, PPM) KMY_FZ(ND, WENOZ)
-  KMY_FZ_ND(1)
-  KMY_FZ_ND(2)
-  KMY_FZ_ND(3)
+#define KMY_FZ_ND(ND, M) KMY_FZ(ND, FOG, M) KMY_FZ(ND, PLM, M) KMY_FZ(ND, PPM, M) KMY_FZ(ND, WENOZ, M)
+  KMY_FZ_ND(1, false)
+  KMY_FZ_ND(2, false)
+  KMY_FZ_ND(3, false)
+  KMY_FZ_ND(2, true)
+  KMY_FZ_ND(3, true)
 #undef KMY_FZ_ND
 #undef KMY_FZ
   c->err = "no fused kernel for this configuration";

@@ -189,6 +189,14 @@ int launch_compute_emf(kmy_ctx *c, Container &md0);
 int launch_flux_divergence(kmy_ctx *c, Container &md0, Container &dudt);
 int launch_apply_dudt(kmy_ctx *c, Container &base, Container &md0, Container &md1,
                       Container &dudt, double beta, double dt, const double *dt_dev);
+// constrained-transport pieces of a stage that the fused stage leaves to
+// separate kernels
+int ensure_flux(kmy_ctx *c);
+const char *fused_ct_unsupported(const kmy_ctx *c);  // kmy_fused.cu
+int launch_flux_halo(kmy_ctx *c);
+int launch_flux_stokes(kmy_ctx *c, Container &md0, Container &dudt);
+int launch_apply_faces(kmy_ctx *c, Container &base, Container &md0, Container &md1, Container &dudt,
+                       double beta, double dt, const double *dt_dev);
 int launch_prepare_primitive(kmy_ctx *c, Container &md1);
 int launch_estimate_dt(kmy_ctx *c, Container &md, bool reset);
 int launch_fill_derived(kmy_ctx *c, Container &md);

@@ -263,14 +263,16 @@ static void face_flux_dir(kmy_ctx *c, int dir, const S *cc, const S *prim, const
   c->launches++;
 }
 
+// Face flux storage, [dir][ncc][nb * Pf], allocated on first use.
+int ensure_flux(kmy_ctx *c) {
+  if (c->flux) return KMY_OK;
+  return dalloc(c, &c->flux, c->esz * 3 * c->ncc * size_t(c->m.nb) * c->m.Pf);
+}
+
 template <typename S>
 static int compute_fluxes_t(kmy_ctx *c, Container &md0) {
   const MeshDesc &m = c->m;
-  if (!c->flux) {
-    const size_t bytes = c->esz * 3 * c->ncc * size_t(m.nb) * m.Pf;
-    const int rc = dalloc(c, &c->flux, bytes);
-    if (rc) return rc;
-  }
+  if (const int rc = ensure_flux(c)) return rc;
   const S *cc = (const S *)md0.cc, *prim = (const S *)c->prim, *fc = (const S *)md0.fc;
   S *flux = (S *)c->flux;
   const int rec = c->prm.recon, rie = c->prm.riemann;
@@ -295,6 +297,65 @@ static int compute_fluxes_t(kmy_ctx *c, Container &md0) {
 
 int launch_compute_fluxes(kmy_ctx *c, Container &md0) {
   return c->esz == 8 ? compute_fluxes_t<double>(c, md0) : compute_fluxes_t<float>(c, md0);
+}
+
+// ---------------------------------------------------------------------------
+// Ghost-layer transverse field fluxes for the edge EMFs.  The fused stage
+// computes face fluxes on interior faces only; the EMF of an edge on a block
+// face also reads F_a[B_t] one cell row outside the block across t.  On a
+// single-level mesh with periodic or outflow boundaries that row is the
+// interior row of the block owning it (or the boundary row itself, for
+// outflow), as the boundary exchange would have filled the cells the flux
+// came from, so the flux is copied from there.  One thread per ghost-layer
+// face: face direction a, transverse axis t, side, the a-face index and the
+// remaining axis c.
+template <typename S>
+__global__ void k_flux_halo(MeshDesc m, S *flux, int a, int t, int na, int nc) {
+  const int cax = 3 - a - t;
+  const long long tt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long per = 2LL * na * nc;
+  if (tt >= per * m.nb) return;
+  const int b = int(tt / per);
+  int r = int(tt - (long long)b * per);
+  const int side = r / (na * nc);
+  r -= side * na * nc;
+  const int ia = r % na, ic = r / na;
+  int lb[3] = {block_loc(m, b, 0), block_loc(m, b, 1), block_loc(m, b, 2)};
+  // destination: ghost row -1 or nx_t across t
+  int L[3];
+  L[a] = ia;
+  L[cax] = ic;
+  L[t] = side ? m.nx[t] : -1;
+  // source: the interior row that ghost row maps to
+  bool flip = false;
+  const int G = lb[t] * m.nx[t] + L[t];
+  const int M = map_index(G, m.mesh_nx[t], m.bc[t][side], flip);
+  const int ob = M / m.nx[t];
+  int Ls[3] = {L[0], L[1], L[2]};
+  Ls[t] = M - ob * m.nx[t];
+  int sb[3] = {lb[0], lb[1], lb[2]};
+  sb[t] = ob;
+  const int bs = sb[0] + m.nbx[0] * (sb[1] + m.nbx[1] * sb[2]);
+  const long long NF = (long long)m.nb * m.Pf;
+  S *F = flux + ((long long)a * 8 + CMAGC0 + t) * NF;
+  F[(long long)b * m.Pf + fidx(m, L[2] + m.g[2], L[1] + m.g[1], L[0] + m.g[0])] =
+      F[(long long)bs * m.Pf + fidx(m, Ls[2] + m.g[2], Ls[1] + m.g[1], Ls[0] + m.g[0])];
+}
+
+int launch_flux_halo(kmy_ctx *c) {
+  const MeshDesc &m = c->m;
+  for (int a = 0; a < m.ndim; a++)
+    for (int t = 0; t < m.ndim; t++) {
+      if (t == a) continue;
+      const int na = m.nx[a] + 1, nc = m.nx[3 - a - t];
+      const long long tot = 2LL * na * nc * m.nb;
+      if (c->esz == 8)
+        k_flux_halo<double><<<nblk(tot), kThreads, 0, c->stream>>>(m, (double *)c->flux, a, t, na, nc);
+      else
+        k_flux_halo<float><<<nblk(tot), kThreads, 0, c->stream>>>(m, (float *)c->flux, a, t, na, nc);
+      c->launches++;
+    }
+  return cuda_check(c, cudaGetLastError(), "flux_halo");
 }
 
 // ---------------------------------------------------------------------------
@@ -415,23 +476,29 @@ int launch_flux_divergence(kmy_ctx *c, Container &md0, Container &dudt) {
     k_flux_divergence<float><<<nblk(n), kThreads, 0, c->stream>>>(m, (const float *)c->flux,
                                                                     (float *)dudt.cc, c->ncc);
   c->launches++;
-  if (c->prm.mhd && m.ndim > 1) {
-    struct FE { int face, ne, e0, e1; };
-    const FE l3[3] = {{0, 2, 2, 1}, {1, 2, 2, 0}, {2, 2, 0, 1}};
-    const FE l2[2] = {{0, 1, 2, 0}, {1, 1, 2, 0}};
-    const FE *l = m.ndim > 2 ? l3 : l2;
-    for (int f = 0; f < m.ndim; f++) {
-      const FE fe = l[f];
-      const long long nfc = (long long)(m.nx[0] + (fe.face == 0)) * (m.nx[1] + (fe.face == 1)) *
-                            (m.nx[2] + (fe.face == 2)) * m.nb;
-      if (c->esz == 8)
-        k_flux_stokes<double><<<nblk(nfc), kThreads, 0, c->stream>>>(
-            m, (const double *)md0.emf, (double *)dudt.fc, fe.face, fe.ne, fe.e0, fe.e1);
-      else
-        k_flux_stokes<float><<<nblk(nfc), kThreads, 0, c->stream>>>(
-            m, (const float *)md0.emf, (float *)dudt.fc, fe.face, fe.ne, fe.e0, fe.e1);
-      c->launches++;
-    }
+  if (c->prm.mhd && m.ndim > 1) return launch_flux_stokes(c, md0, dudt);
+  return cuda_check(c, cudaGetLastError(), "flux_divergence");
+}
+
+// FluxStokes for every active face direction: dU/dt of the face field from
+// md0's edge EMFs.
+int launch_flux_stokes(kmy_ctx *c, Container &md0, Container &dudt) {
+  const MeshDesc &m = c->m;
+  struct FE { int face, ne, e0, e1; };
+  const FE l3[3] = {{0, 2, 2, 1}, {1, 2, 2, 0}, {2, 2, 0, 1}};
+  const FE l2[2] = {{0, 1, 2, 0}, {1, 1, 2, 0}};
+  const FE *l = m.ndim > 2 ? l3 : l2;
+  for (int f = 0; f < m.ndim; f++) {
+    const FE fe = l[f];
+    const long long nfc = (long long)(m.nx[0] + (fe.face == 0)) * (m.nx[1] + (fe.face == 1)) *
+                          (m.nx[2] + (fe.face == 2)) * m.nb;
+    if (c->esz == 8)
+      k_flux_stokes<double><<<nblk(nfc), kThreads, 0, c->stream>>>(
+          m, (const double *)md0.emf, (double *)dudt.fc, fe.face, fe.ne, fe.e0, fe.e1);
+    else
+      k_flux_stokes<float><<<nblk(nfc), kThreads, 0, c->stream>>>(
+          m, (const float *)md0.emf, (float *)dudt.fc, fe.face, fe.ne, fe.e0, fe.e1);
+    c->launches++;
   }
   return cuda_check(c, cudaGetLastError(), "flux_divergence");
 }
@@ -508,20 +575,27 @@ int launch_apply_dudt(kmy_ctx *c, Container &base, Container &md0, Container &md
         (float *)md0.ener_lo, (float *)md1.cc, (float *)md1.ener_lo, (const float *)dudt.cc,
         c->ncc, beta, dt, dt_dev, clk);
   c->launches++;
-  if (c->prm.mhd && m.ndim > 1) {
-    for (int face = 0; face < m.ndim; face++) {
-      const long long nfc =
-          (long long)(m.nx[0] + (face == 0)) * (m.nx[1] + (face == 1)) * (m.nx[2] + (face == 2)) * m.nb;
-      if (c->esz == 8)
-        k_apply_faces<double><<<nblk(nfc), kThreads, 0, c->stream>>>(
-            m, (const double *)base.fc, (double *)md0.fc, (double *)md1.fc, (const double *)dudt.fc,
-            face, beta, dt, dt_dev, clk);
-      else
-        k_apply_faces<float><<<nblk(nfc), kThreads, 0, c->stream>>>(
-            m, (const float *)base.fc, (float *)md0.fc, (float *)md1.fc, (const float *)dudt.fc,
-            face, beta, dt, dt_dev, clk);
-      c->launches++;
-    }
+  if (c->prm.mhd && m.ndim > 1) return launch_apply_faces(c, base, md0, md1, dudt, beta, dt, dt_dev);
+  return cuda_check(c, cudaGetLastError(), "apply_dudt");
+}
+
+// The face-field half of ApplyDuDt for every active face direction.
+int launch_apply_faces(kmy_ctx *c, Container &base, Container &md0, Container &md1, Container &dudt,
+                       double beta, double dt, const double *dt_dev) {
+  const MeshDesc &m = c->m;
+  const DevClock *clk = dt_dev ? c->clock : nullptr;
+  for (int face = 0; face < m.ndim; face++) {
+    const long long nfc =
+        (long long)(m.nx[0] + (face == 0)) * (m.nx[1] + (face == 1)) * (m.nx[2] + (face == 2)) * m.nb;
+    if (c->esz == 8)
+      k_apply_faces<double><<<nblk(nfc), kThreads, 0, c->stream>>>(
+          m, (const double *)base.fc, (double *)md0.fc, (double *)md1.fc, (const double *)dudt.fc,
+          face, beta, dt, dt_dev, clk);
+    else
+      k_apply_faces<float><<<nblk(nfc), kThreads, 0, c->stream>>>(
+          m, (const float *)base.fc, (float *)md0.fc, (float *)md1.fc, (const float *)dudt.fc,
+          face, beta, dt, dt_dev, clk);
+    c->launches++;
   }
   return cuda_check(c, cudaGetLastError(), "apply_dudt");
 }

@@ -40,6 +40,18 @@ def test_kh3d_fp32_vs_fp64(kmy_lib, path):
     assert abs(t32["time"] - t64["time"]) <= 1e-5 * t64["time"]
 
 
+@pytest.mark.parametrize("path", ["fused", "tasks"])
+def test_orszag_tang_fp32_vs_fp64(kmy_lib, path):
+    """3D Orszag-Tang with constrained transport, FP32 bulk against FP64."""
+    s32, s64 = _pair(configs.ot_3d(n=32, nb=16, precision="fp32"),
+                     configs.ot_3d(n=32, nb=16, precision="fp64"), "orszag_tang", 5, path)
+    for var, c in [("dens", 0), ("momentum", 0), ("momentum", 1), ("ener", 0), ("magc", 0), ("magc", 1)]:
+        err = rel_l1(s32.interior(s32.export(var, c)), s64.interior(s64.export(var, c)))
+        assert err <= L1_FP32, (var, c, err)
+    # div B of the FP32 face field, evaluated in FP64
+    assert np.abs(s32.interior(s32.export("divb"))).max() < 1e-4
+
+
 @pytest.mark.parametrize("recon,riemann", [("plm", "hll"), ("ppm", "hllc"), ("wenoz", "hllc")])
 def test_vortex2d_fp32_vs_fp64(kmy_lib, recon, riemann):
     s32, s64 = _pair(configs.vortex_2d(n=64, nb=32, recon=recon, riemann=riemann, nghost=3,
