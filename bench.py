@@ -353,7 +353,8 @@ def _evolve_timed(s, stream, tlim=None, nsteps=None):
 def workloads_block(a, device: int, stream) -> dict:
     """The other configurations of the path, each timed through kmy_step on one GPU:
     2D vortex to t=10 (FP64, fused), 3D Orszag-Tang with constrained transport
-    (FP32 bulk, per-task kernels), and the 2D blast on an adaptive mesh to t=0.2."""
+    (FP32 bulk; fused stage, and the per-task path beside it), and the 2D blast
+    on an adaptive mesh to t=0.2."""
     import kamayan_b200
     from kamayan_b200 import configs
 
@@ -373,17 +374,21 @@ def workloads_block(a, device: int, stream) -> dict:
                              "l1_density_vs_exact": s.vortex_error("dens"),
                              "config": "128^2 in 4x64^2, g=2, PLM(MC)+HLL, RK2, CFL 0.8, t=10"}
     s.close()
-    # c3: Orszag-Tang 192^3, 216 blocks of 32^3, CT, PPM+HLL, RK2, FP32 bulk
+    # c3: Orszag-Tang 192^3, 216 blocks of 32^3, CT, PPM+HLL, RK2, FP32 bulk;
+    # the fused stage (cells) + EMF / face-update kernels, and the per-task path
     n3 = min(a.n, 192)
-    s = solver(configs.ot_3d(n=n3, nb=32, precision="fp32"), "orszag_tang", "tasks")
-    _evolve_timed(s, stream, nsteps=2)
-    ms, upd, steps, _ = _evolve_timed(s, stream, nsteps=max(3, a.steps // 4))
-    divb = s.export("divb")
+    ot = {}
+    for path in ("fused", "tasks"):
+        s = solver(configs.ot_3d(n=n3, nb=32, precision="fp32"), "orszag_tang", path)
+        _evolve_timed(s, stream, nsteps=2)
+        ms, upd, steps, _ = _evolve_timed(s, stream, nsteps=max(3, a.steps // 4))
+        ot[path] = (upd / (ms / 1e3), steps, ms / steps, float(abs(s.interior(s.export("divb"))).max()))
+        s.close()
     out["orszag_tang_3d_ct_fp32"] = {
-        "cell_updates_per_s": upd / (ms / 1e3), "steps": steps, "ms_per_step": ms / steps,
-        "max_abs_divb": float(abs(s.interior(divb)).max()),
-        "config": f"{n3}^3 in 32^3 blocks, g=4, CT, PPM(MC)+HLL, RK2, CFL 0.3, per-task kernels"}
-    s.close()
+        "cell_updates_per_s": ot["fused"][0], "steps": ot["fused"][1], "ms_per_step": ot["fused"][2],
+        "max_abs_divb": ot["fused"][3],
+        "tasks_cell_updates_per_s": ot["tasks"][0], "tasks_ms_per_step": ot["tasks"][2],
+        "config": f"{n3}^3 in 32^3 blocks, g=4, CT, PPM(MC)+HLL, RK2, CFL 0.3, fused stage"}
     # c4: blast on an adaptive mesh, 128^2 base in 16^2 blocks, 3 levels, Loehner on density
     s = solver(configs.blast_2d_amr(), "blast", "tasks")
     ms, upd, steps, nbs = _evolve_timed(s, stream, tlim=0.2)

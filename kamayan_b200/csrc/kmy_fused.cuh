@@ -32,7 +32,9 @@ struct FusedShape {
   static constexpr int H = W + 1;
   static constexpr int B[3] = {NDIM == 3 ? 8 : NDIM == 2 ? 16 : 128, NDIM == 3 ? 8 : NDIM == 2 ? 16 : 1,
                                NDIM == 3 ? 8 : 1};
-  static constexpr int NT = 256;
+  // 3D MHD: 288 threads, so the 288 faces of a chunk's Riemann phase take
+  // one round (at 256 one warp ran a second round alone)
+  static constexpr int NT = (MHD && NDIM == 3) ? 288 : 256;
   static constexpr int NCELL = B[0] * B[1] * B[2];
   static constexpr int CPT = (NCELL + NT - 1) / NT;
   static constexpr int region(int d) { return (B[d] + 2 * H) * (NCELL / B[d]); }
@@ -58,10 +60,11 @@ struct FusedShape {
   // Each cell is reconstructed once (both faces, shared smoothness
   // indicators) into shared memory and the Riemann problems read from there.
   // In 3D FP64 the transverse plane goes through in two chunks, which keeps
-  // the reconstruction buffers small enough for two CTAs per SM.
+  // the reconstruction buffers small enough for two CTAs per SM; 3D FP32 MHD
+  // (ten reconstructed variables) does the same for three.
   template <typename S>
   static constexpr int nchunk() {
-    return (sizeof(S) == 8 && NDIM == 3) ? 2 : 1;
+    return (NDIM == 3 && (sizeof(S) == 8 || MHD)) ? 2 : 1;
   }
   // Face fluxes reuse the primitive tile with one chunk; with several they
   // need their own buffer (the tile is still being read).
@@ -378,14 +381,15 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
   const int tid = threadIdx.x;
 
   // FP32 reconstructs two cells per thread in packed arithmetic, (r, q) and
-  // (r, q + NRC/2).  The grid is halved along its slowest axis of extent > 1,
-  // so the partner's region cell lies a constant PO further.  rofs holds the
-  // region offset of each cell q of the first half.
+  // (r, q + NRC/2).  The chunk's grid is halved along its slowest axis of
+  // extent > 1, so the partner's region cell lies a constant PO further.
+  // rofs holds the region offset of each cell q of the first half of chunk 0;
+  // chunk ch adds its origin's offset.
   constexpr int PA = C2 > 1 ? 2 : (C1 > 1 ? 1 : 0);
   constexpr int HALF = NRC / 2;
   constexpr int PO = PA == 2 ? (C2 / 2) * E0 * E1 : PA == 1 ? (C1 / 2) * E0 : C0 / 2;
   if constexpr (sizeof(S) == 4) {
-    static_assert(NCH == 1 && (PA == 2 ? C2 : PA == 1 ? C1 : C0) % 2 == 0, "pairs split one even axis of one chunk");
+    static_assert((PA == 2 ? C2 : PA == 1 ? C1 : C0) % 2 == 0, "pairs split an even axis of the chunk");
     static_assert(Sh::REG_MAX < 65536, "region offsets are 16-bit");
     for (int q = tid; q < HALF; q += Sh::NT) {
       const int x = q % C0, y = (q / C0) % C1, z = q / (C0 * C1);
@@ -403,10 +407,11 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
     // 2. both face values of every (primitive, cell) of the chunk
     if constexpr (sizeof(S) == 4) {
       // item it = r * HALF + q, stepping by NT without divisions
+      const S *sc = sp + E0 * (c1 + E1 * c2);  // the chunk's origin in the region
       int r = tid / HALF, q = tid - (tid / HALF) * HALF;
 #pragma unroll 2
       for (; r < Sh::NR;) {
-        const S *c = sp + r * RM + rofs[q];
+        const S *c = sc + r * RM + rofs[q];
         float2 s[5];
 #pragma unroll
         for (int k = 0; k < 5; k++)
@@ -447,10 +452,32 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
     __syncthreads();
 
     // 3. Riemann flux at the chunk's DIR faces; the face at position f joins
-    // reconstruction cells f (its low cell, position f-1) and f+1
-    // FP32 pairs faces across the slowest transverse axis of even extent
-    // (none in 1D); the partner lies LQO further in the reconstruction grid
-    // and GFO further in the face grid.
+    // reconstruction cells f (its low cell, position f-1) and f+1.
+    // MHD: the face (x, y, z) of the chunk's face grid sits at block-local
+    // cell coordinates L (the face between cells L-1 and L along DIR); its
+    // offset in the face arrays, clamped into the block for faces of partial
+    // bricks (which no owned cell uses), and whether this brick writes its
+    // flux for the edge EMFs (each interior face once).
+    auto face_at = [&](int x, int y, int z, long long &fo) -> bool {
+      const MeshDesc &m = a.m;
+      const int L[3] = {o[0] + x, o[1] + y + c1, o[2] + z + c2};
+      constexpr int BD = DIR == 0 ? B0 : DIR == 1 ? B1 : B2;
+      bool own = L[DIR] <= m.nx[DIR] && (L[DIR] - o[DIR] < BD || L[DIR] == m.nx[DIR]);
+      int c[3];
+#pragma unroll
+      for (int t = 0; t < 3; t++) {
+        const int hi = m.nx[t] - (t == DIR ? 0 : 1);
+        if (t != DIR) own = own && L[t] <= hi;
+        c[t] = min(L[t], hi);
+      }
+      fo = (long long)b * m.Pf + ((long long)(c[2] + m.g[2]) * m.nf[1] + (c[1] + m.g[1])) * m.nf[0] + (c[0] + m.g[0]);
+      return own;
+    };
+    // FP32 hydro pairs faces across the slowest transverse axis of even
+    // extent (none in 1D); the partner lies LQO further in the
+    // reconstruction grid and GFO further in the face grid.  (A packed MHD
+    // HLL solver measured slower than the scalar one: more registers, one
+    // CTA per SM fewer.)
     constexpr int QA = (sizeof(S) != 4 || MHD) ? -1
                        : (G2 > 1 && G2 % 2 == 0) ? 2
                        : (G1 > 1 && G1 % 2 == 0) ? 1
@@ -488,27 +515,12 @@ __device__ __forceinline__ void fz_direction2(const FusedArgs<S> &a, const FzTab
           vL[r] = rp[r * RC + lq];
           vR[r] = rm[r * RC + lq + RST];
         }
-        // MHD: block-local cell coordinates of the face (the face between
-        // cells L-1 and L along DIR) and its offset in the face arrays
-        const int L0 = o[0] + x, L1 = o[1] + y + c1, L2 = o[2] + z + c2;
         long long fo = 0;
         bool own = false;
         if constexpr (MHD) {
-          const MeshDesc &m = a.m;
-          const int Ld = DIR == 0 ? L0 : DIR == 1 ? L1 : L2;
-          const int f = Ld - o[DIR];
-          constexpr int BD = DIR == 0 ? B0 : DIR == 1 ? B1 : B2;
-          own = Ld <= m.nx[DIR] && (f < BD || Ld == m.nx[DIR]);
-#pragma unroll
-          for (int t = 0; t < 3; t++)
-            if (t != DIR) own = own && (t == 0 ? L0 : t == 1 ? L1 : L2) < m.nx[t];
-          // clamped into the block for faces of partial bricks, which no
-          // owned cell uses
-          const int c0 = min(L0, m.nx[0] - (DIR == 0 ? 0 : 1)), c1_ = min(L1, m.nx[1] - (DIR == 1 ? 0 : 1)),
-                    c2_ = min(L2, m.nx[2] - (DIR == 2 ? 0 : 1));
-          fo = (long long)b * m.Pf + ((long long)(c2_ + m.g[2]) * m.nf[1] + (c1_ + m.g[1])) * m.nf[0] + (c0 + m.g[0]);
+          own = face_at(x, y, z, fo);
           // CT: the normal component is the face field (hydro_add_flux_tasks.cpp:343-346)
-          const S bn = a.fc0[(long long)DIR * m.nb * m.Pf + fo];
+          const S bn = a.fc0[(long long)DIR * a.m.nb * a.m.Pf + fo];
           vL[RMAGC0 + DIR] = bn;
           vR[RMAGC0 + DIR] = bn;
         }

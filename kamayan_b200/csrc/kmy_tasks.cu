@@ -47,6 +47,30 @@ __device__ __forceinline__ void store_ener(S *cc, float *lo, long long stride, l
   }
 }
 
+// Flat thread index t (< per * nblocks) -> block b and cell (i, j, k) of an
+// n0 x n1 x (per / (n0 n1)) range.  Unsigned 32-bit division whenever the
+// numbers fit, which every launch of a mesh below 2^32 cells does; 64-bit
+// integer division is a long software sequence on the GPU.
+__device__ __forceinline__ void unflatten(long long t, long long per, int n0, int n1, int &b, int &i, int &j,
+                                          int &k) {
+  if (t < (1LL << 32) && per < (1LL << 32)) {
+    const unsigned u = unsigned(t), p = unsigned(per);
+    const unsigned bb = u / p, r = u - bb * p;
+    const unsigned q = r / unsigned(n0);
+    b = int(bb);
+    i = int(r - q * unsigned(n0));
+    j = int(q % unsigned(n1));
+    k = int(q / unsigned(n1));
+  } else {
+    b = int(t / per);
+    long long r = t - (long long)b * per;
+    i = int(r % n0);
+    r /= n0;
+    j = int(r % n1);
+    k = int(r / n1);
+  }
+}
+
 static unsigned nblk(long long n) { return unsigned((n + kThreads - 1) / kThreads); }
 
 // ---------------------------------------------------------------------------
@@ -65,12 +89,8 @@ template <typename S>
 __global__ void k_fill_ghost_cells(MeshDesc m, S *cc, float *lo, S *prim, int ncc) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)m.nb * m.P) return;
-  const int b = int(t / m.P);
-  long long r = t - (long long)b * m.P;
-  const int i = int(r % m.np[0]);
-  r /= m.np[0];
-  const int j = int(r % m.np[1]);
-  const int k = int(r / m.np[1]);
+  int b, i, j, k;
+  unflatten(t, m.P, m.np[0], m.np[1], b, i, j, k);
   const int loc[3] = {i, j, k};
   bool interior = true;
   for (int d = 0; d < 3; d++)
@@ -111,12 +131,8 @@ template <typename S>
 __global__ void k_fill_ghost_faces(MeshDesc m, S *fc, int e) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)m.nb * m.Pf) return;
-  const int b = int(t / m.Pf);
-  long long r = t - (long long)b * m.Pf;
-  const int i = int(r % m.nf[0]);
-  r /= m.nf[0];
-  const int j = int(r % m.nf[1]);
-  const int k = int(r / m.nf[1]);
+  int b, i, j, k;
+  unflatten(t, m.Pf, m.nf[0], m.nf[1], b, i, j, k);
   const int loc[3] = {i, j, k};
   for (int d = 0; d < 3; d++)
     if (loc[d] >= m.np[d] + (d == e ? 1 : 0)) return;  // outside this element's extent
@@ -186,12 +202,11 @@ __global__ void k_face_flux(MeshDesc m, int limiter, const S *cc, const S *prim,
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)n0 * n1 * n2;
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = lo0 + int(r % n0);
-  r /= n0;
-  const int j = lo1 + int(r % n1);
-  const int k = lo2 + int(r / n1);
+  int b, i, j, k;
+  unflatten(t, per, n0, n1, b, i, j, k);
+  i += lo0;
+  j += lo1;
+  k += lo2;
   const long long NP = (long long)m.nb * m.P;
   const long long base = (long long)b * m.P + cidx(m, k, j, i);
   const long long st = DIR == 0 ? 1 : DIR == 1 ? m.np[0] : (long long)m.np[0] * m.np[1];
@@ -366,12 +381,11 @@ __global__ void k_edge_emf(MeshDesc m, const S *flux, S *emf, int e, int n0, int
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)n0 * n1 * n2;
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % n0);
-  r /= n0;
-  const int j = m.g[1] + int(r % n1);
-  const int k = m.g[2] + int(r / n1);
+  int b, i, j, k;
+  unflatten(t, per, n0, n1, b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NF = (long long)m.nb * m.Pf;
   const long long bo = (long long)b * m.Pf;
   auto F = [&](int dir, int bcomp, int kk, int jj, int ii) {
@@ -413,12 +427,11 @@ __global__ void k_flux_divergence(MeshDesc m, const S *flux, S *du, int ncc) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)m.nx[0] * m.nx[1] * m.nx[2];
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % m.nx[0]);
-  r /= m.nx[0];
-  const int j = m.g[1] + int(r % m.nx[1]);
-  const int k = m.g[2] + int(r / m.nx[1]);
+  int b, i, j, k;
+  unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NF = (long long)m.nb * m.Pf, NP = (long long)m.nb * m.P;
   const long long bo = (long long)b * m.Pf;
   for (int v = 0; v < ncc; v++) {
@@ -440,12 +453,11 @@ __global__ void k_flux_stokes(MeshDesc m, const S *emf, S *dufc, int face, int n
   const int n0 = m.nx[0] + (face == 0), n1 = m.nx[1] + (face == 1), n2 = m.nx[2] + (face == 2);
   const long long per = (long long)n0 * n1 * n2;
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % n0);
-  r /= n0;
-  const int j = m.g[1] + int(r % n1);
-  const int k = m.g[2] + int(r / n1);
+  int b, i, j, k;
+  unflatten(t, per, n0, n1, b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NF = (long long)m.nb * m.Pf, bo = (long long)b * m.Pf;
   S out = S(0);
   const int edges[2] = {e0, e1};
@@ -513,12 +525,11 @@ __global__ void k_apply_cells(MeshDesc m, const S *ub, const float *ublo, S *u0,
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)m.nx[0] * m.nx[1] * m.nx[2];
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % m.nx[0]);
-  r /= m.nx[0];
-  const int j = m.g[1] + int(r % m.nx[1]);
-  const int k = m.g[2] + int(r / m.nx[1]);
+  int b, i, j, k;
+  unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NP = (long long)m.nb * m.P;
   const long long n = (long long)b * m.P + cidx(m, k, j, i);
   const double h = dt_dev ? *dt_dev : dt;
@@ -545,12 +556,11 @@ __global__ void k_apply_faces(MeshDesc m, const S *fb, S *f0, S *f1, const S *df
   const int n0 = m.nx[0] + (face == 0), n1 = m.nx[1] + (face == 1), n2 = m.nx[2] + (face == 2);
   const long long per = (long long)n0 * n1 * n2;
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % n0);
-  r /= n0;
-  const int j = m.g[1] + int(r % n1);
-  const int k = m.g[2] + int(r / n1);
+  int b, i, j, k;
+  unflatten(t, per, n0, n1, b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NF = (long long)m.nb * m.Pf;
   const long long n = face * NF + (long long)b * m.Pf + fidx(m, k, j, i);
   const double h = dt_dev ? *dt_dev : dt;
@@ -627,12 +637,11 @@ __global__ void k_prepare_primitive(MeshDesc m, EosParams eos, S *cc, const floa
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)m.nx[0] * m.nx[1] * m.nx[2];
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % m.nx[0]);
-  r /= m.nx[0];
-  const int j = m.g[1] + int(r % m.nx[1]);
-  const int k = m.g[2] + int(r / m.nx[1]);
+  int b, i, j, k;
+  unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NP = (long long)m.nb * m.P;
   const long long n = (long long)b * m.P + cidx(m, k, j, i);
   S B[3] = {S(0), S(0), S(0)};
@@ -704,12 +713,11 @@ __global__ void k_estimate_dt(MeshDesc m, const S *cc, const S *prim, DevClock *
   const long long per = (long long)m.nx[0] * m.nx[1] * m.nx[2];
   double dtl = INFINITY;
   if (t < per * m.nb) {
-    const int b = int(t / per);
-    long long r = t - (long long)b * per;
-    const int i = m.g[0] + int(r % m.nx[0]);
-    r /= m.nx[0];
-    const int j = m.g[1] + int(r % m.nx[1]);
-    const int k = m.g[2] + int(r / m.nx[1]);
+    int b, i, j, k;
+    unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
+    i += m.g[0];
+    j += m.g[1];
+    k += m.g[2];
     const long long NP = (long long)m.nb * m.P;
     const long long n = (long long)b * m.P + cidx(m, k, j, i);
     S V[MHD ? 10 : 7];
@@ -810,12 +818,11 @@ __global__ void k_divb(MeshDesc m, const S *fc, double *divb) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)m.nx[0] * m.nx[1] * m.nx[2];
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % m.nx[0]);
-  r /= m.nx[0];
-  const int j = m.g[1] + int(r % m.nx[1]);
-  const int k = m.g[2] + int(r / m.nx[1]);
+  int b, i, j, k;
+  unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NF = (long long)m.nb * m.Pf, bo = (long long)b * m.Pf;
   double d = 0.;
   for (int dir = 0; dir < m.ndim; dir++) {
@@ -845,12 +852,11 @@ __global__ void k_eos_init(MeshDesc m, EosParams eos, const S *cc, S *prim) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)m.nx[0] * m.nx[1] * m.nx[2];
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % m.nx[0]);
-  r /= m.nx[0];
-  const int j = m.g[1] + int(r % m.nx[1]);
-  const int k = m.g[2] + int(r / m.nx[1]);
+  int b, i, j, k;
+  unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NP = (long long)m.nb * m.P;
   const long long n = (long long)b * m.P + cidx(m, k, j, i);
   const S rho = cc[n];
@@ -879,12 +885,11 @@ __global__ void k_prim2cons(MeshDesc m, S *cc, float *lo, const S *fc, const S *
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)m.nx[0] * m.nx[1] * m.nx[2];
   if (t >= per * m.nb) return;
-  const int b = int(t / per);
-  long long r = t - (long long)b * per;
-  const int i = m.g[0] + int(r % m.nx[0]);
-  r /= m.nx[0];
-  const int j = m.g[1] + int(r % m.nx[1]);
-  const int k = m.g[2] + int(r / m.nx[1]);
+  int b, i, j, k;
+  unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
   const long long NP = (long long)m.nb * m.P;
   const long long n = (long long)b * m.P + cidx(m, k, j, i);
   S V[MHD ? 10 : 7], U[MHD ? 8 : 5];
@@ -960,12 +965,11 @@ __global__ void k_cons_sums(MeshDesc m, const S *cc, const float *lo, int ncc, d
     double s = 0.0, cm = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
          t += (long long)gridDim.x * blockDim.x) {
-      const int b = int(t / per);
-      long long r = t - (long long)b * per;
-      const int i = m.g[0] + int(r % m.nx[0]);
-      r /= m.nx[0];
-      const int j = m.g[1] + int(r % m.nx[1]);
-      const int k = m.g[2] + int(r / m.nx[1]);
+      int b, i, j, k;
+      unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
+      i += m.g[0];
+      j += m.g[1];
+      k += m.g[2];
       const long long n = (long long)b * m.P + cidx(m, k, j, i);
       const double x = (v == CENER ? load_ener(cc, lo, NP, n) : double(cc[v * NP + n])) * blk_vol(m, b);
       two_sum(s, cm, x);
@@ -1032,12 +1036,8 @@ __global__ void k_vortex_err(MeshDesc m, const S *cc, const S *prim, int var, in
   double s = 0.0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
        t += (long long)gridDim.x * blockDim.x) {
-    const int b = int(t / per);
-    long long r = t - (long long)b * per;
-    const int i = int(r % m.nx[0]);
-    r /= m.nx[0];
-    const int j = int(r % m.nx[1]);
-    const int k = int(r / m.nx[1]);
+    int b, i, j, k;
+    unflatten(t, per, m.nx[0], m.nx[1], b, i, j, k);
     const long long n = (long long)b * m.P + cidx(m, k + m.g[2], j + m.g[1], i + m.g[0]);
     const double x = m.xmin[0] + (double(blk_loc(m, b, 0) * m.nx[0] + i) + 0.5) * blk_dx(m, b, 0);
     const double y = m.xmin[1] + (double(blk_loc(m, b, 1) * m.nx[1] + j) + 0.5) * blk_dx(m, b, 1);
