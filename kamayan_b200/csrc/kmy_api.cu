@@ -730,23 +730,19 @@ int kmy_task_stage(kmy_ctx *c, int stage, double dt) {
 // are current (after set-up, an import, the task path or a previous fused
 // stage) and writes those of its output to c->prim_alt; the buffers swap.
 // Constrained transport: the fused stage updates the cells and writes the
-// transverse field fluxes; the edge EMFs, the face update and the
-// primitives (which need the new cell-centred field) follow as separate
-// kernels, in the order of the task list (hydro_add_flux_tasks.cpp,
-// grid.cpp:353-381, primconsflux.cpp:82-142).
+// transverse field fluxes; the face update (edge EMFs, Stokes, ApplyDuDt in
+// one kernel per face direction) and the primitives (which need the new
+// cell-centred field) follow as separate kernels, in the order of the task
+// list (hydro_add_flux_tasks.cpp, grid.cpp:353-381, primconsflux.cpp:82-142).
 static int fused_stage_ct(kmy_ctx *c, int stage) {
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());
-  Container *dup = find_container(c, "dUdt");
-  if (!dup) return KMY_ERR_OOM;
   Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
   const bool stored = c->prims_valid || c->prims_interior;
   const double beta = c->prm.beta[stage - 1];
   int rc = launch_fused_stage(c, base, md0, md1, beta, stored, false);
   if (!rc) rc = launch_flux_halo(c);
-  if (!rc) rc = launch_compute_emf(c, md0);
-  if (!rc) rc = launch_flux_stokes(c, md0, *dup);
-  if (!rc) rc = launch_apply_faces(c, base, md0, md1, *dup, beta, -1.0, &c->clock->dt);
+  if (!rc) rc = launch_ct_faces(c, base, md0, md1, beta);
   if (!rc) rc = launch_prepare_primitive(c, md1);
   if (!rc && stage == ns) {
     rc = launch_estimate_dt(c, base, true);

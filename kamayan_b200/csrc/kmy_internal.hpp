@@ -197,6 +197,7 @@ int launch_flux_halo(kmy_ctx *c);
 int launch_flux_stokes(kmy_ctx *c, Container &md0, Container &dudt);
 int launch_apply_faces(kmy_ctx *c, Container &base, Container &md0, Container &md1, Container &dudt,
                        double beta, double dt, const double *dt_dev);
+int launch_ct_faces(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta);
 int launch_prepare_primitive(kmy_ctx *c, Container &md1);
 int launch_estimate_dt(kmy_ctx *c, Container &md, bool reset);
 int launch_fill_derived(kmy_ctx *c, Container &md);

@@ -611,6 +611,89 @@ int launch_apply_faces(kmy_ctx *c, Container &base, Container &md0, Container &m
 }
 
 // ---------------------------------------------------------------------------
+// The face update of a constrained-transport stage in one kernel per face
+// direction: each face's edge EMFs from the face fluxes (CalculateEMF's
+// arithmetic average, as k_edge_emf), their Stokes sum (FluxStokes, as
+// k_flux_stokes) and the low-storage update (ApplyDuDt, as k_apply_faces),
+// with the same expressions in the same order, so EMFs and face values agree
+// bit for bit with those three kernels.  The EMF and dU/dt arrays are not
+// written.  Edges on block faces read the ghost-layer fluxes of k_flux_halo.
+template <typename S>
+__device__ __forceinline__ S edge_emf(const MeshDesc &m, const S *flux, long long bo, int e, int k, int j, int i) {
+  const long long NF = (long long)m.nb * m.Pf;
+  auto F = [&](int dir, int bcomp, int kk, int jj, int ii) {
+    return flux[((long long)dir * 8 + CMAGC0 + bcomp) * NF + bo + fidx(m, kk, jj, ii)];
+  };
+  if (e == 2)
+    return S(1.0) * S(0.25) * (F(1, 0, k, j, i - 1) + F(1, 0, k, j, i) - F(0, 1, k, j - 1, i) - F(0, 1, k, j, i));
+  if (e == 0)
+    return S(1.0) * S(0.25) * (F(2, 1, k, j - 1, i) + F(2, 1, k, j, i) - F(1, 2, k - 1, j, i) - F(1, 2, k, j, i));
+  return S(1.0) * S(0.25) * (F(0, 2, k - 1, j, i) + F(0, 2, k, j, i) - F(2, 0, k, j, i - 1) - F(2, 0, k, j, i));
+}
+
+template <typename S>
+__global__ void k_ct_faces(MeshDesc m, const S *flux, const S *fb, S *f0, S *f1, int face, int ne, int e0,
+                           int e1, double beta, const double *dt_dev, const DevClock *clock) {
+  if (clock->done) return;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int n0 = m.nx[0] + (face == 0), n1 = m.nx[1] + (face == 1), n2 = m.nx[2] + (face == 2);
+  const long long per = (long long)n0 * n1 * n2;
+  if (t >= per * m.nb) return;
+  int b, i, j, k;
+  unflatten(t, per, n0, n1, b, i, j, k);
+  i += m.g[0];
+  j += m.g[1];
+  k += m.g[2];
+  const long long NF = (long long)m.nb * m.Pf, bo = (long long)b * m.Pf;
+  S out = S(0);
+  const int edges[2] = {e0, e1};
+  for (int q = 0; q < ne; q++) {
+    const int edge = edges[q];
+    int axis;  // AxisFromFaceEdge, i=0 j=1 k=2
+    if (face == 0) axis = edge == 2 ? 1 : 2;
+    else if (face == 1) axis = edge == 2 ? 0 : 2;
+    else axis = edge == 0 ? 1 : 0;
+    int ijk[3] = {i, j, k};
+    ijk[axis] += 1;
+    const S sign = ((axis + 1) % 3 == edge) ? S(1.0) : S(-1.0);
+    const S L = S(blk_dx(m, b, edge));
+    const S Ea = edge_emf(m, flux, bo, edge, k, j, i);
+    const S Eb = edge_emf(m, flux, bo, edge, ijk[2], ijk[1], ijk[0]);
+    out += sign * (L * Ea - L * Eb);
+  }
+  out *= S(1.) / (S(blk_area(m, b, face)) + S(1.e-36));
+  const long long n = face * NF + bo + fidx(m, k, j, i);
+  const double h = *dt_dev;
+  const S bt = S(beta);
+  const S x0 = bt * fb[n] + (S(1.0) - bt) * f0[n];
+  f0[n] = x0;
+  f1[n] = x0 + bt * S(h) * out;
+}
+
+int launch_ct_faces(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta) {
+  const MeshDesc &m = c->m;
+  struct FE { int face, ne, e0, e1; };
+  const FE l3[3] = {{0, 2, 2, 1}, {1, 2, 2, 0}, {2, 2, 0, 1}};
+  const FE l2[2] = {{0, 1, 2, 0}, {1, 1, 2, 0}};
+  const FE *l = m.ndim > 2 ? l3 : l2;
+  for (int f = 0; f < m.ndim; f++) {
+    const FE fe = l[f];
+    const long long nfc = (long long)(m.nx[0] + (fe.face == 0)) * (m.nx[1] + (fe.face == 1)) *
+                          (m.nx[2] + (fe.face == 2)) * m.nb;
+    if (c->esz == 8)
+      k_ct_faces<double><<<nblk(nfc), kThreads, 0, c->stream>>>(
+          m, (const double *)c->flux, (const double *)base.fc, (double *)md0.fc, (double *)md1.fc, fe.face,
+          fe.ne, fe.e0, fe.e1, beta, &c->clock->dt, c->clock);
+    else
+      k_ct_faces<float><<<nblk(nfc), kThreads, 0, c->stream>>>(
+          m, (const float *)c->flux, (const float *)base.fc, (float *)md0.fc, (float *)md1.fc, fe.face, fe.ne,
+          fe.e0, fe.e1, beta, &c->clock->dt, c->clock);
+    c->launches++;
+  }
+  return cuda_check(c, cudaGetLastError(), "ct_faces");
+}
+
+// ---------------------------------------------------------------------------
 // CT face -> cell average (primconsflux.cpp:102-129)
 template <typename S>
 __device__ __forceinline__ void face_average(const MeshDesc &m, const S *fc, int b, int k, int j,
