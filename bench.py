@@ -12,9 +12,9 @@ batched into one launch per stage, timed with CUDA events on the solver's
 stream.  Beside it: the FP64 fused path, the FP64 per-task path (the
 reference task list, one kernel per task) and the FP32-vs-FP64 density L1.
 ``e2e``: the same metric through the C ABI with host buffers: import of the
-initial conserved state from pinned host memory (finalize derives the
-primitives), K x kmy_step (each returns dt to the host), export of the final
-conserved state.
+initial conserved state (interior cells, FP64) from pinned host memory
+(finalize derives the primitives and fills the ghost zones), K x kmy_step
+(each returns dt to the host), export of the final conserved state.
 
 ``--impl reference`` times the reference's CPU path (the C++ restatement in
 oracle/, all host threads) on a bounded sample of the same workload.
@@ -224,25 +224,27 @@ def make_solver(a, precision: str, device: int, stream):
 
 
 def e2e_solve(a, device: int, stream, K: int):
-    """Initial state from pinned host memory -> K x kmy_step -> final state to pinned host."""
+    """Initial state from pinned host memory -> K x kmy_step -> final state to pinned host.
+
+    The conserved state moves as interior cells (kmy_import_interior /
+    kmy_export_interior, the layout of Parthenon's phdf outputs); finalize
+    derives the primitives and fills the ghost zones on the device."""
     import torch
 
     import kamayan_b200
 
     src = make_solver(a, "fp64", device, stream)
-    # the conserved state in; finalize derives the primitives on the device
-    names_in = [("dens", 0), ("momentum", 0), ("momentum", 1), ("momentum", 2), ("ener", 0)]
-    names_out = names_in
+    names = [("dens", 0), ("momentum", 0), ("momentum", 1), ("momentum", 2), ("ener", 0)]
     n = 1
-    for x in src.cell_shape:
+    for x in src.interior_shape:
         n *= x
     host_in = {}
-    for v, c in names_in:
+    for v, c in names:
         t = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        src.export_ptr(v, t.data_ptr(), n, c)
+        src.export_interior_ptr(v, t.data_ptr(), n, c)
         host_in[(v, c)] = t
     src.close()
-    host_out = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in names_out}
+    host_out = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in names}
     from kamayan_b200 import configs
 
     s = kamayan_b200.Solver(configs.kh_3d(n=a.n, nb=a.nb, precision="fp32"), device=device)
@@ -252,18 +254,18 @@ def e2e_solve(a, device: int, stream, K: int):
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     for (v, c), t in host_in.items():
-        s.import_ptr(v, t.data_ptr(), n, c)
+        s.import_interior_ptr(v, t.data_ptr(), n, c)
     s.finalize_import()
     for _ in range(K):
         s.step()
     for (v, c), t in host_out.items():
-        s.export_ptr(v, t.data_ptr(), n, c)
+        s.export_interior_ptr(v, t.data_ptr(), n, c)
     t1.record(stream)
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
     s.close()
-    h2d = 8 * n * len(names_in)
-    d2h = 8 * n * len(names_out) + 48 * K
+    h2d = 8 * n * len(names)
+    d2h = 8 * n * len(names) + 48 * K
     return ms, h2d, d2h
 
 
@@ -499,8 +501,8 @@ def main():
         "dtype": "f32", "data": "synthetic", "config": workload_config(a, ws),
         "e2e": {"value": ws * cells * K / (e2e_ms / 1e3), "unit": METRIC,
                 "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
-                "what": "kmy_import_var of the conserved state (pinned host) + finalize + K x kmy_step + "
-                        "kmy_export_var of the conserved state, FP32"},
+                "what": "kmy_import_interior of the conserved state (FP64 interior cells, pinned host) + "
+                        "finalize + K x kmy_step + kmy_export_interior of the conserved state, FP32 solve"},
         "gpu_launches": r32["launches"],
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
                      "frac": ach32 / peak, "traffic": traffic, "peak_kind": peak_kind,

@@ -30,7 +30,8 @@ STATUS = {
 # Every entry point declared in include/kmy_hydro.h.
 EXPORTS = (
     "kmy_create", "kmy_destroy", "kmy_last_error", "kmy_get_info", "kmy_set_stream", "kmy_sync",
-    "kmy_import_var", "kmy_export_var", "kmy_finalize_import", "kmy_pgen",
+    "kmy_import_var", "kmy_export_var", "kmy_import_interior", "kmy_export_interior",
+    "kmy_finalize_import", "kmy_pgen",
     "kmy_compute_fluxes", "kmy_compute_emf", "kmy_flux_divergence", "kmy_apply_dudt",
     "kmy_prepare_primitive", "kmy_fill_ghosts", "kmy_estimate_dt", "kmy_fill_derived",
     "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_end_step", "kmy_get_time",
@@ -81,6 +82,8 @@ def lib() -> ctypes.CDLL:
         L.kmy_sync.argtypes = [vp]
         L.kmy_import_var.argtypes = [vp, cp, cp, i, _dp, sz]
         L.kmy_export_var.argtypes = [vp, cp, cp, i, _dp, sz]
+        L.kmy_import_interior.argtypes = [vp, cp, cp, i, _dp, sz]
+        L.kmy_export_interior.argtypes = [vp, cp, cp, i, _dp, sz]
         L.kmy_finalize_import.argtypes = [vp]
         L.kmy_pgen.argtypes = [vp, cp]
         for n in ("kmy_compute_fluxes", "kmy_compute_emf", "kmy_prepare_primitive",
@@ -226,6 +229,32 @@ class Solver:
     def export_ptr(self, var: str, ptr: int, n: int, comp: int = 0, container: str = "base") -> None:
         self._check(lib().kmy_export_var(self._h, container.encode(), var.encode(), comp,
                                          ctypes.cast(ptr, _dp), n))
+
+    @property
+    def interior_shape(self):
+        i = self.info
+        return (i.nblocks, i.nx[2], i.nx[1], i.nx[0])
+
+    def export_interior(self, var: str, comp: int = 0, container: str = "base") -> np.ndarray:
+        """Interior cells only, (nblocks, nk, nj, ni) (kmy_export_interior)."""
+        out = np.empty(self.interior_shape, dtype=np.float64)
+        self._check(lib().kmy_export_interior(self._h, container.encode(), var.encode(), comp,
+                                              _ptr(out), out.size))
+        return out
+
+    def import_interior(self, var: str, arr, comp: int = 0, container: str = "base") -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        self._check(lib().kmy_import_interior(self._h, container.encode(), var.encode(), comp,
+                                              _ptr(a), a.size))
+
+    def import_interior_ptr(self, var: str, ptr: int, n: int, comp: int = 0, container: str = "base") -> None:
+        """Import n interior-cell doubles from host address ptr (e.g. a pinned buffer)."""
+        self._check(lib().kmy_import_interior(self._h, container.encode(), var.encode(), comp,
+                                              ctypes.cast(ptr, _dp), n))
+
+    def export_interior_ptr(self, var: str, ptr: int, n: int, comp: int = 0, container: str = "base") -> None:
+        self._check(lib().kmy_export_interior(self._h, container.encode(), var.encode(), comp,
+                                              ctypes.cast(ptr, _dp), n))
 
     def finalize_import(self) -> None:
         self._check(lib().kmy_finalize_import(self._h))

@@ -565,6 +565,107 @@ int kmy_export_var(kmy_ctx *c, const char *container, const char *var, int comp,
   return rc;
 }
 
+// Interior cells only, packed block-major then (k, j, i): scatter from a
+// host-order staging buffer into the ghost-padded layout, and the gather
+// back.  One thread per interior cell.
+__global__ void k_store_interior(MeshDesc m, const double *src, void *dst, float *lo, int f32) {
+  const size_t per = size_t(m.nx[0]) * m.nx[1] * m.nx[2];
+  const size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  if (t >= per * m.nb) return;
+  const size_t b = t / per, r = t - b * per;
+  const size_t i = r % m.nx[0], q = r / m.nx[0], j = q % m.nx[1], k = q / m.nx[1];
+  const size_t n = b * m.P + ((k + m.g[2]) * m.np[1] + (j + m.g[1])) * m.np[0] + (i + m.g[0]);
+  const double v = src[t];
+  if (f32) {
+    const float hi = float(v);
+    static_cast<float *>(dst)[n] = hi;
+    if (lo) lo[n] = float(v - double(hi));
+  } else {
+    static_cast<double *>(dst)[n] = v;
+  }
+}
+__global__ void k_load_interior(MeshDesc m, const void *src, const float *lo, double *dst, int f32) {
+  const size_t per = size_t(m.nx[0]) * m.nx[1] * m.nx[2];
+  const size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  if (t >= per * m.nb) return;
+  const size_t b = t / per, r = t - b * per;
+  const size_t i = r % m.nx[0], q = r / m.nx[0], j = q % m.nx[1], k = q / m.nx[1];
+  const size_t n = b * m.P + ((k + m.g[2]) * m.np[1] + (j + m.g[1])) * m.np[0] + (i + m.g[0]);
+  if (f32) {
+    double v = double(static_cast<const float *>(src)[n]);
+    if (lo) v += double(lo[n]);
+    dst[t] = v;
+  } else {
+    dst[t] = static_cast<const double *>(src)[n];
+  }
+}
+
+// Shared checks of the interior transfers: a cell variable and the interior
+// cell count.
+static int resolve_interior(kmy_ctx *c, const char *container, const char *var, int comp, size_t n,
+                            VarRef &r) {
+  int rc = resolve(c, container, var, comp, r);
+  if (rc) return rc;
+  const MeshDesc &m = c->m;
+  if (r.n != size_t(m.nb) * m.P) {
+    c->err = "interior transfers cover cell variables";
+    return KMY_ERR_BAD_PARAM;
+  }
+  const size_t ni = size_t(m.nb) * m.nx[0] * m.nx[1] * m.nx[2];
+  if (n != ni) {
+    c->err = "size mismatch: expected " + std::to_string(ni) + " interior cells";
+    return KMY_ERR_BAD_PARAM;
+  }
+  return KMY_OK;
+}
+
+int kmy_import_interior(kmy_ctx *c, const char *container, const char *var, int comp, const double *host,
+                        size_t n) {
+  if (!c || !host) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  VarRef r;
+  int rc = resolve_interior(c, container, var, comp, n, r);
+  if (rc) return rc;
+  const std::string vn(var);
+  if (vn == "velocity" || vn == "pres" || vn == "bulk modulus" || vn == "eint" || vn == "temp")
+    c->prims_imported = true;
+  double *stage = nullptr;
+  rc = cuda_check(c, cudaMallocAsync(reinterpret_cast<void **>(&stage), n * 8, c->stream), "stage");
+  if (rc) return rc;
+  rc = cuda_check(c, cudaMemcpyAsync(stage, host, n * 8, cudaMemcpyHostToDevice, c->stream), "import");
+  if (!rc) {
+    const int f32 = (r.is_double || c->esz == 8) ? 0 : 1;
+    k_store_interior<<<unsigned((n + 255) / 256), 256, 0, c->stream>>>(c->m, stage, r.p, f32 ? r.lo : nullptr, f32);
+    c->launches++;
+    rc = cuda_check(c, cudaGetLastError(), "k_store_interior");
+  }
+  cudaFreeAsync(stage, c->stream);
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "import sync");
+  c->prims_valid = true;
+  return rc;
+}
+
+int kmy_export_interior(kmy_ctx *c, const char *container, const char *var, int comp, double *host, size_t n) {
+  if (!c || !host) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  VarRef r;
+  int rc = resolve_interior(c, container, var, comp, n, r);
+  if (rc) return rc;
+  rc = materialize(c);
+  if (rc) return rc;
+  double *stage = nullptr;
+  rc = cuda_check(c, cudaMallocAsync(reinterpret_cast<void **>(&stage), n * 8, c->stream), "stage");
+  if (rc) return rc;
+  const int f32 = (r.is_double || c->esz == 8) ? 0 : 1;
+  k_load_interior<<<unsigned((n + 255) / 256), 256, 0, c->stream>>>(c->m, r.p, f32 ? r.lo : nullptr, stage, f32);
+  c->launches++;
+  rc = cuda_check(c, cudaGetLastError(), "k_load_interior");
+  if (!rc) rc = cuda_check(c, cudaMemcpyAsync(host, stage, n * 8, cudaMemcpyDeviceToHost, c->stream), "export");
+  cudaFreeAsync(stage, c->stream);
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "export sync");
+  return rc;
+}
+
 int kmy_finalize_import(kmy_ctx *c) {
   if (!c) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
