@@ -140,6 +140,7 @@ class Solver:
             if rc:
                 raise KmyError(rc, "kmy_create rejected the deck (see stderr)")
         self._h = h
+        self._lib = lib()  # kept so close() still works while the interpreter shuts down
         self._info = Info()
         self.ndim = self.info.ndim
 
@@ -190,7 +191,7 @@ class Solver:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            lib().kmy_destroy(self._h)
+            self._lib.kmy_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -370,10 +371,11 @@ class Server:
         if rc:
             raise KmyError(rc, "kmy_server_create failed")
         self._h = h
+        self._lib = lib()
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            lib().kmy_server_destroy(self._h)
+            self._lib.kmy_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

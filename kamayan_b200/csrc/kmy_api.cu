@@ -452,6 +452,7 @@ int kmy_create(const char *deck, int device, kmy_ctx **out) {
 int kmy_destroy(kmy_ctx *c) {
   if (!c) return KMY_OK;
   cudaSetDevice(c->device);
+  if (c->evolve_exec) cudaGraphExecDestroy(c->evolve_exec);
   for (void *p : c->allocations) cudaFreeAsync(p, c->stream);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -936,6 +937,77 @@ int kmy_step(kmy_ctx *c, double *dt_taken) {
   return KMY_OK;
 }
 
+// kmy_evolve queues fused hydro steps in chunks of kChunk; the chunk runs as
+// one CUDA graph (its 4 x kChunk or so launches cost one submission).  A
+// graph replays the kernel arguments it was captured with, so it is keyed by
+// the host-side state those arguments come from: the primitive buffers and
+// containers (an even number of stages swaps them back), the flags that pick
+// stored primitives, and the time parameters of the dt controller.  The first
+// chunk after any change of that state runs uncaptured (first-use
+// allocations, flags settling); the next one is captured and replayed until
+// the state changes again.
+static constexpr int kChunk = 8;
+
+static std::string evolve_key(const kmy_ctx *c) {
+  std::string k;
+  auto add = [&](const void *p, size_t n) { k.append(static_cast<const char *>(p), n); };
+  add(&c->prim, sizeof(c->prim));
+  add(&c->prim_alt, sizeof(c->prim_alt));
+  for (const auto &kv : c->md) add(&kv.second.cc, sizeof(kv.second.cc));
+  const bool flags[2] = {c->prims_valid, c->prims_interior};
+  add(flags, sizeof(flags));
+  add(&c->prm.tp, sizeof(c->prm.tp));
+  add(&c->stream, sizeof(c->stream));
+  return k;
+}
+
+// Run one chunk of fused steps through the cached graph, capturing it first
+// when the state is steady.  *ran is false when the caller should step
+// uncaptured instead.
+static int evolve_chunk_graph(kmy_ctx *c, bool *ran) {
+  *ran = false;
+  const std::string key = evolve_key(c);
+  if (c->evolve_exec && key == c->evolve_key) {
+    c->launches += c->evolve_launches;
+    *ran = true;
+    return cuda_check(c, cudaGraphLaunch(c->evolve_exec, c->stream), "evolve graph");
+  }
+  if (c->evolve_exec) {
+    cudaGraphExecDestroy(c->evolve_exec);
+    c->evolve_exec = nullptr;
+  }
+  if (key != c->evolve_seen) {  // first chunk in this state: run it uncaptured
+    c->evolve_seen = key;
+    return KMY_OK;
+  }
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();  // e.g. the legacy default stream, which cannot be captured
+    return KMY_OK;
+  }
+  const int64_t l0 = c->launches;
+  int rc = KMY_OK;
+  for (int i = 0; i < kChunk && !rc; i++) rc = step_async(c);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (!rc) rc = cuda_check(c, e, "evolve capture");
+  cudaGraphExec_t exec = nullptr;
+  if (!rc) rc = cuda_check(c, cudaGraphInstantiate(&exec, g, 0), "evolve instantiate");
+  if (g) cudaGraphDestroy(g);
+  if (rc) return rc;
+  // the captured chunk has not run yet; it runs now, and is kept when the
+  // state after it is the state it started from
+  rc = cuda_check(c, cudaGraphLaunch(exec, c->stream), "evolve graph");
+  if (!rc && evolve_key(c) == key) {
+    c->evolve_exec = exec;
+    c->evolve_key = key;
+    c->evolve_launches = c->launches - l0;
+  } else {
+    cudaGraphExecDestroy(exec);
+  }
+  *ran = !rc;
+  return rc;
+}
+
 int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
   if (!c) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
@@ -950,8 +1022,13 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
     // of a constrained-transport stage) do not check the clock, so those
     // step one at a time; an adaptive mesh reads its tags back every step
     // anyway.
-    const int chunk = steps_fused(c) && !c->prm.mhd ? 8 : 1;
-    for (int i = 0; i < chunk && !rc && (nlim < 0 || n < nlim); i++, n++) rc = step_async(c);
+    const int chunk = steps_fused(c) && !c->prm.mhd ? kChunk : 1;
+    bool ran = false;
+    if (chunk == kChunk && (nlim < 0 || nlim - n >= kChunk)) {
+      rc = evolve_chunk_graph(c, &ran);
+      if (ran) n += kChunk;
+    }
+    for (int i = 0; !ran && i < chunk && !rc && (nlim < 0 || n < nlim); i++, n++) rc = step_async(c);
     if (rc) break;
     rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "evolve");

@@ -21,6 +21,8 @@
 // hydro_time_step.cpp:19-64.
 #pragma once
 
+#include <atomic>
+
 #include "../../include/kmy_hydro.h"
 #include "kmy_internal.hpp"
 
@@ -822,8 +824,15 @@ int fused_launch(kmy_ctx *c, FusedArgs<S> a) {
   const long long grid = (long long)a.nbr[0] * a.nbr[1] * a.nbr[2] * m.nb;
   const size_t smem = Sh::template smem_bytes<S>();
   auto kern = k_fused_stage<S, NDIM, RECON, RIEMANN, MHD>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return cuda_check(c, e, "fused smem attribute");
+  // the shared-memory opt-in once per device and kernel, so a stream capture
+  // (kmy_evolve's graphs) sees launches only
+  static std::atomic<unsigned> opted{0};
+  const unsigned bit = c->device < 32 ? 1u << c->device : 0u;
+  if (!bit || !(opted.load() & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return cuda_check(c, e, "fused smem attribute");
+    opted.fetch_or(bit);
+  }
   kern<<<unsigned(grid), Sh::NT, smem, c->stream>>>(a);
   c->launches++;
   return cuda_check(c, cudaGetLastError(), "fused stage");

@@ -175,6 +175,11 @@ struct kmy_ctx {
   int path = 0;              // 0 fused, 1 tasks
   kmy::AmrHost amr;          // adaptive mesh (task path only)
   int64_t launches = 0;
+  // kmy_evolve's chunk of fused steps as a CUDA graph, and the host-side
+  // state it was captured from (kmy_api.cu:evolve_chunk_graph)
+  cudaGraphExec_t evolve_exec = nullptr;
+  std::string evolve_key, evolve_seen;
+  int64_t evolve_launches = 0;
   std::string err;
   std::string deck_text;  // the deck the context was created from (restart files carry it)
   std::vector<void *> allocations;
