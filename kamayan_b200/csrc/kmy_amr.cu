@@ -399,14 +399,20 @@ __device__ __forceinline__ void store_value(S *arr, float *lo, long long n, doub
 template <typename S>
 __global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, float *lo, S *prim, int ncc,
                                   int *err) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)m.nb * m.P) return;
-  const int b = int(t / m.P);
-  long long r = t - (long long)b * m.P;
-  const int i = int(r % m.np[0]);
-  r /= m.np[0];
-  const int j = int(r % m.np[1]);
-  const int k = int(r / m.np[1]);
+  // one thread per (padded cell, variable): blockIdx.y runs over the ncc
+  // conserved variables, then the NPRIM primitives, so the level-value
+  // evaluations of a ghost cell's variables run side by side
+  const unsigned per = unsigned(m.nb) * unsigned(m.P);  // cells of all blocks (< 2^32)
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per) return;
+  const int v = blockIdx.y;
+  const unsigned P = unsigned(m.P);
+  const int b = int(t / P);
+  unsigned r = t - unsigned(b) * P;
+  const int i = int(r % unsigned(m.np[0]));
+  r /= unsigned(m.np[0]);
+  const int j = int(r % unsigned(m.np[1]));
+  const int k = int(r / unsigned(m.np[1]));
   const int loc[3] = {i, j, k};
   bool interior = true;
   for (int d = 0; d < 3; d++)
@@ -418,6 +424,13 @@ __global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, flo
   const long long NP = (long long)m.nb * m.P;
   const long long dst = (long long)b * m.P + cidx(m, k, j, i);
   constexpr bool F32 = sizeof(S) == 4;
+  const bool is_cc = v < ncc;
+  // the variable, its vector component (-1: scalar) and, for FP32 energy,
+  // its low words
+  S *arr = is_cc ? cc + v * NP : prim + (v - ncc) * NP;
+  const int fd = is_cc ? ((v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1))
+                       : (v - ncc <= PVEL2 ? v - ncc : -1);
+  float *vlo = (F32 && is_cc && v == CENER) ? lo : nullptr;
 
   int M[3] = {0, 0, 0}, bx[3];
   bool flip[3] = {false, false, false};
@@ -427,33 +440,17 @@ __global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, flo
   if (e >= 0) {
     const long long s = (long long)e * m.P + cidx(m, M[2] - bx[2] * m.nx[2] + m.g[2],
                                                   M[1] - bx[1] * m.nx[1] + m.g[1], M[0] - bx[0] * m.nx[0] + m.g[0]);
-    for (int v = 0; v < ncc; v++) {
-      S val = cc[v * NP + s];
-      if (v >= CMOM0 && v <= CMOM2 && flip[v - CMOM0]) val = -val;
-      if (v >= CMAGC0 && flip[v - CMAGC0]) val = -val;
-      cc[v * NP + dst] = val;
-    }
+    S val = arr[s];
+    if (fd >= 0 && flip[fd]) val = -val;
+    arr[dst] = val;
     if constexpr (F32) {
-      if (lo) lo[dst] = lo[s];
-    }
-    for (int v = 0; v < NPRIM; v++) {
-      S val = prim[v * NP + s];
-      if (v <= PVEL2 && flip[v]) val = -val;
-      prim[v * NP + dst] = val;
+      if (vlo) vlo[dst] = vlo[s];
     }
     return;
   }
-  for (int v = 0; v < ncc; v++) {
-    const Field f{cc + v * NP, (F32 && v == CENER) ? lo : nullptr, F32};
-    const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1);
-    const double val = level_value<kMaxDepth>(m, L, G[0], G[1], G[2], f, fd, err);
-    store_value<S>(cc + v * NP, v == CENER ? lo : nullptr, dst, val);
-  }
-  for (int v = 0; v < NPRIM; v++) {
-    const Field f{prim + v * NP, nullptr, F32};
-    const double val = level_value<kMaxDepth>(m, L, G[0], G[1], G[2], f, v <= PVEL2 ? v : -1, err);
-    store_value<S>(prim + v * NP, nullptr, dst, val);
-  }
+  const Field f{arr, vlo, F32};
+  const double val = level_value<kMaxDepth>(m, L, G[0], G[1], G[2], f, fd, err);
+  store_value<S>(arr, vlo, dst, val);
 }
 
 // Flux correction: a coarse block's boundary face whose neighbour across it
@@ -529,8 +526,9 @@ __global__ void k_flux_correct(const __grid_constant__ MeshDesc m, S *flux, int 
 __global__ void k_amr_tag(const __grid_constant__ MeshDesc m, Field f, double refine_tol, double derefine_tol,
                           double filter, int max_level, int combine, int *tags) {
   __shared__ int flag_sh;
+  __shared__ unsigned long long max_sh;
   const int b = blockIdx.x;
-  if (threadIdx.x == 0) flag_sh = -1;
+  if (threadIdx.x == 0) max_sh = 0ull;
   __syncthreads();
   const int nd = m.ndim;
   const double dxq[3] = {blk_dx(m, b, 0), blk_dx(m, b, 1), blk_dx(m, b, 2)};
@@ -539,40 +537,43 @@ __global__ void k_amr_tag(const __grid_constant__ MeshDesc m, Field f, double re
   auto U = [&](long long n) { return fetch(f, base + n); };
   // central first derivative along p at cell n
   auto Dv = [&](int p, long long n) { return 0.5 * (U(n + st[p]) - U(n - st[p])) / dxq[p]; };
-  const int rows = m.nx[1] * m.nx[2];
-  int flag_row_max = -1;
-  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
-    const int j = m.g[1] + r % m.nx[1], k = m.g[2] + r / m.nx[1];
-    double max_err_2 = 0.;
-    for (int i = m.g[0]; i < m.g[0] + m.nx[0]; i++) {
-      const long long n = cidx(m, k, j, i);
-      double numerator = 0.0, denominator = 1.e-12;
-      for (int q = 0; q < nd; q++) {
-        const long long sq = st[q];
-        for (int p = 0; p < nd; p++) {
-          const long long sp = st[p];
-          const double dpp = Dv(p, n + sq), dpm = Dv(p, n - sq);
-          const double num = 0.5 * (dpp - dpm) / dxq[q];
-          numerator += num * num;
-          const double denom =
-              0.5 * (fabs(dpp) + fabs(dpm)) / dxq[p] +
-              filter * (fabs(U(n + sq)) + fabs(U(n - sq)) + fabs(U(n - sp)) + fabs(U(n + sp))) / (dxq[q] * dxq[p]);
-          denominator += denom * denom;
-        }
-      }
-      if (denominator != 0.0) {
-        const double ratio = numerator / denominator;
-        max_err_2 = (max_err_2 < ratio) ? ratio : max_err_2;
+  // One thread per cell.  The reference flags each row by its largest error
+  // and the block by the largest row flag; the flag grows with the error, so
+  // that is the flag of the block's largest error, taken here as the maximum
+  // of the squared ratios (non-negative doubles order as their bit patterns).
+  const int ncell = m.nx[0] * m.nx[1] * m.nx[2];
+  double max_err_2 = 0.;
+  for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
+    const int i = m.g[0] + c % m.nx[0], j = m.g[1] + (c / m.nx[0]) % m.nx[1], k = m.g[2] + c / (m.nx[0] * m.nx[1]);
+    const long long n = cidx(m, k, j, i);
+    double numerator = 0.0, denominator = 1.e-12;
+    for (int q = 0; q < nd; q++) {
+      const long long sq = st[q];
+      for (int p = 0; p < nd; p++) {
+        const long long sp = st[p];
+        const double dpp = Dv(p, n + sq), dpm = Dv(p, n - sq);
+        const double num = 0.5 * (dpp - dpm) / dxq[q];
+        numerator += num * num;
+        const double denom =
+            0.5 * (fabs(dpp) + fabs(dpm)) / dxq[p] +
+            filter * (fabs(U(n + sq)) + fabs(U(n - sq)) + fabs(U(n - sp)) + fabs(U(n + sp))) / (dxq[q] * dxq[p]);
+        denominator += denom * denom;
       }
     }
-    const double max_err = sqrt(max_err_2);
+    if (denominator != 0.0) {
+      const double ratio = numerator / denominator;
+      max_err_2 = (max_err_2 < ratio) ? ratio : max_err_2;
+    }
+  }
+  atomicMax(&max_sh, (unsigned long long)__double_as_longlong(max_err_2));
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double max_err = sqrt(__longlong_as_double((long long)max_sh));
     int flag = 0;
     if (max_err > refine_tol && m.blev[b] < max_level) flag = 1;
     if (max_err < derefine_tol) flag = -1;
-    flag_row_max = max(flag_row_max, flag);
+    flag_sh = flag;
   }
-  atomicMax(&flag_sh, flag_row_max);
-  __syncthreads();
   if (threadIdx.x == 0) tags[b] = combine ? max(tags[b], flag_sh) : flag_sh;
 }
 
@@ -843,12 +844,17 @@ int amr_setup(kmy_ctx *c) {
 int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct) {
   const MeshDesc &m = c->m;
   const long long n = (long long)m.nb * m.P;
+  if (n >= (1LL << 32)) {
+    c->err = "adaptive mesh: more than 2^32 padded cells";
+    return KMY_ERR_BAD_PARAM;
+  }
+  const dim3 grid(nblk(n), unsigned(c->ncc + NPRIM));
   if (c->esz == 8)
-    k_amr_fill_ghosts<double><<<nblk(n), kThreads, 0, c->stream>>>(m, (double *)ct.cc, nullptr, (double *)c->prim,
-                                                                   c->ncc, c->amr.d_err);
+    k_amr_fill_ghosts<double><<<grid, kThreads, 0, c->stream>>>(m, (double *)ct.cc, nullptr, (double *)c->prim,
+                                                                c->ncc, c->amr.d_err);
   else
-    k_amr_fill_ghosts<float><<<nblk(n), kThreads, 0, c->stream>>>(m, (float *)ct.cc, (float *)ct.ener_lo,
-                                                                  (float *)c->prim, c->ncc, c->amr.d_err);
+    k_amr_fill_ghosts<float><<<grid, kThreads, 0, c->stream>>>(m, (float *)ct.cc, (float *)ct.ener_lo,
+                                                               (float *)c->prim, c->ncc, c->amr.d_err);
   c->launches++;
   if (c->prm.mhd) {
     const long long nf = (long long)m.nb * m.Pf;
@@ -987,7 +993,9 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
   };
   for (int b = 0; b < nb; b++)
     if (tags[b] == 1 && a.lev[b] < a.max_level) split({a.lev[b], a.loc[3 * b], a.loc[3 * b + 1], a.loc[3 * b + 2]});
-  for (bool again = true; again;) {  // 2:1 balance
+  // 2:1 balance.  Only splits can unbalance a balanced tree (derefinement
+  // below checks its neighbours), so a step without splits skips the pass.
+  for (bool again = changed || !a.balanced; again;) {
     again = false;
     std::vector<Key> keys;
     for (auto &kv : leaf) keys.push_back(kv.first);
@@ -1006,6 +1014,7 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
           }
     }
   }
+  a.balanced = true;
   if (allow_derefine) {
     std::map<Key, int> parents;
     for (auto &kv : leaf) {
@@ -1144,6 +1153,7 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
 namespace kmy {
 
 int amr_adopt_leaves(kmy_ctx *c) {
+  c->amr.balanced = false;
   for (auto &kv : c->md) {
     dfree(c, kv.second.cc);
     dfree(c, kv.second.ener_lo);

@@ -143,6 +143,7 @@ struct AmrHost {
   std::vector<int> lev;  // per leaf
   std::vector<int> loc;  // 3 per leaf
   std::vector<int> cnt;  // consecutive derefine tags per leaf
+  bool balanced = false;  // the leaf list is known to be 2:1 balanced
   int *d_blev = nullptr, *d_bloc = nullptr, *d_tabs = nullptr, *d_tags = nullptr;
   int *d_err = nullptr;  // set by a level-value recursion that ran out of depth
   void *d_emf_tmp = nullptr;  // EMFs as computed, read by the edge correction
