@@ -583,15 +583,18 @@ template <typename S>
 __global__ void k_amr_remap(const __grid_constant__ MeshDesc mo, const S *occ, const float *olo, const S *oprim,
                             int nnew, const int *nlev, const int *nloc, S *ncc_out, float *nlo, S *nprim, int ncc,
                             int *err) {
-  const long long cells = (long long)mo.nx[0] * mo.nx[1] * mo.nx[2];
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= cells * nnew) return;
+  // one thread per (new interior cell, variable): blockIdx.y runs over the
+  // ncc conserved variables, then the NPRIM primitives
+  const unsigned cells = unsigned(mo.nx[0]) * unsigned(mo.nx[1]) * unsigned(mo.nx[2]);
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cells * unsigned(nnew)) return;
+  const int v = blockIdx.y;
   const int q = int(t / cells);
-  long long r = t - (long long)q * cells;
-  const int i = mo.g[0] + int(r % mo.nx[0]);
-  r /= mo.nx[0];
-  const int j = mo.g[1] + int(r % mo.nx[1]);
-  const int k = mo.g[2] + int(r / mo.nx[1]);
+  unsigned r = t - unsigned(q) * cells;
+  const int i = mo.g[0] + int(r % unsigned(mo.nx[0]));
+  r /= unsigned(mo.nx[0]);
+  const int j = mo.g[1] + int(r % unsigned(mo.nx[1]));
+  const int k = mo.g[2] + int(r / unsigned(mo.nx[1]));
   const int G0 = nloc[3 * q] * mo.nx[0] + (i - mo.g[0]);
   const int G1 = nloc[3 * q + 1] * mo.nx[1] + (j - mo.g[1]);
   const int G2 = nloc[3 * q + 2] * mo.nx[2] + (k - mo.g[2]);
@@ -599,16 +602,16 @@ __global__ void k_amr_remap(const __grid_constant__ MeshDesc mo, const S *occ, c
   constexpr bool F32 = sizeof(S) == 4;
   const long long NPo = (long long)mo.nb * mo.P, NPn = (long long)nnew * mo.P;
   const long long dst = (long long)q * mo.P + cidx(mo, k, j, i);
-  for (int v = 0; v < ncc; v++) {
+  if (v < ncc) {
     const Field f{occ + v * NPo, (F32 && v == CENER) ? olo : nullptr, F32};
     const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1);
     const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, fd, err);
     store_value<S>(ncc_out + v * NPn, v == CENER ? nlo : nullptr, dst, val);
-  }
-  for (int v = 0; v < NPRIM; v++) {
-    const Field f{oprim + v * NPo, nullptr, F32};
-    const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, v <= PVEL2 ? v : -1, err);
-    store_value<S>(nprim + v * NPn, nullptr, dst, val);
+  } else {
+    const int pv = v - ncc;
+    const Field f{oprim + pv * NPo, nullptr, F32};
+    const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, pv <= PVEL2 ? pv : -1, err);
+    store_value<S>(nprim + pv * NPn, nullptr, dst, val);
   }
 }
 
@@ -1089,12 +1092,17 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
   if (rc) return rc;
   Container &ob = c->md["base"];
   const long long cells = (long long)m.nx[0] * m.nx[1] * m.nx[2] * nnew;
+  if (cells >= (1LL << 32)) {
+    c->err = "adaptive mesh: more than 2^32 cells";
+    return KMY_ERR_BAD_PARAM;
+  }
+  const dim3 rgrid(nblk(cells), unsigned(c->ncc + NPRIM));
   if (c->esz == 8)
-    k_amr_remap<double><<<nblk(cells), kThreads, 0, c->stream>>>(
+    k_amr_remap<double><<<rgrid, kThreads, 0, c->stream>>>(
         mo, (const double *)ob.cc, nullptr, (const double *)c->prim, nnew, d_nlev, d_nloc, (double *)nb_ct.cc,
         nullptr, (double *)nprim, c->ncc, a.d_err);
   else
-    k_amr_remap<float><<<nblk(cells), kThreads, 0, c->stream>>>(
+    k_amr_remap<float><<<rgrid, kThreads, 0, c->stream>>>(
         mo, (const float *)ob.cc, (const float *)ob.ener_lo, (const float *)c->prim, nnew, d_nlev, d_nloc,
         (float *)nb_ct.cc, (float *)nb_ct.ener_lo, (float *)nprim, c->ncc, a.d_err);
   c->launches++;
