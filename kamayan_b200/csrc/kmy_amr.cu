@@ -37,6 +37,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxDepth = 12;               // unrolled depth of the level value
+// CTAs per SM the level-value kernels keep resident.  The recursive
+// evaluation otherwise takes all 255 registers (one CTA per SM); bounded, its
+// rarely entered deep frames spill instead.
+constexpr int kLvBlocks = 4;
 constexpr long long kMaxTable = 1ll << 26;  // level-table entries over all levels
 
 unsigned nblk(long long n) { return unsigned((n + kThreads - 1) / kThreads); }
@@ -95,6 +99,32 @@ __device__ __forceinline__ double grad_minmod(double fc, double fm, double fp, d
   return 0.5 * (sm + sp) * ((agp < agm) ? agp : agm);
 }
 
+template <int D>
+__device__ __noinline__ double level_value(const MeshDesc &m, int L, int G0, int G1, int G2, const Field &f,
+                                           int flipdim, int *err);
+
+// level_value with its common case inline: a position that holds a leaf at
+// level L is fetched directly, and only restriction or prolongation enters the
+// recursive (register-heavy, non-inlined) evaluation.  Same arithmetic.
+template <int D>
+__device__ __forceinline__ double level_value_at(const MeshDesc &m, int L, int G0, int G1, int G2, const Field &f,
+                                                 int flipdim, int *err) {
+  const int G[3] = {G0, G1, G2};
+  int M[3] = {0, 0, 0};
+  bool flip[3] = {false, false, false};
+  for (int d = 0; d < m.ndim; d++) M[d] = amr_map(G[d], m.mesh_nx[d] << L, m.bc[d][G[d] < 0 ? 0 : 1], flip[d]);
+  int bx[3];
+  for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
+  const int e = table_at(m, L, bx);
+  if (e >= 0) {
+    const double sgn = (flipdim >= 0 && flip[flipdim]) ? -1.0 : 1.0;
+    return sgn * fetch(f, (long long)e * m.P + cidx(m, M[2] - bx[2] * m.nx[2] + m.g[2],
+                                                    M[1] - bx[1] * m.nx[1] + m.g[1],
+                                                    M[0] - bx[0] * m.nx[0] + m.g[0]));
+  }
+  return level_value<D>(m, L, G0, G1, G2, f, flipdim, err);
+}
+
 // Value of field f at level L, global cell G; flipdim is the vector component
 // the field carries (its sign flips across reflecting boundaries) or -1.
 template <int D>
@@ -129,7 +159,7 @@ __device__ __noinline__ double level_value(const MeshDesc &m, int L, int G0, int
           for (int oi = 0; oi < 2; oi++) {
             const int q = ok * 4 + oj * 2 + oi;
             v[q] = vol;
-            t[q] = vol * level_value<D - 1>(m, L + 1, 2 * M[0] + oi, nd > 1 ? 2 * M[1] + oj : 0,
+            t[q] = vol * level_value_at<D - 1>(m, L + 1, 2 * M[0] + oi, nd > 1 ? 2 * M[1] + oj : 0,
                                             nd > 2 ? 2 * M[2] + ok : 0, f, flipdim, err);
           }
       return sgn * restrict8(t, v);
@@ -144,7 +174,7 @@ __device__ __noinline__ double level_value(const MeshDesc &m, int L, int G0, int
       Mc[d] = M[d] >> 1;
       o[d] = M[d] & 1;
     }
-    const double fc = level_value<D - 1>(m, L - 1, Mc[0], Mc[1], Mc[2], f, flipdim, err);
+    const double fc = level_value_at<D - 1>(m, L - 1, Mc[0], Mc[1], Mc[2], f, flipdim, err);
     double gq[3] = {0, 0, 0}, dfm[3] = {0, 0, 0}, dfp[3] = {0, 0, 0};
     for (int d = 0; d < nd; d++) {
       const double dxc = m.dx[d] / double(1 << (L - 1)), dxf = m.dx[d] / double(1 << L);
@@ -152,8 +182,8 @@ __device__ __noinline__ double level_value(const MeshDesc &m, int L, int G0, int
       int Gm[3] = {Mc[0], Mc[1], Mc[2]}, Gp[3] = {Mc[0], Mc[1], Mc[2]};
       Gm[d] -= 1;
       Gp[d] += 1;
-      const double fm = level_value<D - 1>(m, L - 1, Gm[0], Gm[1], Gm[2], f, flipdim, err);
-      const double fp = level_value<D - 1>(m, L - 1, Gp[0], Gp[1], Gp[2], f, flipdim, err);
+      const double fm = level_value_at<D - 1>(m, L - 1, Gm[0], Gm[1], Gm[2], f, flipdim, err);
+      const double fp = level_value_at<D - 1>(m, L - 1, Gp[0], Gp[1], Gp[2], f, flipdim, err);
       const double xm = x0 + (double(Mc[d] - 1) + 0.5) * dxc;
       const double xc = x0 + (double(Mc[d]) + 0.5) * dxc;
       const double xp = x0 + (double(Mc[d] + 1) + 0.5) * dxc;
@@ -397,7 +427,7 @@ __device__ __forceinline__ void store_value(S *arr, float *lo, long long n, doub
 // ghost whose same-level position holds a leaf (the common case) copies it
 // directly; the rest restrict or prolongate.  Reads interior cells only.
 template <typename S>
-__global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, float *lo, S *prim, int ncc,
+__global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, float *lo, S *prim, int ncc,
                                   int *err) {
   // one thread per (padded cell, variable): blockIdx.y runs over the ncc
   // conserved variables, then the NPRIM primitives, so the level-value
@@ -449,7 +479,7 @@ __global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, flo
     return;
   }
   const Field f{arr, vlo, F32};
-  const double val = level_value<kMaxDepth>(m, L, G[0], G[1], G[2], f, fd, err);
+  const double val = level_value_at<kMaxDepth>(m, L, G[0], G[1], G[2], f, fd, err);
   store_value<S>(arr, vlo, dst, val);
 }
 
@@ -580,7 +610,7 @@ __global__ void k_amr_tag(const __grid_constant__ MeshDesc m, Field f, double re
 // Remap after a remesh: every interior cell of the new leaves takes the level
 // value of the old mesh (copy, prolongation or restriction).
 template <typename S>
-__global__ void k_amr_remap(const __grid_constant__ MeshDesc mo, const S *occ, const float *olo, const S *oprim,
+__global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_remap(const __grid_constant__ MeshDesc mo, const S *occ, const float *olo, const S *oprim,
                             int nnew, const int *nlev, const int *nloc, S *ncc_out, float *nlo, S *nprim, int ncc,
                             int *err) {
   // one thread per (new interior cell, variable): blockIdx.y runs over the
@@ -605,12 +635,12 @@ __global__ void k_amr_remap(const __grid_constant__ MeshDesc mo, const S *occ, c
   if (v < ncc) {
     const Field f{occ + v * NPo, (F32 && v == CENER) ? olo : nullptr, F32};
     const int fd = (v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1);
-    const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, fd, err);
+    const double val = level_value_at<kMaxDepth>(mo, L, G0, G1, G2, f, fd, err);
     store_value<S>(ncc_out + v * NPn, v == CENER ? nlo : nullptr, dst, val);
   } else {
     const int pv = v - ncc;
     const Field f{oprim + pv * NPo, nullptr, F32};
-    const double val = level_value<kMaxDepth>(mo, L, G0, G1, G2, f, pv <= PVEL2 ? pv : -1, err);
+    const double val = level_value_at<kMaxDepth>(mo, L, G0, G1, G2, f, pv <= PVEL2 ? pv : -1, err);
     store_value<S>(nprim + pv * NPn, nullptr, dst, val);
   }
 }
