@@ -618,25 +618,23 @@ int launch_apply_faces(kmy_ctx *c, Container &base, Container &md0, Container &m
 // with the same expressions in the same order, so EMFs and face values agree
 // bit for bit with those three kernels.  The EMF and dU/dt arrays are not
 // written.  Edges on block faces read the ghost-layer fluxes of k_flux_halo.
+
+// Edge EMF of edge direction E at in-block face-array offset p: the
+// arithmetic average of CalculateEMF, with k_edge_emf's expression.  Fa / Fb
+// are the block's flux arrays of the two terms: E = 2 reads F_y[B_x] and
+// F_x[B_y], E = 0 F_z[B_y] and F_y[B_z], E = 1 F_x[B_z] and F_z[B_x]; sa / sb
+// are the face-array strides the terms shift along (i, j or k).
 template <typename S>
-__device__ __forceinline__ S edge_emf(const MeshDesc &m, const S *flux, long long bo, int e, int k, int j, int i) {
-  const long long NF = (long long)m.nb * m.Pf;
-  auto F = [&](int dir, int bcomp, int kk, int jj, int ii) {
-    return flux[((long long)dir * 8 + CMAGC0 + bcomp) * NF + bo + fidx(m, kk, jj, ii)];
-  };
-  if (e == 2)
-    return S(1.0) * S(0.25) * (F(1, 0, k, j, i - 1) + F(1, 0, k, j, i) - F(0, 1, k, j - 1, i) - F(0, 1, k, j, i));
-  if (e == 0)
-    return S(1.0) * S(0.25) * (F(2, 1, k, j - 1, i) + F(2, 1, k, j, i) - F(1, 2, k - 1, j, i) - F(1, 2, k, j, i));
-  return S(1.0) * S(0.25) * (F(0, 2, k - 1, j, i) + F(0, 2, k, j, i) - F(2, 0, k, j, i - 1) - F(2, 0, k, j, i));
+__device__ __forceinline__ S edge_emf_at(const S *Fa, const S *Fb, unsigned p, unsigned sa, unsigned sb) {
+  return S(1.0) * S(0.25) * (Fa[p - sa] + Fa[p] - Fb[p - sb] - Fb[p]);
 }
 
-template <typename S>
-__global__ void k_ct_faces(MeshDesc m, const S *flux, const S *fb, S *f0, S *f1, int face, int ne, int e0,
-                           int e1, double beta, const double *dt_dev, const DevClock *clock) {
+template <typename S, int FACE>
+__global__ void k_ct_faces(MeshDesc m, const S *flux, const S *fb, S *f0, S *f1, double beta,
+                           const double *dt_dev, const DevClock *clock) {
   if (clock->done) return;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int n0 = m.nx[0] + (face == 0), n1 = m.nx[1] + (face == 1), n2 = m.nx[2] + (face == 2);
+  const int n0 = m.nx[0] + (FACE == 0), n1 = m.nx[1] + (FACE == 1), n2 = m.nx[2] + (FACE == 2);
   const long long per = (long long)n0 * n1 * n2;
   if (t >= per * m.nb) return;
   int b, i, j, k;
@@ -645,24 +643,43 @@ __global__ void k_ct_faces(MeshDesc m, const S *flux, const S *fb, S *f0, S *f1,
   j += m.g[1];
   k += m.g[2];
   const long long NF = (long long)m.nb * m.Pf, bo = (long long)b * m.Pf;
-  S out = S(0);
-  const int edges[2] = {e0, e1};
-  for (int q = 0; q < ne; q++) {
-    const int edge = edges[q];
-    int axis;  // AxisFromFaceEdge, i=0 j=1 k=2
-    if (face == 0) axis = edge == 2 ? 1 : 2;
-    else if (face == 1) axis = edge == 2 ? 0 : 2;
-    else axis = edge == 0 ? 1 : 0;
-    int ijk[3] = {i, j, k};
-    ijk[axis] += 1;
+  // in-block face-array offsets (a block's face arrays hold fewer than 2^32)
+  const unsigned si = 1, sj = unsigned(m.nf[0]), sk = unsigned(m.nf[0]) * unsigned(m.nf[1]);
+  const unsigned p = (unsigned(k) * unsigned(m.nf[1]) + unsigned(j)) * unsigned(m.nf[0]) + unsigned(i);
+  auto Fp = [&](int dir, int bcomp) { return flux + ((long long)dir * 8 + CMAGC0 + bcomp) * NF + bo; };
+  // The face's edges in FluxStokes order (grid_update.hpp:80-137): edge
+  // direction, the axis its second EMF sits one node further along, and the
+  // sign; in 2D only the z edges.
+  auto stokes = [&](int edge, int axis) -> S {
+    const unsigned sax = axis == 0 ? si : axis == 1 ? sj : sk;
     const S sign = ((axis + 1) % 3 == edge) ? S(1.0) : S(-1.0);
     const S L = S(blk_dx(m, b, edge));
-    const S Ea = edge_emf(m, flux, bo, edge, k, j, i);
-    const S Eb = edge_emf(m, flux, bo, edge, ijk[2], ijk[1], ijk[0]);
-    out += sign * (L * Ea - L * Eb);
+    S Ea, Eb;
+    if (edge == 2) {
+      Ea = edge_emf_at(Fp(1, 0), Fp(0, 1), p, si, sj);
+      Eb = edge_emf_at(Fp(1, 0), Fp(0, 1), p + sax, si, sj);
+    } else if (edge == 0) {
+      Ea = edge_emf_at(Fp(2, 1), Fp(1, 2), p, sj, sk);
+      Eb = edge_emf_at(Fp(2, 1), Fp(1, 2), p + sax, sj, sk);
+    } else {
+      Ea = edge_emf_at(Fp(0, 2), Fp(2, 0), p, sk, si);
+      Eb = edge_emf_at(Fp(0, 2), Fp(2, 0), p + sax, sk, si);
+    }
+    return sign * (L * Ea - L * Eb);
+  };
+  S out = S(0);
+  if (FACE == 0) {
+    out += stokes(2, 1);
+    if (m.ndim > 2) out += stokes(1, 2);
+  } else if (FACE == 1) {
+    out += stokes(2, 0);
+    if (m.ndim > 2) out += stokes(0, 2);
+  } else {
+    out += stokes(0, 1);
+    out += stokes(1, 0);
   }
-  out *= S(1.) / (S(blk_area(m, b, face)) + S(1.e-36));
-  const long long n = face * NF + bo + fidx(m, k, j, i);
+  out *= S(1.) / (S(blk_area(m, b, FACE)) + S(1.e-36));
+  const long long n = FACE * NF + bo + p;
   const double h = *dt_dev;
   const S bt = S(beta);
   const S x0 = bt * fb[n] + (S(1.0) - bt) * f0[n];
@@ -672,22 +689,23 @@ __global__ void k_ct_faces(MeshDesc m, const S *flux, const S *fb, S *f0, S *f1,
 
 int launch_ct_faces(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta) {
   const MeshDesc &m = c->m;
-  struct FE { int face, ne, e0, e1; };
-  const FE l3[3] = {{0, 2, 2, 1}, {1, 2, 2, 0}, {2, 2, 0, 1}};
-  const FE l2[2] = {{0, 1, 2, 0}, {1, 1, 2, 0}};
-  const FE *l = m.ndim > 2 ? l3 : l2;
   for (int f = 0; f < m.ndim; f++) {
-    const FE fe = l[f];
-    const long long nfc = (long long)(m.nx[0] + (fe.face == 0)) * (m.nx[1] + (fe.face == 1)) *
-                          (m.nx[2] + (fe.face == 2)) * m.nb;
-    if (c->esz == 8)
-      k_ct_faces<double><<<nblk(nfc), kThreads, 0, c->stream>>>(
-          m, (const double *)c->flux, (const double *)base.fc, (double *)md0.fc, (double *)md1.fc, fe.face,
-          fe.ne, fe.e0, fe.e1, beta, &c->clock->dt, c->clock);
-    else
-      k_ct_faces<float><<<nblk(nfc), kThreads, 0, c->stream>>>(
-          m, (const float *)c->flux, (const float *)base.fc, (float *)md0.fc, (float *)md1.fc, fe.face, fe.ne,
-          fe.e0, fe.e1, beta, &c->clock->dt, c->clock);
+    const long long nfc =
+        (long long)(m.nx[0] + (f == 0)) * (m.nx[1] + (f == 1)) * (m.nx[2] + (f == 2)) * m.nb;
+#define KMY_CTF(S_, F_)                                                                                    \
+  k_ct_faces<S_, F_><<<nblk(nfc), kThreads, 0, c->stream>>>(m, (const S_ *)c->flux, (const S_ *)base.fc, \
+                                                            (S_ *)md0.fc, (S_ *)md1.fc, beta,            \
+                                                            &c->clock->dt, c->clock)
+    if (c->esz == 8) {
+      if (f == 0) KMY_CTF(double, 0);
+      else if (f == 1) KMY_CTF(double, 1);
+      else KMY_CTF(double, 2);
+    } else {
+      if (f == 0) KMY_CTF(float, 0);
+      else if (f == 1) KMY_CTF(float, 1);
+      else KMY_CTF(float, 2);
+    }
+#undef KMY_CTF
     c->launches++;
   }
   return cuda_check(c, cudaGetLastError(), "ct_faces");
