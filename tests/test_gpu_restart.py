@@ -49,6 +49,14 @@ def test_restart_ct_tasks(kmy_lib, tmp_path):
     _same(a, b, CONS + [("mag", 0), ("mag", 1), ("magc", 0)])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_restart_ct_fused(kmy_lib, tmp_path, precision):
+    # the fused CT stage resumes from the saved primitives, faces and clock
+    deck = configs.ot_3d(n=24, nb=12, precision=precision)
+    a, b = _run(deck, "orszag_tang", 3, 3, "fused", tmp_path)
+    _same(a, b, CONS + [("mag", 0), ("mag", 2), ("magc", 1)])
+
+
 def test_restart_adaptive_mesh(kmy_lib, tmp_path):
     deck = configs.blast_2d_amr(n=64, nb=8, derefine_count=2)
     a, b = _run(deck, "blast", 20, 20, "tasks", tmp_path)
