@@ -478,9 +478,195 @@ __global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_fill_ghosts(const _
     }
     return;
   }
+  // not a leaf at its level: the ghost plan's kernel fills it
+  (void)err;
+}
+
+// ---------------------------------------------------------------------------
+// Ghost plan.  The ghost cells whose position is not a leaf at their level
+// (fine/coarse boundaries) are listed once per table upload, each with the
+// cells its restriction or prolongation reads when every one of them is a
+// leaf one level away (the usual case), so a ghost fill reads them directly
+// instead of walking the tree per variable and stage.  Deeper cases keep the
+// recursive evaluation.  The arithmetic below is level_value's, term for term.
+struct GhostPlan {
+  long long dst;      // ghost cell, offset in [nb][P]
+  long long src[8];   // restriction: the 2^d children (index ok*4 + oj*2 + oi);
+                      // prolongation: the coarse cell, then its - / + neighbours per axis
+  int kind;           // 1 restriction, 2 prolongation, 3 recursive evaluation at fill time
+  int flips;          // bits 0-2: the ghost position's mirrored axes; prolongation:
+                      // bits 3(k+1)+d those of source k
+  int L;              // level of the ghost position
+  int M[3];           // its mapped position at L (kind 3: the unmapped global position)
+};
+
+// Offset of the leaf holding position P at level L, or -1 when no leaf does;
+// fl gets the axes the boundary map mirrored.
+__device__ __forceinline__ long long plan_leaf(const MeshDesc &m, int L, int P0, int P1, int P2, int &fl) {
+  const int G[3] = {P0, P1, P2};
+  int M[3] = {0, 0, 0}, bx[3];
+  bool flip[3] = {false, false, false};
+  for (int d = 0; d < m.ndim; d++) M[d] = amr_map(G[d], m.mesh_nx[d] << L, m.bc[d][G[d] < 0 ? 0 : 1], flip[d]);
+  for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
+  const int e = table_at(m, L, bx);
+  fl = (flip[0] ? 1 : 0) | (flip[1] ? 2 : 0) | (flip[2] ? 4 : 0);
+  if (e < 0) return -1;
+  return (long long)e * m.P + cidx(m, M[2] - bx[2] * m.nx[2] + m.g[2], M[1] - bx[1] * m.nx[1] + m.g[1],
+                                   M[0] - bx[0] * m.nx[0] + m.g[0]);
+}
+
+// The plan entry of padded cell t, or false when t is interior or its
+// position holds a leaf (the copy path of k_amr_fill_ghosts).
+__device__ __forceinline__ bool plan_entry(const MeshDesc &m, unsigned t, GhostPlan &g) {
+  const unsigned P = unsigned(m.P);
+  const int b = int(t / P);
+  unsigned r = t - unsigned(b) * P;
+  const int loc[3] = {int(r % unsigned(m.np[0])), int((r / unsigned(m.np[0])) % unsigned(m.np[1])),
+                      int(r / (unsigned(m.np[0]) * unsigned(m.np[1])))};
+  bool interior = true;
+  for (int d = 0; d < 3; d++)
+    if (loc[d] < m.g[d] || loc[d] >= m.g[d] + m.nx[d]) interior = false;
+  if (interior) return false;
+  const int L = m.blev[b];
+  int G[3];
+  for (int d = 0; d < 3; d++) G[d] = m.bloc[3 * b + d] * m.nx[d] + (loc[d] - m.g[d]);
+  int ftop;
+  if (plan_leaf(m, L, G[0], G[1], G[2], ftop) >= 0) return false;
+  int M[3] = {0, 0, 0}, bx[3];
+  bool flip[3] = {false, false, false};
+  for (int d = 0; d < m.ndim; d++) M[d] = amr_map(G[d], m.mesh_nx[d] << L, m.bc[d][G[d] < 0 ? 0 : 1], flip[d]);
+  for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
+  const int e = table_at(m, L, bx);
+  const int nd = m.ndim;
+  g.dst = (long long)b * m.P + cidx(m, loc[2], loc[1], loc[0]);
+  g.L = L;
+  g.flips = ftop;
+  for (int q = 0; q < 8; q++) g.src[q] = 0;
+  for (int d = 0; d < 3; d++) g.M[d] = M[d];
+  bool leaves = true;
+  if (e == -1) {  // covered by finer leaves: the children at L+1
+    g.kind = 1;
+    for (int ok = 0; ok < 1 + (nd > 2); ok++)
+      for (int oj = 0; oj < 1 + (nd > 1); oj++)
+        for (int oi = 0; oi < 2; oi++) {
+          int fl;
+          const long long s = plan_leaf(m, L + 1, 2 * M[0] + oi, nd > 1 ? 2 * M[1] + oj : 0, nd > 2 ? 2 * M[2] + ok : 0, fl);
+          if (s < 0) leaves = false;
+          g.src[ok * 4 + oj * 2 + oi] = s;
+        }
+  } else if (L > 0) {  // covered by a coarser leaf: the coarse cell and its neighbours
+    g.kind = 2;
+    int Mc[3] = {0, 0, 0};
+    for (int d = 0; d < nd; d++) Mc[d] = M[d] >> 1;
+    int fl;
+    g.src[0] = plan_leaf(m, L - 1, Mc[0], Mc[1], Mc[2], fl);
+    if (g.src[0] < 0) leaves = false;
+    g.flips |= fl << 3;
+    for (int d = 0; d < nd; d++) {
+      int Gm[3] = {Mc[0], Mc[1], Mc[2]}, Gp[3] = {Mc[0], Mc[1], Mc[2]};
+      Gm[d] -= 1;
+      Gp[d] += 1;
+      g.src[1 + 2 * d] = plan_leaf(m, L - 1, Gm[0], Gm[1], Gm[2], fl);
+      g.flips |= fl << (3 * (2 + 2 * d));
+      if (g.src[1 + 2 * d] < 0) leaves = false;
+      g.src[2 + 2 * d] = plan_leaf(m, L - 1, Gp[0], Gp[1], Gp[2], fl);
+      g.flips |= fl << (3 * (3 + 2 * d));
+      if (g.src[2 + 2 * d] < 0) leaves = false;
+    }
+  } else {
+    leaves = false;
+  }
+  if (!leaves) {  // deeper than one level: the fill evaluates it recursively
+    g.kind = 3;
+    for (int d = 0; d < 3; d++) g.M[d] = G[d];
+  }
+  return true;
+}
+
+__global__ void k_amr_plan(const __grid_constant__ MeshDesc m, GhostPlan *plan, int *count) {
+  const unsigned per = unsigned(m.nb) * unsigned(m.P);
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per) return;
+  GhostPlan g;
+  if (!plan_entry(m, t, g)) return;
+  const int q = atomicAdd(count, 1);
+  if (plan) plan[q] = g;
+}
+
+// The planned ghost cells, one thread per (entry, variable) as in
+// k_amr_fill_ghosts.
+template <typename S>
+__global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_fill_plan(const __grid_constant__ MeshDesc m,
+                                                                       const GhostPlan *plan, int nplan, S *cc,
+                                                                       float *lo, S *prim, int ncc, int *err) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nplan) return;
+  const int v = blockIdx.y;
+  const GhostPlan &g = plan[q];
+  const long long NP = (long long)m.nb * m.P;
+  constexpr bool F32 = sizeof(S) == 4;
+  const bool is_cc = v < ncc;
+  S *arr = is_cc ? cc + v * NP : prim + (v - ncc) * NP;
+  const int fd = is_cc ? ((v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1))
+                       : (v - ncc <= PVEL2 ? v - ncc : -1);
+  float *vlo = (F32 && is_cc && v == CENER) ? lo : nullptr;
   const Field f{arr, vlo, F32};
-  const double val = level_value_at<kMaxDepth>(m, L, G[0], G[1], G[2], f, fd, err);
-  store_value<S>(arr, vlo, dst, val);
+  const int L = g.L, nd = m.ndim;
+  if (g.kind == 3) {
+    store_value<S>(arr, vlo, g.dst, level_value_at<kMaxDepth>(m, L, g.M[0], g.M[1], g.M[2], f, fd, err));
+    return;
+  }
+  auto sgn = [&](int k) { return (fd >= 0 && ((g.flips >> (3 * k + fd)) & 1)) ? -1.0 : 1.0; };
+  double val;
+  if (g.kind == 1) {
+    double t[8] = {0, 0, 0, 0, 0, 0, 0, 0}, vv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double vol = 1.0;
+    for (int d = 0; d < 3; d++) vol *= d < nd ? m.dx[d] / double(1 << (L + 1)) : m.dx[d];
+    for (int ok = 0; ok < 1 + (nd > 2); ok++)
+      for (int oj = 0; oj < 1 + (nd > 1); oj++)
+        for (int oi = 0; oi < 2; oi++) {
+          const int c = ok * 4 + oj * 2 + oi;
+          vv[c] = vol;
+          t[c] = vol * fetch(f, g.src[c]);
+        }
+    val = sgn(0) * restrict8(t, vv);
+  } else {
+    int Mc[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+    for (int d = 0; d < nd; d++) {
+      Mc[d] = g.M[d] >> 1;
+      o[d] = g.M[d] & 1;
+    }
+    const double fc = sgn(1) * fetch(f, g.src[0]);
+    double gq[3] = {0, 0, 0}, dfm[3] = {0, 0, 0}, dfp[3] = {0, 0, 0};
+    for (int d = 0; d < nd; d++) {
+      const double dxc = m.dx[d] / double(1 << (L - 1)), dxf = m.dx[d] / double(1 << L);
+      const double x0 = m.xmin[d];
+      const double fm = sgn(2 + 2 * d) * fetch(f, g.src[1 + 2 * d]);
+      const double fp = sgn(3 + 2 * d) * fetch(f, g.src[2 + 2 * d]);
+      const double xm = x0 + (double(Mc[d] - 1) + 0.5) * dxc;
+      const double xc = x0 + (double(Mc[d]) + 0.5) * dxc;
+      const double xp = x0 + (double(Mc[d] + 1) + 0.5) * dxc;
+      const double dxm = xc - xm, dxp = xp - xc;
+      dfm[d] = xc - (x0 + (double(2 * Mc[d]) + 0.5) * dxf);
+      dfp[d] = (x0 + (double(2 * Mc[d] + 1) + 0.5) * dxf) - xc;
+      gq[d] = grad_minmod(fc, fm, fp, dxm, dxp);
+    }
+    const double g1 = gq[0], g2 = gq[1], g3 = gq[2];
+    const double d1m = dfm[0], d1p = dfp[0], d2m = dfm[1], d2p = dfp[1], d3m = dfm[2], d3p = dfp[2];
+    double pv;
+    switch (o[0] + 2 * o[1] + 4 * o[2]) {
+      case 0: pv = fc - (g1 * d1m + g2 * d2m + g3 * d3m); break;
+      case 1: pv = fc + (g1 * d1p - g2 * d2m - g3 * d3m); break;
+      case 2: pv = fc - (g1 * d1m - g2 * d2p + g3 * d3m); break;
+      case 3: pv = fc + (g1 * d1p + g2 * d2p - g3 * d3m); break;
+      case 4: pv = fc - (g1 * d1m + g2 * d2m - g3 * d3p); break;
+      case 5: pv = fc + (g1 * d1p - g2 * d2m + g3 * d3p); break;
+      case 6: pv = fc - (g1 * d1m - g2 * d2p - g3 * d3p); break;
+      default: pv = fc + (g1 * d1p + g2 * d2p + g3 * d3p); break;
+    }
+    val = sgn(0) * pv;
+  }
+  store_value<S>(arr, vlo, g.dst, val);
 }
 
 // Flux correction: a coarse block's boundary face whose neighbour across it
@@ -854,7 +1040,32 @@ int amr_upload(kmy_ctx *c) {
   m.bloc = a.d_bloc;
   m.tabs = a.d_tabs;
   m.nlev = nlev;
-  return KMY_OK;
+  // the ghost plan of the new tables: count, allocate, fill
+  dfree(c, a.d_plan);
+  a.d_plan = nullptr;
+  a.plan_n = 0;
+  if (!a.d_plan_n) rc = dalloc(c, reinterpret_cast<void **>(&a.d_plan_n), sizeof(int));
+  const long long cells = (long long)m.nb * m.P;
+  int count = 0;
+  if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, sizeof(int), c->stream), "plan count");
+  if (!rc) {
+    k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, nullptr, a.d_plan_n);
+    c->launches++;
+    rc = cuda_check(c, cudaMemcpyAsync(&count, a.d_plan_n, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                    "plan count");
+  }
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "plan count");
+  if (!rc && count > 0) {
+    rc = dalloc(c, &a.d_plan, sizeof(GhostPlan) * size_t(count));
+    if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, sizeof(int), c->stream), "plan fill");
+    if (!rc) {
+      k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, static_cast<GhostPlan *>(a.d_plan), a.d_plan_n);
+      c->launches++;
+      rc = cuda_check(c, cudaGetLastError(), "plan fill");
+    }
+    a.plan_n = count;
+  }
+  return rc;
 }
 
 // Initial leaves: every block of the root grid at level 0, lexicographic.
@@ -889,6 +1100,18 @@ int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct) {
     k_amr_fill_ghosts<float><<<grid, kThreads, 0, c->stream>>>(m, (float *)ct.cc, (float *)ct.ener_lo,
                                                                (float *)c->prim, c->ncc, c->amr.d_err);
   c->launches++;
+  const int np = c->amr.plan_n;
+  if (np > 0) {
+    const dim3 pgrid(nblk(np), unsigned(c->ncc + NPRIM));
+    const GhostPlan *plan = static_cast<const GhostPlan *>(c->amr.d_plan);
+    if (c->esz == 8)
+      k_amr_fill_plan<double><<<pgrid, kThreads, 0, c->stream>>>(m, plan, np, (double *)ct.cc, nullptr,
+                                                                 (double *)c->prim, c->ncc, c->amr.d_err);
+    else
+      k_amr_fill_plan<float><<<pgrid, kThreads, 0, c->stream>>>(m, plan, np, (float *)ct.cc, (float *)ct.ener_lo,
+                                                                (float *)c->prim, c->ncc, c->amr.d_err);
+    c->launches++;
+  }
   if (c->prm.mhd) {
     const long long nf = (long long)m.nb * m.Pf;
     for (int e = 0; e < m.ndim; e++) {

@@ -147,6 +147,11 @@ struct AmrHost {
   int *d_blev = nullptr, *d_bloc = nullptr, *d_tabs = nullptr, *d_tags = nullptr;
   int *d_err = nullptr;  // set by a level-value recursion that ran out of depth
   void *d_emf_tmp = nullptr;  // EMFs as computed, read by the edge correction
+  // ghost cells whose position is not a leaf at their level, with the cells
+  // their restriction or prolongation reads (rebuilt at every table upload)
+  void *d_plan = nullptr;
+  int *d_plan_n = nullptr;
+  int plan_n = 0;
   size_t emf_tmp_bytes = 0;
 };
 
