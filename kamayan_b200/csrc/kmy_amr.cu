@@ -423,15 +423,14 @@ __device__ __forceinline__ void store_value(S *arr, float *lo, long long n, doub
   }
 }
 
-// Ghost cells of every block from the level value of the cell they cover.  A
-// ghost whose same-level position holds a leaf (the common case) copies it
-// directly; the rest restrict or prolongate.  Reads interior cells only.
+// Ghost cells of every block whose same-level position holds a leaf (the
+// common case): a copy of that cell, mirrored components negated across a
+// reflecting boundary.  The other ghost cells are the ghost plan's
+// (k_amr_fill_plan).  Reads interior cells only.
 template <typename S>
-__global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, float *lo, S *prim, int ncc,
-                                  int *err) {
+__global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, float *lo, S *prim, int ncc) {
   // one thread per (padded cell, variable): blockIdx.y runs over the ncc
-  // conserved variables, then the NPRIM primitives, so the level-value
-  // evaluations of a ghost cell's variables run side by side
+  // conserved variables, then the NPRIM primitives
   const unsigned per = unsigned(m.nb) * unsigned(m.P);  // cells of all blocks (< 2^32)
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= per) return;
@@ -479,7 +478,6 @@ __global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_fill_ghosts(const _
     return;
   }
   // not a leaf at its level: the ghost plan's kernel fills it
-  (void)err;
 }
 
 // ---------------------------------------------------------------------------
@@ -1095,10 +1093,10 @@ int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct) {
   const dim3 grid(nblk(n), unsigned(c->ncc + NPRIM));
   if (c->esz == 8)
     k_amr_fill_ghosts<double><<<grid, kThreads, 0, c->stream>>>(m, (double *)ct.cc, nullptr, (double *)c->prim,
-                                                                c->ncc, c->amr.d_err);
+                                                                c->ncc);
   else
     k_amr_fill_ghosts<float><<<grid, kThreads, 0, c->stream>>>(m, (float *)ct.cc, (float *)ct.ener_lo,
-                                                               (float *)c->prim, c->ncc, c->amr.d_err);
+                                                               (float *)c->prim, c->ncc);
   c->launches++;
   const int np = c->amr.plan_n;
   if (np > 0) {
