@@ -482,40 +482,106 @@ __global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, flo
 
 // ---------------------------------------------------------------------------
 // Ghost plan.  The ghost cells whose position is not a leaf at their level
-// (fine/coarse boundaries) are listed once per table upload, each with the
-// cells its restriction or prolongation reads when every one of them is a
-// leaf one level away (the usual case), so a ghost fill reads them directly
-// instead of walking the tree per variable and stage.  Deeper cases keep the
-// recursive evaluation.  The arithmetic below is level_value's, term for term.
+// (fine/coarse boundaries) are listed once per table upload with the cells
+// their restriction or prolongation reads, so a ghost fill reads them
+// directly instead of walking the tree per variable and stage.  A source
+// that is no leaf either but is itself one restriction or prolongation of
+// leaves (a prolongation's coarse neighbour where the levels change again,
+// near block corners) becomes an inner entry: its value goes to a scratch
+// slot first and the outer entry reads it there.  Anything deeper keeps the
+// recursive evaluation.  The arithmetic is level_value's, term for term.
 struct GhostPlan {
-  long long dst;      // ghost cell, offset in [nb][P]
+  long long dst;      // outer entry: ghost cell, offset in [nb][P]; inner entry: scratch slot
   long long src[8];   // restriction: the 2^d children (index ok*4 + oj*2 + oi);
-                      // prolongation: the coarse cell, then its - / + neighbours per axis
+                      // prolongation: the coarse cell, then its - / + neighbours per axis;
+                      // >= 0 a leaf cell's offset, < 0 scratch slot -src - 1
   int kind;           // 1 restriction, 2 prolongation, 3 recursive evaluation at fill time
-  int flips;          // bits 0-2: the ghost position's mirrored axes; prolongation:
-                      // bits 3(k+1)+d those of source k
-  int L;              // level of the ghost position
+  int flips;          // bits 0-2: the ghost position's mirrored axes (0 for inner entries);
+                      // prolongation: bits 3(k+1)+d those of source k
+  int L;              // level of the position
   int M[3];           // its mapped position at L (kind 3: the unmapped global position)
 };
 
-// Offset of the leaf holding position P at level L, or -1 when no leaf does;
-// fl gets the axes the boundary map mirrored.
-__device__ __forceinline__ long long plan_leaf(const MeshDesc &m, int L, int P0, int P1, int P2, int &fl) {
-  const int G[3] = {P0, P1, P2};
-  int M[3] = {0, 0, 0}, bx[3];
+// Mapped position M, mirrored axes fl and table entry of global position P
+// at level L.
+__device__ __forceinline__ int plan_map(const MeshDesc &m, int L, const int P[3], int M[3], int &fl) {
   bool flip[3] = {false, false, false};
-  for (int d = 0; d < m.ndim; d++) M[d] = amr_map(G[d], m.mesh_nx[d] << L, m.bc[d][G[d] < 0 ? 0 : 1], flip[d]);
+  M[0] = M[1] = M[2] = 0;
+  for (int d = 0; d < m.ndim; d++) M[d] = amr_map(P[d], m.mesh_nx[d] << L, m.bc[d][P[d] < 0 ? 0 : 1], flip[d]);
+  int bx[3];
   for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
-  const int e = table_at(m, L, bx);
   fl = (flip[0] ? 1 : 0) | (flip[1] ? 2 : 0) | (flip[2] ? 4 : 0);
+  return table_at(m, L, bx);
+}
+
+// Offset of the leaf holding global position P at level L, or -1 when no
+// leaf does; fl gets the axes the boundary map mirrored.
+__device__ __forceinline__ long long plan_leaf(const MeshDesc &m, int L, const int P[3], int &fl) {
+  int M[3];
+  const int e = plan_map(m, L, P, M, fl);
   if (e < 0) return -1;
+  int bx[3];
+  for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
   return (long long)e * m.P + cidx(m, M[2] - bx[2] * m.nx[2] + m.g[2], M[1] - bx[1] * m.nx[1] + m.g[1],
                                    M[0] - bx[0] * m.nx[0] + m.g[0]);
 }
 
-// The plan entry of padded cell t, or false when t is interior or its
-// position holds a leaf (the copy path of k_amr_fill_ghosts).
-__device__ __forceinline__ bool plan_entry(const MeshDesc &m, unsigned t, GhostPlan &g) {
+// Level and global position P of source k of a restriction (kind 1) or a
+// prolongation (kind 2) at mapped position M of level L.
+__device__ __forceinline__ int plan_source(const MeshDesc &m, int kind, int L, const int M[3], int k, int P[3]) {
+  const int nd = m.ndim;
+  if (kind == 1) {
+    P[0] = 2 * M[0] + (k & 1);
+    P[1] = nd > 1 ? 2 * M[1] + ((k >> 1) & 1) : 0;
+    P[2] = nd > 2 ? 2 * M[2] + ((k >> 2) & 1) : 0;
+    return L + 1;
+  }
+  for (int d = 0; d < 3; d++) P[d] = d < nd ? M[d] >> 1 : 0;
+  if (k > 0) P[(k - 1) >> 1] += (k & 1) ? -1 : 1;  // k = 1 + 2d: the - neighbour, 2 + 2d: the +
+  return L - 1;
+}
+
+// Kind and sources of mapped position M at level L, whose table entry e is
+// no leaf: a leaf source gets its offset, any other -1 and its bit in the
+// returned mask.  kind 3 when neither restriction nor prolongation applies
+// (a level-0 position without a leaf, which the recursion reports).
+__device__ __forceinline__ unsigned plan_node(const MeshDesc &m, int L, const int M[3], int e, GhostPlan &g) {
+  g.L = L;
+  for (int d = 0; d < 3; d++) g.M[d] = M[d];
+  for (int q = 0; q < 8; q++) g.src[q] = 0;
+  g.flips = 0;
+  if (e == -1) g.kind = 1;
+  else if (L > 0) g.kind = 2;
+  else {
+    g.kind = 3;
+    return 0;
+  }
+  const int ns = g.kind == 1 ? 1 << m.ndim : 1 + 2 * m.ndim;
+  unsigned miss = 0;
+  for (int k = 0; k < ns; k++) {
+    int P[3], fl;
+    const int Ls = plan_source(m, g.kind, L, M, k, P);
+    g.src[k] = plan_leaf(m, Ls, P, fl);
+    if (g.kind == 2) g.flips |= fl << (3 * (k + 1));
+    if (g.src[k] < 0) miss |= 1u << k;
+  }
+  return miss;
+}
+
+// Inner entry for source k of g, which is no leaf: true when it is one
+// restriction or prolongation of leaves.
+__device__ __forceinline__ bool plan_inner(const MeshDesc &m, const GhostPlan &g, int k, GhostPlan &in) {
+  int P[3], M[3], fl;
+  const int Ls = plan_source(m, g.kind, g.L, g.M, k, P);
+  const int e = plan_map(m, Ls, P, M, fl);
+  if (e >= 0) return false;
+  return plan_node(m, Ls, M, e, in) == 0 && in.kind != 3;
+}
+
+// Outer entry of padded cell t, or false when t is interior or its position
+// holds a leaf (the copy path of k_amr_fill_ghosts).  miss: the sources that
+// need an inner entry; kind 3 when one of them is deeper still.
+__device__ __forceinline__ bool plan_entry(const MeshDesc &m, unsigned t, GhostPlan &g, unsigned &miss) {
   const unsigned P = unsigned(m.P);
   const int b = int(t / P);
   unsigned r = t - unsigned(b) * P;
@@ -526,96 +592,99 @@ __device__ __forceinline__ bool plan_entry(const MeshDesc &m, unsigned t, GhostP
     if (loc[d] < m.g[d] || loc[d] >= m.g[d] + m.nx[d]) interior = false;
   if (interior) return false;
   const int L = m.blev[b];
-  int G[3];
+  int G[3], M[3], ftop;
   for (int d = 0; d < 3; d++) G[d] = m.bloc[3 * b + d] * m.nx[d] + (loc[d] - m.g[d]);
-  int ftop;
-  if (plan_leaf(m, L, G[0], G[1], G[2], ftop) >= 0) return false;
-  int M[3] = {0, 0, 0}, bx[3];
-  bool flip[3] = {false, false, false};
-  for (int d = 0; d < m.ndim; d++) M[d] = amr_map(G[d], m.mesh_nx[d] << L, m.bc[d][G[d] < 0 ? 0 : 1], flip[d]);
-  for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
-  const int e = table_at(m, L, bx);
-  const int nd = m.ndim;
+  const int e = plan_map(m, L, G, M, ftop);
+  if (e >= 0) return false;
+  miss = plan_node(m, L, M, e, g);
   g.dst = (long long)b * m.P + cidx(m, loc[2], loc[1], loc[0]);
-  g.L = L;
-  g.flips = ftop;
-  for (int q = 0; q < 8; q++) g.src[q] = 0;
-  for (int d = 0; d < 3; d++) g.M[d] = M[d];
-  bool leaves = true;
-  if (e == -1) {  // covered by finer leaves: the children at L+1
-    g.kind = 1;
-    for (int ok = 0; ok < 1 + (nd > 2); ok++)
-      for (int oj = 0; oj < 1 + (nd > 1); oj++)
-        for (int oi = 0; oi < 2; oi++) {
-          int fl;
-          const long long s = plan_leaf(m, L + 1, 2 * M[0] + oi, nd > 1 ? 2 * M[1] + oj : 0, nd > 2 ? 2 * M[2] + ok : 0, fl);
-          if (s < 0) leaves = false;
-          g.src[ok * 4 + oj * 2 + oi] = s;
-        }
-  } else if (L > 0) {  // covered by a coarser leaf: the coarse cell and its neighbours
-    g.kind = 2;
-    int Mc[3] = {0, 0, 0};
-    for (int d = 0; d < nd; d++) Mc[d] = M[d] >> 1;
-    int fl;
-    g.src[0] = plan_leaf(m, L - 1, Mc[0], Mc[1], Mc[2], fl);
-    if (g.src[0] < 0) leaves = false;
-    g.flips |= fl << 3;
-    for (int d = 0; d < nd; d++) {
-      int Gm[3] = {Mc[0], Mc[1], Mc[2]}, Gp[3] = {Mc[0], Mc[1], Mc[2]};
-      Gm[d] -= 1;
-      Gp[d] += 1;
-      g.src[1 + 2 * d] = plan_leaf(m, L - 1, Gm[0], Gm[1], Gm[2], fl);
-      g.flips |= fl << (3 * (2 + 2 * d));
-      if (g.src[1 + 2 * d] < 0) leaves = false;
-      g.src[2 + 2 * d] = plan_leaf(m, L - 1, Gp[0], Gp[1], Gp[2], fl);
-      g.flips |= fl << (3 * (3 + 2 * d));
-      if (g.src[2 + 2 * d] < 0) leaves = false;
-    }
-  } else {
-    leaves = false;
+  g.flips |= ftop;
+  for (int k = 0; k < 8 && g.kind != 3; k++) {
+    GhostPlan in;
+    if (((miss >> k) & 1) && !plan_inner(m, g, k, in)) g.kind = 3;
   }
-  if (!leaves) {  // deeper than one level: the fill evaluates it recursively
-    g.kind = 3;
+  if (g.kind == 3) {
+    miss = 0;
     for (int d = 0; d < 3; d++) g.M[d] = G[d];
   }
   return true;
 }
 
-__global__ void k_amr_plan(const __grid_constant__ MeshDesc m, GhostPlan *plan, int *count) {
+// count[0] counts the outer entries read directly, count[1] the recursive
+// ones and count[2] the inner entries.  The fill pass stores them at
+// [0, n0), [n0, n0 + n1) and [n0 + n1, ...), so a warp of the direct fill
+// never waits on a recursion.
+__global__ void k_amr_plan(const __grid_constant__ MeshDesc m, GhostPlan *plan, int *count, int n0, int n1) {
   const unsigned per = unsigned(m.nb) * unsigned(m.P);
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= per) return;
   GhostPlan g;
-  if (!plan_entry(m, t, g)) return;
+  unsigned miss;
+  if (!plan_entry(m, t, g, miss)) return;
+  if (g.kind == 3) {
+    const int q = atomicAdd(count + 1, 1);
+    if (plan) plan[n0 + q] = g;
+    return;
+  }
+  int slot = miss ? atomicAdd(count + 2, __popc(miss)) : 0;
+  if (plan) {
+    for (int k = 0; k < 8; k++) {
+      if (!((miss >> k) & 1)) continue;
+      GhostPlan in;
+      plan_inner(m, g, k, in);
+      in.dst = slot;
+      plan[n0 + n1 + slot] = in;
+      g.src[k] = -1 - (long long)slot;
+      slot++;
+    }
+  }
   const int q = atomicAdd(count, 1);
   if (plan) plan[q] = g;
 }
 
-// The planned ghost cells, one thread per (entry, variable) as in
-// k_amr_fill_ghosts.
+// The variable v of the fill kernels (blockIdx.y: the ncc conserved
+// variables, then the NPRIM primitives): its array, vector component (-1:
+// scalar) and, for FP32 energy, low words.
 template <typename S>
-__global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_fill_plan(const __grid_constant__ MeshDesc m,
-                                                                       const GhostPlan *plan, int nplan, S *cc,
-                                                                       float *lo, S *prim, int ncc, int *err) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nplan) return;
-  const int v = blockIdx.y;
-  const GhostPlan &g = plan[q];
-  const long long NP = (long long)m.nb * m.P;
-  constexpr bool F32 = sizeof(S) == 4;
-  const bool is_cc = v < ncc;
-  S *arr = is_cc ? cc + v * NP : prim + (v - ncc) * NP;
-  const int fd = is_cc ? ((v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1))
-                       : (v - ncc <= PVEL2 ? v - ncc : -1);
-  float *vlo = (F32 && is_cc && v == CENER) ? lo : nullptr;
-  const Field f{arr, vlo, F32};
-  const int L = g.L, nd = m.ndim;
-  if (g.kind == 3) {
-    store_value<S>(arr, vlo, g.dst, level_value_at<kMaxDepth>(m, L, g.M[0], g.M[1], g.M[2], f, fd, err));
-    return;
+struct FillVar {
+  S *arr;
+  float *lo;
+  int fd;
+  __device__ __forceinline__ FillVar(const MeshDesc &m, int v, S *cc, float *clo, S *prim, int ncc) {
+    const long long NP = (long long)m.nb * m.P;
+    const bool is_cc = v < ncc;
+    arr = is_cc ? cc + v * NP : prim + (v - ncc) * NP;
+    fd = is_cc ? ((v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1))
+               : (v - ncc <= PVEL2 ? v - ncc : -1);
+    lo = (sizeof(S) == 4 && is_cc && v == CENER) ? clo : nullptr;
   }
+};
+
+// The plan's recursive entries [q0, q0 + n): level_value at the ghost
+// position, one thread per (entry, variable).
+template <typename S>
+__global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_fill_plan_deep(const __grid_constant__ MeshDesc m,
+                                                                            const GhostPlan *plan, int q0, int n,
+                                                                            S *cc, float *lo, S *prim, int ncc,
+                                                                            int *err) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const FillVar<S> fv(m, blockIdx.y, cc, lo, prim, ncc);
+  const GhostPlan &g = plan[q0 + q];
+  const Field f{fv.arr, fv.lo, sizeof(S) == 4};
+  store_value<S>(fv.arr, fv.lo, g.dst, level_value_at<kMaxDepth>(m, g.L, g.M[0], g.M[1], g.M[2], f, fv.fd, err));
+}
+
+// Value of a restriction (kind 1) or prolongation (kind 2) entry for field f
+// (vector component fd); scr holds this variable's scratch slots.
+__device__ __forceinline__ double plan_value(const MeshDesc &m, const GhostPlan &g, const Field &f, int fd,
+                                             const double *scr) {
+  const int L = g.L, nd = m.ndim;
+  auto src = [&](int k) {
+    const long long s = g.src[k];
+    return s >= 0 ? fetch(f, s) : scr[-s - 1];
+  };
   auto sgn = [&](int k) { return (fd >= 0 && ((g.flips >> (3 * k + fd)) & 1)) ? -1.0 : 1.0; };
-  double val;
   if (g.kind == 1) {
     double t[8] = {0, 0, 0, 0, 0, 0, 0, 0}, vv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double vol = 1.0;
@@ -625,46 +694,62 @@ __global__ void __launch_bounds__(kThreads, kLvBlocks) k_amr_fill_plan(const __g
         for (int oi = 0; oi < 2; oi++) {
           const int c = ok * 4 + oj * 2 + oi;
           vv[c] = vol;
-          t[c] = vol * fetch(f, g.src[c]);
+          t[c] = vol * src(c);
         }
-    val = sgn(0) * restrict8(t, vv);
-  } else {
-    int Mc[3] = {0, 0, 0}, o[3] = {0, 0, 0};
-    for (int d = 0; d < nd; d++) {
-      Mc[d] = g.M[d] >> 1;
-      o[d] = g.M[d] & 1;
-    }
-    const double fc = sgn(1) * fetch(f, g.src[0]);
-    double gq[3] = {0, 0, 0}, dfm[3] = {0, 0, 0}, dfp[3] = {0, 0, 0};
-    for (int d = 0; d < nd; d++) {
-      const double dxc = m.dx[d] / double(1 << (L - 1)), dxf = m.dx[d] / double(1 << L);
-      const double x0 = m.xmin[d];
-      const double fm = sgn(2 + 2 * d) * fetch(f, g.src[1 + 2 * d]);
-      const double fp = sgn(3 + 2 * d) * fetch(f, g.src[2 + 2 * d]);
-      const double xm = x0 + (double(Mc[d] - 1) + 0.5) * dxc;
-      const double xc = x0 + (double(Mc[d]) + 0.5) * dxc;
-      const double xp = x0 + (double(Mc[d] + 1) + 0.5) * dxc;
-      const double dxm = xc - xm, dxp = xp - xc;
-      dfm[d] = xc - (x0 + (double(2 * Mc[d]) + 0.5) * dxf);
-      dfp[d] = (x0 + (double(2 * Mc[d] + 1) + 0.5) * dxf) - xc;
-      gq[d] = grad_minmod(fc, fm, fp, dxm, dxp);
-    }
-    const double g1 = gq[0], g2 = gq[1], g3 = gq[2];
-    const double d1m = dfm[0], d1p = dfp[0], d2m = dfm[1], d2p = dfp[1], d3m = dfm[2], d3p = dfp[2];
-    double pv;
-    switch (o[0] + 2 * o[1] + 4 * o[2]) {
-      case 0: pv = fc - (g1 * d1m + g2 * d2m + g3 * d3m); break;
-      case 1: pv = fc + (g1 * d1p - g2 * d2m - g3 * d3m); break;
-      case 2: pv = fc - (g1 * d1m - g2 * d2p + g3 * d3m); break;
-      case 3: pv = fc + (g1 * d1p + g2 * d2p - g3 * d3m); break;
-      case 4: pv = fc - (g1 * d1m + g2 * d2m - g3 * d3p); break;
-      case 5: pv = fc + (g1 * d1p - g2 * d2m + g3 * d3p); break;
-      case 6: pv = fc - (g1 * d1m - g2 * d2p - g3 * d3p); break;
-      default: pv = fc + (g1 * d1p + g2 * d2p + g3 * d3p); break;
-    }
-    val = sgn(0) * pv;
+    return sgn(0) * restrict8(t, vv);
   }
-  store_value<S>(arr, vlo, g.dst, val);
+  int Mc[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+  for (int d = 0; d < nd; d++) {
+    Mc[d] = g.M[d] >> 1;
+    o[d] = g.M[d] & 1;
+  }
+  const double fc = sgn(1) * src(0);
+  double gq[3] = {0, 0, 0}, dfm[3] = {0, 0, 0}, dfp[3] = {0, 0, 0};
+  for (int d = 0; d < nd; d++) {
+    const double dxc = m.dx[d] / double(1 << (L - 1)), dxf = m.dx[d] / double(1 << L);
+    const double x0 = m.xmin[d];
+    const double fm = sgn(2 + 2 * d) * src(1 + 2 * d);
+    const double fp = sgn(3 + 2 * d) * src(2 + 2 * d);
+    const double xm = x0 + (double(Mc[d] - 1) + 0.5) * dxc;
+    const double xc = x0 + (double(Mc[d]) + 0.5) * dxc;
+    const double xp = x0 + (double(Mc[d] + 1) + 0.5) * dxc;
+    const double dxm = xc - xm, dxp = xp - xc;
+    dfm[d] = xc - (x0 + (double(2 * Mc[d]) + 0.5) * dxf);
+    dfp[d] = (x0 + (double(2 * Mc[d] + 1) + 0.5) * dxf) - xc;
+    gq[d] = grad_minmod(fc, fm, fp, dxm, dxp);
+  }
+  const double g1 = gq[0], g2 = gq[1], g3 = gq[2];
+  const double d1m = dfm[0], d1p = dfp[0], d2m = dfm[1], d2p = dfp[1], d3m = dfm[2], d3p = dfp[2];
+  double pv;
+  switch (o[0] + 2 * o[1] + 4 * o[2]) {
+    case 0: pv = fc - (g1 * d1m + g2 * d2m + g3 * d3m); break;
+    case 1: pv = fc + (g1 * d1p - g2 * d2m - g3 * d3m); break;
+    case 2: pv = fc - (g1 * d1m - g2 * d2p + g3 * d3m); break;
+    case 3: pv = fc + (g1 * d1p + g2 * d2p - g3 * d3m); break;
+    case 4: pv = fc - (g1 * d1m + g2 * d2m - g3 * d3p); break;
+    case 5: pv = fc + (g1 * d1p - g2 * d2m + g3 * d3p); break;
+    case 6: pv = fc - (g1 * d1m - g2 * d2p - g3 * d3p); break;
+    default: pv = fc + (g1 * d1p + g2 * d2p + g3 * d3p); break;
+  }
+  return sgn(0) * pv;
+}
+
+// Plan entries [q0, q0 + n), one thread per (entry, variable) as in
+// k_amr_fill_ghosts.  INNER: the inner entries, into the scratch slots
+// ([variable][nscr] doubles); otherwise the direct outer entries, into their
+// ghost cells.
+template <typename S, bool INNER>
+__global__ void k_amr_fill_plan(const __grid_constant__ MeshDesc m, const GhostPlan *plan, int q0, int n, S *cc,
+                                float *lo, S *prim, int ncc, double *scratch, int nscr) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const FillVar<S> fv(m, blockIdx.y, cc, lo, prim, ncc);
+  const GhostPlan &g = plan[q0 + q];
+  const Field f{fv.arr, fv.lo, sizeof(S) == 4};
+  double *scr = scratch + (long long)blockIdx.y * nscr;
+  const double val = plan_value(m, g, f, fv.fd, scr);
+  if constexpr (INNER) scr[g.dst] = val;
+  else store_value<S>(fv.arr, fv.lo, g.dst, val);
 }
 
 // Flux correction: a coarse block's boundary face whose neighbour across it
@@ -1040,28 +1125,36 @@ int amr_upload(kmy_ctx *c) {
   m.nlev = nlev;
   // the ghost plan of the new tables: count, allocate, fill
   dfree(c, a.d_plan);
+  dfree(c, a.d_plan_scr);
   a.d_plan = nullptr;
-  a.plan_n = 0;
-  if (!a.d_plan_n) rc = dalloc(c, reinterpret_cast<void **>(&a.d_plan_n), sizeof(int));
+  a.d_plan_scr = nullptr;
+  a.plan_n = a.plan_deep = a.plan_inner = 0;
+  if (!a.d_plan_n) rc = dalloc(c, reinterpret_cast<void **>(&a.d_plan_n), 3 * sizeof(int));
   const long long cells = (long long)m.nb * m.P;
-  int count = 0;
-  if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, sizeof(int), c->stream), "plan count");
+  int count[3] = {0, 0, 0};
+  if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, 3 * sizeof(int), c->stream), "plan count");
   if (!rc) {
-    k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, nullptr, a.d_plan_n);
+    k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, nullptr, a.d_plan_n, 0, 0);
     c->launches++;
-    rc = cuda_check(c, cudaMemcpyAsync(&count, a.d_plan_n, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+    rc = cuda_check(c, cudaMemcpyAsync(count, a.d_plan_n, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream),
                     "plan count");
   }
   if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "plan count");
-  if (!rc && count > 0) {
-    rc = dalloc(c, &a.d_plan, sizeof(GhostPlan) * size_t(count));
-    if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, sizeof(int), c->stream), "plan fill");
+  const long long nplan = (long long)count[0] + count[1] + count[2];
+  if (!rc && nplan > 0) {
+    rc = dalloc(c, &a.d_plan, sizeof(GhostPlan) * size_t(nplan));
+    if (!rc && count[2] > 0)
+      rc = dalloc(c, reinterpret_cast<void **>(&a.d_plan_scr), sizeof(double) * size_t(c->ncc + NPRIM) * count[2]);
+    if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, 3 * sizeof(int), c->stream), "plan fill");
     if (!rc) {
-      k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, static_cast<GhostPlan *>(a.d_plan), a.d_plan_n);
+      k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, static_cast<GhostPlan *>(a.d_plan), a.d_plan_n,
+                                                          count[0], count[1]);
       c->launches++;
       rc = cuda_check(c, cudaGetLastError(), "plan fill");
     }
-    a.plan_n = count;
+    a.plan_n = count[0];
+    a.plan_deep = count[1];
+    a.plan_inner = count[2];
   }
   return rc;
 }
@@ -1098,16 +1191,42 @@ int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct) {
     k_amr_fill_ghosts<float><<<grid, kThreads, 0, c->stream>>>(m, (float *)ct.cc, (float *)ct.ener_lo,
                                                                (float *)c->prim, c->ncc);
   c->launches++;
-  const int np = c->amr.plan_n;
-  if (np > 0) {
-    const dim3 pgrid(nblk(np), unsigned(c->ncc + NPRIM));
-    const GhostPlan *plan = static_cast<const GhostPlan *>(c->amr.d_plan);
+  const GhostPlan *plan = static_cast<const GhostPlan *>(c->amr.d_plan);
+  const int n0 = c->amr.plan_n, n1 = c->amr.plan_deep, n2 = c->amr.plan_inner;
+  double *scr = c->amr.d_plan_scr;
+  const unsigned nvar = unsigned(c->ncc + NPRIM);
+  // inner entries first: the direct ones read their scratch slots
+  if (n2 > 0) {
+    const dim3 pgrid(nblk(n2), nvar);
     if (c->esz == 8)
-      k_amr_fill_plan<double><<<pgrid, kThreads, 0, c->stream>>>(m, plan, np, (double *)ct.cc, nullptr,
-                                                                 (double *)c->prim, c->ncc, c->amr.d_err);
+      k_amr_fill_plan<double, true><<<pgrid, kThreads, 0, c->stream>>>(m, plan, n0 + n1, n2, (double *)ct.cc,
+                                                                       nullptr, (double *)c->prim, c->ncc, scr, n2);
     else
-      k_amr_fill_plan<float><<<pgrid, kThreads, 0, c->stream>>>(m, plan, np, (float *)ct.cc, (float *)ct.ener_lo,
-                                                                (float *)c->prim, c->ncc, c->amr.d_err);
+      k_amr_fill_plan<float, true><<<pgrid, kThreads, 0, c->stream>>>(m, plan, n0 + n1, n2, (float *)ct.cc,
+                                                                      (float *)ct.ener_lo, (float *)c->prim, c->ncc,
+                                                                      scr, n2);
+    c->launches++;
+  }
+  if (n0 > 0) {
+    const dim3 pgrid(nblk(n0), nvar);
+    if (c->esz == 8)
+      k_amr_fill_plan<double, false><<<pgrid, kThreads, 0, c->stream>>>(m, plan, 0, n0, (double *)ct.cc, nullptr,
+                                                                        (double *)c->prim, c->ncc, scr, n2);
+    else
+      k_amr_fill_plan<float, false><<<pgrid, kThreads, 0, c->stream>>>(m, plan, 0, n0, (float *)ct.cc,
+                                                                       (float *)ct.ener_lo, (float *)c->prim,
+                                                                       c->ncc, scr, n2);
+    c->launches++;
+  }
+  if (n1 > 0) {
+    const dim3 pgrid(nblk(n1), nvar);
+    if (c->esz == 8)
+      k_amr_fill_plan_deep<double><<<pgrid, kThreads, 0, c->stream>>>(m, plan, n0, n1, (double *)ct.cc, nullptr,
+                                                                      (double *)c->prim, c->ncc, c->amr.d_err);
+    else
+      k_amr_fill_plan_deep<float><<<pgrid, kThreads, 0, c->stream>>>(m, plan, n0, n1, (float *)ct.cc,
+                                                                     (float *)ct.ener_lo, (float *)c->prim, c->ncc,
+                                                                     c->amr.d_err);
     c->launches++;
   }
   if (c->prm.mhd) {
@@ -1210,12 +1329,17 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
     c->err = "adaptive mesh: a level-value evaluation exceeded its depth or call budget (mesh not 2:1 balanced)";
     return KMY_ERR_STATE;
   }
+  // derefinement counts; a step with no split candidate, a balanced tree and
+  // no leaf due for derefinement leaves the mesh as it is
+  bool any = !a.balanced;
+  for (int b = 0; b < nb; b++) {
+    a.cnt[b] = tags[b] == -1 ? a.cnt[b] + 1 : 0;
+    if ((tags[b] == 1 && a.lev[b] < a.max_level) || (a.lev[b] > 0 && a.cnt[b] >= a.derefine_count)) any = true;
+  }
+  if (!any) return KMY_OK;
   typedef std::array<int, 4> Key;  // level, location
   std::map<Key, int> leaf;         // -> old leaf id, -1 for a new leaf
-  for (int b = 0; b < nb; b++) {
-    leaf[{a.lev[b], a.loc[3 * b], a.loc[3 * b + 1], a.loc[3 * b + 2]}] = b;
-    a.cnt[b] = tags[b] == -1 ? a.cnt[b] + 1 : 0;
-  }
+  for (int b = 0; b < nb; b++) leaf[{a.lev[b], a.loc[3 * b], a.loc[3 * b + 1], a.loc[3 * b + 2]}] = b;
   bool changed = false;
   auto child = [&](const Key &p, int o) {
     return Key{p[0] + 1, 2 * p[1] + (o & 1), nd > 1 ? 2 * p[2] + ((o >> 1) & 1) : 0,

@@ -149,9 +149,13 @@ struct AmrHost {
   void *d_emf_tmp = nullptr;  // EMFs as computed, read by the edge correction
   // ghost cells whose position is not a leaf at their level, with the cells
   // their restriction or prolongation reads (rebuilt at every table upload)
+  // (entries [0, plan_n) are read directly, the next plan_deep evaluated
+  // recursively, the last plan_inner are inner entries whose values the
+  // direct ones read from d_plan_scr, [variable][plan_inner] doubles)
   void *d_plan = nullptr;
-  int *d_plan_n = nullptr;
-  int plan_n = 0;
+  int *d_plan_n = nullptr;  // three counters: direct, recursive, inner
+  double *d_plan_scr = nullptr;
+  int plan_n = 0, plan_deep = 0, plan_inner = 0;
   size_t emf_tmp_bytes = 0;
 };
 

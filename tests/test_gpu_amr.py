@@ -54,10 +54,19 @@ def test_initial_refinement_on_pressure(kmy_lib, oracle_mod):
     assert abs(s.time["dt"] - o.time["dt"]) <= 1e-14 * o.time["dt"]
 
 
-def test_level_exchange_bit_identical(kmy_lib, oracle_mod):
+@pytest.mark.parametrize("bc", ["outflow", "reflecting", "periodic"])
+def test_level_exchange_bit_identical(kmy_lib, oracle_mod, bc):
     # identical interiors on an identical 3-level mesh: every ghost cell (copy,
-    # restriction of finer leaves, minmod prolongation) matches bit for bit
+    # restriction of finer leaves, minmod prolongation, and the corners where
+    # a prolongation's coarse neighbour is itself restricted or prolongated)
+    # matches bit for bit, mirrored components included
     deck = configs.blast_2d_amr(n=64, nb=8, field="pres")
+    for ax in "12":
+        deck.set("parthenon/mesh", f"ix{ax}_bc", bc).set("parthenon/mesh", f"ox{ax}_bc", bc)
+        if bc != "outflow":
+            # the blast (centred on the origin) near the low corner, so the
+            # refined levels reach the boundary and its mapped ghost cells
+            deck.set("parthenon/mesh", f"x{ax}min", -0.125).set("parthenon/mesh", f"x{ax}max", 0.875)
     o, s = _pair(deck)
     _same_blocks(o, s)
     for var, c in CONS + PRIMS:
