@@ -338,52 +338,22 @@ def serving_block(a, device: int) -> dict:
     }
 
 
-def _evolve_timed(s, stream, tlim=None, nsteps=None):
-    """Step to tlim (or nsteps) with kmy_step; device time between two events on the
-    solver's stream, and the interior cells advanced (block counts change under AMR)."""
+def _evolve_run(s, stream, tlim: float = 1e30, nlim: int = -1):
+    """kmy_evolve to tlim (or nlim steps) in one call; device time between two
+    events on the solver's stream, the zone-cycles the library counted (each
+    step's interior cells on the mesh it ran on, so block-count changes under
+    AMR are included) and the steps taken."""
     import torch
 
-    cells_per_block = 1
-    for x in s.info.nx:
-        cells_per_block *= x
-    torch.cuda.synchronize()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    updates, steps, nbs = 0, 0, []
-    t0.record(stream)
-    while True:
-        if nsteps is not None and steps >= nsteps:
-            break
-        if tlim is not None and s.time["time"] >= tlim * (1 - 1e-14):
-            break
-        nb = s.nblocks
-        s.step()
-        updates += nb * cells_per_block
-        nbs.append(nb)
-        steps += 1
-    t1.record(stream)
-    torch.cuda.synchronize()
-    return t0.elapsed_time(t1), updates, steps, nbs
-
-
-def _evolve_run(s, stream, tlim: float):
-    """kmy_evolve to tlim on a fixed mesh; device time between two events on the
-    solver's stream, the interior cells advanced and the steps taken."""
-    import torch
-
-    cells = s.nblocks
-    for x in s.info.nx:
-        cells *= x
-    n0 = s.time["ncycle"]
+    n0, z0 = s.time["ncycle"], s.zone_cycles
     torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
-    s.evolve(tlim)
+    s.evolve(tlim, nlim)
     t1.record(stream)
     torch.cuda.synchronize()
-    steps = s.time["ncycle"] - n0
-    return t0.elapsed_time(t1), cells * steps, steps
+    return t0.elapsed_time(t1), s.zone_cycles - z0, s.time["ncycle"] - n0
 
 
 def workloads_block(a, device: int, stream) -> dict:
@@ -417,8 +387,8 @@ def workloads_block(a, device: int, stream) -> dict:
     ot = {}
     for path in ("fused", "tasks"):
         s = solver(configs.ot_3d(n=n3, nb=32, precision="fp32"), "orszag_tang", path)
-        _evolve_timed(s, stream, nsteps=2)
-        ms, upd, steps, _ = _evolve_timed(s, stream, nsteps=max(3, a.steps // 4))
+        _evolve_run(s, stream, nlim=2)
+        ms, upd, steps = _evolve_run(s, stream, nlim=max(3, a.steps // 4))
         ot[path] = (upd / (ms / 1e3), steps, ms / steps, float(abs(s.interior(s.export("divb"))).max()))
         s.close()
     out["orszag_tang_3d_ct_fp32"] = {
@@ -428,10 +398,11 @@ def workloads_block(a, device: int, stream) -> dict:
         "config": f"{n3}^3 in 32^3 blocks, g=4, CT, PPM(MC)+HLL, RK2, CFL 0.3, fused stage"}
     # c4: blast on an adaptive mesh, 128^2 base in 16^2 blocks, 3 levels, Loehner on density
     s = solver(configs.blast_2d_amr(), "blast", "tasks")
-    ms, upd, steps, nbs = _evolve_timed(s, stream, tlim=0.2)
+    nb0 = s.nblocks
+    ms, upd, steps = _evolve_run(s, stream, tlim=0.2)
     out["blast_2d_amr_fp64"] = {
         "cell_updates_per_s": upd / (ms / 1e3), "steps": steps, "seconds": ms / 1e3,
-        "blocks_min_max": [min(nbs), max(nbs)], "blocks_final": s.nblocks,
+        "blocks_initial": nb0, "blocks_final": s.nblocks,
         "config": "128^2 base in 16^2 blocks, 3 levels, Loehner dens 0.3/0.05, PLM(MC)+HLLC, RK2, t=0.2"}
     s.close()
     return out

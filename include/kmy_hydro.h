@@ -156,6 +156,11 @@ int kmy_evolve(kmy_ctx *ctx, double tlim, int nlim, int *nsteps);
 int kmy_end_step(kmy_ctx *ctx);
 /* Simulation clock: time, next dt, last dt estimate, cycle count. */
 int kmy_get_time(const kmy_ctx *ctx, double *time, double *dt, double *dt_est, int *ncycle);
+/* Zone-cycles since set-up: the interior cells of each completed step's mesh
+ * (before its remesh), summed over the steps.  Divided by wall time it is the
+ * zone-cycles/wall_second figure the reference's driver prints every
+ * ncycle_out cycles (src/driver/kamayan_driver.cpp:63-78). */
+int kmy_zone_cycles(const kmy_ctx *ctx, int64_t *out);
 /* Leaf blocks in block order: refinement level (levels[b]) and logical
  * location at that level (locations[3b..3b+2], i j k).  Fills at most
  * max_blocks entries; *nblocks receives the block count.  Single-level meshes

@@ -35,6 +35,7 @@ EXPORTS = (
     "kmy_compute_fluxes", "kmy_compute_emf", "kmy_flux_divergence", "kmy_apply_dudt",
     "kmy_prepare_primitive", "kmy_fill_ghosts", "kmy_estimate_dt", "kmy_fill_derived",
     "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_end_step", "kmy_get_time",
+    "kmy_zone_cycles",
     "kmy_get_blocks", "kmy_set_dt", "kmy_save_restart", "kmy_load_restart",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
     "kmy_conserved_sums_noalloc",
@@ -106,6 +107,7 @@ def lib() -> ctypes.CDLL:
         L.kmy_vortex_error.argtypes = [vp, i, i, _dp]
         L.kmy_conserved_sums.argtypes = [vp, cp, _dp]
         L.kmy_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.kmy_zone_cycles.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         ip3 = ctypes.POINTER(ctypes.c_int)
         L.kmy_conserved_sums_noalloc.argtypes = [vp, i, i, ip3, ip3, ip3, d, vp, vp]
         i64p = ctypes.POINTER(ctypes.c_int64)
@@ -344,6 +346,14 @@ class Solver:
         out = np.zeros(self.info.ncons)
         self._check(lib().kmy_conserved_sums(self._h, md.encode(), _ptr(out)))
         return out
+
+    @property
+    def zone_cycles(self) -> int:
+        """Interior cells x completed steps since set-up (each step counted on
+        the mesh it ran on)."""
+        n = ctypes.c_int64()
+        self._check(lib().kmy_zone_cycles(self._h, ctypes.byref(n)))
+        return n.value
 
     @property
     def launch_count(self) -> int:

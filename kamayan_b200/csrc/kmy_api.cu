@@ -910,13 +910,18 @@ static bool steps_fused(const kmy_ctx *c) {
   return c->path == 0 && !c->amr.on && (!c->prm.mhd || !fused_ct_unsupported(c));
 }
 
+static long long interior_cells(const kmy_ctx *c) {
+  return (long long)c->m.nb * c->m.nx[0] * c->m.nx[1] * c->m.nx[2];
+}
+
 static int step_async(kmy_ctx *c) {
   const int ns = int(c->prm.beta.size());
+  const long long cells = interior_cells(c);  // before a remesh changes the mesh
   int rc = KMY_OK;
   const bool fused = steps_fused(c);
   for (int s = 1; s <= ns && !rc; s++) rc = fused ? fused_stage(c, s) : task_stage(c, s, -1.0);
   if (!rc && c->amr.on) rc = amr_after_step(c);
-  if (!rc) rc = launch_dt_controller(c, 0);
+  if (!rc) rc = launch_dt_controller(c, 0, cells);
   return rc;
 }
 
@@ -1047,8 +1052,9 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
 int kmy_end_step(kmy_ctx *c) {
   if (!c) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
+  const long long cells = interior_cells(c);
   int rc = c->amr.on ? amr_after_step(c) : KMY_OK;
-  if (!rc) rc = launch_dt_controller(c, 0);
+  if (!rc) rc = launch_dt_controller(c, 0, cells);
   return rc;
 }
 
@@ -1074,6 +1080,17 @@ int kmy_get_time(const kmy_ctx *c, double *time, double *dt, double *dt_est, int
   if (dt) *dt = h.dt;
   if (dt_est) *dt_est = h.dt_est;
   if (ncycle) *ncycle = h.ncycle;
+  return KMY_OK;
+}
+
+int kmy_zone_cycles(const kmy_ctx *c, int64_t *out) {
+  if (!c || !out) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  DevClock h;
+  cudaError_t e = cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return KMY_ERR_CUDA;
+  *out = int64_t(h.zone_cycles);
   return KMY_OK;
 }
 

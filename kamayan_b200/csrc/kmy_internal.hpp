@@ -78,6 +78,7 @@ struct DevClock {
   int ncycle;
   int done;         // time >= tlim: stage kernels become no-ops
   int status;       // KMY_ERR_NONFINITE when the estimate was not finite/positive
+  unsigned long long zone_cycles;  // interior cells x completed steps, summed over the steps
 };
 
 struct TimeParams {
@@ -219,7 +220,9 @@ int launch_fill_derived(kmy_ctx *c, Container &md);
 int launch_eos_init(kmy_ctx *c, Container &md);
 int launch_convert_to_conserved(kmy_ctx *c, Container &md);
 // mode 0: after a step; 1: initial dt from the estimate; 2: clamp pending dt to tlim
-int launch_dt_controller(kmy_ctx *c, int mode);
+// cells: interior cells of the step the controller completes (mode 0); -1
+// takes the current mesh's.
+int launch_dt_controller(kmy_ctx *c, int mode, long long cells = -1);
 int launch_conserved_sums(kmy_ctx *c, Container &md, double *host_out);
 int launch_vortex_error(kmy_ctx *c, int var, int comp, double *host_out);
 int launch_set_energy_split(kmy_ctx *c, Container &ct);

@@ -11,7 +11,7 @@
 // counters.  Stage containers, fluxes and EMFs are rebuilt by every step and
 // are not saved.  The file carries the deck, so a restart needs nothing else.
 //
-// Layout (native byte order): magic "KMYRST01", then int32 fields, int64
+// Layout (native byte order): magic "KMYRST02", then int32 fields, int64
 // sizes, the deck text, the leaf list, raw structs, raw device arrays.
 #include <cstdio>
 #include <cstring>
@@ -25,7 +25,7 @@ using kmy::Container;
 
 namespace {
 
-constexpr char kMagic[8] = {'K', 'M', 'Y', 'R', 'S', 'T', '0', '1'};
+constexpr char kMagic[8] = {'K', 'M', 'Y', 'R', 'S', 'T', '0', '2'};
 constexpr size_t kChunk = size_t(64) << 20;  // device <-> file staging chunk
 
 struct Header {

@@ -870,7 +870,7 @@ int launch_estimate_dt(kmy_ctx *c, Container &md, bool reset) {
 }
 
 // Parthenon EvolutionDriver::SetGlobalTimeStep, restated (single thread).
-__global__ void k_dt_controller(DevClock *clk, TimeParams tp, int mode) {
+__global__ void k_dt_controller(DevClock *clk, TimeParams tp, int mode, long long cells) {
   double dtmin;
   const unsigned long long bits = clk->dtmin_bits;
   dtmin = __longlong_as_double((long long)bits);
@@ -883,10 +883,12 @@ __global__ void k_dt_controller(DevClock *clk, TimeParams tp, int mode) {
   if (mode == 0) {
     if (clk->done) return;
     advance_clock(clk, tp);
+    clk->zone_cycles += (unsigned long long)cells;
     return;
   } else {
     clk->time = 0.0;
     clk->ncycle = 0;
+    clk->zone_cycles = 0;
     clk->dt = big;
     clk->dt_taken = 0.0;
     clk->status = 0;
@@ -906,8 +908,10 @@ __global__ void k_dt_controller(DevClock *clk, TimeParams tp, int mode) {
   clk->dtmin_bits = 0x7FF0000000000000ull;  // the next step's CFL minimum starts at +inf
 }
 
-int launch_dt_controller(kmy_ctx *c, int mode) {
-  k_dt_controller<<<1, 1, 0, c->stream>>>(c->clock, c->prm.tp, mode);
+int launch_dt_controller(kmy_ctx *c, int mode, long long cells) {
+  const MeshDesc &m = c->m;
+  if (cells < 0) cells = (long long)m.nb * m.nx[0] * m.nx[1] * m.nx[2];
+  k_dt_controller<<<1, 1, 0, c->stream>>>(c->clock, c->prm.tp, mode, cells);
   c->launches++;
   return cuda_check(c, cudaGetLastError(), "dt_controller");
 }

@@ -184,3 +184,27 @@ def test_two_criteria_take_the_larger_tag(kmy_lib, oracle_mod):
         _same_blocks(o, s)
     res = compare(o, s)
     assert all(v <= TOL_NSTEP for v in res.values()), res
+
+
+def test_zone_cycles_count_each_step_on_its_mesh(kmy_lib):
+    # the zone-cycle counter adds each step's interior cells before its
+    # remesh, through kmy_step and through kmy_evolve alike
+    from kamayan_b200 import Solver
+
+    deck = configs.blast_2d_amr(n=64, nb=8, derefine_count=2)
+    s = Solver(deck.text())
+    s.set_path("tasks")
+    s.pgen("blast")
+    assert s.zone_cycles == 0
+    per_block = 8 * 8
+    expect, counts = 0, set()
+    for _ in range(60):  # derefinement within 60 steps: test_derefinement_happens
+        counts.add(s.nblocks)
+        expect += s.nblocks * per_block
+        s.step()
+    assert s.zone_cycles == expect
+    assert len(counts) > 1, "the mesh never changed"
+    n0, z0 = s.time["ncycle"], s.zone_cycles
+    nb = s.nblocks
+    s.evolve(1e30, 1)
+    assert s.time["ncycle"] == n0 + 1 and s.zone_cycles == z0 + nb * per_block
