@@ -423,63 +423,6 @@ __device__ __forceinline__ void store_value(S *arr, float *lo, long long n, doub
   }
 }
 
-// Ghost cells of every block whose same-level position holds a leaf (the
-// common case): a copy of that cell, mirrored components negated across a
-// reflecting boundary.  The other ghost cells are the ghost plan's
-// (k_amr_fill_plan).  Reads interior cells only.
-template <typename S>
-__global__ void k_amr_fill_ghosts(const __grid_constant__ MeshDesc m, S *cc, float *lo, S *prim, int ncc) {
-  // one thread per (padded cell, variable): blockIdx.y runs over the ncc
-  // conserved variables, then the NPRIM primitives
-  const unsigned per = unsigned(m.nb) * unsigned(m.P);  // cells of all blocks (< 2^32)
-  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= per) return;
-  const int v = blockIdx.y;
-  const unsigned P = unsigned(m.P);
-  const int b = int(t / P);
-  unsigned r = t - unsigned(b) * P;
-  const int i = int(r % unsigned(m.np[0]));
-  r /= unsigned(m.np[0]);
-  const int j = int(r % unsigned(m.np[1]));
-  const int k = int(r / unsigned(m.np[1]));
-  const int loc[3] = {i, j, k};
-  bool interior = true;
-  for (int d = 0; d < 3; d++)
-    if (loc[d] < m.g[d] || loc[d] >= m.g[d] + m.nx[d]) interior = false;
-  if (interior) return;
-  const int L = m.blev[b];
-  int G[3];
-  for (int d = 0; d < 3; d++) G[d] = m.bloc[3 * b + d] * m.nx[d] + (loc[d] - m.g[d]);
-  const long long NP = (long long)m.nb * m.P;
-  const long long dst = (long long)b * m.P + cidx(m, k, j, i);
-  constexpr bool F32 = sizeof(S) == 4;
-  const bool is_cc = v < ncc;
-  // the variable, its vector component (-1: scalar) and, for FP32 energy,
-  // its low words
-  S *arr = is_cc ? cc + v * NP : prim + (v - ncc) * NP;
-  const int fd = is_cc ? ((v >= CMOM0 && v <= CMOM2) ? v - CMOM0 : (v >= CMAGC0 ? v - CMAGC0 : -1))
-                       : (v - ncc <= PVEL2 ? v - ncc : -1);
-  float *vlo = (F32 && is_cc && v == CENER) ? lo : nullptr;
-
-  int M[3] = {0, 0, 0}, bx[3];
-  bool flip[3] = {false, false, false};
-  for (int d = 0; d < m.ndim; d++) M[d] = amr_map(G[d], m.mesh_nx[d] << L, m.bc[d][G[d] < 0 ? 0 : 1], flip[d]);
-  for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
-  const int e = table_at(m, L, bx);
-  if (e >= 0) {
-    const long long s = (long long)e * m.P + cidx(m, M[2] - bx[2] * m.nx[2] + m.g[2],
-                                                  M[1] - bx[1] * m.nx[1] + m.g[1], M[0] - bx[0] * m.nx[0] + m.g[0]);
-    S val = arr[s];
-    if (fd >= 0 && flip[fd]) val = -val;
-    arr[dst] = val;
-    if constexpr (F32) {
-      if (vlo) vlo[dst] = vlo[s];
-    }
-    return;
-  }
-  // not a leaf at its level: the ghost plan's kernel fills it
-}
-
 // ---------------------------------------------------------------------------
 // Ghost plan.  The ghost cells whose position is not a leaf at their level
 // (fine/coarse boundaries) are listed once per table upload with the cells
@@ -578,10 +521,18 @@ __device__ __forceinline__ bool plan_inner(const MeshDesc &m, const GhostPlan &g
   return plan_node(m, Ls, M, e, in) == 0 && in.kind != 3;
 }
 
-// Outer entry of padded cell t, or false when t is interior or its position
-// holds a leaf (the copy path of k_amr_fill_ghosts).  miss: the sources that
-// need an inner entry; kind 3 when one of them is deeper still.
-__device__ __forceinline__ bool plan_entry(const MeshDesc &m, unsigned t, GhostPlan &g, unsigned &miss) {
+// Same-level ghost copies (the common case): the ghost cell, the leaf cell
+// holding its position, and the axes the boundary map mirrored.
+struct GhostCopy {
+  long long dst, src;
+  int flips;
+};
+
+// Padded cell t: 0 when interior; 1 when its position holds a leaf at its
+// level (cp: the copy); 2 otherwise (g: the outer entry; miss: the sources
+// that need an inner entry; kind 3 when one of them is deeper still).
+__device__ __forceinline__ int plan_entry(const MeshDesc &m, unsigned t, GhostPlan &g, unsigned &miss,
+                                          GhostCopy &cp) {
   const unsigned P = unsigned(m.P);
   const int b = int(t / P);
   unsigned r = t - unsigned(b) * P;
@@ -590,14 +541,23 @@ __device__ __forceinline__ bool plan_entry(const MeshDesc &m, unsigned t, GhostP
   bool interior = true;
   for (int d = 0; d < 3; d++)
     if (loc[d] < m.g[d] || loc[d] >= m.g[d] + m.nx[d]) interior = false;
-  if (interior) return false;
+  if (interior) return 0;
   const int L = m.blev[b];
   int G[3], M[3], ftop;
   for (int d = 0; d < 3; d++) G[d] = m.bloc[3 * b + d] * m.nx[d] + (loc[d] - m.g[d]);
   const int e = plan_map(m, L, G, M, ftop);
-  if (e >= 0) return false;
+  const long long dst = (long long)b * m.P + cidx(m, loc[2], loc[1], loc[0]);
+  if (e >= 0) {
+    int bx[3];
+    for (int d = 0; d < 3; d++) bx[d] = M[d] / m.nx[d];
+    cp.dst = dst;
+    cp.src = (long long)e * m.P + cidx(m, M[2] - bx[2] * m.nx[2] + m.g[2], M[1] - bx[1] * m.nx[1] + m.g[1],
+                                       M[0] - bx[0] * m.nx[0] + m.g[0]);
+    cp.flips = ftop;
+    return 1;
+  }
   miss = plan_node(m, L, M, e, g);
-  g.dst = (long long)b * m.P + cidx(m, loc[2], loc[1], loc[0]);
+  g.dst = dst;
   g.flips |= ftop;
   for (int k = 0; k < 8 && g.kind != 3; k++) {
     GhostPlan in;
@@ -607,20 +567,28 @@ __device__ __forceinline__ bool plan_entry(const MeshDesc &m, unsigned t, GhostP
     miss = 0;
     for (int d = 0; d < 3; d++) g.M[d] = G[d];
   }
-  return true;
+  return 2;
 }
 
 // count[0] counts the outer entries read directly, count[1] the recursive
-// ones and count[2] the inner entries.  The fill pass stores them at
-// [0, n0), [n0, n0 + n1) and [n0 + n1, ...), so a warp of the direct fill
-// never waits on a recursion.
-__global__ void k_amr_plan(const __grid_constant__ MeshDesc m, GhostPlan *plan, int *count, int n0, int n1) {
+// ones, count[2] the inner entries and count[3] the copies.  The fill pass
+// stores the plan entries at [0, n0), [n0, n0 + n1) and [n0 + n1, ...), so a
+// warp of the direct fill never waits on a recursion, and the copies apart.
+__global__ void k_amr_plan(const __grid_constant__ MeshDesc m, GhostPlan *plan, GhostCopy *copies, int *count,
+                           int n0, int n1) {
   const unsigned per = unsigned(m.nb) * unsigned(m.P);
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= per) return;
   GhostPlan g;
-  unsigned miss;
-  if (!plan_entry(m, t, g, miss)) return;
+  GhostCopy cp;
+  unsigned miss = 0;
+  const int what = plan_entry(m, t, g, miss, cp);
+  if (what == 0) return;
+  if (what == 1) {
+    const int q = atomicAdd(count + 3, 1);
+    if (copies) copies[q] = cp;
+    return;
+  }
   if (g.kind == 3) {
     const int q = atomicAdd(count + 1, 1);
     if (plan) plan[n0 + q] = g;
@@ -659,6 +627,24 @@ struct FillVar {
     lo = (sizeof(S) == 4 && is_cc && v == CENER) ? clo : nullptr;
   }
 };
+
+// The same-level ghost copies: a copy of the leaf cell, mirrored components
+// negated across a reflecting boundary; one thread per (copy, variable).
+// Reads interior cells only.
+template <typename S>
+__global__ void k_amr_fill_copy(const __grid_constant__ MeshDesc m, const GhostCopy *copies, int n, S *cc,
+                                float *lo, S *prim, int ncc) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const FillVar<S> fv(m, blockIdx.y, cc, lo, prim, ncc);
+  const GhostCopy cp = copies[q];
+  S val = fv.arr[cp.src];
+  if (fv.fd >= 0 && ((cp.flips >> fv.fd) & 1)) val = -val;
+  fv.arr[cp.dst] = val;
+  if constexpr (sizeof(S) == 4) {
+    if (fv.lo) fv.lo[cp.dst] = fv.lo[cp.src];
+  }
+}
 
 // The plan's recursive entries [q0, q0 + n): level_value at the ghost
 // position, one thread per (entry, variable).
@@ -734,8 +720,7 @@ __device__ __forceinline__ double plan_value(const MeshDesc &m, const GhostPlan 
   return sgn(0) * pv;
 }
 
-// Plan entries [q0, q0 + n), one thread per (entry, variable) as in
-// k_amr_fill_ghosts.  INNER: the inner entries, into the scratch slots
+// Plan entries [q0, q0 + n), one thread per (entry, variable).  INNER: the inner entries, into the scratch slots
 // ([variable][nscr] doubles); otherwise the direct outer entries, into their
 // ghost cells.
 template <typename S, bool INNER>
@@ -1126,35 +1111,45 @@ int amr_upload(kmy_ctx *c) {
   // the ghost plan of the new tables: count, allocate, fill
   dfree(c, a.d_plan);
   dfree(c, a.d_plan_scr);
+  dfree(c, a.d_copy);
   a.d_plan = nullptr;
   a.d_plan_scr = nullptr;
-  a.plan_n = a.plan_deep = a.plan_inner = 0;
-  if (!a.d_plan_n) rc = dalloc(c, reinterpret_cast<void **>(&a.d_plan_n), 3 * sizeof(int));
+  a.d_copy = nullptr;
+  a.plan_n = a.plan_deep = a.plan_inner = a.copy_n = 0;
   const long long cells = (long long)m.nb * m.P;
-  int count[3] = {0, 0, 0};
-  if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, 3 * sizeof(int), c->stream), "plan count");
+  if (cells >= (1LL << 32)) {
+    c->err = "adaptive mesh: more than 2^32 padded cells";
+    return KMY_ERR_BAD_PARAM;
+  }
+  if (!a.d_plan_n) rc = dalloc(c, reinterpret_cast<void **>(&a.d_plan_n), 4 * sizeof(int));
+  int count[4] = {0, 0, 0, 0};
+  if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, 4 * sizeof(int), c->stream), "plan count");
   if (!rc) {
-    k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, nullptr, a.d_plan_n, 0, 0);
+    k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, nullptr, nullptr, a.d_plan_n, 0, 0);
     c->launches++;
-    rc = cuda_check(c, cudaMemcpyAsync(count, a.d_plan_n, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+    rc = cuda_check(c, cudaMemcpyAsync(count, a.d_plan_n, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream),
                     "plan count");
   }
   if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "plan count");
+  if (rc) return rc;
   const long long nplan = (long long)count[0] + count[1] + count[2];
-  if (!rc && nplan > 0) {
-    rc = dalloc(c, &a.d_plan, sizeof(GhostPlan) * size_t(nplan));
-    if (!rc && count[2] > 0)
-      rc = dalloc(c, reinterpret_cast<void **>(&a.d_plan_scr), sizeof(double) * size_t(c->ncc + NPRIM) * count[2]);
-    if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, 3 * sizeof(int), c->stream), "plan fill");
-    if (!rc) {
-      k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, static_cast<GhostPlan *>(a.d_plan), a.d_plan_n,
-                                                          count[0], count[1]);
-      c->launches++;
-      rc = cuda_check(c, cudaGetLastError(), "plan fill");
-    }
+  if (nplan > 0) rc = dalloc(c, &a.d_plan, sizeof(GhostPlan) * size_t(nplan));
+  if (!rc && count[2] > 0)
+    rc = dalloc(c, reinterpret_cast<void **>(&a.d_plan_scr), sizeof(double) * size_t(c->ncc + NPRIM) * count[2]);
+  if (!rc && count[3] > 0) rc = dalloc(c, &a.d_copy, sizeof(GhostCopy) * size_t(count[3]));
+  if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, 4 * sizeof(int), c->stream), "plan fill");
+  if (!rc && (nplan > 0 || count[3] > 0)) {
+    k_amr_plan<<<nblk(cells), kThreads, 0, c->stream>>>(m, static_cast<GhostPlan *>(a.d_plan),
+                                                        static_cast<GhostCopy *>(a.d_copy), a.d_plan_n, count[0],
+                                                        count[1]);
+    c->launches++;
+    rc = cuda_check(c, cudaGetLastError(), "plan fill");
+  }
+  if (!rc) {
     a.plan_n = count[0];
     a.plan_deep = count[1];
     a.plan_inner = count[2];
+    a.copy_n = count[3];
   }
   return rc;
 }
@@ -1178,23 +1173,22 @@ int amr_setup(kmy_ctx *c) {
 
 int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct) {
   const MeshDesc &m = c->m;
-  const long long n = (long long)m.nb * m.P;
-  if (n >= (1LL << 32)) {
-    c->err = "adaptive mesh: more than 2^32 padded cells";
-    return KMY_ERR_BAD_PARAM;
-  }
-  const dim3 grid(nblk(n), unsigned(c->ncc + NPRIM));
-  if (c->esz == 8)
-    k_amr_fill_ghosts<double><<<grid, kThreads, 0, c->stream>>>(m, (double *)ct.cc, nullptr, (double *)c->prim,
-                                                                c->ncc);
-  else
-    k_amr_fill_ghosts<float><<<grid, kThreads, 0, c->stream>>>(m, (float *)ct.cc, (float *)ct.ener_lo,
+  const unsigned nvar = unsigned(c->ncc + NPRIM);
+  const int ncp = c->amr.copy_n;
+  if (ncp > 0) {
+    const dim3 grid(nblk(ncp), nvar);
+    const GhostCopy *cp = static_cast<const GhostCopy *>(c->amr.d_copy);
+    if (c->esz == 8)
+      k_amr_fill_copy<double><<<grid, kThreads, 0, c->stream>>>(m, cp, ncp, (double *)ct.cc, nullptr,
+                                                                (double *)c->prim, c->ncc);
+    else
+      k_amr_fill_copy<float><<<grid, kThreads, 0, c->stream>>>(m, cp, ncp, (float *)ct.cc, (float *)ct.ener_lo,
                                                                (float *)c->prim, c->ncc);
-  c->launches++;
+    c->launches++;
+  }
   const GhostPlan *plan = static_cast<const GhostPlan *>(c->amr.d_plan);
   const int n0 = c->amr.plan_n, n1 = c->amr.plan_deep, n2 = c->amr.plan_inner;
   double *scr = c->amr.d_plan_scr;
-  const unsigned nvar = unsigned(c->ncc + NPRIM);
   // inner entries first: the direct ones read their scratch slots
   if (n2 > 0) {
     const dim3 pgrid(nblk(n2), nvar);

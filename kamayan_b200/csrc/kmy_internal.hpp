@@ -154,9 +154,12 @@ struct AmrHost {
   // recursively, the last plan_inner are inner entries whose values the
   // direct ones read from d_plan_scr, [variable][plan_inner] doubles)
   void *d_plan = nullptr;
-  int *d_plan_n = nullptr;  // three counters: direct, recursive, inner
+  int *d_plan_n = nullptr;  // four counters: direct, recursive, inner, copies
   double *d_plan_scr = nullptr;
   int plan_n = 0, plan_deep = 0, plan_inner = 0;
+  // ghost cells whose same-level position holds a leaf, with that leaf cell
+  void *d_copy = nullptr;
+  int copy_n = 0;
   size_t emf_tmp_bytes = 0;
 };
 
