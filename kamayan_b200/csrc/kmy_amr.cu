@@ -1053,6 +1053,7 @@ uint64_t morton_key(int x0, int y0, int z0, int level, int maxl) {
 
 // Level tables and leaf arrays to the device; MeshDesc points at them.
 int amr_upload(kmy_ctx *c) {
+  c->amr.gen++;
   AmrHost &a = c->amr;
   MeshDesc &m = c->m;
   const int nb = int(a.lev.size());
@@ -1312,13 +1313,15 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
   const int nd = m.ndim;
   const int nb = m.nb;
   *changed_out = false;
-  std::vector<int> tags(nb);
-  int err = 0;
-  int rc = cuda_check(c, cudaMemcpyAsync(tags.data(), a.d_tags, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream),
+  int *pin = static_cast<int *>(host_pin(c, sizeof(int) * (size_t(nb) + 1)));
+  if (!pin) return KMY_ERR_OOM;
+  int rc = cuda_check(c, cudaMemcpyAsync(pin + 1, a.d_tags, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream),
                       "amr tags");
-  if (!rc) rc = cuda_check(c, cudaMemcpyAsync(&err, a.d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "amr err");
+  if (!rc) rc = cuda_check(c, cudaMemcpyAsync(pin, a.d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "amr err");
   if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "amr tags sync");
   if (rc) return rc;
+  const int err = pin[0];
+  const std::vector<int> tags(pin + 1, pin + 1 + nb);
   if (err) {
     c->err = "adaptive mesh: a level-value evaluation exceeded its depth or call budget (mesh not 2:1 balanced)";
     return KMY_ERR_STATE;

@@ -1,5 +1,6 @@
 // kmy_api.cu -- C ABI of libkmy_hydro: contexts, deck parameters, MeshData
 // import/export and the RK driver (stage sequencing + device dt controller).
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -276,6 +277,22 @@ int dalloc(kmy_ctx *c, void **p, size_t bytes) {
   return cuda_check(c, cudaMemsetAsync(*p, 0, bytes, c->stream), "memset");
 }
 
+void *host_pin(kmy_ctx *c, size_t bytes) {
+  if (bytes <= c->h_pin_bytes) return c->h_pin;
+  if (c->h_pin) cudaFreeHost(c->h_pin);
+  c->h_pin = nullptr;
+  c->h_pin_bytes = 0;
+  const size_t n = std::max(bytes, size_t(4096));
+  if (cudaMallocHost(&c->h_pin, n) != cudaSuccess) {
+    cudaGetLastError();
+    c->h_pin = nullptr;
+    c->err = "pinned host allocation of " + std::to_string(n) + " bytes failed";
+    return nullptr;
+  }
+  c->h_pin_bytes = n;
+  return c->h_pin;
+}
+
 void dfree(kmy_ctx *c, void *p) {
   if (!p) return;
   for (size_t i = 0; i < c->allocations.size(); i++)
@@ -456,6 +473,7 @@ int kmy_destroy(kmy_ctx *c) {
   for (void *p : c->allocations) cudaFreeAsync(p, c->stream);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (c->h_pin) cudaFreeHost(c->h_pin);
   delete c;
   return KMY_OK;
 }
@@ -914,14 +932,36 @@ static long long interior_cells(const kmy_ctx *c) {
   return (long long)c->m.nb * c->m.nx[0] * c->m.nx[1] * c->m.nx[2];
 }
 
-static int step_async(kmy_ctx *c) {
+static int stages_async(kmy_ctx *c) {
   const int ns = int(c->prm.beta.size());
-  const long long cells = interior_cells(c);  // before a remesh changes the mesh
   int rc = KMY_OK;
   const bool fused = steps_fused(c);
   for (int s = 1; s <= ns && !rc; s++) rc = fused ? fused_stage(c, s) : task_stage(c, s, -1.0);
-  if (!rc && c->amr.on) rc = amr_after_step(c);
+  return rc;
+}
+
+// After a step's stages: the tree update on an adaptive mesh, then the dt
+// controller, which counts the step's cells (taken before the remesh).
+static int finish_step(kmy_ctx *c, long long cells) {
+  int rc = c->amr.on ? amr_after_step(c) : KMY_OK;
   if (!rc) rc = launch_dt_controller(c, 0, cells);
+  return rc;
+}
+
+static int step_async(kmy_ctx *c) {
+  const long long cells = interior_cells(c);
+  int rc = stages_async(c);
+  if (!rc) rc = finish_step(c, cells);
+  return rc;
+}
+
+// The device clock through the pinned staging (synchronizes the stream).
+static int read_clock(kmy_ctx *c, DevClock &h, const char *what) {
+  DevClock *pin = static_cast<DevClock *>(host_pin(c, sizeof(DevClock)));
+  if (!pin) return KMY_ERR_OOM;
+  int rc = cuda_check(c, cudaMemcpyAsync(pin, c->clock, sizeof(DevClock), cudaMemcpyDeviceToHost, c->stream), what);
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), what);
+  if (!rc) h = *pin;
   return rc;
 }
 
@@ -931,8 +971,7 @@ int kmy_step(kmy_ctx *c, double *dt_taken) {
   int rc = step_async(c);
   if (rc) return rc;
   DevClock h;
-  rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
-  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "step");
+  rc = read_clock(c, h, "step");
   if (rc) return rc;
   if (dt_taken) *dt_taken = h.dt_taken;
   if (h.status) {
@@ -950,12 +989,17 @@ int kmy_step(kmy_ctx *c, double *dt_taken) {
 // stored primitives, and the time parameters of the dt controller.  The first
 // chunk after any change of that state runs uncaptured (first-use
 // allocations, flags settling); the next one is captured and replayed until
-// the state changes again.
+// the state changes again.  An adaptive mesh steps one at a time (the host
+// reads its tags after every step), so there the graph holds the stages of
+// one step, and its key adds the mesh generation (every table upload changes
+// the block list, the ghost plan and the buffers) and the flux buffer.
 static constexpr int kChunk = 8;
 
 static std::string evolve_key(const kmy_ctx *c) {
   std::string k;
   auto add = [&](const void *p, size_t n) { k.append(static_cast<const char *>(p), n); };
+  const char kind = c->amr.on ? 'a' : 'f';
+  add(&kind, 1);
   add(&c->prim, sizeof(c->prim));
   add(&c->prim_alt, sizeof(c->prim_alt));
   for (const auto &kv : c->md) add(&kv.second.cc, sizeof(kv.second.cc));
@@ -963,13 +1007,16 @@ static std::string evolve_key(const kmy_ctx *c) {
   add(flags, sizeof(flags));
   add(&c->prm.tp, sizeof(c->prm.tp));
   add(&c->stream, sizeof(c->stream));
+  if (c->amr.on) {
+    add(&c->amr.gen, sizeof(c->amr.gen));
+    add(&c->flux, sizeof(c->flux));
+  }
   return k;
 }
 
-// Run one chunk of fused steps through the cached graph, capturing it first
-// when the state is steady.  *ran is false when the caller should step
-// uncaptured instead.
-static int evolve_chunk_graph(kmy_ctx *c, bool *ran) {
+// Run `body` through the cached graph, capturing it first when the state is
+// steady.  *ran is false when the caller should run it uncaptured instead.
+static int graph_run(kmy_ctx *c, const std::function<int()> &body, bool *ran) {
   *ran = false;
   const std::string key = evolve_key(c);
   if (c->evolve_exec && key == c->evolve_key) {
@@ -981,7 +1028,7 @@ static int evolve_chunk_graph(kmy_ctx *c, bool *ran) {
     cudaGraphExecDestroy(c->evolve_exec);
     c->evolve_exec = nullptr;
   }
-  if (key != c->evolve_seen) {  // first chunk in this state: run it uncaptured
+  if (key != c->evolve_seen) {  // first run in this state: uncaptured
     c->evolve_seen = key;
     return KMY_OK;
   }
@@ -990,8 +1037,7 @@ static int evolve_chunk_graph(kmy_ctx *c, bool *ran) {
     return KMY_OK;
   }
   const int64_t l0 = c->launches;
-  int rc = KMY_OK;
-  for (int i = 0; i < kChunk && !rc; i++) rc = step_async(c);
+  int rc = body();
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (!rc) rc = cuda_check(c, e, "evolve capture");
@@ -999,7 +1045,7 @@ static int evolve_chunk_graph(kmy_ctx *c, bool *ran) {
   if (!rc) rc = cuda_check(c, cudaGraphInstantiate(&exec, g, 0), "evolve instantiate");
   if (g) cudaGraphDestroy(g);
   if (rc) return rc;
-  // the captured chunk has not run yet; it runs now, and is kept when the
+  // the captured work has not run yet; it runs now, and is kept when the
   // state after it is the state it started from
   rc = cuda_check(c, cudaGraphLaunch(exec, c->stream), "evolve graph");
   if (!rc && evolve_key(c) == key) {
@@ -1030,13 +1076,23 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
     const int chunk = steps_fused(c) && !c->prm.mhd ? kChunk : 1;
     bool ran = false;
     if (chunk == kChunk && (nlim < 0 || nlim - n >= kChunk)) {
-      rc = evolve_chunk_graph(c, &ran);
+      rc = graph_run(c, [&] {
+        int r = KMY_OK;
+        for (int i = 0; i < kChunk && !r; i++) r = step_async(c);
+        return r;
+      }, &ran);
       if (ran) n += kChunk;
+    } else if (c->amr.on && (nlim < 0 || n < nlim)) {
+      const long long cells = interior_cells(c);
+      rc = graph_run(c, [&] { return stages_async(c); }, &ran);
+      if (!rc && !ran) rc = stages_async(c);
+      if (!rc) rc = finish_step(c, cells);
+      n++;
+      ran = true;
     }
     for (int i = 0; !ran && i < chunk && !rc && (nlim < 0 || n < nlim); i++, n++) rc = step_async(c);
     if (rc) break;
-    rc = cuda_check(c, cudaMemcpyAsync(&h, c->clock, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
-    if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "evolve");
+    rc = read_clock(c, h, "evolve");
     if (rc) break;
     if (h.status) {
       c->err = "non-finite or non-positive time-step estimate";
@@ -1052,10 +1108,7 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
 int kmy_end_step(kmy_ctx *c) {
   if (!c) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
-  const long long cells = interior_cells(c);
-  int rc = c->amr.on ? amr_after_step(c) : KMY_OK;
-  if (!rc) rc = launch_dt_controller(c, 0, cells);
-  return rc;
+  return finish_step(c, interior_cells(c));
 }
 
 int kmy_get_blocks(const kmy_ctx *c, int *levels, int *locations, int max_blocks, int *nblocks) {

@@ -160,6 +160,7 @@ struct AmrHost {
   // ghost cells whose same-level position holds a leaf, with that leaf cell
   void *d_copy = nullptr;
   int copy_n = 0;
+  int64_t gen = 0;  // table uploads so far (a captured step is only valid for one)
   size_t emf_tmp_bytes = 0;
 };
 
@@ -190,10 +191,13 @@ struct kmy_ctx {
   kmy::AmrHost amr;          // adaptive mesh (task path only)
   int64_t launches = 0;
   // kmy_evolve's chunk of fused steps as a CUDA graph, and the host-side
-  // state it was captured from (kmy_api.cu:evolve_chunk_graph)
+  // state it was captured from (kmy_api.cu:graph_run)
   cudaGraphExec_t evolve_exec = nullptr;
   std::string evolve_key, evolve_seen;
   int64_t evolve_launches = 0;
+  // pinned host staging for the per-step reads (clock, tags), grown on demand
+  void *h_pin = nullptr;
+  size_t h_pin_bytes = 0;
   std::string err;
   std::string deck_text;  // the deck the context was created from (restart files carry it)
   std::vector<void *> allocations;
@@ -203,6 +207,9 @@ namespace kmy {
 
 // ---- kernels (kmy_tasks.cu) ----
 int launch_fill_ghosts(kmy_ctx *c, Container &ct);
+// Pinned host staging of at least `bytes` (kmy_api.cu); valid until the next
+// call, so every user synchronizes before it returns.
+void *host_pin(kmy_ctx *c, size_t bytes);
 int launch_compute_fluxes(kmy_ctx *c, Container &md0);
 int launch_compute_emf(kmy_ctx *c, Container &md0);
 int launch_flux_divergence(kmy_ctx *c, Container &md0, Container &dudt);

@@ -208,3 +208,27 @@ def test_zone_cycles_count_each_step_on_its_mesh(kmy_lib):
     nb = s.nblocks
     s.evolve(1e30, 1)
     assert s.time["ncycle"] == n0 + 1 and s.zone_cycles == z0 + nb * per_block
+
+
+def test_evolve_graph_matches_steps(kmy_lib):
+    # kmy_evolve replays each adaptive step's stages from a CUDA graph
+    # (captured again after every remesh); kmy_step launches them one by one.
+    # Same meshes, same bits.
+    from kamayan_b200 import Solver
+
+    deck = configs.blast_2d_amr(n=64, nb=8, derefine_count=2)
+    sa, sb = Solver(deck.text()), Solver(deck.text())
+    for s in (sa, sb):
+        s.set_path("tasks")
+        s.pgen("blast")
+    for _ in range(60):
+        sa.step()
+    sb.evolve(1e30, 60)
+    assert sa.time == sb.time and sa.time["ncycle"] == 60
+    la, ca = sa.blocks()
+    lb, cb = sb.blocks()
+    assert np.array_equal(la, lb) and np.array_equal(ca, cb)
+    for var, c in CONS + PRIMS:
+        a, b = sa.export(var, c), sb.export(var, c)
+        assert np.array_equal(a, b), f"{var}{c}: max |diff| {np.abs(a - b).max()}"
+    assert sa.zone_cycles == sb.zone_cycles
