@@ -739,19 +739,26 @@ __global__ void k_amr_fill_plan(const __grid_constant__ MeshDesc m, const GhostP
 
 // Flux correction: a coarse block's boundary face whose neighbour across it
 // is finer takes the area-weighted restriction of the 2^(d-1) fine face
-// fluxes.  One thread per (block, direction, side, face); reads fine blocks'
-// boundary faces and writes coarse blocks' boundary faces only.
-template <typename S>
-__global__ void k_flux_correct(const __grid_constant__ MeshDesc m, S *flux, int ncc, int F) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)m.nb * 6 * F) return;
+// fluxes.  The faces and their fine faces are listed once per table upload
+// (k_flux_plan, one thread per (block, direction, side, face)); the fix
+// reads fine blocks' boundary faces and writes coarse blocks' boundary
+// faces only.
+struct FluxFix {
+  long long dst;     // coarse face, offset in [nb][Pf]
+  long long src[8];  // fine faces, slot off[2]*4 + off[1]*2 + off[0] (transverse offsets)
+  double vv[8];      // their areas; 0 for unused slots
+  int d;             // face direction
+};
+
+__device__ __forceinline__ bool flux_fix_entry(const MeshDesc &m, long long t, int F, FluxFix &fx) {
+  if (t >= (long long)m.nb * 6 * F) return false;
   const int b = int(t / (6ll * F));
   const int rr = int(t - (long long)b * 6 * F);
   const int d = (rr / F) >> 1, s = (rr / F) & 1, a = rr % F;
-  if (d >= m.ndim) return;
+  if (d >= m.ndim) return false;
   const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
   const int a1 = a % m.nx[t1], a2 = a / m.nx[t1];
-  if (a2 >= m.nx[t2]) return;
+  if (a2 >= m.nx[t2]) return false;
   const int L = m.blev[b];
   const int *bl = m.bloc + 3 * b;
   // the cell across the face, at level L
@@ -760,15 +767,16 @@ __global__ void k_flux_correct(const __grid_constant__ MeshDesc m, S *flux, int 
   Gn[t1] = bl[t1] * m.nx[t1] + a1;
   Gn[t2] = bl[t2] * m.nx[t2] + a2;
   const int N = m.mesh_nx[d] << L;
-  if ((Gn[d] < 0 || Gn[d] >= N) && m.bc[d][s] != BC_PERIODIC) return;
+  if ((Gn[d] < 0 || Gn[d] >= N) && m.bc[d][s] != BC_PERIODIC) return false;
   bool fl = false;
   Gn[d] = amr_map(Gn[d], N, m.bc[d][s], fl);
   int bxn[3];
   for (int q = 0; q < 3; q++) bxn[q] = Gn[q] / m.nx[q];
-  if (table_at(m, L, bxn) != -1) return;  // not finer across this face
-  const long long NF = (long long)m.nb * m.Pf;
-  double vv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  long long src[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // flux index of the fine face, per slot
+  if (table_at(m, L, bxn) != -1) return false;  // not finer across this face
+  for (int q = 0; q < 8; q++) {
+    fx.vv[q] = 0.0;
+    fx.src[q] = 0;
+  }
   for (int o2 = 0; o2 < 1 + (t2 < m.ndim); o2++)
     for (int o1 = 0; o1 < 1 + (t1 < m.ndim); o1++) {
       int Gf[3];
@@ -781,27 +789,47 @@ __global__ void k_flux_correct(const __grid_constant__ MeshDesc m, S *flux, int 
       int bf[3], lf[3];
       for (int q = 0; q < 3; q++) bf[q] = Gf[q] / m.nx[q];
       const int e = table_at(m, L + 1, bf);
-      if (e < 0) return;  // not a leaf one level finer: the mesh is not 2:1 balanced
+      if (e < 0) return false;  // not a leaf one level finer: the mesh is not 2:1 balanced
       for (int q = 0; q < 3; q++) lf[q] = Gf[q] - bf[q] * m.nx[q] + m.g[q];
       if (!s) lf[d] += 1;  // the fine cell's high face
       int off[3] = {0, 0, 0};
       off[t1] = o1;
       off[t2] = o2;
       const int slot = off[2] * 4 + off[1] * 2 + off[0];
-      vv[slot] = blk_area(m, e, d);
-      src[slot] = (long long)e * m.Pf + fidx(m, lf[2], lf[1], lf[0]);
+      fx.vv[slot] = blk_area(m, e, d);
+      fx.src[slot] = (long long)e * m.Pf + fidx(m, lf[2], lf[1], lf[0]);
     }
   int lc[3];
   lc[d] = m.g[d] + (s ? m.nx[d] : 0);
   lc[t1] = m.g[t1] + a1;
   lc[t2] = m.g[t2] + a2;
-  const long long dst = (long long)b * m.Pf + fidx(m, lc[2], lc[1], lc[0]);
-  for (int v = 0; v < ncc; v++) {
-    const S *fv = flux + ((long long)d * ncc + v) * NF;
-    double tt[8];
-    for (int q = 0; q < 8; q++) tt[q] = vv[q] > 0.0 ? vv[q] * double(fv[src[q]]) : 0.0;
-    flux[((long long)d * ncc + v) * NF + dst] = S(restrict8(tt, vv));
-  }
+  fx.dst = (long long)b * m.Pf + fidx(m, lc[2], lc[1], lc[0]);
+  fx.d = d;
+  return true;
+}
+
+// Count (fixes null) or list the flux fixes of the current tables.
+__global__ void k_flux_plan(const __grid_constant__ MeshDesc m, int F, FluxFix *fixes, int *count) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  FluxFix fx;
+  if (!flux_fix_entry(m, t, F, fx)) return;
+  const int q = atomicAdd(count, 1);
+  if (fixes) fixes[q] = fx;
+}
+
+// One thread per (fix, conserved variable).
+template <typename S>
+__global__ void k_flux_correct(const __grid_constant__ MeshDesc m, const FluxFix *fixes, int n, S *flux, int ncc) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int v = blockIdx.y;
+  const FluxFix &fx = fixes[q];
+  const long long NF = (long long)m.nb * m.Pf;
+  S *fv = flux + ((long long)fx.d * ncc + v) * NF;
+  double tt[8], vv[8];
+  for (int k = 0; k < 8; k++) vv[k] = fx.vv[k];
+  for (int k = 0; k < 8; k++) tt[k] = vv[k] > 0.0 ? vv[k] * double(fv[fx.src[k]]) : 0.0;
+  fv[fx.dst] = S(restrict8(tt, vv));
 }
 
 // AMRLoehner on one field of a container: one CTA per block, one thread per
@@ -1152,6 +1180,32 @@ int amr_upload(kmy_ctx *c) {
     a.plan_inner = count[2];
     a.copy_n = count[3];
   }
+  // the flux fixes of the new tables: count, allocate, fill
+  dfree(c, a.d_fix);
+  a.d_fix = nullptr;
+  a.fix_n = 0;
+  int F = 1;
+  for (int d = 0; d < m.ndim; d++) F = std::max(F, m.nx[(d + 1) % 3] * m.nx[(d + 2) % 3]);
+  const long long nfix = (long long)m.nb * 6 * F;
+  int nf = 0;
+  if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, sizeof(int), c->stream), "flux plan count");
+  if (!rc) {
+    k_flux_plan<<<nblk(nfix), kThreads, 0, c->stream>>>(m, F, nullptr, a.d_plan_n);
+    c->launches++;
+    rc = cuda_check(c, cudaMemcpyAsync(&nf, a.d_plan_n, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                    "flux plan count");
+  }
+  if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "flux plan count");
+  if (!rc && nf > 0) {
+    rc = dalloc(c, &a.d_fix, sizeof(FluxFix) * size_t(nf));
+    if (!rc) rc = cuda_check(c, cudaMemsetAsync(a.d_plan_n, 0, sizeof(int), c->stream), "flux plan");
+    if (!rc) {
+      k_flux_plan<<<nblk(nfix), kThreads, 0, c->stream>>>(m, F, static_cast<FluxFix *>(a.d_fix), a.d_plan_n);
+      c->launches++;
+      rc = cuda_check(c, cudaGetLastError(), "flux plan");
+    }
+    if (!rc) a.fix_n = nf;
+  }
   return rc;
 }
 
@@ -1267,14 +1321,14 @@ int launch_emf_correct(kmy_ctx *c, Container &md0) {
 
 int launch_flux_correct(kmy_ctx *c) {
   const MeshDesc &m = c->m;
-  if (!c->flux) return KMY_OK;
-  int F = 1;
-  for (int d = 0; d < m.ndim; d++) F = std::max(F, m.nx[(d + 1) % 3] * m.nx[(d + 2) % 3]);
-  const long long n = (long long)m.nb * 6 * F;
+  const int n = c->amr.fix_n;
+  if (!c->flux || n == 0) return KMY_OK;
+  const dim3 grid(nblk(n), unsigned(c->ncc));
+  const FluxFix *fx = static_cast<const FluxFix *>(c->amr.d_fix);
   if (c->esz == 8)
-    k_flux_correct<double><<<nblk(n), kThreads, 0, c->stream>>>(m, (double *)c->flux, c->ncc, F);
+    k_flux_correct<double><<<grid, kThreads, 0, c->stream>>>(m, fx, n, (double *)c->flux, c->ncc);
   else
-    k_flux_correct<float><<<nblk(n), kThreads, 0, c->stream>>>(m, (float *)c->flux, c->ncc, F);
+    k_flux_correct<float><<<grid, kThreads, 0, c->stream>>>(m, fx, n, (float *)c->flux, c->ncc);
   c->launches++;
   return cuda_check(c, cudaGetLastError(), "flux_correct");
 }

@@ -160,6 +160,10 @@ struct AmrHost {
   // ghost cells whose same-level position holds a leaf, with that leaf cell
   void *d_copy = nullptr;
   int copy_n = 0;
+  // coarse boundary faces whose neighbour is finer, with the fine faces their
+  // flux is restricted from
+  void *d_fix = nullptr;
+  int fix_n = 0;
   int64_t gen = 0;  // table uploads so far (a captured step is only valid for one)
   size_t emf_tmp_bytes = 0;
 };
