@@ -816,9 +816,15 @@ static int task_stage(kmy_ctx *c, int stage, double dt) {
   if (!rc && c->amr.on) rc = launch_flux_correct(c);
   if (!rc) rc = launch_compute_emf(c, md0);
   if (!rc && c->amr.on) rc = launch_emf_correct(c, md0);
-  if (!rc) rc = launch_flux_divergence(c, md0, du);
-  if (!rc) rc = launch_apply_dudt(c, base, md0, md1, du, c->prm.beta[stage - 1], dt,
-                                  dt < 0 ? &c->clock->dt : nullptr);
+  // An adaptive hydro mesh has no fused stage; its divergence and update
+  // share one pass.  Elsewhere the task list's kernels stay separate.
+  if (c->amr.on && !c->prm.mhd) {
+    if (!rc) rc = launch_div_apply(c, base, md0, md1, c->prm.beta[stage - 1], dt, dt < 0 ? &c->clock->dt : nullptr);
+  } else {
+    if (!rc) rc = launch_flux_divergence(c, md0, du);
+    if (!rc) rc = launch_apply_dudt(c, base, md0, md1, du, c->prm.beta[stage - 1], dt,
+                                    dt < 0 ? &c->clock->dt : nullptr);
+  }
   if (!rc) rc = launch_prepare_primitive(c, md1);
   if (!rc && stage == ns) {
     rc = launch_estimate_dt(c, base, true);

@@ -217,6 +217,9 @@ void *host_pin(kmy_ctx *c, size_t bytes);
 int launch_compute_fluxes(kmy_ctx *c, Container &md0);
 int launch_compute_emf(kmy_ctx *c, Container &md0);
 int launch_flux_divergence(kmy_ctx *c, Container &md0, Container &dudt);
+// Flux divergence and the cell update in one pass (adaptive hydro meshes).
+int launch_div_apply(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, double dt,
+                     const double *dt_dev);
 int launch_apply_dudt(kmy_ctx *c, Container &base, Container &md0, Container &md1,
                       Container &dudt, double beta, double dt, const double *dt_dev);
 // constrained-transport pieces of a stage that the fused stage leaves to
