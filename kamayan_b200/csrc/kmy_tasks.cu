@@ -551,7 +551,9 @@ __global__ void k_apply_cells(MeshDesc m, const S *ub, const float *ublo, S *u0,
 // FluxDivergence then ApplyDuDt of the cell variables in one pass, for
 // adaptive hydro meshes (which have no fused stage): the expressions and
 // their order are those of k_flux_divergence and k_apply_cells, with dU/dt
-// held in a register instead of the dUdt container.
+// held in a register instead of the dUdt container.  One thread per (cell,
+// variable): an adaptive mesh can hold fewer cells than the GPU has thread
+// slots, and independent variables keep more loads in flight.
 template <typename S>
 __global__ void k_div_apply(MeshDesc m, const S *flux, const S *ub, const float *ublo, S *u0, float *u0lo, S *u1,
                             float *u1lo, int ncc, double beta, double dt, const double *dt_dev,
@@ -569,27 +571,26 @@ __global__ void k_div_apply(MeshDesc m, const S *flux, const S *ub, const float 
   const long long bo = (long long)b * m.Pf;
   const long long n = (long long)b * m.P + cidx(m, k, j, i);
   const double h = dt_dev ? *dt_dev : dt;
-  for (int v = 0; v < ncc; v++) {
-    S d = S(0);
-    for (int dir = 0; dir < m.ndim; dir++) {
-      const int kp = k + (dir == 2), jp = j + (dir == 1), ip = i + (dir == 0);
-      const S A = S(blk_area(m, b, dir));
-      const S *F = flux + ((long long)dir * ncc + v) * NF + bo;
-      d -= (A * F[fidx(m, kp, jp, ip)] - A * F[fidx(m, k, j, i)]);
-    }
-    const S du = d / S(blk_vol(m, b));
-    if (sizeof(S) == 4 && v == CENER) {
-      const double eb = load_ener(ub, ublo, NP, n), e0 = load_ener(u0, u0lo, NP, n);
-      const double e0n = beta * eb + (1.0 - beta) * e0;
-      store_ener(u0, u0lo, NP, n, e0n);
-      store_ener(u1, u1lo, NP, n, e0n + beta * h * double(du));
-      continue;
-    }
-    const S bt = S(beta);
-    const S x0 = bt * ub[v * NP + n] + (S(1.0) - bt) * u0[v * NP + n];
-    u0[v * NP + n] = x0;
-    u1[v * NP + n] = x0 + bt * S(h) * du;
+  const int v = blockIdx.y;
+  S d = S(0);
+  for (int dir = 0; dir < m.ndim; dir++) {
+    const int kp = k + (dir == 2), jp = j + (dir == 1), ip = i + (dir == 0);
+    const S A = S(blk_area(m, b, dir));
+    const S *F = flux + ((long long)dir * ncc + v) * NF + bo;
+    d -= (A * F[fidx(m, kp, jp, ip)] - A * F[fidx(m, k, j, i)]);
   }
+  const S du = d / S(blk_vol(m, b));
+  if (sizeof(S) == 4 && v == CENER) {
+    const double eb = load_ener(ub, ublo, NP, n), e0 = load_ener(u0, u0lo, NP, n);
+    const double e0n = beta * eb + (1.0 - beta) * e0;
+    store_ener(u0, u0lo, NP, n, e0n);
+    store_ener(u1, u1lo, NP, n, e0n + beta * h * double(du));
+    return;
+  }
+  const S bt = S(beta);
+  const S x0 = bt * ub[v * NP + n] + (S(1.0) - bt) * u0[v * NP + n];
+  u0[v * NP + n] = x0;
+  u1[v * NP + n] = x0 + bt * S(h) * du;
 }
 
 int launch_div_apply(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, double dt,
@@ -597,12 +598,13 @@ int launch_div_apply(kmy_ctx *c, Container &base, Container &md0, Container &md1
   const MeshDesc &m = c->m;
   const long long n = (long long)m.nx[0] * m.nx[1] * m.nx[2] * m.nb;
   const DevClock *clk = dt_dev ? c->clock : nullptr;
+  const dim3 grid(nblk(n), unsigned(c->ncc));
   if (c->esz == 8)
-    k_div_apply<double><<<nblk(n), kThreads, 0, c->stream>>>(
+    k_div_apply<double><<<grid, kThreads, 0, c->stream>>>(
         m, (const double *)c->flux, (const double *)base.cc, nullptr, (double *)md0.cc, nullptr,
         (double *)md1.cc, nullptr, c->ncc, beta, dt, dt_dev, clk);
   else
-    k_div_apply<float><<<nblk(n), kThreads, 0, c->stream>>>(
+    k_div_apply<float><<<grid, kThreads, 0, c->stream>>>(
         m, (const float *)c->flux, (const float *)base.cc, (const float *)base.ener_lo, (float *)md0.cc,
         (float *)md0.ener_lo, (float *)md1.cc, (float *)md1.ener_lo, c->ncc, beta, dt, dt_dev, clk);
   c->launches++;
