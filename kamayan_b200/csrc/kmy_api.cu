@@ -116,6 +116,9 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   const std::string prec = p.str("kamayan_b200/precision", "fp64");
   if (!one_of(prec, {"fp64", "fp32"})) return bad("kamayan_b200/precision: " + prec);
   p.precision = prec == "fp32" ? 32 : 64;
+  const std::string sk = p.str("kamayan_b200/stage_kernel", "auto");
+  if (!one_of(sk, {"auto", "brick", "slab"})) return bad("kamayan_b200/stage_kernel: " + sk);
+  p.stage_kernel = sk == "auto" ? 0 : sk == "brick" ? 1 : 2;
 
   const std::string integ = p.str("parthenon/time/integrator", "rk2");
   if (integ == "rk1") p.beta = {1.0};
@@ -533,6 +536,7 @@ int kmy_import_var(kmy_ctx *c, const char *container, const char *var, int comp,
   const std::string vn(var);
   if (vn == "velocity" || vn == "pres" || vn == "bulk modulus" || vn == "eint" || vn == "temp")
     c->prims_imported = true;
+  if (Container *w = find_container(c, container)) w->ghosts = false;
   if (r.is_double || c->esz == 8) {
     rc = cuda_check(c, cudaMemcpyAsync(r.p, host, n * 8, cudaMemcpyHostToDevice, c->stream), "import copy");
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "import sync");
@@ -648,6 +652,7 @@ int kmy_import_interior(kmy_ctx *c, const char *container, const char *var, int 
   const std::string vn(var);
   if (vn == "velocity" || vn == "pres" || vn == "bulk modulus" || vn == "eint" || vn == "temp")
     c->prims_imported = true;
+  if (Container *w = find_container(c, container)) w->ghosts = false;
   double *stage = nullptr;
   rc = cuda_check(c, cudaMallocAsync(reinterpret_cast<void **>(&stage), n * 8, c->stream), "stage");
   if (rc) return rc;
@@ -764,6 +769,7 @@ int kmy_apply_dudt(kmy_ctx *c, const char *base, const char *md0, const char *md
   KMY_CONTAINER(a0, md0);
   KMY_CONTAINER(a1, md1);
   KMY_CONTAINER(d, dudt);
+  a1->ghosts = false;
   return launch_apply_dudt(c, *b, *a0, *a1, *d, beta, dt, nullptr);
 }
 int kmy_prepare_primitive(kmy_ctx *c, const char *md1) {
@@ -812,6 +818,7 @@ static int task_stage(kmy_ctx *c, int stage, double dt) {
     if (rc) return rc;
     c->prims_valid = true;
   }
+  md1.ghosts = false;
   int rc = launch_compute_fluxes(c, md0);
   if (!rc && c->amr.on) rc = launch_flux_correct(c);
   if (!rc) rc = launch_compute_emf(c, md0);
@@ -866,6 +873,7 @@ static int fused_stage_ct(kmy_ctx *c, int stage) {
   Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
   const bool stored = c->prims_valid || c->prims_interior;
   const double beta = c->prm.beta[stage - 1];
+  md1.ghosts = false;
   int rc = launch_fused_stage(c, base, md0, md1, beta, stored, false);
   if (!rc) rc = launch_flux_halo(c);
   if (!rc) rc = launch_ct_faces(c, base, md0, md1, beta);
@@ -880,8 +888,44 @@ static int fused_stage_ct(kmy_ctx *c, int stage) {
   return rc;
 }
 
+// Whether the hydro stage runs the z-streamed kernel (kmy_slab_f32.cu): by
+// default wherever it applies (FP32, 3D, 32-cell rows), or as the deck's
+// <kamayan_b200> stage_kernel asks.
+static bool use_slab(const kmy_ctx *c) {
+  if (c->prm.stage_kernel == 1) return false;
+  return !slab_unsupported(c);
+}
+
+// One stage through the z-streamed kernel.  rk1 updates base in place, and
+// the kernel reads its input's neighbouring blocks while it writes, so rk1
+// writes a scratch container and the two swap roles afterwards.
+static int slab_stage(kmy_ctx *c, int stage) {
+  const auto &nm = c->prm.stage_name;
+  const int ns = int(c->prm.beta.size());
+  int rc;
+  if (ns == 1) {
+    if (!c->md.count("1") && make_container(c, "1")) return KMY_ERR_OOM;
+    Container &base = c->md["base"], &out = c->md["1"];
+    rc = launch_slab_stage(c, base, base, out, c->prm.beta[0], true);
+    if (!rc) std::swap(c->md["base"], c->md["1"]);
+  } else {
+    Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
+    rc = launch_slab_stage(c, base, md0, md1, c->prm.beta[stage - 1], stage == ns);
+  }
+  c->prims_interior = false;
+  c->prims_valid = false;
+  return rc;
+}
+
 static int fused_stage(kmy_ctx *c, int stage) {
   if (c->prm.mhd) return fused_stage_ct(c, stage);
+  if (c->prm.stage_kernel == 2) {
+    if (const char *why = slab_unsupported(c)) {
+      c->err = std::string("stage_kernel = slab: ") + why;
+      return KMY_ERR_BAD_PARAM;
+    }
+  }
+  if (use_slab(c)) return slab_stage(c, stage);
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());
   // FP32 stages keep their output's primitives (kmy_fused.cu)
@@ -896,10 +940,12 @@ static int fused_stage(kmy_ctx *c, int stage) {
     // container and the two swap roles afterwards.
     if (!c->md.count("1") && make_container(c, "1")) return KMY_ERR_OOM;
     Container &base = c->md["base"], &out = c->md["1"];
+    out.ghosts = false;
     rc = launch_fused_stage(c, base, base, out, c->prm.beta[0], stored, true);
     if (!rc) std::swap(c->md["base"], c->md["1"]);
   } else {
     Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
+    md1.ghosts = false;
     rc = launch_fused_stage(c, base, md0, md1, c->prm.beta[stage - 1], stored, stage == ns);
   }
   if (!rc && keep) std::swap(c->prim, c->prim_alt);
@@ -971,6 +1017,17 @@ static int read_clock(kmy_ctx *c, DevClock &h, const char *what) {
   return rc;
 }
 
+// The device clock's status word: a non-finite or non-positive CFL estimate
+// (the dt controller), or a stage kernel's bounded wait that gave up.
+static int clock_status(kmy_ctx *c, int status) {
+  if (status == KMY_ERR_TIMEOUT) {
+    c->err = "a stage kernel's bounded wait for its staged tiles gave up";
+    return KMY_ERR_TIMEOUT;
+  }
+  c->err = "non-finite or non-positive time-step estimate";
+  return KMY_ERR_NONFINITE;
+}
+
 int kmy_step(kmy_ctx *c, double *dt_taken) {
   if (!c) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
@@ -980,10 +1037,7 @@ int kmy_step(kmy_ctx *c, double *dt_taken) {
   rc = read_clock(c, h, "step");
   if (rc) return rc;
   if (dt_taken) *dt_taken = h.dt_taken;
-  if (h.status) {
-    c->err = "non-finite or non-positive time-step estimate";
-    return KMY_ERR_NONFINITE;
-  }
+  if (h.status) return clock_status(c, h.status);
   return KMY_OK;
 }
 
@@ -1101,8 +1155,7 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
     rc = read_clock(c, h, "evolve");
     if (rc) break;
     if (h.status) {
-      c->err = "non-finite or non-positive time-step estimate";
-      rc = KMY_ERR_NONFINITE;
+      rc = clock_status(c, h.status);
       break;
     }
     if (h.done || (nlim >= 0 && n >= nlim)) break;

@@ -117,6 +117,9 @@ struct Params {
   std::vector<double> beta;
   std::vector<std::string> stage_name;
   int precision = 64;
+  // fused hydro stage kernel: 0 auto (the z-streamed stage where it applies),
+  // 1 brick stage, 2 z-streamed stage (error where it does not apply)
+  int stage_kernel = 0;
   TimeParams tp{};
   std::map<std::string, std::string> deck;
   double real(const std::string &k, double d) const;
@@ -129,6 +132,10 @@ struct Container {
   void *ener_lo = nullptr;// [nb][P] float low word of E (FP32 path only)
   void *fc = nullptr;     // [3][nb][Pf] face "mag" (CT only)
   void *emf = nullptr;    // [3][nb][Pf] edge EMFs (CT only)
+  // the face ghosts of the conserved state hold their owners' values (set by
+  // a ghost fill or a z-streamed stage that wrote this container, cleared by
+  // every other writer); the z-streamed stage stages its input through them
+  bool ghosts = false;
 };
 
 // Host side of an adaptive mesh: the leaf list and the refinement parameters.
@@ -246,6 +253,10 @@ int launch_set_energy_split(kmy_ctx *c, Container &ct);
 // ---- fused stage (kmy_fused.cu) ----
 int launch_fused_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1,
                        double beta, bool stored_prims, bool last);
+// ---- z-streamed FP32 3D stage (kmy_slab_f32.cu) ----
+// Why the z-streamed stage cannot run this context, or null.
+const char *slab_unsupported(const kmy_ctx *c);
+int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, bool last);
 // ---- problem generators (kmy_pgen.cu) ----
 int launch_pgen(kmy_ctx *c, const std::string &problem);
 

@@ -200,6 +200,7 @@ int kmy_load_restart(const char *path, int device, kmy_ctx **out) {
                                 "restart clock");
   const size_t n = size_t(c->m.nb) * c->m.P, nf = size_t(c->m.nb) * c->m.Pf;
   Container &b = c->md["base"];
+  b.ghosts = false;
   if (!rc) rc = load_array(c, in.f, b.cc, c->esz * c->ncc * n);
   if (!rc && c->esz == 4) rc = load_array(c, in.f, b.ener_lo, 4 * n);
   if (!rc) rc = load_array(c, in.f, c->prim, c->esz * kmy::NPRIM * n);

@@ -187,7 +187,9 @@ int launch_fill_ghosts(kmy_ctx *c, Container &ct) {
       c->launches++;
     }
   }
-  return cuda_check(c, cudaGetLastError(), "fill_ghosts");
+  const int rc = cuda_check(c, cudaGetLastError(), "fill_ghosts");
+  ct.ghosts = rc == KMY_OK;
+  return rc;
 }
 
 // ---------------------------------------------------------------------------
