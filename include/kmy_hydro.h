@@ -197,6 +197,43 @@ int kmy_conserved_sums(kmy_ctx *ctx, const char *md, double *out);
 
 /* Number of this library's kernels launched on the context since creation. */
 int kmy_launch_count(const kmy_ctx *ctx, int64_t *out);
+/* Number of kmy_evolve chunks (or adaptive steps) that replayed a cached CUDA
+ * graph instead of launching their kernels one by one. */
+int kmy_graph_replays(const kmy_ctx *ctx, int64_t *out);
+
+/* ---- stage-kernel autotuner -------------------------------------------------
+ * The reference chooses its flux loop strategy by a runtime parameter
+ * (<hydro> ReconstructionStrategy, src/physics/hydro/hydro.cpp:75-79).  Here
+ * the stage kernel is chosen by measurement: "brick" (brick-tiled fused
+ * stage), "slab16" / "slab8" (z-streamed FP32 3D stage with TMA-staged plane
+ * pairs, tiles of 16 or 8 rows).  kmy_autotune times every candidate that
+ * applies to the context on its current state (stage 1 into a scratch
+ * container, so the solve does not advance), applies the fastest and caches
+ * it under (device name, configuration key).  The deck option
+ * <kamayan_b200> stage_kernel = tune does the same at the first stage (from
+ * the cache when it holds the key).  results[i]: candidate name, mean stage
+ * time in ms, and whether it applies (ms < 0 when it does not). */
+typedef struct {
+  char name[16];
+  double ms;
+  int applies;
+} kmy_tune_result;
+int kmy_autotune(kmy_ctx *ctx, int reps, kmy_tune_result *results, int max_results, int *n_results);
+/* The stage kernel the context's next fused stage runs: "brick", "slab16",
+ * "slab8", "tune" (not yet chosen) or "tasks". */
+int kmy_stage_kernel(const kmy_ctx *ctx, char *name, size_t n);
+/* Configuration part of the tuner's cache key for a deck (host only: parses
+ * the deck, needs no GPU).  The cache key is "<device name> | <this>". */
+int kmy_tune_key(const char *deck, char *buf, size_t n);
+/* The process-wide tuning cache: put/get one entry (choice must be a
+ * candidate name), clear, and save to / load from a text file with one
+ * "key<TAB>choice<TAB>ms" line per entry (malformed lines are skipped).
+ * kmy_tune_cache_get returns KMY_ERR_STATE when the key is absent. */
+int kmy_tune_cache_put(const char *key, const char *choice, double ms);
+int kmy_tune_cache_get(const char *key, char *choice, size_t n, double *ms);
+int kmy_tune_cache_clear(void);
+int kmy_tune_cache_save(const char *path);
+int kmy_tune_cache_load(const char *path);
 
 /* ---- serving loop: continuously batched independent solves ----------------
  * No counterpart in the reference (which runs one mesh per process).  A
@@ -238,8 +275,10 @@ int kmy_server_stats(const kmy_server *srv, double *out);
  *           cells of cons[v] * cell_volume
  *   stream: cudaStream_t to launch on (NULL = default stream)
  * ncons above 8 (the scratch array's capacity) returns KMY_ERR_BAD_PARAM.
- * The first call on a device looks up the scratch array's device address with
- * that device current; make that first call before any stream capture.  Calls
+ * The first call in a CUDA context looks up the scratch array's device
+ * address in that context (the address is valid for that context only; a
+ * device reset starts a new context, whose first call looks it up again);
+ * make that first call before any stream capture.  Calls
  * share the scratch array: calls that overlap on the GPU race and must be
  * serialised by the caller. */
 int kmy_conserved_sums_noalloc(const double *cons, int ncons, int nblocks,

@@ -38,6 +38,8 @@ EXPORTS = (
     "kmy_zone_cycles",
     "kmy_get_blocks", "kmy_set_dt", "kmy_save_restart", "kmy_load_restart",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
+    "kmy_graph_replays", "kmy_autotune", "kmy_stage_kernel", "kmy_tune_key", "kmy_tune_cache_put",
+    "kmy_tune_cache_get", "kmy_tune_cache_clear", "kmy_tune_cache_save", "kmy_tune_cache_load",
     "kmy_conserved_sums_noalloc",
     "kmy_server_create", "kmy_server_destroy", "kmy_server_last_error", "kmy_server_submit",
     "kmy_server_tick", "kmy_server_poll", "kmy_server_export", "kmy_server_release",
@@ -49,6 +51,10 @@ class KmyError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS.get(code, code)}: {msg}")
         self.code = code
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 16), ("ms", ctypes.c_double), ("applies", ctypes.c_int)]
 
 
 class Info(ctypes.Structure):
@@ -108,6 +114,15 @@ def lib() -> ctypes.CDLL:
         L.kmy_conserved_sums.argtypes = [vp, cp, _dp]
         L.kmy_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.kmy_zone_cycles.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.kmy_graph_replays.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.kmy_autotune.argtypes = [vp, i, ctypes.POINTER(TuneResult), i, ctypes.POINTER(i)]
+        L.kmy_stage_kernel.argtypes = [vp, cp, sz]
+        L.kmy_tune_key.argtypes = [cp, cp, sz]
+        L.kmy_tune_cache_put.argtypes = [cp, cp, d]
+        L.kmy_tune_cache_get.argtypes = [cp, cp, sz, _dp]
+        L.kmy_tune_cache_clear.argtypes = []
+        L.kmy_tune_cache_save.argtypes = [cp]
+        L.kmy_tune_cache_load.argtypes = [cp]
         ip3 = ctypes.POINTER(ctypes.c_int)
         L.kmy_conserved_sums_noalloc.argtypes = [vp, i, i, ip3, ip3, ip3, d, vp, vp]
         i64p = ctypes.POINTER(ctypes.c_int64)
@@ -361,6 +376,27 @@ class Solver:
         self._check(lib().kmy_launch_count(self._h, ctypes.byref(n)))
         return n.value
 
+    @property
+    def graph_replays(self) -> int:
+        """kmy_evolve chunks (adaptive steps) that replayed a cached CUDA graph."""
+        n = ctypes.c_int64()
+        self._check(lib().kmy_graph_replays(self._h, ctypes.byref(n)))
+        return n.value
+
+    def autotune(self, reps: int = 5) -> dict:
+        """Time every stage kernel that applies on the current state, apply
+        and cache the fastest; {name: ms per stage (None where it does not apply)}."""
+        res = (TuneResult * 8)()
+        n = ctypes.c_int()
+        self._check(lib().kmy_autotune(self._h, reps, res, 8, ctypes.byref(n)))
+        return {res[k].name.decode(): (res[k].ms if res[k].applies else None) for k in range(n.value)}
+
+    @property
+    def stage_kernel(self) -> str:
+        buf = ctypes.create_string_buffer(64)
+        self._check(lib().kmy_stage_kernel(self._h, buf, 64))
+        return buf.value.decode()
+
     def interior(self, arr: np.ndarray) -> np.ndarray:
         i = self.info
         g = i.nghost
@@ -434,3 +470,48 @@ class Server:
         out = np.zeros(8)
         self._check(lib().kmy_server_stats(self._h, _ptr(out)))
         return dict(zip(self.STATS, out.tolist()))
+
+
+# ---- the stage-kernel tuner's cache (host only; no GPU needed) --------------
+def tune_key(deck) -> str:
+    """Configuration part of the tuner's cache key for a deck."""
+    buf = ctypes.create_string_buffer(256)
+    text = deck.text() if isinstance(deck, Deck) else deck
+    rc = lib().kmy_tune_key(text.encode(), buf, 256)
+    if rc:
+        raise KmyError(rc, "kmy_tune_key")
+    return buf.value.decode()
+
+
+def tune_cache_put(key: str, choice: str, ms: float = 0.0) -> None:
+    rc = lib().kmy_tune_cache_put(key.encode(), choice.encode(), ms)
+    if rc:
+        raise KmyError(rc, f"kmy_tune_cache_put {choice!r}")
+
+
+def tune_cache_get(key: str):
+    """(choice, ms) for a key, or None."""
+    buf = ctypes.create_string_buffer(32)
+    ms = ctypes.c_double()
+    rc = lib().kmy_tune_cache_get(key.encode(), buf, 32, ctypes.byref(ms))
+    if rc == 6:
+        return None
+    if rc:
+        raise KmyError(rc, "kmy_tune_cache_get")
+    return buf.value.decode(), ms.value
+
+
+def tune_cache_clear() -> None:
+    lib().kmy_tune_cache_clear()
+
+
+def tune_cache_save(path: str) -> None:
+    rc = lib().kmy_tune_cache_save(str(path).encode())
+    if rc:
+        raise KmyError(rc, f"kmy_tune_cache_save {path}")
+
+
+def tune_cache_load(path: str) -> None:
+    rc = lib().kmy_tune_cache_load(str(path).encode())
+    if rc:
+        raise KmyError(rc, f"kmy_tune_cache_load {path}")

@@ -117,8 +117,11 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   if (!one_of(prec, {"fp64", "fp32"})) return bad("kamayan_b200/precision: " + prec);
   p.precision = prec == "fp32" ? 32 : 64;
   const std::string sk = p.str("kamayan_b200/stage_kernel", "auto");
-  if (!one_of(sk, {"auto", "brick", "slab"})) return bad("kamayan_b200/stage_kernel: " + sk);
-  p.stage_kernel = sk == "auto" ? 0 : sk == "brick" ? 1 : 2;
+  if (!one_of(sk, {"auto", "brick", "slab", "tune"})) return bad("kamayan_b200/stage_kernel: " + sk);
+  p.stage_kernel = sk == "auto" ? 0 : sk == "brick" ? 1 : sk == "slab" ? 2 : 3;
+  const std::string sr = p.str("kamayan_b200/slab_rows", "auto");
+  if (!one_of(sr, {"auto", "8", "16"})) return bad("kamayan_b200/slab_rows: " + sr);
+  p.slab_rows = sr == "auto" ? 0 : std::stoi(sr);
 
   const std::string integ = p.str("parthenon/time/integrator", "rk2");
   if (integ == "rk1") p.beta = {1.0};
@@ -222,6 +225,8 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   c->esz = p.precision == 32 ? 4 : 8;
   return KMY_OK;
 }
+
+int parse_deck(kmy_ctx *tmp, const char *deck) { return setup_params(tmp, deck); }
 
 // Device bytes a fused-path context for `deck` allocates at kmy_create, and
 // the deck's kernel class.  Host-only: parses and validates the deck.
@@ -919,6 +924,19 @@ static int slab_stage(kmy_ctx *c, int stage) {
 
 static int fused_stage(kmy_ctx *c, int stage) {
   if (c->prm.mhd) return fused_stage_ct(c, stage);
+  if (c->prm.stage_kernel == 3) {
+    // stage_kernel = tune: the cached choice for this device and
+    // configuration, else a tuning run now (never inside a stream capture:
+    // kmy_evolve runs its first chunk uncaptured, and a capture keeps the
+    // default choice until then)
+    if (!tune_lookup(c)) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      cudaStreamIsCapturing(c->stream, &cs);
+      if (cs == cudaStreamCaptureStatusNone) {
+        if (const int rc = tune_run(c, 5, nullptr)) return rc;
+      }
+    }
+  }
   if (c->prm.stage_kernel == 2) {
     if (const char *why = slab_unsupported(c)) {
       c->err = std::string("stage_kernel = slab: ") + why;
@@ -1065,7 +1083,15 @@ static std::string evolve_key(const kmy_ctx *c) {
   for (const auto &kv : c->md) add(&kv.second.cc, sizeof(kv.second.cc));
   const bool flags[2] = {c->prims_valid, c->prims_interior};
   add(flags, sizeof(flags));
-  add(&c->prm.tp, sizeof(c->prm.tp));
+  // the time parameters field by field (the struct's tail padding is not state)
+  const TimeParams &tp = c->prm.tp;
+  for (const double *d : {&tp.tlim, &tp.dt_factor, &tp.dt_init, &tp.dt_ceil, &tp.dt_user, &tp.dt_floor,
+                          &tp.cfl_over_ndim})
+    add(d, sizeof(double));
+  add(&tp.nlim, sizeof(tp.nlim));
+  // the stage kernel (the tuner may change it after the first chunk)
+  add(&c->prm.stage_kernel, sizeof(int));
+  add(&c->prm.slab_rows, sizeof(int));
   add(&c->stream, sizeof(c->stream));
   if (c->amr.on) {
     add(&c->amr.gen, sizeof(c->amr.gen));
@@ -1081,6 +1107,7 @@ static int graph_run(kmy_ctx *c, const std::function<int()> &body, bool *ran) {
   const std::string key = evolve_key(c);
   if (c->evolve_exec && key == c->evolve_key) {
     c->launches += c->evolve_launches;
+    c->graph_replays++;
     *ran = true;
     return cuda_check(c, cudaGraphLaunch(c->evolve_exec, c->stream), "evolve graph");
   }
@@ -1233,6 +1260,12 @@ int kmy_conserved_sums(kmy_ctx *c, const char *md, double *out) {
   cudaSetDevice(c->device);
   KMY_CONTAINER(a, md);
   return launch_conserved_sums(c, *a, out);
+}
+
+int kmy_graph_replays(const kmy_ctx *c, int64_t *out) {
+  if (!c || !out) return KMY_ERR_BAD_PARAM;
+  *out = c->graph_replays;
+  return KMY_OK;
 }
 
 int kmy_launch_count(const kmy_ctx *c, int64_t *out) {

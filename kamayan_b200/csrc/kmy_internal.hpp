@@ -118,8 +118,11 @@ struct Params {
   std::vector<std::string> stage_name;
   int precision = 64;
   // fused hydro stage kernel: 0 auto (the z-streamed stage where it applies),
-  // 1 brick stage, 2 z-streamed stage (error where it does not apply)
+  // 1 brick stage, 2 z-streamed stage (error where it does not apply),
+  // 3 tune (the autotuner's cached or measured choice, kmy_tune.cu)
   int stage_kernel = 0;
+  // rows per tile of the z-streamed stage: 0 auto, 8 or 16
+  int slab_rows = 0;
   TimeParams tp{};
   std::map<std::string, std::string> deck;
   double real(const std::string &k, double d) const;
@@ -206,6 +209,7 @@ struct kmy_ctx {
   cudaGraphExec_t evolve_exec = nullptr;
   std::string evolve_key, evolve_seen;
   int64_t evolve_launches = 0;
+  int64_t graph_replays = 0;  // launches of a cached graph (kmy_graph_replays)
   // pinned host staging for the per-step reads (clock, tags), grown on demand
   void *h_pin = nullptr;
   size_t h_pin_bytes = 0;
@@ -256,7 +260,16 @@ int launch_fused_stage(kmy_ctx *c, Container &base, Container &md0, Container &m
 // ---- z-streamed FP32 3D stage (kmy_slab_f32.cu) ----
 // Why the z-streamed stage cannot run this context, or null.
 const char *slab_unsupported(const kmy_ctx *c);
+// Rows per tile the z-streamed stage uses for this context (8 or 16).
+int slab_rows(const kmy_ctx *c);
 int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, bool last);
+// ---- stage-kernel autotuner (kmy_tune.cu) ----
+std::string tune_config_key(const kmy_ctx *c);
+int tune_apply(kmy_ctx *c, const std::string &choice);
+int tune_run(kmy_ctx *c, int reps, std::vector<std::pair<std::string, double>> *results);
+bool tune_lookup(kmy_ctx *c);
+// Parse and validate a deck into a context that owns no device resources.
+int parse_deck(kmy_ctx *tmp, const char *deck);
 // ---- problem generators (kmy_pgen.cu) ----
 int launch_pgen(kmy_ctx *c, const std::string &problem);
 

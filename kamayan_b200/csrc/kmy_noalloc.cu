@@ -12,15 +12,19 @@
 //
 // The array is a fixed, modest size (kNoallocMaxVars x kNoallocCtas pairs of
 // doubles, 75.8 KiB) and every GPU that loads this library holds it until the
-// process exits.  All calls on a device share it and it keeps the previous
+// process exits.  Its device address is looked up once per CUDA context, on
+// the first call made with that context current (a device reset starts a new
+// context, which looks it up again).  All calls on a device share it and it keeps the previous
 // call's contents: each call overwrites every partial slot it reads, so
 // nothing needs clearing, but calls whose kernels overlap on the GPU (two
 // streams, or two host threads) race on it and must be serialised by the
 // caller.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
+#include <map>
 #include <mutex>
 
 #include "../../include/kmy_hydro.h"
@@ -31,31 +35,62 @@ namespace {
 constexpr int kNoallocMaxVars = 8;   // cell conserved components: 5 hydro, 8 with CT
 constexpr int kNoallocCtas = 592;    // 4 CTAs per SM on 148 SMs
 constexpr int kNoallocThreads = 256;
-constexpr int kMaxDevices = 64;
 
 // (sum, compensation) per (variable, CTA).  Host code must not pass this name
 // to a kernel: on the host it is only a stand-in for the device symbol.
 __device__ __align__(256) double g_sum_scratch[2 * kNoallocMaxVars * kNoallocCtas];
 
 std::mutex g_setup_mutex;
-double *g_scratch_dev[kMaxDevices] = {};
+// Device address of g_sum_scratch per CUDA context (by context id): a device
+// reset destroys the primary context and the module is loaded again, possibly
+// at another address, in the new context, which then gets its own lookup.
+std::map<unsigned long long, double *> g_scratch_dev;
 
-// Device address of g_sum_scratch on the current device, looked up once per
-// device with that device current.
-int scratch_address(int device, double **out) {
-  if (device < 0 || device >= kMaxDevices) return KMY_ERR_BAD_PARAM;
+using CtxGetCurrent = CUresult (*)(CUcontext *);
+using CtxGetId = CUresult (*)(CUcontext, unsigned long long *);
+
+template <typename F>
+F driver_fn(const char *name) {
+  void *p = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return reinterpret_cast<F>(p);
+}
+
+// Id of the context current on this thread (0 if none is current yet).
+unsigned long long current_context_id() {
+  static CtxGetCurrent get_current = driver_fn<CtxGetCurrent>("cuCtxGetCurrent");
+  static CtxGetId get_id = driver_fn<CtxGetId>("cuCtxGetId");
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of g_sum_scratch in the current context, looked up with
+// cudaGetSymbolAddress the first time a context calls (which also makes the
+// runtime's context current if it was not yet).
+int scratch_address(double **out) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_dev[device]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_sum_scratch);
-    if (e != cudaSuccess || !p) {
-      std::fprintf(stderr, "kmy_conserved_sums_noalloc: cudaGetSymbolAddress failed: %s\n",
-                   cudaGetErrorString(e));
-      return KMY_ERR_CUDA;
+  unsigned long long id = current_context_id();
+  if (id) {
+    auto it = g_scratch_dev.find(id);
+    if (it != g_scratch_dev.end()) {
+      *out = it->second;
+      return KMY_OK;
     }
-    g_scratch_dev[device] = static_cast<double *>(p);
   }
-  *out = g_scratch_dev[device];
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_sum_scratch);
+  if (e != cudaSuccess || !p) {
+    std::fprintf(stderr, "kmy_conserved_sums_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+    return KMY_ERR_CUDA;
+  }
+  if (!id) id = current_context_id();
+  if (id) g_scratch_dev[id] = static_cast<double *>(p);
+  *out = static_cast<double *>(p);
   return KMY_OK;
 }
 
@@ -147,10 +182,8 @@ extern "C" int kmy_conserved_sums_noalloc(const double *cons, int ncons, int nbl
     L.g[d] = nghost[d];
     L.P *= ncells_pad[d];
   }
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess) return KMY_ERR_CUDA;
   double *scratch = nullptr;
-  int rc = scratch_address(device, &scratch);
+  int rc = scratch_address(&scratch);
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   k_noalloc_partials<<<kNoallocCtas, kNoallocThreads, 0, s>>>(L, cons, cell_volume, scratch);

@@ -1,9 +1,11 @@
 // kmy_slab.cuh -- one RK stage of 3D hydro in FP32, streamed through each
 // meshblock along z with TMA-staged plane pairs.
 //
-// Work item: one meshblock b and one tile of TY = 16 rows (y) by the block's
-// full 32-cell width (x).  A persistent grid (one CTA of 512 threads per SM)
-// strides over the (block, tile) work list.  Thread t owns the column
+// Work item: one meshblock b and one tile of TY rows (y) by the block's full
+// 32-cell width (x).  A persistent grid strides over the (block, tile) work
+// list: TY = 16 runs one CTA of 512 threads per SM, TY = 8 two CTAs of 256
+// (they fill each other's barrier waits; the staged halo rows cost more).
+// Thread t owns the column
 // (x = t % 32, y = oy + t / 32) and walks it along z two planes at a time, so
 // every FP32 operation of the z sweep works on a float2 of planes (k, k+1)
 // (sm_100's FADD2/FMUL2/FFMA2 issue one instruction for both lanes).
@@ -14,8 +16,10 @@
 // the x and y halos are the block's own ghost zones.  The previous stage's
 // epilogue keeps those current (it writes every cell it updates into the
 // face ghosts that hold it, periodic, outflow or reflect as Parthenon's
-// boundary exchange would).  Loads run one pair ahead on an mbarrier per
-// slot; the staging costs no per-cell address arithmetic.
+// boundary exchange would).  The loads of the next pair are issued as soon as
+// the raw slot is converted and land while the CTA works on the current pair
+// (one mbarrier, bounded waits); the staging costs no per-cell address
+// arithmetic.
 //
 // Per pair the CTA then
 //   1. converts the pair to primitives (rho, v, P, e_int; e_int = E - e_kin in
@@ -53,21 +57,26 @@ namespace kmy {
 namespace slab {
 
 constexpr int NX = 32;            // interior cells along x (one warp per row)
-constexpr int TY = 16;            // rows per tile
-constexpr int NT = NX * TY;       // threads per CTA, one column each
 constexpr int HH = 3;             // staged halo cells on each side
 constexpr int PC = NX + 2 * HH;   // 38 staged columns
-constexpr int PR = TY + 2 * HH;   // 22 staged rows
 constexpr int NV = 6;             // reconstructed: rho, v0, v1, v2, P, e_int
 constexpr int NCV = 5;            // conserved components
 enum : int { SD = 0, SV0 = 1, SPRES = 4, SEINT = 5 };
 
+// Tile of TY rows (16: one CTA of 512 threads per SM; 8: two CTAs of 256).
 // x sweep: reconstruction cells -1 .. 32 (34) per row, 33 faces per row;
-// y sweep: cells -1 .. 16 (18) per column, 17 faces per column.
-constexpr int RXC = NX + 2, RYC = TY + 2;
-constexpr int REC_N = (RXC * TY > RYC * NX ? RXC * TY : RYC * NX);  // 576 float2 per variable and side
-constexpr int FX_N = (NX + 1) * TY, FY_N = NX * (TY + 1);
-constexpr int FLX_N = FX_N > FY_N ? FX_N : FY_N;                    // 544 float2 per component
+// y sweep: cells -1 .. TY (TY + 2) per column, TY + 1 faces per column.
+template <int TY_>
+struct Tile {
+  static constexpr int TY = TY_;
+  static constexpr int NT = NX * TY;      // threads, one column each
+  static constexpr int PR = TY + 2 * HH;  // staged rows
+  static constexpr int CTAS = TY == 8 ? 2 : 1;  // CTAs per SM the plan is sized for
+  static constexpr int RXC = NX + 2, RYC = TY + 2;
+  static constexpr int REC_N = RXC * TY > RYC * NX ? RXC * TY : RYC * NX;  // float2 per variable and side
+  static constexpr int FX_N = (NX + 1) * TY, FY_N = NX * (TY + 1);
+  static constexpr int FLX_N = FX_N > FY_N ? FX_N : FY_N;                  // float2 per component
+};
 
 struct Args {
   MeshDesc m;
@@ -87,23 +96,28 @@ struct Args {
   int nitems;        // blocks x tiles
 };
 
-// Shared-memory plan (bytes), the same on host and device.
+// Shared-memory plan (bytes), the same on host and device: one raw slot (the
+// stage input of one plane pair as the tensor loads deliver it), the
+// interleaved primitives of the centre pair, the reconstructed face values
+// and the face fluxes of one sweep, the mbarrier and reduction scratch.
+template <int TY>
 struct Smem {
+  using T = Tile<TY>;
   int np0;
   __host__ __device__ explicit Smem(int np0_) : np0(np0_) {}
   __host__ __device__ static constexpr int rup(int x) { return (x + 127) & ~127; }
-  __host__ __device__ int raw_plane() const { return PR * np0; }              // floats
+  __host__ __device__ int raw_plane() const { return T::PR * np0; }           // floats
   __host__ __device__ int raw_var() const { return 2 * raw_plane(); }         // floats
   __host__ __device__ int cc_bytes() const { return NCV * raw_var() * 4; }
   __host__ __device__ int lo_off() const { return rup(cc_bytes()); }
   __host__ __device__ int lo_bytes() const { return raw_var() * 4; }
   __host__ __device__ int slot_bytes() const { return rup(lo_off() + lo_bytes()); }
-  __host__ __device__ int prim_off() const { return 2 * slot_bytes(); }
-  __host__ __device__ static constexpr int prim_bytes() { return NV * PR * PC * 8; }
+  __host__ __device__ int prim_off() const { return slot_bytes(); }
+  __host__ __device__ static constexpr int prim_bytes() { return NV * T::PR * PC * 8; }
   __host__ __device__ int rec_off() const { return prim_off() + prim_bytes(); }
-  __host__ __device__ static constexpr int rec_bytes() { return 2 * NV * REC_N * 8; }
+  __host__ __device__ static constexpr int rec_bytes() { return 2 * NV * T::REC_N * 8; }
   __host__ __device__ int flx_off() const { return rec_off() + rec_bytes(); }
-  __host__ __device__ static constexpr int flx_bytes() { return NCV * FLX_N * 8; }
+  __host__ __device__ static constexpr int flx_bytes() { return NCV * T::FLX_N * 8; }
   __host__ __device__ int bar_off() const { return flx_off() + flx_bytes(); }
   __host__ __device__ int total() const { return bar_off() + 256; }
   // bytes one plane pair brings in (both tensor loads)
@@ -175,13 +189,10 @@ __device__ __forceinline__ float exp_scale(float x) {
 //    e0 - e1 and e2 - e1 written through the second differences u_k of the
 //    smoothness indicators (one subtraction each instead of a 3-term stencil);
 //  * the indicators are scaled by 12/13 (u^2 + (3/13) v^2), which leaves the
-//    ratios tau / beta_k unchanged, and then by the power of two that puts the
-//    largest into [1, 2);
-//  * the reference's eps = 1e-36 becomes a floor of 1e-12 on the scaled
-//    indicators: below it a stencil's weight already dominates by more than
-//    1e24 and the FP32 sum no longer changes.  With the floor the product of
-//    the three lies in [1e-36, 8], so one reciprocal gives all three ratios;
-//    the two normalisations take one reciprocal each.
+//    ratios tau / (eps + beta_k) unchanged up to eps;
+//  * each ratio takes one reciprocal and is capped at 1e15 so its square
+//    stays finite in FP32: at that ratio the stencil already holds the whole
+//    weight.
 __device__ __forceinline__ void WenoZPair(const float2 (&s)[5], float2 &vM, float2 &vP) {
   const float2 a = s[0], b = s[1], c = s[2], d = s[3], e = s[4];
   const float2 m2 = p2(-2.f), m4 = p2(-4.f);
@@ -192,24 +203,18 @@ __device__ __forceinline__ void WenoZPair(const float2 (&s)[5], float2 &vM, floa
   const float2 v0 = pfma(m4, b, padd(a, c3));
   const float2 v1 = psub2(b, d);
   const float2 v2 = pfma(m4, d, padd(e, c3));
-  const float2 k = p2(3.f / 13.f);
-  float2 b0 = pfma(u0, u0, pmul(pmul(k, v0), v0));
-  float2 b1 = pfma(u1, u1, pmul(pmul(k, v1), v1));
-  float2 b2 = pfma(u2, u2, pmul(pmul(k, v2), v2));
-  const float2 sc = make_float2(exp_scale(fmaxf(b0.x, fmaxf(b1.x, b2.x))), exp_scale(fmaxf(b0.y, fmaxf(b1.y, b2.y))));
-  b0 = pmul(b0, sc);
-  b1 = pmul(b1, sc);
-  b2 = pmul(b2, sc);
-  const float2 ts = psub2(b2, b0);
-  const float fl = 1.e-12f;
-  const float2 D0 = make_float2(fmaxf(b0.x, fl), fmaxf(b0.y, fl));
-  const float2 D1 = make_float2(fmaxf(b1.x, fl), fmaxf(b1.y, fl));
-  const float2 D2 = make_float2(fmaxf(b2.x, fl), fmaxf(b2.y, fl));
-  const float2 D01 = pmul(D0, D1);
-  const float2 tR = pmul(ts, prcp(pmul(D01, D2)));
-  const float2 r0 = pmul(tR, pmul(D1, D2)), r1 = pmul(tR, pmul(D0, D2)), r2 = pmul(tR, D01);
+  const float2 k = p2(3.f / 13.f), eps = p2(1.e-36f);
+  const float2 D0 = pfma(u0, u0, pfma(pmul(k, v0), v0, eps));
+  const float2 D1 = pfma(u1, u1, pfma(pmul(k, v1), v1, eps));
+  const float2 D2 = pfma(u2, u2, pfma(pmul(k, v2), v2, eps));
+  const float2 tau = psub2(D2, D0);
+  const float cap = 1.e15f;
+  const float2 r0 = pmul(tau, prcp(D0)), r1 = pmul(tau, prcp(D1)), r2 = pmul(tau, prcp(D2));
+  const float2 r0c = make_float2(fminf(fabsf(r0.x), cap), fminf(fabsf(r0.y), cap));
+  const float2 r1c = make_float2(fminf(fabsf(r1.x), cap), fminf(fabsf(r1.y), cap));
+  const float2 r2c = make_float2(fminf(fabsf(r2.x), cap), fminf(fabsf(r2.y), cap));
   const float2 one = p2(1.f);
-  const float2 q0 = pfma(r0, r0, one), q1 = pfma(r1, r1, one), q2 = pfma(r2, r2, one);
+  const float2 q0 = pfma(r0c, r0c, one), q1 = pfma(r1c, r1c, one), q2 = pfma(r2c, r2c, one);
   const float2 g0 = psub2(u0, u1), g2 = psub2(u2, u1);
   const float2 inner = pfma(p2(1.f / 12.f), u1, c);
   const float2 ep1 = pfma(p2(-0.25f), v1, inner), em1 = pfma(p2(0.25f), v1, inner);
@@ -256,8 +261,10 @@ __device__ __forceinline__ void SlabRiemann2(const float2 *vL, const float2 *vR,
   const float2 uL = vL[SV0 + DIR1], uR = vR[SV0 + DIR1];
   const float2 gPL = pmul(p2(gam), vL[SPRES]), gPR = pmul(p2(gam), vR[SPRES]);
   const float2 tL = pmul(gPL, vL[SD]), tR = pmul(gPR, vR[SD]);
-  const float2 cfL = pmul(gPL, make_float2(rsqrt_approx(fmaxf(tL.x, tiny)), rsqrt_approx(fmaxf(tL.y, tiny))));
-  const float2 cfR = pmul(gPR, make_float2(rsqrt_approx(fmaxf(tR.x, tiny)), rsqrt_approx(fmaxf(tR.y, tiny))));
+  // (+ FLT_MIN keeps the reciprocal square root finite where P = 0)
+  const float2 tLs = padd(tL, p2(tiny)), tRs = padd(tR, p2(tiny));
+  const float2 cfL = pmul(gPL, make_float2(rsqrt_approx(tLs.x), rsqrt_approx(tLs.y)));
+  const float2 cfR = pmul(gPR, make_float2(rsqrt_approx(tRs.x), rsqrt_approx(tRs.y)));
   const float2 mL = psub2(uL, cfL), mR = psub2(uR, cfR), pL = padd(uL, cfL), pR = padd(uR, cfR);
   const float2 sL = make_float2(fminf(-tiny, fminf(mL.x, mR.x)), fminf(-tiny, fminf(mL.y, mR.y)));
   const float2 sR = make_float2(fmaxf(tiny, fmaxf(pL.x, pR.x)), fmaxf(tiny, fmaxf(pL.y, pR.y)));
@@ -401,18 +408,20 @@ __device__ __forceinline__ void ghost_push_axis(const Args &a, int d, int b, con
 }
 
 // ---------------------------------------------------------------------------
-template <int RECON, int RIEMANN>
-__global__ void __launch_bounds__(NT, 1)
+template <int TY_, int RECON, int RIEMANN>
+__global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
     k_slab_stage(const __grid_constant__ CUtensorMap tm_cc, const __grid_constant__ CUtensorMap tm_lo,
                  const __grid_constant__ Args a) {
+  using T = Tile<TY_>;
+  constexpr int TY = T::TY, NT = T::NT, PR = T::PR, RXC = T::RXC, REC_N = T::REC_N, FLX_N = T::FLX_N;
   extern __shared__ __align__(128) unsigned char smem[];
   const MeshDesc &m = a.m;
-  const Smem L(m.np[0]);
+  const Smem<TY_> L(m.np[0]);
   const int tid = threadIdx.x, lane = tid & 31, wr = tid >> 5;
   const int np0 = m.np[0], gx = m.g[0], nz = m.nx[2], nz2 = nz / 2;
-  // raw slot s (s = pair & 1): the conserved box, then the energy low words
-  auto raw = [&](int s) { return reinterpret_cast<float *>(smem + s * L.slot_bytes()); };
-  auto rawlo = [&](int s) { return reinterpret_cast<float *>(smem + s * L.slot_bytes() + L.lo_off()); };
+  // the raw slot: the conserved box of a plane pair, then its energy low words
+  float *const rawcc = reinterpret_cast<float *>(smem);
+  float *const rawlo = reinterpret_cast<float *>(smem + L.lo_off());
   float2 *prim = reinterpret_cast<float2 *>(smem + L.prim_off());   // [NV][PR][PC]
   float2 *rm = reinterpret_cast<float2 *>(smem + L.rec_off());      // [NV][REC_N]
   float2 *rp = rm + NV * REC_N;
@@ -428,14 +437,14 @@ __global__ void __launch_bounds__(NT, 1)
   const float vol = float(m.vol);
   const float bt = float(a.beta);
   const int RV = L.raw_var(), RPL = L.raw_plane();
+  const long long plane_st = (long long)np0 * m.np[1];
 
   if (tid == 0) {
     mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  unsigned phase = 0u;  // bit s: parity of slot s's next completion
+  unsigned phase = 0u;  // parity of the slot's next completion
   double dtl = INFINITY;
   bool failed = false;
 
@@ -443,11 +452,10 @@ __global__ void __launch_bounds__(NT, 1)
     const int b = item / a.nty, ty = item - b * a.nty;
     const int oy = ty * TY;
     const int lb[3] = {b % m.nbx[0], (b / m.nbx[0]) % m.nbx[1], b / (m.nbx[0] * m.nbx[1])};
-    const int row0 = oy + m.g[1] - HH;  // first staged padded row
+    const int row0 = oy + m.g[1] - HH;     // first staged padded row
     const int zc0 = b * m.np[2] + m.g[2];  // tensor plane coordinate of interior plane 0
     // this thread's column: interior (x, y) = (lane, oy + wr)
     const long long col = (long long)b * m.P + (long long)(oy + wr + m.g[1]) * np0 + (lane + gx);
-    const long long plane_st = (long long)np0 * m.np[1];
 
     if (done) {
       // a stage queued after the run reached tlim leaves the state as it is
@@ -469,29 +477,31 @@ __global__ void __launch_bounds__(NT, 1)
       continue;
     }
 
+    // the tensor loads of a plane pair into the raw slot (free: the pair
+    // before it was converted before the last barrier)
     auto issue = [&](int pair) {
       if (tid == 0) {
-        const int s = pair & 1;
         fence_proxy_async();
-        mbar_expect_tx(&bar[s], unsigned(L.tx_bytes()));
-        tma_load_4d(raw(s), &tm_cc, 0, row0 / a.rgroup, zc0 + 2 * pair, 0, &bar[s]);
-        tma_load_3d(rawlo(s), &tm_lo, 0, row0 / a.rgroup, zc0 + 2 * pair, &bar[s]);
+        mbar_expect_tx(&bar[0], unsigned(L.tx_bytes()));
+        tma_load_4d(rawcc, &tm_cc, 0, row0 / a.rgroup, zc0 + 2 * pair, 0, &bar[0]);
+        tma_load_3d(rawlo, &tm_lo, 0, row0 / a.rgroup, zc0 + 2 * pair, &bar[0]);
       }
     };
-    // wait for a pair: thread 0 waits (bounded) and the CTA learns the outcome at the barrier
-    auto wait_pair = [&](int pair) -> bool {
-      const int s = pair & 1;
-      const unsigned par = (phase >> s) & 1u;
-      phase ^= 1u << s;
-      if (tid == 0) *flag = mbar_wait(&bar[s], par) ? 0 : 1;
-      __syncthreads();
+    // thread 0's bounded wait for the pair; the CTA reads the outcome after its
+    // next barrier and then acquires the pair with a wait that returns at once
+    auto wait_start = [&]() {
+      if (tid == 0) *flag = mbar_wait(&bar[0], phase) ? 0 : 1;
+    };
+    auto wait_finish = [&]() -> bool {
+      const unsigned par = phase;
+      phase ^= 1u;
       if (*flag) return false;
-      mbar_wait(&bar[s], par);  // completes at once: the phase has flipped
+      mbar_wait(&bar[0], par);
       return true;
     };
     // own column of a pair -> primitives (float2 over the two planes)
-    auto convert_own = [&](int pair, float2 (&W)[NV], bool keep) {
-      const float *r = raw(pair & 1), *rl = rawlo(pair & 1);
+    auto convert_own = [&](float2 (&W)[NV], bool keep) {
+      const float *r = rawcc, *rl = rawlo;
       const int o = (wr + HH) * np0 + lane + gx;
       float V0[NV], V1[NV];
       slab_prim(a.gm1, r[o], r[RV + o], r[2 * RV + o], r[3 * RV + o], r[4 * RV + o], rl[o], V0);
@@ -505,8 +515,8 @@ __global__ void __launch_bounds__(NT, 1)
       }
     };
     // the x and y halo cells of a centre pair
-    auto convert_halo = [&](int pair) {
-      const float *r = raw(pair & 1), *rl = rawlo(pair & 1);
+    auto convert_halo = [&]() {
+      const float *r = rawcc, *rl = rawlo;
       if (tid < 6 * TY + 6 * NX) {
         int rr, cc;
         if (tid < 6 * TY) {
@@ -528,186 +538,149 @@ __global__ void __launch_bounds__(NT, 1)
         for (int v = 0; v < NV; v++) prim[(v * PR + rr) * PC + cc] = make_float2(V0[v], V1[v]);
       }
     };
+    auto recon_x = [&](int v, int r, int xx) {
+      const float2 *c = prim + (v * PR + r + HH) * PC + xx;
+      float2 s[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) s[q] = c[q];
+      float2 vm, vp;
+      ReconPair<RECON>(a.limiter, s, vm, vp);
+      rm[v * REC_N + r * RXC + xx] = vm;
+      rp[v * REC_N + r * RXC + xx] = vp;
+    };
+    auto riemann_x = [&](int r, int f) {
+      float2 vL[NV], vR[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        vL[v] = rp[v * REC_N + r * RXC + f];
+        vR[v] = rm[v * REC_N + r * RXC + f + 1];
+      }
+      float2 F[NCV];
+      SlabRiemann2<RIEMANN, 0>(vL, vR, a.gam, F);
+#pragma unroll
+      for (int v = 0; v < NCV; v++) flx[v * FLX_N + r * (NX + 1) + f] = F[v];
+    };
+    auto recon_y = [&](int v, int yy, int x) {
+      const float2 *c = prim + (v * PR + yy) * PC + x + HH;
+      float2 s[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) s[q] = c[q * PC];
+      float2 vm, vp;
+      ReconPair<RECON>(a.limiter, s, vm, vp);
+      rm[v * REC_N + yy * NX + x] = vm;
+      rp[v * REC_N + yy * NX + x] = vp;
+    };
+    auto riemann_y = [&](int f, int x) {
+      float2 vL[NV], vR[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        vL[v] = rp[v * REC_N + f * NX + x];
+        vR[v] = rm[v * REC_N + (f + 1) * NX + x];
+      }
+      float2 F[NCV];
+      SlabRiemann2<RIEMANN, 1>(vL, vR, a.gam, F);
+#pragma unroll
+      for (int v = 0; v < NCV; v++) flx[v * FLX_N + f * NX + x] = F[v];
+    };
 
-    // the z window: planes (2j-2, 2j-1), (2j, 2j+1); carried z-face state
-    float2 W0[NV], W1[NV], W2[NV];
+    // z window: planes (2j-2, 2j-1), (2j, 2j+1).  Carried between steps:
+    // vPc = z face value vP of cell 2j-1; Fc = z flux at face 2j-3/2 and
+    // duc = x+y divergence of cell 2j-1 (both for the pending update of cell
+    // 2j-1); du = x+y divergence of the step's planes (y part added in the
+    // next step's first phase); zF = the step's z fluxes.
+    float2 W0[NV], W1[NV];
     float vPc[NV], Fc[NCV], duc[NCV];
+    float2 du[NCV], zF[NCV];
 #pragma unroll
     for (int v = 0; v < NV; v++) vPc[v] = 0.f;
 #pragma unroll
-    for (int v = 0; v < NCV; v++) Fc[v] = duc[v] = 0.f;
-
-    issue(-2);
-    issue(-1);
-    if (!wait_pair(-2)) {
-      failed = true;
-      break;
+    for (int v = 0; v < NCV; v++) {
+      Fc[v] = duc[v] = 0.f;
+      du[v] = zF[v] = p2(0.f);
     }
-    convert_own(-2, W0, false);
-    __syncthreads();
-    issue(0);
-    if (!wait_pair(-1)) {
-      failed = true;
-      break;
-    }
-    convert_own(-1, W1, false);
-    __syncthreads();
 
-    for (int j = -1; j <= nz2; j++) {
-      if (j + 2 <= nz2 + 1) issue(j + 2);
-      // L2 prefetch of the rows this step's update reads
-      {
-        const int z0 = 2 * j - 1;
-        if (lane < 24 && z0 + 1 >= 0 && z0 < nz) {
-          const int arr = lane % 12, pl = lane / 12;
-          const int z = z0 + pl;
-          if (z >= 0 && z < nz) {
-            const float *base = arr < 5 ? a.ub + arr * NP : arr == 5 ? a.ublo : arr < 11 ? a.u0 + (arr - 6) * NP : a.u0lo;
-            const float *p = base + (long long)b * m.P + (long long)(z + m.g[2]) * plane_st +
-                             (long long)(oy + wr + m.g[1]) * np0;
-            const uintptr_t lo = uintptr_t(p) & ~uintptr_t(15);
-            const unsigned bytes = unsigned(((uintptr_t(p + np0) & ~uintptr_t(15)) - lo));
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(bytes) : "memory");
+    // inputs of the pending update (cells 2j-3, 2j-2 at step j), loaded at the
+    // end of the previous step so the loads complete during its last barrier
+    bool ok[2] = {false, false};
+    long long n[2] = {0, 0};
+    float zb[2][NCV], z0[2][NCV], zblo[2], z0lo[2];
+    auto load_update = [&](int zlo) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int z = zlo + h;
+        ok[h] = z >= 0 && z < nz;
+        n[h] = col + (long long)(z + m.g[2]) * plane_st;
+        if (ok[h]) {
+#pragma unroll
+          for (int v = 0; v < NCV; v++) {
+            zb[h][v] = a.ub[v * NP + n[h]];
+            z0[h][v] = a.u0[v * NP + n[h]];
           }
+          zblo[h] = a.ublo[n[h]];
+          z0lo[h] = a.u0lo[n[h]];
         }
       }
-      float2 du[NCV];
-#pragma unroll
-      for (int v = 0; v < NCV; v++) du[v] = p2(0.f);
+    };
 
-      if (j >= 0 && j < nz2) {
-        // ---- x sweep ----
-        auto recon_x = [&](int v, int r, int xx) {
-          const float2 *c = prim + (v * PR + r + HH) * PC + xx;
-          float2 s[5];
-#pragma unroll
-          for (int q = 0; q < 5; q++) s[q] = c[q];
-          float2 vm, vp;
-          ReconPair<RECON>(a.limiter, s, vm, vp);
-          rm[v * REC_N + r * RXC + xx] = vm;
-          rp[v * REC_N + r * RXC + xx] = vp;
-        };
-#pragma unroll 1
-        for (int v = 0; v < NV; v++) recon_x(v, wr, lane);
-        if (tid < NV * TY * 2) recon_x(tid >> 5, (tid & 31) >> 1, NX + (tid & 1));
-        __syncthreads();
-        auto riemann_x = [&](int r, int f) {
-          float2 vL[NV], vR[NV];
-#pragma unroll
-          for (int v = 0; v < NV; v++) {
-            vL[v] = rp[v * REC_N + r * RXC + f];
-            vR[v] = rm[v * REC_N + r * RXC + f + 1];
-          }
-          float2 F[NCV];
-          SlabRiemann2<RIEMANN, 0>(vL, vR, a.gam, F);
-#pragma unroll
-          for (int v = 0; v < NCV; v++) flx[v * FLX_N + r * (NX + 1) + f] = F[v];
-        };
-        riemann_x(wr, lane);
-        if (tid < TY) riemann_x(tid, NX);
-        __syncthreads();
-#pragma unroll
-        for (int v = 0; v < NCV; v++) {
-          const float2 lo = flx[v * FLX_N + wr * (NX + 1) + lane], hi = flx[v * FLX_N + wr * (NX + 1) + lane + 1];
-          du[v] = psub2(du[v], psub2(pmul(p2(A0), hi), pmul(p2(A0), lo)));
-        }
-        // ---- y sweep ----
-        auto recon_y = [&](int v, int yy, int x) {
-          const float2 *c = prim + (v * PR + yy) * PC + x + HH;
-          float2 s[5];
-#pragma unroll
-          for (int q = 0; q < 5; q++) s[q] = c[q * PC];
-          float2 vm, vp;
-          ReconPair<RECON>(a.limiter, s, vm, vp);
-          rm[v * REC_N + yy * NX + x] = vm;
-          rp[v * REC_N + yy * NX + x] = vp;
-        };
-#pragma unroll 1
-        for (int v = 0; v < NV; v++) recon_y(v, wr, lane);
-        if (tid < NV * 2 * NX) recon_y(tid >> 6, TY + ((tid >> 5) & 1), lane);
-        __syncthreads();
-        auto riemann_y = [&](int f, int x) {
-          float2 vL[NV], vR[NV];
-#pragma unroll
-          for (int v = 0; v < NV; v++) {
-            vL[v] = rp[v * REC_N + f * NX + x];
-            vR[v] = rm[v * REC_N + (f + 1) * NX + x];
-          }
-          float2 F[NCV];
-          SlabRiemann2<RIEMANN, 1>(vL, vR, a.gam, F);
-#pragma unroll
-          for (int v = 0; v < NCV; v++) flx[v * FLX_N + f * NX + x] = F[v];
-        };
-        riemann_y(wr, lane);
-        if (tid < NX) riemann_y(TY, tid);
-        __syncthreads();
+    issue(-2);
+    wait_start();
+    __syncthreads();
+    if (!wait_finish()) {
+      failed = true;
+      break;
+    }
+    convert_own(W0, false);
+    __syncthreads();
+    issue(-1);
+    wait_start();
+    __syncthreads();
+    if (!wait_finish()) {
+      failed = true;
+      break;
+    }
+    convert_own(W1, false);
+    __syncthreads();
+
+    for (int j = -1; j <= nz2 + 1; j++) {
+      const bool centre = j >= 0 && j < nz2;
+      // ---- phase A: the pending update of cells (2j-3, 2j-2), the next
+      // pair's loads, x reconstruction of this step's planes ----
+      if (j - 1 >= 0 && j - 1 < nz2) {
+        // y divergence of step j-1's planes
 #pragma unroll
         for (int v = 0; v < NCV; v++) {
           const float2 lo = flx[v * FLX_N + wr * NX + lane], hi = flx[v * FLX_N + (wr + 1) * NX + lane];
           du[v] = psub2(du[v], psub2(pmul(p2(A1), hi), pmul(p2(A1), lo)));
         }
       }
-
-      // ---- next pair: convert (own column into the window, and the halo if it is a centre pair) ----
-      if (!wait_pair(j + 1)) {
-        failed = true;
-        break;
-      }
-      const bool centre = j + 1 >= 0 && j + 1 < nz2;
-      convert_own(j + 1, W2, centre);
-      if (centre) convert_halo(j + 1);
-
-      // ---- z sweep in registers: cells (2j, 2j+1), faces 2j - 1/2 and 2j + 1/2 ----
-      float2 vm[NV], vp[NV];
-#pragma unroll
-      for (int v = 0; v < NV; v++) {
-        const float2 s[5] = {W0[v], make_float2(W0[v].y, W1[v].x), W1[v], make_float2(W1[v].y, W2[v].x), W2[v]};
-        ReconPair<RECON>(a.limiter, s, vm[v], vp[v]);
-      }
-      float2 vL[NV];
-#pragma unroll
-      for (int v = 0; v < NV; v++) vL[v] = make_float2(vPc[v], vp[v].x);
-      float2 F[NCV];
-      SlabRiemann2<RIEMANN, 2>(vL, vm, a.gam, F);
-
-      // ---- update of cells 2j-1 (lane x) and 2j (lane y) ----
-      {
-        float2 dz[NCV];
+      if (j >= 1) {
+        float dz[2][NCV];
 #pragma unroll
         for (int v = 0; v < NCV; v++) {
-          // z contributions: -A (F+ - F-), after x and y as the reference sums them
-          const float dA = duc[v] - (A2 * F[v].x - A2 * Fc[v]);
-          const float dB = du[v].x - (A2 * F[v].y - A2 * F[v].x);
-          dz[v] = make_float2(dA, dB);
+          // z contributions -A (F+ - F-) after x and y, as the reference sums them
+          dz[0][v] = duc[v] - (A2 * zF[v].x - A2 * Fc[v]);
+          dz[1][v] = du[v].x - (A2 * zF[v].y - A2 * zF[v].x);
         }
+        const int zlo = 2 * j - 3;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-          const int z = 2 * j - 1 + h;
-          if (z < 0 || z >= nz) continue;
-          const long long n = col + (long long)(z + m.g[2]) * plane_st;
-          float zb[NCV], z0[NCV];
-#pragma unroll
-          for (int v = 0; v < NCV; v++) {
-            zb[v] = a.ub[v * NP + n];
-            z0[v] = a.u0[v * NP + n];
-          }
-          const float zblo = a.ublo[n], z0lo = a.u0lo[n];
+          if (!ok[h]) continue;
           GhostVal gv;
 #pragma unroll
           for (int v = 0; v < NCV; v++) {
-            const float dudt = (h == 0 ? dz[v].x : dz[v].y) / vol;
+            const float dudt = dz[h][v] / vol;
             if (v == CENER) {
-              const double eb = double(zb[v]) + double(zblo), e0 = double(z0[v]) + double(z0lo);
+              const double eb = double(zb[h][v]) + double(zblo[h]), e0 = double(z0[h][v]) + double(z0lo[h]);
               const double e1 = (a.beta * eb + (1.0 - a.beta) * e0) + a.beta * dt * double(dudt);
               gv.v[v] = float(e1);
               gv.lo = float(e1 - double(gv.v[v]));
             } else {
-              gv.v[v] = (bt * zb[v] + (1.f - bt) * z0[v]) + bt * float(dt) * dudt;
+              gv.v[v] = (bt * zb[h][v] + (1.f - bt) * z0[h][v]) + bt * float(dt) * dudt;
             }
-            a.u1[v * NP + n] = gv.v[v];
+            a.u1[v * NP + n[h]] = gv.v[v];
           }
-          a.u1lo[n] = gv.lo;
-          const int pc[3] = {lane + gx, oy + wr + m.g[1], z + m.g[2]};
+          a.u1lo[n[h]] = gv.lo;
+          const int pc[3] = {lane + gx, oy + wr + m.g[1], zlo + h + m.g[2]};
 #pragma unroll
           for (int d = 0; d < 3; d++) ghost_push_axis(a, d, b, lb, pc, gv);
           if (a.last) {
@@ -723,18 +696,73 @@ __global__ void __launch_bounds__(NT, 1)
           }
         }
       }
-      // carry to the next pair
-#pragma unroll
-      for (int v = 0; v < NV; v++) {
-        vPc[v] = vp[v].y;
-        W0[v] = W1[v];
-        W1[v] = W2[v];
-      }
+      if (j > nz2) break;
+      // the pending update of cell 2j-1 in the next step takes these
 #pragma unroll
       for (int v = 0; v < NCV; v++) {
-        Fc[v] = F[v].y;
+        Fc[v] = zF[v].y;
         duc[v] = du[v].y;
+        du[v] = p2(0.f);
       }
+      issue(j + 1);
+      if (centre) {
+#pragma unroll 2
+        for (int v = 0; v < NV; v++) recon_x(v, wr, lane);
+        if (tid < NV * TY * 2) recon_x(tid / (2 * TY), (tid % (2 * TY)) >> 1, NX + (tid & 1));
+      }
+      __syncthreads();
+      // ---- phase B: x Riemann fluxes ----
+      if (centre) {
+        riemann_x(wr, lane);
+        if (tid < TY) riemann_x(tid, NX);
+      }
+      __syncthreads();
+      // ---- phase C: x divergence, y reconstruction, wait for the next pair ----
+      if (centre) {
+#pragma unroll
+        for (int v = 0; v < NCV; v++) {
+          const float2 lo = flx[v * FLX_N + wr * (NX + 1) + lane], hi = flx[v * FLX_N + wr * (NX + 1) + lane + 1];
+          du[v] = psub2(du[v], psub2(pmul(p2(A0), hi), pmul(p2(A0), lo)));
+        }
+#pragma unroll 2
+        for (int v = 0; v < NV; v++) recon_y(v, wr, lane);
+        for (int it = tid; it < NV * 2 * NX; it += NT) recon_y(it >> 6, TY + ((it >> 5) & 1), lane);
+      }
+      wait_start();
+      __syncthreads();
+      // ---- phase D: y Riemann fluxes, the next pair's primitives, the z sweep ----
+      if (!wait_finish()) {
+        failed = true;
+        break;
+      }
+      if (centre) {
+        riemann_y(wr, lane);
+        if (tid < NX) riemann_y(TY, tid);
+      }
+      const bool next_centre = j + 1 >= 0 && j + 1 < nz2;
+      float2 W2[NV];
+      convert_own(W2, next_centre);
+      if (next_centre) convert_halo();
+      {
+        // cells (2j, 2j+1) of the column, faces 2j - 1/2 and 2j + 1/2
+        float2 vm[NV], vp[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+          const float2 s[5] = {W0[v], make_float2(W0[v].y, W1[v].x), W1[v], make_float2(W1[v].y, W2[v].x), W2[v]};
+          ReconPair<RECON>(a.limiter, s, vm[v], vp[v]);
+        }
+        float2 vL[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) vL[v] = make_float2(vPc[v], vp[v].x);
+        SlabRiemann2<RIEMANN, 2>(vL, vm, a.gam, zF);
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+          vPc[v] = vp[v].y;
+          W0[v] = W1[v];
+          W1[v] = W2[v];
+        }
+      }
+      load_update(2 * j - 1);
       __syncthreads();
     }
   }

@@ -38,8 +38,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn(std::string *err) {
 }
 
 // Tensor map over one container array: dims (row group, row groups, planes of
-// all blocks [, variables]); the box is one tile's 22 staged rows of two planes.
-int make_map(kmy_ctx *c, CUtensorMap *map, const void *base, int nvar) {
+// all blocks [, variables]); the box is one tile's staged rows of two planes.
+int make_map(kmy_ctx *c, CUtensorMap *map, const void *base, int nvar, int staged_rows) {
   const MeshDesc &m = c->m;
   const int R = row_group(m.np[0]);
   auto fn = encode_fn(&c->err);
@@ -48,7 +48,7 @@ int make_map(kmy_ctx *c, CUtensorMap *map, const void *base, int nvar) {
                         cuuint64_t(nvar)};
   cuuint64_t strides[3] = {cuuint64_t(R) * m.np[0] * 4, cuuint64_t(m.np[0]) * m.np[1] * 4,
                            cuuint64_t(m.nb) * m.P * 4};
-  cuuint32_t box[4] = {cuuint32_t(R * m.np[0]), cuuint32_t(slab::PR / R), 2u, cuuint32_t(nvar)};
+  cuuint32_t box[4] = {cuuint32_t(R * m.np[0]), cuuint32_t(staged_rows / R), 2u, cuuint32_t(nvar)};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   const cuuint32_t rank = nvar > 1 ? 4 : 3;
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<void *>(base), dims, strides, box, estr,
@@ -72,10 +72,10 @@ int sm_count(int device) {
   return v;
 }
 
-template <int RECON, int RIEMANN>
+template <int TY, int RECON, int RIEMANN>
 int launch_kind(kmy_ctx *c, const CUtensorMap &mc, const CUtensorMap &ml, const slab::Args &a, int grid,
                 size_t smem) {
-  auto kern = slab::k_slab_stage<RECON, RIEMANN>;
+  auto kern = slab::k_slab_stage<TY, RECON, RIEMANN>;
   // the shared-memory opt-in once per device, so a stream capture sees launches only
   static std::atomic<unsigned long long> opted{0};
   const unsigned long long bit = c->device < 64 ? 1ull << c->device : 0ull;
@@ -84,12 +84,20 @@ int launch_kind(kmy_ctx *c, const CUtensorMap &mc, const CUtensorMap &ml, const 
     if (e != cudaSuccess) return cuda_check(c, e, "slab smem attribute");
     opted.fetch_or(bit);
   }
-  kern<<<unsigned(grid), slab::NT, smem, c->stream>>>(mc, ml, a);
+  kern<<<unsigned(grid), slab::Tile<TY>::NT, smem, c->stream>>>(mc, ml, a);
   c->launches++;
   return cuda_check(c, cudaGetLastError(), "slab stage");
 }
 
 }  // namespace
+
+// Rows per tile for this context: the deck's (or the tuner's) choice, else 16
+// where the block height allows it (measured faster than 8 on the 256^3
+// WENO-Z workload), else 8.
+int slab_rows(const kmy_ctx *c) {
+  if (c->prm.slab_rows) return c->prm.slab_rows;
+  return c->m.nx[1] % 16 == 0 ? 16 : 8;
+}
 
 const char *slab_unsupported(const kmy_ctx *c) {
   const MeshDesc &m = c->m;
@@ -98,17 +106,19 @@ const char *slab_unsupported(const kmy_ctx *c) {
   if (c->prm.mhd) return "constrained transport runs the brick stage";
   if (c->amr.on) return "adaptive meshes run the per-task kernels";
   if (m.nx[0] != slab::NX) return "the z-streamed stage needs 32 cells per block along x";
-  if (m.nx[1] % slab::TY != 0) return "the z-streamed stage needs a multiple of 16 cells per block along y";
+  const int ty = slab_rows(c);
+  if (m.nx[1] % ty != 0) return "the block height is not a multiple of the tile's rows";
   if (m.nx[2] % 2 != 0) return "the z-streamed stage needs an even block size along z";
   for (int d = 0; d < 3; d++)
     if (m.g[d] < slab::HH) return "the z-streamed stage needs 3 or more ghost cells";
   const int R = row_group(m.np[0]);
   if (!R) return "padded rows do not group into 16-byte multiples";
-  if ((m.g[1] - slab::HH) % R || slab::PR % R || m.np[1] % R || slab::TY % R)
+  if ((m.g[1] - slab::HH) % R || (ty + 2 * slab::HH) % R || m.np[1] % R || ty % R)
     return "staged rows do not align with the row groups";
   if ((size_t(m.np[0]) * m.np[1] * 4) % 16) return "padded planes are not a multiple of 16 bytes";
   if ((long long)m.np[2] * m.nb >= (1ll << 31)) return "too many planes for a tensor map";
-  if (slab::Smem(m.np[0]).total() > 227 * 1024) return "padded rows too long for the shared-memory plan";
+  const int need = ty == 8 ? slab::Smem<8>(m.np[0]).total() * 2 : slab::Smem<16>(m.np[0]).total();
+  if (need > 227 * 1024) return "padded rows too long for the shared-memory plan";
   return nullptr;
 }
 
@@ -124,8 +134,9 @@ int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md
   CUtensorMap mc, ml;
   std::memset(&mc, 0, sizeof(mc));
   std::memset(&ml, 0, sizeof(ml));
-  if (int rc = make_map(c, &mc, md0.cc, slab::NCV)) return rc;
-  if (int rc = make_map(c, &ml, md0.ener_lo, 1)) return rc;
+  const int ty = slab_rows(c);
+  if (int rc = make_map(c, &mc, md0.cc, slab::NCV, ty + 2 * slab::HH)) return rc;
+  if (int rc = make_map(c, &ml, md0.ener_lo, 1, ty + 2 * slab::HH)) return rc;
   slab::Args a{};
   a.m = m;
   a.gm1 = float(c->eos.gm1);
@@ -141,26 +152,34 @@ int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md
   a.beta = beta;
   a.clock = c->clock;
   a.rgroup = row_group(m.np[0]);
-  a.nty = m.nx[1] / slab::TY;
+  a.nty = m.nx[1] / ty;
   a.nitems = m.nb * a.nty;
-  const int grid = std::min(a.nitems, sm_count(c->device));
-  const size_t smem = size_t(slab::Smem(m.np[0]).total());
+  const int ctas = ty == 8 ? slab::Tile<8>::CTAS : slab::Tile<16>::CTAS;
+  const int grid = std::min(a.nitems, sm_count(c->device) * ctas);
+  const size_t smem = size_t(ty == 8 ? slab::Smem<8>(m.np[0]).total() : slab::Smem<16>(m.np[0]).total());
   if (last) {
     k_reset_dtmin_slab<<<1, 1, 0, c->stream>>>(c->clock);
     c->launches++;
   }
   int rc;
   const int rec = c->prm.recon, rie = c->prm.riemann;
+#define KMY_SLAB_TY(TY, RC)                                                               \
+  rc = rie == HLL ? launch_kind<TY, RC, HLL>(c, mc, ml, a, grid, smem)                    \
+                  : launch_kind<TY, RC, HLLC>(c, mc, ml, a, grid, smem);
 #define KMY_SLAB(RC)                                                                      \
   if (rec == RC) {                                                                        \
-    rc = rie == HLL ? launch_kind<RC, HLL>(c, mc, ml, a, grid, smem)                      \
-                    : launch_kind<RC, HLLC>(c, mc, ml, a, grid, smem);                    \
+    if (ty == 8) {                                                                        \
+      KMY_SLAB_TY(8, RC)                                                                  \
+    } else {                                                                              \
+      KMY_SLAB_TY(16, RC)                                                                 \
+    }                                                                                     \
   } else
   KMY_SLAB(FOG) KMY_SLAB(PLM) KMY_SLAB(PPM) KMY_SLAB(WENOZ) {
     c->err = "no slab kernel for this reconstruction";
     return KMY_ERR_BAD_PARAM;
   }
 #undef KMY_SLAB
+#undef KMY_SLAB_TY
   md1.ghosts = rc == KMY_OK;
   return rc;
 }

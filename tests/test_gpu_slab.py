@@ -194,3 +194,51 @@ def test_slab_rejected_where_it_does_not_apply(kmy_lib):
     s.pgen("kelvin_helmholtz")
     with pytest.raises(K.KmyError):
         s.step()
+
+
+@pytest.mark.parametrize("rows", ["8", "16"])
+def test_slab_tile_rows(kmy_lib, rows):
+    """Both tile heights (two 256-thread CTAs or one 512-thread CTA per SM)
+    against FP64, and their face ghosts against the exchange."""
+    d = kh()
+    d.set("kamayan_b200", "slab_rows", rows)
+    s32 = run(d, 6)
+    assert s32.stage_kernel == f"slab{rows}"
+    s64 = run(kh(precision="fp64", kernel="auto"), 6)
+    for var, c in CONS:
+        err = rel_l1(s32.interior(s32.export(var, c)), s64.interior(s64.export(var, c)))
+        assert err <= bar(var, c), (rows, var, c, err)
+
+
+def test_autotune_picks_the_fastest_and_caches(kmy_lib):
+    K.tune_cache_clear()
+    s = K.Solver(kh(kernel="tune"))
+    s.pgen("kelvin_helmholtz")
+    assert s.stage_kernel == "tune"
+    res = s.autotune(reps=3)
+    timed = {k: v for k, v in res.items() if v is not None}
+    assert set(timed) == {"brick", "slab16", "slab8"}
+    assert all(v > 0 for v in timed.values())
+    assert s.stage_kernel == min(timed, key=timed.get)
+    # the tuned kernel steps correctly
+    for _ in range(4):
+        s.step()
+    ref = run(kh(precision="fp64", kernel="auto"), 4)
+    assert rel_l1(s.interior(s.export("dens")), ref.interior(ref.export("dens"))) <= L1_FP32
+    # a second context of the same configuration takes the cached choice at its first stage
+    key = f"{s._dev_name} | {K.tune_key(kh())}" if hasattr(s, "_dev_name") else None
+    t = K.Solver(kh(kernel="tune"))
+    t.pgen("kelvin_helmholtz")
+    n0 = t.launch_count
+    t.rk_stage(1)
+    assert t.stage_kernel == s.stage_kernel
+    # no tuning launches: the stage (and a dt reset at most) ran
+    assert t.launch_count - n0 <= 3
+    del key
+
+
+def test_evolve_replays_graphs(kmy_lib):
+    a = K.Solver(kh(nlim=60))
+    a.pgen("kelvin_helmholtz")
+    a.evolve(1e30, 40)
+    assert a.graph_replays > 0

@@ -29,9 +29,12 @@ def test_noalloc_sums_match_context_sums_twice(kmy_lib):
     import kamayan_b200 as K
     from kamayan_b200 import configs
 
-    s = K.Solver(configs.kh_3d(n=32, nb=16))
+    # 128^3 interior cells: more than the kernel's 151,552 threads, so each
+    # thread's grid-stride loop and its compensated sum run several times
+    s = K.Solver(configs.kh_3d(n=128, nb=32))
     s.pgen("kelvin_helmholtz")
     s.step()
+    assert s.info.nblocks * 32 ** 3 > 4 * 592 * 256
     ref = s.conserved_sums()
     inf = s.info
     vol = inf.dx[0] * inf.dx[1] * inf.dx[2]
