@@ -4,20 +4,28 @@
 Workload: 3D Kelvin-Helmholtz, gamma 1.4, periodic unit cube, 256^3 cells in
 512 meshblocks of 32^3 with 3 ghost cells, WENO-Z + HLLC, RK3, CFL 0.4,
 synthetic initial state (seeded shear-layer perturbation).  A step is one full
-RK3 time step over the whole mesh (three fused stage launches + the device dt
+RK3 time step over the whole mesh (three stage launches + the device dt
 controller).  Metric: cell-updates/s = interior cells x steps / time.
 
-``value``: the FP32 bulk path (FP64 energy recovery and sums), all 512 blocks
-batched into one launch per stage, timed with CUDA events on the solver's
-stream.  Beside it: the FP64 fused path, the FP64 per-task path (the
-reference task list, one kernel per task) and the FP32-vs-FP64 density L1.
-``e2e``: the same metric through the C ABI with host buffers: import of the
-initial conserved state (interior cells, FP64) from pinned host memory
-(finalize derives the primitives and fills the ghost zones), K x kmy_step
-(each returns dt to the host), export of the final conserved state.
+``value``: the FP32 bulk path (FP64 energy recovery and sums), every block in
+one persistent launch per stage, the stage kernel chosen by the library's
+autotuner (``config.stage_kernel``), timed with CUDA events on the solver's
+stream.  Beside it: the FP64 stage with one launch per mesh, the plain
+per-block FP64 path (one launch per meshblock per stage), the FP64 per-task
+path (the reference task list, one kernel per task) and the FP32-vs-FP64
+density L1.  ``e2e``: the same metric through the C ABI with host buffers:
+import of the initial conserved state (interior cells, FP64) from pinned host
+memory (finalize derives the primitives and fills the ghost zones),
+K x kmy_step (each returns dt to the host), export of the final conserved
+state.
+
+``roofline``: the stage kernel against HBM (algorithmic bytes per launch over
+its CUDA-event time, of the measured copy bandwidth), with its issue-slot and
+FP32-pipe fractions from the per-cell counters of its ncu profile
+(profiles/stage_counters.txt) at the sampled SM clock.
 
 ``--impl reference`` times the reference's CPU path (the C++ restatement in
-oracle/, all host threads) on a bounded sample of the same workload.
+oracle/, host-tuned build, all host threads) on the same 256^3 workload.
 
 Multi-GPU (torchrun): the path does not shard here, so every rank runs an
 independent replica; the time is the max over ranks and ``value`` the sum.
@@ -57,6 +65,8 @@ def args():
                     help="skip the vortex / Orszag-Tang / adaptive-blast measurements")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
                     help="time one precision only (profiling captures); prints its own line")
+    ap.add_argument("--kernel", choices=["brick", "slab", "tune"], default=None,
+                    help="stage kernel for --only runs (default: the library's choice)")
     return ap.parse_args()
 
 
@@ -227,11 +237,16 @@ def time_solver(s, stream, K: int, W: int, ws: int, tasks: bool = False, sampler
             "launches": s.launch_count - launches0, "clocks": clocks}
 
 
-def make_solver(a, precision: str, device: int, stream):
+def make_solver(a, precision: str, device: int, stream, **opts):
+    """The workload's solver; opts are <kamayan_b200> deck options
+    (stage_kernel, slab_rows, launch)."""
     import kamayan_b200
     from kamayan_b200 import configs
 
-    s = kamayan_b200.Solver(configs.kh_3d(n=a.n, nb=a.nb, precision=precision), device=device)
+    d = configs.kh_3d(n=a.n, nb=a.nb, precision=precision)
+    for k, v in opts.items():
+        d.set("kamayan_b200", k, v)
+    s = kamayan_b200.Solver(d, device=device)
     s.set_stream(stream.cuda_stream)
     s.pgen("kelvin_helmholtz")
     return s
@@ -283,14 +298,14 @@ def e2e_solve(a, device: int, stream, K: int):
     return ms, h2d, d2h
 
 
-def load_traffic(precision: str, a):
-    """DRAM bytes per fused-stage launch from the committed ncu summary, scaled to this mesh."""
-    p = ROOT / "profiles" / "fused_stage_traffic.txt"
-    if not p.exists():
-        return None
+def stage_counters(kernel: str):
+    """Per-cell counters of a stage kernel from its committed ncu summary
+    (profiles/stage_counters.txt): DRAM bytes, warp instructions issued, and
+    FMA- and XU-pipe busy SM-cycles, per interior cell and stage launch."""
+    p = ROOT / "profiles" / "stage_counters.txt"
     try:
-        d = json.loads(p.read_text())[precision]
-        return d["bytes_per_cell"] * a.n ** 3
+        k = json.loads(p.read_text())["kernels"]
+        return k.get(kernel) or k.get(kernel + "_fp32")
     except Exception:
         return None
 
@@ -304,10 +319,10 @@ def peaks():
 
 
 def cpu_baseline(sample_n: int, min_seconds: float, max_steps: int, steps: int = 1,
-                 workload: str = "kh_3d", nb: int = 32, warmup: int = 1):
+                 workload: str = "kh_3d", nb: int = 32, warmup: int = 1, threads: int = 0):
     cmd = [sys.executable, "-m", "oracle.cpu_bench", "--workload", workload, "--n", str(sample_n),
            "--nb", str(nb), "--steps", str(steps), "--warmup", str(warmup), "--min-seconds", str(min_seconds),
-           "--max-steps", str(max_steps)]
+           "--max-steps", str(max_steps), "--threads", str(threads), "--build", "native"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
     if r.returncode != 0:
         return {"error": r.stderr[-400:]}
@@ -413,18 +428,22 @@ def main_reference(a):
     # and need no process group
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    cb = cpu_baseline(128, 20.0, 200, steps=max(1, min(a.steps, 3)))
+    # the full workload (256^3 in 512 blocks of 32^3), all host threads,
+    # host-tuned build; a step takes a few seconds, so K is bounded
+    steps = max(1, min(a.steps, 3))
+    cb = cpu_baseline(a.n, 0.0, steps, steps=steps, nb=a.nb, warmup=1)
     cfg = workload_config(a, a.gpus)
     line = {
         "impl": "reference", "metric": METRIC, "value": cb.get("value"), "unit": METRIC,
         "n_gpus": a.gpus, "steps": cb.get("steps"), "warmup": 1, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": cb.get("value"), "unit": METRIC, "cores": cb.get("threads"),
-                         "kind": "port", "sample": cb.get("sample")},
+                         "kind": "port", "sample": cb.get("sample"), "cpu": cb.get("cpu"),
+                         "build": cb.get("build")},
         "e2e": {"value": cb.get("value"), "unit": METRIC, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "note": "reference's own build is unavailable (un-vendored Parthenon/Kokkos); "
-                "timed: the C++ restatement of its CPU path, OpenMP over meshblocks",
+                "timed: the C++ restatement of its CPU path, OpenMP over meshblocks, on the same workload",
     }
     print(json.dumps(line), flush=True)
 
@@ -444,24 +463,28 @@ def main():
     ns = 3
 
     if a.only:
-        s1 = make_solver(a, a.only, device, stream)
+        s1 = make_solver(a, a.only, device, stream, **({"stage_kernel": a.kernel} if a.kernel else {}))
         r1 = time_solver(s1, stream, K, W, ws)
+        kern = s1.stage_kernel
         s1.close()
         tot = allreduce_max(r1["total_ms"], ws)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": job_value(ws, cells, K, tot), "unit": METRIC,
                               "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": tot / K,
-                              "dtype": "f32" if a.only == "fp32" else "f64",
+                              "dtype": "f32" if a.only == "fp32" else "f64", "stage_kernel": kern,
                               "launch_ms_avg": r1["stage_ms_avg"], "config": workload_config(a, ws),
                               "note": "single-precision profiling run; not the headline line"}),
                   flush=True)
         return
 
-    # headline: FP32 bulk path, fused stages over all blocks
-    s32 = make_solver(a, "fp32", device, stream)
+    # headline: FP32 bulk path, the stage kernel the autotuner picks for this
+    # device and configuration (timed on the solver's state before the warm-up)
+    s32 = make_solver(a, "fp32", device, stream, stage_kernel="tune")
+    tuning = s32.autotune(reps=3)
+    kernel = s32.stage_kernel
     sampler = ClockSampler(device)
     r32 = time_solver(s32, stream, K, W, ws, sampler=sampler)
-    # FP64 fused
+    # FP64, one launch per stage over the whole mesh
     s64 = make_solver(a, "fp64", device, stream)
     r64 = time_solver(s64, stream, K, W, ws)
     import numpy as np
@@ -472,6 +495,12 @@ def main():
     t32, t64 = s32.time["time"], s64.time["time"]
     s32.close()
     s64.close()
+    # the plain per-block FP64 path: the same stage kernel, one launch per
+    # meshblock per stage
+    Kp = max(2, K // 4)
+    spb = make_solver(a, "fp64", device, stream, launch="per_block")
+    rpb = time_solver(spb, stream, Kp, W, ws)
+    spb.close()
     # FP64 per-task path (the reference task list as separate kernels)
     rt = None
     if not a.no_tasks:
@@ -483,42 +512,62 @@ def main():
 
     tot32 = allreduce_max(r32["total_ms"], ws)
     tot64 = allreduce_max(r64["total_ms"], ws)
+    totpb = allreduce_max(rpb["total_ms"], ws)
     e2e_ms = allreduce_max(e2e_ms, ws)
     value = job_value(ws, cells, K, tot32)
     v64 = job_value(ws, cells, K, tot64)
+    vpb = job_value(ws, cells, Kp, totpb)
     vt = None
     if rt:
         Kt = max(2, K // 4)
         vt = ws * cells * Kt / (allreduce_max(rt["total_ms"], ws) / 1e3)
 
-    # roofline of the dominant kernel (the fused stage): algorithmic bytes per
+    # roofline of the dominant kernel (the stage): algorithmic bytes per
     # launch = cells x words x bytes, words = 10 (stage 1) or 15 (stages 2, 3)
-    # (5 conserved words per cell; the FP32 path's extra energy low word is not counted)
+    # (5 conserved words per cell; the FP32 path's energy low word not counted)
     words_avg = (10 + 15 * (ns - 1)) / ns
     alg32 = cells * words_avg * 4
     alg64 = cells * words_avg * 8
     peak, peak_kind = peaks()
-    ach32 = alg32 / (r32["stage_ms_avg"] / 1e3) / 1e9
+    launch_s = r32["stage_ms_avg"] / 1e3
+    ach32 = alg32 / launch_s / 1e9
     ach64 = alg64 / (r64["stage_ms_avg"] / 1e3) / 1e9
-    traffic = load_traffic("fp32", a)
+    ctr = stage_counters(kernel)
+    clk = r32["clocks"] or {}
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    roof = {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
+            "traffic": (ctr["dram_bytes_per_cell"] * cells) if ctr else None, "peak_kind": peak_kind,
+            "kernel": kernel, "alg_bytes_per_launch": alg32, "launch_ms_avg": r32["stage_ms_avg"]}
+    if ctr:
+        cyc = launch_s * mhz * 1e6 * sms  # SM-cycles of one launch
+        roof["issue"] = {"frac": ctr["warp_inst_per_cell"] * cells / (cyc * 4),
+                         "what": "warp instructions issued / (4 schedulers x SMs x cycles of the launch)"}
+        if "fma_pipe_sm_cycles_per_cell" in ctr:
+            roof["fp32_pipe"] = {"frac": ctr["fma_pipe_sm_cycles_per_cell"] * cells / cyc,
+                                 "xu_frac": ctr["xu_pipe_sm_cycles_per_cell"] * cells / cyc,
+                                 "what": "FMA-pipe (and reciprocal/XU-pipe) busy SM-cycles / SM-cycles of the launch"}
+        roof["counters"] = f"profiles/stage_counters.txt ({ctr.get('source', '')})"
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": K, "warmup": W,
         "ms_per_step": tot32 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic", "config": workload_config(a, ws),
+        "dtype": "f32", "data": "synthetic", "config": dict(workload_config(a, ws), stage_kernel=kernel),
         "e2e": {"value": job_value(ws, cells, K, e2e_ms), "unit": METRIC,
                 "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
                 "what": "kmy_import_interior of the conserved state (FP64 interior cells, pinned host) + "
                         "finalize + K x kmy_step + kmy_export_interior of the conserved state, FP32 solve"},
         "gpu_launches": r32["launches"],
-        "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
-                     "frac": ach32 / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "k_fused_stage<float,3,WENOZ,HLLC>",
-                     "alg_bytes_per_launch": alg32, "launch_ms_avg": r32["stage_ms_avg"]},
+        "roofline": roof,
         "clocks": r32["clocks"],
+        "tuning": {k: v for k, v in tuning.items()},
         "fp64_fused": {"value": v64, "ms_per_step": tot64 / K, "launch_ms_avg": r64["stage_ms_avg"],
                        "roofline_achieved_gbs": ach64, "frac": ach64 / peak},
+        "fp64_per_block": {"value": vpb, "ms_per_step": totpb / Kp, "steps": Kp,
+                           "what": "the FP64 brick stage launched once per meshblock per stage"},
         "fp64_tasks": ({"value": vt, "ms_per_step": rt["total_ms"] / max(2, K // 4)} if rt else None),
+        "fp32_over_fp64_per_block": value / vpb,
+        "fp32_over_fp64_fused": value / v64,
         "l1_density_fp32_vs_fp64": l1,
         "sim_time_fp32_fp64": [t32, t64],
     }
@@ -536,9 +585,14 @@ def main():
     if a.serve > 0:
         line["serving"] = serving_block(a, device)
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
-        cb = cpu_baseline(128, 10.0, 200)
+        # the same 256^3 workload on all host threads (one step after one
+        # warm-up step), and on one core a 128^3 sample of it
+        cb = cpu_baseline(a.n, 0.0, 1, steps=1, nb=a.nb, warmup=1)
+        c1 = cpu_baseline(128, 0.0, 1, steps=1, nb=a.nb, warmup=0, threads=1)
         line["cpu_baseline"] = {"value": cb.get("value"), "unit": METRIC, "cores": cb.get("threads"),
-                                "kind": "port", "sample": cb.get("sample")}
+                                "kind": "port", "sample": cb.get("sample"), "cpu": cb.get("cpu"),
+                                "build": cb.get("build"),
+                                "one_core": {"value": c1.get("value"), "sample": c1.get("sample")}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -122,6 +122,10 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   const std::string sr = p.str("kamayan_b200/slab_rows", "auto");
   if (!one_of(sr, {"auto", "8", "16"})) return bad("kamayan_b200/slab_rows: " + sr);
   p.slab_rows = sr == "auto" ? 0 : std::stoi(sr);
+  const std::string ln = p.str("kamayan_b200/launch", "batched");
+  if (!one_of(ln, {"batched", "per_block"})) return bad("kamayan_b200/launch: " + ln);
+  p.per_block = ln == "per_block";
+  if (p.per_block && p.stage_kernel == 0) p.stage_kernel = 1;  // the per-block launches are of the brick stage
 
   const std::string integ = p.str("parthenon/time/integrator", "rk2");
   if (integ == "rk1") p.beta = {1.0};

@@ -102,6 +102,7 @@ struct FusedArgs {
   int nbr[3];
   const S *fc0;  // MHD: face field of the stage input (the Riemann problems' normal B)
   S *flux;       // MHD: face fluxes for the edge EMFs, layout [dir][8][nb * Pf]
+  int b0;        // first block of the launch (per-block launches; 0 when one launch covers the mesh)
 };
 
 // Global index -> interior index under the physical boundary of that side.
@@ -723,12 +724,12 @@ __device__ __forceinline__ void fused_passthrough(const FusedArgs<S> &a, int b, 
 template <typename S, int NDIM, int RECON, int RIEMANN, bool MHD>
 __global__ void __launch_bounds__(FusedShape<NDIM, RECON, MHD>::NT) k_fused_stage(FusedArgs<S> a) {
   const int nbrick = a.nbr[0] * a.nbr[1] * a.nbr[2];
-  const int b = blockIdx.x / nbrick;
+  const int bl = blockIdx.x / nbrick, b = a.b0 + bl;
   if (a.clock->done) {
-    fused_passthrough<S, NDIM, RECON, MHD>(a, b, blockIdx.x - b * nbrick);
+    fused_passthrough<S, NDIM, RECON, MHD>(a, b, blockIdx.x - bl * nbrick);
     return;
   }
-  fused_brick<S, NDIM, RECON, RIEMANN, true, MHD>(a, b, blockIdx.x - b * nbrick, a.clock->dt);
+  fused_brick<S, NDIM, RECON, RIEMANN, true, MHD>(a, b, blockIdx.x - bl * nbrick, a.clock->dt);
 }
 
 // ---------------------------------------------------------------------------
@@ -833,6 +834,17 @@ int fused_launch(kmy_ctx *c, FusedArgs<S> a) {
     if (e != cudaSuccess) return cuda_check(c, e, "fused smem attribute");
     opted.fetch_or(bit);
   }
+  if (c->prm.per_block && !MHD) {
+    // one launch per meshblock, as a caller that steps blocks one at a time would
+    const int per = a.nbr[0] * a.nbr[1] * a.nbr[2];
+    for (int b = 0; b < m.nb; b++) {
+      a.b0 = b;
+      kern<<<unsigned(per), Sh::NT, smem, c->stream>>>(a);
+      c->launches++;
+    }
+    return cuda_check(c, cudaGetLastError(), "fused stage");
+  }
+  a.b0 = 0;
   kern<<<unsigned(grid), Sh::NT, smem, c->stream>>>(a);
   c->launches++;
   return cuda_check(c, cudaGetLastError(), "fused stage");

@@ -123,6 +123,9 @@ struct Params {
   int stage_kernel = 0;
   // rows per tile of the z-streamed stage: 0 auto, 8 or 16
   int slab_rows = 0;
+  // hydro brick stage launched once per meshblock instead of once per mesh
+  // (<kamayan_b200> launch = per_block; the plain per-block GPU baseline)
+  bool per_block = false;
   TimeParams tp{};
   std::map<std::string, std::string> deck;
   double real(const std::string &k, double d) const;

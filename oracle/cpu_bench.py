@@ -2,7 +2,10 @@
 
 Runs as its own process (``python -m oracle.cpu_bench``) so the oracle's
 OpenMP runtime never shares a process with CUDA or torch.  Prints one JSON
-object: cell-updates/s over the timed steps, the thread count and the sample.
+object: cell-updates/s over the timed steps, the thread count, the CPU model,
+the build and the sample.  ``--build native`` times the host-tuned build
+(-O3 -march=native, compiled on this machine first); ``parity`` the portable
+parity build.
 """
 from __future__ import annotations
 
@@ -19,6 +22,16 @@ from kamayan_b200 import configs  # noqa: E402
 from oracle import oracle  # noqa: E402
 
 
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="kh_3d")
@@ -29,9 +42,11 @@ def main() -> None:
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--min-seconds", type=float, default=0.0, help="keep stepping until this long")
     ap.add_argument("--max-steps", type=int, default=1000)
+    ap.add_argument("--build", choices=["native", "parity"], default="native")
     a = ap.parse_args()
     threads = a.threads or len(os.sched_getaffinity(0))
     os.environ["OMP_NUM_THREADS"] = str(threads)
+    oracle.use_native = a.build == "native"
     if a.workload == "kh_3d":
         deck, prob = configs.kh_3d(n=a.n, nb=a.nb), "kelvin_helmholtz"
     elif a.workload == "vortex_2d":
@@ -59,7 +74,9 @@ def main() -> None:
     a.steps = done
     cells = a.n ** ndim
     print(json.dumps({"value": updates / el, "unit": "cell-updates/s", "seconds": el,
-                      "steps": a.steps, "cells": cells, "threads": threads,
+                      "steps": a.steps, "cells": cells, "threads": threads, "cpu": cpu_model(),
+                      "build": ("-O3 -march=native -ffp-contract=off" if a.build == "native"
+                                else "-O3 -march=x86-64-v2 -ffp-contract=off"),
                       "sample": f"{a.workload} {a.n}^{ndim} in {a.nb}^{ndim} blocks, {a.steps} steps "
                                 f"after {a.warmup} warm-up"}))
 

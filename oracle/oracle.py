@@ -16,6 +16,27 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "libkmy_oracle.so"
+# the host-tuned timing build (oracle/Makefile target `native`), which
+# cpu_bench selects before the first load; the parity build otherwise.  It is
+# built per host CPU (model and flags) so a copy from another machine is never
+# loaded.
+use_native = False
+
+
+def _host_tag() -> str:
+    import hashlib
+
+    info = ""
+    try:
+        lines = Path("/proc/cpuinfo").read_text().splitlines()
+        info = "\n".join(sorted({ln for ln in lines if ln.startswith(("model name", "flags"))}))
+    except OSError:
+        pass
+    return hashlib.sha1(info.encode()).hexdigest()[:12]
+
+
+def native_lib() -> Path:
+    return HERE / "_build" / "native" / _host_tag() / "libkmy_oracle.so"
 
 RECON = {"fog": 0, "plm": 1, "ppm": 2, "wenoz": 3}
 LIMITER = {"minmod": 0, "van_leer": 1, "mc": 2}
@@ -31,12 +52,23 @@ def build() -> Path:
     return LIB
 
 
+def build_native() -> Path:
+    """Compile the host-tuned timing build (-march=native) for this machine."""
+    out = native_lib()
+    subprocess.run(["make", "-s", "-C", str(HERE), "native", f"NATIVE_DIR={out.parent}"], check=True)
+    return out
+
+
 def lib():
     global _lib
     if _lib is None:
-        if not LIB.exists():
-            build()
-        L = ctypes.CDLL(str(LIB))
+        if use_native:
+            path = build_native()
+        else:
+            if not LIB.exists():
+                build()
+            path = LIB
+        L = ctypes.CDLL(str(path))
         L.kmyo_create.restype = ctypes.c_void_p
         L.kmyo_create.argtypes = [ctypes.c_char_p]
         L.kmyo_destroy.argtypes = [ctypes.c_void_p]
