@@ -66,7 +66,7 @@ typedef struct {
  * Loehner tagging and a remesh after each step.
  * Replaces: InitEnv/InitPackages parameter setup (src/kamayan/kamayan.cpp:20-138),
  * hydro::SetupParams (src/physics/hydro/hydro.cpp:51-92),
- * grid::SetupParams (src/grid/grid.cpp:169-262),
+ * grid::SetupParams (src/grid/grid.cpp:29-122),
  * driver::SetupParams (src/driver/kamayan_driver.cpp:23-81). */
 int kmy_create(const char *deck, int device, kmy_ctx **out);
 int kmy_destroy(kmy_ctx *ctx);
@@ -112,7 +112,7 @@ int kmy_finalize_import(kmy_ctx *ctx);
 /* Device problem generators: "isentropic_vortex", "kelvin_helmholtz",
  * "orszag_tang", "blast", "sedov".  Problem parameters come from the deck.
  * Replaces: ProblemGenerator + MeshPostInitialization
- * (src/problems/isentropic_vortex.cpp:307-377, src/problems/sedov.cpp:104-143,
+ * (src/problems/isentropic_vortex.cpp:105-175, src/problems/sedov.cpp:104-143,
  *  src/physics/hydro/primconsflux.cpp:145-148, src/physics/material_properties/eos/eos.cpp:165-168). */
 int kmy_pgen(kmy_ctx *ctx, const char *problem);
 
@@ -121,9 +121,9 @@ int kmy_pgen(kmy_ctx *ctx, const char *problem);
 int kmy_compute_fluxes(kmy_ctx *ctx, const char *md0);
 /* hydro::AddFluxTasks -> CalculateEMF (src/physics/hydro/hydro_add_flux_tasks.cpp:405-442) */
 int kmy_compute_emf(kmy_ctx *ctx, const char *md0);
-/* grid::FluxesToDuDt (src/grid/grid.cpp:348-351; src/grid/grid_update.hpp:15-137) */
+/* grid::FluxesToDuDt (src/grid/grid.cpp:208-211; src/grid/grid_update.hpp:15-137) */
 int kmy_flux_divergence(kmy_ctx *ctx, const char *md0, const char *dudt);
-/* grid::ApplyDuDt (src/grid/grid.cpp:353-423) */
+/* grid::ApplyDuDt (src/grid/grid.cpp:213-283) */
 int kmy_apply_dudt(kmy_ctx *ctx, const char *base, const char *md0, const char *md1,
                    const char *dudt, double beta, double dt);
 /* hydro::PreparePrimitive + eos::PreparePrimitive (src/physics/hydro/primconsflux.cpp:152-155,

@@ -875,7 +875,7 @@ int kmy_task_stage(kmy_ctx *c, int stage, double dt) {
 // transverse field fluxes; the face update (edge EMFs, Stokes, ApplyDuDt in
 // one kernel per face direction) and the primitives (which need the new
 // cell-centred field) follow as separate kernels, in the order of the task
-// list (hydro_add_flux_tasks.cpp, grid.cpp:353-381, primconsflux.cpp:82-142).
+// list (hydro_add_flux_tasks.cpp, grid.cpp:213-241, primconsflux.cpp:82-142).
 static int fused_stage_ct(kmy_ctx *c, int stage) {
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());

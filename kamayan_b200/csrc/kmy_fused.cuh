@@ -17,7 +17,7 @@
 //
 // Arithmetic per cell/face is the same as the per-task kernels
 // (kmy_tasks.cu), which follow hydro_add_flux_tasks.cpp:36-264,
-// grid_update.hpp:15-57, grid.cpp:353-381, primconsflux.cpp:82-142 and
+// grid_update.hpp:15-57, grid.cpp:213-241, primconsflux.cpp:82-142 and
 // hydro_time_step.cpp:19-64.
 #pragma once
 

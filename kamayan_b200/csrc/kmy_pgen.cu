@@ -7,7 +7,7 @@
 //   sedov              src/problems/sedov.cpp:54-63, :75-103
 //   blast              src/problems/mhd_blast.cpp:52-64 (no field)
 //   kelvin_helmholtz   3D shear layer, v,w seeded per global cell (splitmix64)
-//   orszag_tang        3D Orszag-Tang with face B from A_z (isentropic_vortex.cpp:352-375 pattern)
+//   orszag_tang        3D Orszag-Tang with face B from A_z (isentropic_vortex.cpp:150-174 pattern)
 #include <cmath>
 #include <string>
 

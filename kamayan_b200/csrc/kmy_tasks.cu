@@ -518,7 +518,7 @@ int launch_flux_stokes(kmy_ctx *c, Container &md0, Container &dudt) {
 }
 
 // ---------------------------------------------------------------------------
-// ApplyDuDt_impl (grid.cpp:353-381): u0 <- beta*base + (1-beta)*u0 ; u1 <- u0 + beta*dt*du
+// ApplyDuDt_impl (grid.cpp:213-241): u0 <- beta*base + (1-beta)*u0 ; u1 <- u0 + beta*dt*du
 template <typename S>
 __global__ void k_apply_cells(MeshDesc m, const S *ub, const float *ublo, S *u0, float *u0lo,
                               S *u1, float *u1lo, const S *du, int ncc, double beta, double dt,

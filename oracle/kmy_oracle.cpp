@@ -1615,7 +1615,7 @@ void Sim::calc_emf(const std::string &md0name) {
 }
 
 // grid_update.hpp:15-57 (FluxDivergence) and :80-137 (FluxStokes) as wired by
-// grid.cpp:319-346.
+// grid.cpp:179-206.
 void Sim::fluxes_to_dudt(const std::string &md0name, const std::string &dudtname) {
   Container &c = C(md0name);
   Container &du = C(dudtname);
@@ -1985,7 +1985,7 @@ int Sim::pgen_cells(const std::string &problem) {
           pr(PPRES, b)[n] = pres;
         }
   if (ph.mhd) {
-    // face B from a vector potential (isentropic_vortex.cpp:352-375 pattern)
+    // face B from a vector potential (isentropic_vortex.cpp:150-174 pattern)
     const Real mhd_strength = deck.real("isentropic_vortex/mhd_strength", 1.0);
     auto Az = [&](Real x, Real y) {
       if (problem == "isentropic_vortex") {  // isentropic_vortex.hpp:140-144

@@ -3,7 +3,7 @@
 Pins the oracle with the reference's unit and regression tests:
 reconstruction exactness and symmetry (test_reconstruction.cpp:159-194), the
 ideal-gas EOS (test_eos.cpp:55-85), the per-method density-L1 thresholds of
-the vortex at 64^2, t=10 (tests/test_suites/reconstruction/reconstruction.py:188-198)
+the vortex at 64^2, t=10 (tests/test_suites/reconstruction/reconstruction.py:128-135)
 and the WENO-Z/RK2 convergence slope > 1.5
 (tests/test_suites/isentropic_vortex/isentropic_vortex.py:13-60).
 """
