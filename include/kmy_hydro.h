@@ -195,6 +195,19 @@ int kmy_vortex_error(kmy_ctx *ctx, int var, int comp, double *out);
  * interior of `md` times the cell volume: out[0..ncons-1]. */
 int kmy_conserved_sums(kmy_ctx *ctx, const char *md, double *out);
 
+/* Face values (vM at i-1/2, vP at i+1/2) of n five-cell stencils (stencils[5i
+ * .. 5i+4] = cells i-2 .. i+2) from the library's device reconstruction
+ * functions: out[3i] = vM, out[3i+1] = vP, out[3i+2] = 1 when the two lanes of
+ * a packed FP32 form disagreed (else 0).  impl selects the form each stage
+ * kernel uses: 0 FP64 per-task kernels, 1 FP64 brick stage (two-division
+ * WENO-Z), 2 FP32 per lane, 3 FP32 brick stage (packed), 4 FP32 z-streamed
+ * stage (packed).  Needs no context; runs on the current device and
+ * synchronises it.  Counterpart of the reference's device-side Reconstruct
+ * (src/physics/hydro/reconstruction.hpp:11-142) as its unit tests call it
+ * (src/physics/hydro/tests/test_reconstruction.cpp:13-194). */
+int kmy_reconstruct_stencils(const char *reconstruction, const char *slope_limiter, int impl,
+                             const double *stencils, int n, double *out);
+
 /* Number of this library's kernels launched on the context since creation. */
 int kmy_launch_count(const kmy_ctx *ctx, int64_t *out);
 /* Number of kmy_evolve chunks (or adaptive steps) that replayed a cached CUDA

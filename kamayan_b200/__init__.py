@@ -38,7 +38,7 @@ EXPORTS = (
     "kmy_zone_cycles",
     "kmy_get_blocks", "kmy_set_dt", "kmy_save_restart", "kmy_load_restart",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
-    "kmy_graph_replays", "kmy_autotune", "kmy_stage_kernel", "kmy_tune_key", "kmy_tune_cache_put",
+    "kmy_graph_replays", "kmy_reconstruct_stencils", "kmy_autotune", "kmy_stage_kernel", "kmy_tune_key", "kmy_tune_cache_put",
     "kmy_tune_cache_get", "kmy_tune_cache_clear", "kmy_tune_cache_save", "kmy_tune_cache_load",
     "kmy_conserved_sums_noalloc",
     "kmy_server_create", "kmy_server_destroy", "kmy_server_last_error", "kmy_server_submit",
@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
         L.kmy_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.kmy_zone_cycles.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.kmy_graph_replays.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.kmy_reconstruct_stencils.argtypes = [cp, cp, i, _dp, i, _dp]
         L.kmy_autotune.argtypes = [vp, i, ctypes.POINTER(TuneResult), i, ctypes.POINTER(i)]
         L.kmy_stage_kernel.argtypes = [vp, cp, sz]
         L.kmy_tune_key.argtypes = [cp, cp, sz]
@@ -515,3 +516,18 @@ def tune_cache_load(path: str) -> None:
     rc = lib().kmy_tune_cache_load(str(path).encode())
     if rc:
         raise KmyError(rc, f"kmy_tune_cache_load {path}")
+
+
+# ---- the device reconstruction functions on a batch of stencils --------------
+RECON_IMPLS = {"fp64_tasks": 0, "fp64_brick": 1, "fp32_lane": 2, "fp32_brick": 3, "fp32_slab": 4}
+
+
+def reconstruct_stencils(reconstruction: str, slope_limiter: str, impl: str, stencils) -> np.ndarray:
+    """(n, 3) array of (vM, vP, lanes-disagree flag) for n 5-cell stencils."""
+    st = np.ascontiguousarray(np.asarray(stencils, dtype=np.float64).reshape(-1, 5))
+    out = np.zeros((st.shape[0], 3))
+    rc = lib().kmy_reconstruct_stencils(reconstruction.encode(), slope_limiter.encode(), RECON_IMPLS[impl],
+                                        _ptr(st), st.shape[0], _ptr(out))
+    if rc:
+        raise KmyError(rc, "kmy_reconstruct_stencils")
+    return out

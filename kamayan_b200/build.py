@@ -34,6 +34,10 @@ EXTRA_FLAGS = {
     # same arithmetic as the single-mesh FP32 stage, so a solve gives the same
     # bits alone and inside a batch
     "kmy_batch_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+    # the z-streamed FP32 stage, and the device reconstruction functions as the
+    # FP32 stage kernels compile them
+    "kmy_slab_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+    "kmy_kat.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     # adaptive mesh: no FMA contraction, so prolongation, restriction and the
     # refinement estimator round exactly as written (tags are threshold tests)
     "kmy_amr.cu": ["-fmad=false"],
