@@ -26,7 +26,9 @@ typedef enum {
   KMY_ERR_NONFINITE = 3, /* NaN/inf or non-positive density/pressure detected */
   KMY_ERR_TIMEOUT = 4,   /* a bounded device wait gave up */
   KMY_ERR_CUDA = 5,      /* CUDA runtime error (see kmy_last_error) */
-  KMY_ERR_STATE = 6      /* call out of order (e.g. no state yet) */
+  KMY_ERR_STATE = 6,     /* call out of order (e.g. no state yet) */
+  KMY_ERR_DT_RANGE = 7   /* dt below dt_min for dt_min_cycle_limit cycles, or above dt_max for
+                            dt_max_cycle_limit (Parthenon's fatal, kamayan_driver.cpp:43-54) */
 } kmy_status;
 
 typedef struct kmy_ctx kmy_ctx;
@@ -54,8 +56,9 @@ typedef struct {
  * tlim, nlim, dt_*), <hydro> (reconstruction, slope_limiter, riemann, cfl,
  * ReconstructionVars, ReconstructionStrategy, EMF_averaging), <physics> (MHD),
  * <material/single> (gamma, Abar, eos_type), <eos> (mode_init), plus
- * <kamayan_b200> (precision = fp64|fp32).  Unknown option values fail with
- * KMY_ERR_BAD_PARAM.
+ * <kamayan_b200> (precision = fp64|fp32; stage_kernel = auto|brick|slab|tune;
+ * slab_rows = auto|8|16; launch = batched|per_block).  Unknown option values
+ * fail with KMY_ERR_BAD_PARAM.
  * Adaptive meshes (hydro and CT): <parthenon/mesh> refinement = adaptive, numlevel
  * (<= 8), derefine_count, and <kamayan/refinement0>, <kamayan/refinement1>, ...
  * blocks, each with field (dens|pres|ener), method = loehner, refine_tol,
@@ -102,6 +105,29 @@ int kmy_import_interior(kmy_ctx *ctx, const char *container, const char *var, in
                         const double *host, size_t n);
 int kmy_export_interior(kmy_ctx *ctx, const char *container, const char *var, int comp,
                         double *host, size_t n);
+/* In-place state on caller-owned device memory.  The reference's slots read
+ * and write the MeshData they are given (src/kamayan/unit.hpp:56-76,
+ * src/grid/grid.hpp:133-135); kmy_bind_container makes a caller's device
+ * arrays the storage of a named container, so every slot above and below
+ * (kmy_compute_fluxes, kmy_flux_divergence, kmy_apply_dudt, kmy_task_stage,
+ * kmy_rk_stage, kmy_step, ...) works on them directly, with no copies.
+ *   cons:    [ncons][nblocks][ncells_pad] of the context's precision (double, or
+ *            float with fp32), i fastest: each conserved component a contiguous
+ *            nblocks x prod(ncells_pad) array, components in the order dens,
+ *            momentum 0-2, ener (, magc 0-2); cons_bytes its size
+ *   ener_lo: fp32 only (else NULL/0): [nblocks][ncells_pad] floats, the low word
+ *            of the total energy (E = ener + ener_lo); zeros for an FP32 energy
+ *   mag:     CT only (else NULL/0): [3][nblocks][nfaces_pad] face field
+ * Arrays start on 16-byte boundaries.  The caller keeps them alive until
+ * kmy_destroy; the context's own arrays for the container are released.
+ * After writing bound arrays from outside, call kmy_finalize_import (ghosts,
+ * primitives, dt).  Single-level meshes only (an adaptive mesh reallocates its
+ * containers as it remeshes).  kmy_bind_primitives does the same for the
+ * primitives shared by all containers, [7][nblocks][ncells_pad] in the order
+ * velocity 0-2, pres, bulk modulus, eint, temp. */
+int kmy_bind_container(kmy_ctx *ctx, const char *container, void *cons, size_t cons_bytes,
+                       void *ener_lo, size_t ener_lo_bytes, void *mag, size_t mag_bytes);
+int kmy_bind_primitives(kmy_ctx *ctx, void *prim, size_t bytes);
 /* Mark imported state complete: prims of "base" are taken as given (as after
  * the reference's MeshPostInitialization) or, when no primitive variable was
  * imported since the last finalize, derived from the conserved state
@@ -210,6 +236,13 @@ int kmy_reconstruct_stencils(const char *reconstruction, const char *slope_limit
 
 /* Number of this library's kernels launched on the context since creation. */
 int kmy_launch_count(const kmy_ctx *ctx, int64_t *out);
+/* Failure-path test hook.  what = "stage_wait", value = 1: the next
+ * z-streamed stage's staged-pair barrier expects more bytes than its tensor
+ * loads deliver and its bounded wait is shortened, so the wait runs out; the
+ * stage stops, sets the device clock's status, and the step returns
+ * KMY_ERR_TIMEOUT.  Nothing faults or hangs; the CUDA context stays usable.
+ * No counterpart in the reference. */
+int kmy_set_fault(kmy_ctx *ctx, const char *what, int value);
 /* Number of kmy_evolve chunks (or adaptive steps) that replayed a cached CUDA
  * graph instead of launching their kernels one by one. */
 int kmy_graph_replays(const kmy_ctx *ctx, int64_t *out);

@@ -25,20 +25,21 @@ STATUS = {
     4: "TIMEOUT",
     5: "CUDA",
     6: "STATE",
+    7: "DT_RANGE",
 }
 
 # Every entry point declared in include/kmy_hydro.h.
 EXPORTS = (
     "kmy_create", "kmy_destroy", "kmy_last_error", "kmy_get_info", "kmy_set_stream", "kmy_sync",
     "kmy_import_var", "kmy_export_var", "kmy_import_interior", "kmy_export_interior",
-    "kmy_finalize_import", "kmy_pgen",
+    "kmy_finalize_import", "kmy_pgen", "kmy_bind_container", "kmy_bind_primitives",
     "kmy_compute_fluxes", "kmy_compute_emf", "kmy_flux_divergence", "kmy_apply_dudt",
     "kmy_prepare_primitive", "kmy_fill_ghosts", "kmy_estimate_dt", "kmy_fill_derived",
     "kmy_task_stage", "kmy_rk_stage", "kmy_step", "kmy_evolve", "kmy_end_step", "kmy_get_time",
     "kmy_zone_cycles",
     "kmy_get_blocks", "kmy_set_dt", "kmy_save_restart", "kmy_load_restart",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
-    "kmy_graph_replays", "kmy_reconstruct_stencils", "kmy_autotune", "kmy_stage_kernel", "kmy_tune_key", "kmy_tune_cache_put",
+    "kmy_graph_replays", "kmy_set_fault", "kmy_reconstruct_stencils", "kmy_autotune", "kmy_stage_kernel", "kmy_tune_key", "kmy_tune_cache_put",
     "kmy_tune_cache_get", "kmy_tune_cache_clear", "kmy_tune_cache_save", "kmy_tune_cache_load",
     "kmy_conserved_sums_noalloc",
     "kmy_server_create", "kmy_server_destroy", "kmy_server_last_error", "kmy_server_submit",
@@ -92,6 +93,8 @@ def lib() -> ctypes.CDLL:
         L.kmy_import_interior.argtypes = [vp, cp, cp, i, _dp, sz]
         L.kmy_export_interior.argtypes = [vp, cp, cp, i, _dp, sz]
         L.kmy_finalize_import.argtypes = [vp]
+        L.kmy_bind_container.argtypes = [vp, cp, vp, sz, vp, sz, vp, sz]
+        L.kmy_bind_primitives.argtypes = [vp, vp, sz]
         L.kmy_pgen.argtypes = [vp, cp]
         for n in ("kmy_compute_fluxes", "kmy_compute_emf", "kmy_prepare_primitive",
                   "kmy_fill_ghosts", "kmy_fill_derived"):
@@ -115,6 +118,7 @@ def lib() -> ctypes.CDLL:
         L.kmy_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.kmy_zone_cycles.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.kmy_graph_replays.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.kmy_set_fault.argtypes = [vp, cp, i]
         L.kmy_reconstruct_stencils.argtypes = [cp, cp, i, _dp, i, _dp]
         L.kmy_autotune.argtypes = [vp, i, ctypes.POINTER(TuneResult), i, ctypes.POINTER(i)]
         L.kmy_stage_kernel.argtypes = [vp, cp, sz]
@@ -275,6 +279,16 @@ class Solver:
         self._check(lib().kmy_export_interior(self._h, container.encode(), var.encode(), comp,
                                               ctypes.cast(ptr, _dp), n))
 
+    def bind_container(self, container: str, cons_ptr: int, cons_bytes: int, ener_lo_ptr: int = 0,
+                       ener_lo_bytes: int = 0, mag_ptr: int = 0, mag_bytes: int = 0) -> None:
+        """Make caller-owned device arrays the storage of a container (kmy_bind_container)."""
+        self._check(lib().kmy_bind_container(self._h, container.encode(), ctypes.c_void_p(cons_ptr), cons_bytes,
+                                             ctypes.c_void_p(ener_lo_ptr or None), ener_lo_bytes,
+                                             ctypes.c_void_p(mag_ptr or None), mag_bytes))
+
+    def bind_primitives(self, prim_ptr: int, nbytes: int) -> None:
+        self._check(lib().kmy_bind_primitives(self._h, ctypes.c_void_p(prim_ptr), nbytes))
+
     def finalize_import(self) -> None:
         self._check(lib().kmy_finalize_import(self._h))
 
@@ -376,6 +390,10 @@ class Solver:
         n = ctypes.c_int64()
         self._check(lib().kmy_launch_count(self._h, ctypes.byref(n)))
         return n.value
+
+    def set_fault(self, what: str, value: int = 1) -> None:
+        """Failure-path test hook (kmy_set_fault)."""
+        self._check(lib().kmy_set_fault(self._h, what.encode(), value))
 
     @property
     def graph_replays(self) -> int:

@@ -144,6 +144,12 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   p.tp.dt_ceil = p.real("parthenon/time/dt_ceil", big);
   p.tp.dt_user = p.real("parthenon/time/dt_user", big);
   p.tp.dt_floor = p.real("parthenon/time/dt_floor", std::numeric_limits<double>::min());
+  p.tp.dt_min = p.real("parthenon/time/dt_min", std::numeric_limits<double>::lowest());
+  p.tp.dt_max = p.real("parthenon/time/dt_max", std::numeric_limits<double>::max());
+  p.tp.dt_min_cycle_limit = p.integer("parthenon/time/dt_min_cycle_limit", 10);
+  p.tp.dt_max_cycle_limit = p.integer("parthenon/time/dt_max_cycle_limit", 1);
+  if (p.tp.dt_min_cycle_limit < 1 || p.tp.dt_max_cycle_limit < 1)
+    return bad("parthenon/time/dt_min_cycle_limit and dt_max_cycle_limit must be positive");
 
   const std::string refine = p.str("parthenon/mesh/refinement", "none");
   if (!one_of(refine, {"none", "static", "adaptive"})) return bad("parthenon/mesh/refinement");
@@ -897,6 +903,25 @@ static int fused_stage_ct(kmy_ctx *c, int stage) {
   return rc;
 }
 
+// rk1 stages write the scratch container "1" (the stage reads neighbouring
+// blocks of its input while it writes); "1" then becomes "base".  A base
+// bound to caller memory keeps its arrays: the result is copied into them.
+static int adopt_rk1_output(kmy_ctx *c) {
+  Container &base = c->md["base"], &out = c->md["1"];
+  if (!base.bound) {
+    std::swap(c->md["base"], c->md["1"]);
+    return KMY_OK;
+  }
+  const size_t n = size_t(c->m.nb) * c->m.P;
+  int rc = cuda_check(c, cudaMemcpyAsync(base.cc, out.cc, c->esz * c->ncc * n, cudaMemcpyDeviceToDevice, c->stream),
+                      "rk1 copy");
+  if (!rc && base.ener_lo)
+    rc = cuda_check(c, cudaMemcpyAsync(base.ener_lo, out.ener_lo, 4 * n, cudaMemcpyDeviceToDevice, c->stream),
+                    "rk1 copy");
+  base.ghosts = out.ghosts;
+  return rc;
+}
+
 // Whether the hydro stage runs the z-streamed kernel (kmy_slab_f32.cu): by
 // default wherever it applies (FP32, 3D, 32-cell rows), or as the deck's
 // <kamayan_b200> stage_kernel asks.
@@ -916,7 +941,7 @@ static int slab_stage(kmy_ctx *c, int stage) {
     if (!c->md.count("1") && make_container(c, "1")) return KMY_ERR_OOM;
     Container &base = c->md["base"], &out = c->md["1"];
     rc = launch_slab_stage(c, base, base, out, c->prm.beta[0], true);
-    if (!rc) std::swap(c->md["base"], c->md["1"]);
+    if (!rc) rc = adopt_rk1_output(c);
   } else {
     Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
     rc = launch_slab_stage(c, base, md0, md1, c->prm.beta[stage - 1], stage == ns);
@@ -950,8 +975,10 @@ static int fused_stage(kmy_ctx *c, int stage) {
   if (use_slab(c)) return slab_stage(c, stage);
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());
-  // FP32 stages keep their output's primitives (kmy_fused.cu)
-  const bool keep = c->esz == 4;
+  // FP32 stages keep their output's primitives (kmy_fused.cu) in a second
+  // buffer that swaps with the first; primitives bound to caller memory stay
+  // where they are, so there every stage converts its input instead
+  const bool keep = c->esz == 4 && !c->prim_bound;
   const bool stored = c->prims_valid || c->prims_interior;
   if (keep && !c->prim_alt && dalloc(c, &c->prim_alt, c->esz * NPRIM * size_t(c->m.nb) * c->m.P))
     return KMY_ERR_OOM;
@@ -964,7 +991,7 @@ static int fused_stage(kmy_ctx *c, int stage) {
     Container &base = c->md["base"], &out = c->md["1"];
     out.ghosts = false;
     rc = launch_fused_stage(c, base, base, out, c->prm.beta[0], stored, true);
-    if (!rc) std::swap(c->md["base"], c->md["1"]);
+    if (!rc) rc = adopt_rk1_output(c);
   } else {
     Container &base = c->md[nm[0]], &md0 = c->md[nm[stage - 1]], &md1 = c->md[nm[stage]];
     md1.ghosts = false;
@@ -1046,6 +1073,10 @@ static int clock_status(kmy_ctx *c, int status) {
     c->err = "a stage kernel's bounded wait for its staged tiles gave up";
     return KMY_ERR_TIMEOUT;
   }
+  if (status == KMY_ERR_DT_RANGE) {
+    c->err = "the time step stayed outside [dt_min, dt_max] for the cycle limit";
+    return KMY_ERR_DT_RANGE;
+  }
   c->err = "non-finite or non-positive time-step estimate";
   return KMY_ERR_NONFINITE;
 }
@@ -1090,9 +1121,9 @@ static std::string evolve_key(const kmy_ctx *c) {
   // the time parameters field by field (the struct's tail padding is not state)
   const TimeParams &tp = c->prm.tp;
   for (const double *d : {&tp.tlim, &tp.dt_factor, &tp.dt_init, &tp.dt_ceil, &tp.dt_user, &tp.dt_floor,
-                          &tp.cfl_over_ndim})
+                          &tp.cfl_over_ndim, &tp.dt_min, &tp.dt_max})
     add(d, sizeof(double));
-  add(&tp.nlim, sizeof(tp.nlim));
+  for (const int *i : {&tp.nlim, &tp.dt_min_cycle_limit, &tp.dt_max_cycle_limit}) add(i, sizeof(int));
   // the stage kernel (the tuner may change it after the first chunk)
   add(&c->prm.stage_kernel, sizeof(int));
   add(&c->prm.slab_rows, sizeof(int));
@@ -1264,6 +1295,81 @@ int kmy_conserved_sums(kmy_ctx *c, const char *md, double *out) {
   cudaSetDevice(c->device);
   KMY_CONTAINER(a, md);
   return launch_conserved_sums(c, *a, out);
+}
+
+static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int kmy_bind_container(kmy_ctx *c, const char *container, void *cons, size_t cons_bytes, void *ener_lo,
+                       size_t ener_lo_bytes, void *mag, size_t mag_bytes) {
+  if (!c || !container || !cons) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  if (c->amr.on) {
+    c->err = "an adaptive mesh reallocates its containers when it remeshes; bind a single-level mesh";
+    return KMY_ERR_BAD_PARAM;
+  }
+  const size_t n = size_t(c->m.nb) * c->m.P, nf = size_t(c->m.nb) * c->m.Pf;
+  const size_t want_cc = c->esz * c->ncc * n, want_lo = c->esz == 4 ? 4 * n : 0,
+               want_mag = c->prm.mhd ? c->esz * 3 * nf : 0;
+  if (cons_bytes != want_cc || ener_lo_bytes != (ener_lo ? want_lo : 0) || (want_lo && !ener_lo) ||
+      mag_bytes != (mag ? want_mag : 0) || (want_mag && !mag)) {
+    c->err = "bind sizes: conserved " + std::to_string(want_cc) + " bytes, energy low words " +
+             std::to_string(want_lo) + ", face field " + std::to_string(want_mag);
+    return KMY_ERR_BAD_PARAM;
+  }
+  if (!aligned16(cons) || (ener_lo && !aligned16(ener_lo)) || (mag && !aligned16(mag))) {
+    c->err = "bound arrays must start on a 16-byte boundary";
+    return KMY_ERR_BAD_PARAM;
+  }
+  Container *ct = find_container(c, container);
+  if (!ct) return KMY_ERR_BAD_PARAM;
+  // the context's own arrays for this container go back to the pool
+  if (!ct->bound) {
+    dfree(c, ct->cc);
+    dfree(c, ct->ener_lo);
+    dfree(c, ct->fc);
+  }
+  ct->cc = cons;
+  ct->ener_lo = ener_lo;
+  if (c->prm.mhd) ct->fc = mag;
+  ct->bound = true;
+  ct->ghosts = false;
+  c->prims_valid = false;
+  c->prims_interior = false;
+  if (c->evolve_exec) {
+    cudaGraphExecDestroy(c->evolve_exec);
+    c->evolve_exec = nullptr;
+  }
+  return KMY_OK;
+}
+
+int kmy_bind_primitives(kmy_ctx *c, void *prim, size_t bytes) {
+  if (!c || !prim) return KMY_ERR_BAD_PARAM;
+  cudaSetDevice(c->device);
+  const size_t want = c->esz * NPRIM * size_t(c->m.nb) * c->m.P;
+  if (c->amr.on || bytes != want || !aligned16(prim)) {
+    c->err = "bind primitives: " + std::to_string(want) + " bytes, 16-byte aligned, single-level mesh";
+    return KMY_ERR_BAD_PARAM;
+  }
+  if (!c->prim_bound) dfree(c, c->prim);
+  c->prim = prim;
+  c->prim_bound = true;
+  c->prims_valid = false;
+  c->prims_interior = false;
+  return KMY_OK;
+}
+
+int kmy_set_fault(kmy_ctx *c, const char *what, int value) {
+  if (!c || !what) return KMY_ERR_BAD_PARAM;
+  if (std::string(what) == "stage_wait") {
+    if (slab_unsupported(c)) {
+      c->err = "stage_wait applies to the z-streamed stage";
+      return KMY_ERR_BAD_PARAM;
+    }
+    c->fault_wait = value ? 1 : 0;
+    return KMY_OK;
+  }
+  c->err = std::string("unknown fault ") + what;
+  return KMY_ERR_BAD_PARAM;
 }
 
 int kmy_graph_replays(const kmy_ctx *c, int64_t *out) {

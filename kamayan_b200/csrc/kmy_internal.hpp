@@ -77,14 +77,22 @@ struct DevClock {
   unsigned long long dtmin_bits;  // atomic min of dx/(|v|+c) (bit pattern of a positive double)
   int ncycle;
   int done;         // time >= tlim: stage kernels become no-ops
-  int status;       // KMY_ERR_NONFINITE when the estimate was not finite/positive
+  int status;       // KMY_ERR_NONFINITE when the estimate was not finite/positive,
+                    // KMY_ERR_DT_RANGE when dt left [dt_min, dt_max] too long,
+                    // KMY_ERR_TIMEOUT when a stage kernel's bounded wait gave up
   unsigned long long zone_cycles;  // interior cells x completed steps, summed over the steps
+  int below_min;    // consecutive cycles with dt < dt_min
+  int above_max;    // consecutive cycles with dt > dt_max
 };
 
 struct TimeParams {
   double tlim, dt_factor, dt_init, dt_ceil, dt_user, dt_floor;
   double cfl_over_ndim;
+  // Parthenon's dt sanity limits: a dt below dt_min for dt_min_cycle_limit
+  // cycles (or above dt_max for dt_max_cycle_limit) ends the run
+  double dt_min, dt_max;
   int nlim;
+  int dt_min_cycle_limit, dt_max_cycle_limit;
 };
 
 // Parthenon EvolutionDriver time update + SetGlobalTimeStep after a step,
@@ -99,7 +107,9 @@ __device__ __forceinline__ void advance_clock(DevClock *clk, const TimeParams &t
   clk->ncycle += 1;
   const double est = dtmin * tp.cfl_over_ndim;
   clk->dt_est = est;
-  if (!(est > 0.0) || !(est < big)) clk->status = 3;  // KMY_ERR_NONFINITE
+  // the first failure stays: a stage that stopped early (a wait that ran
+  // out) leaves no estimate, which is not the cause to report
+  if (clk->status == 0 && (!(est > 0.0) || !(est < big))) clk->status = 3;  // KMY_ERR_NONFINITE
   double nd = clk->dt;
   if (nd < 0.1 * big) nd *= tp.dt_factor;
   nd = fmin(nd, est);
@@ -108,6 +118,13 @@ __device__ __forceinline__ void advance_clock(DevClock *clk, const TimeParams &t
   if (clk->time < tp.tlim && (tp.tlim - clk->time) < nd) nd = tp.tlim - clk->time;
   clk->dt = nd;
   clk->done = clk->time >= tp.tlim;
+  // the dt sanity limits (the reference's parthenon/time dt_min, dt_max and
+  // their cycle limits, src/driver/kamayan_driver.cpp:43-54): the step that
+  // was just taken counts
+  clk->below_min = clk->dt_taken < tp.dt_min ? clk->below_min + 1 : 0;
+  clk->above_max = clk->dt_taken > tp.dt_max ? clk->above_max + 1 : 0;
+  if (clk->status == 0 && (clk->below_min >= tp.dt_min_cycle_limit || clk->above_max >= tp.dt_max_cycle_limit))
+    clk->status = 7;  // KMY_ERR_DT_RANGE
 }
 
 struct Params {
@@ -142,6 +159,8 @@ struct Container {
   // a ghost fill or a z-streamed stage that wrote this container, cleared by
   // every other writer); the z-streamed stage stages its input through them
   bool ghosts = false;
+  // the arrays are the caller's (kmy_bind_container): never freed or moved
+  bool bound = false;
 };
 
 // Host side of an adaptive mesh: the leaf list and the refinement parameters.
@@ -199,6 +218,7 @@ struct kmy_ctx {
   void *prim_alt = nullptr;
   bool prims_interior = false;  // `prim` holds the interior primitives of "base" (ghosts stale)
   bool prims_imported = false;  // a primitive was imported since the last finalize
+  bool prim_bound = false;      // `prim` is the caller's (kmy_bind_primitives): never swapped or freed
   void *flux = nullptr;   // [3][ncc][nb][Pf] face fluxes (S), shared by all containers
   double *divb = nullptr; // [nb][P]
   kmy::DevClock *clock = nullptr;  // device
@@ -213,6 +233,7 @@ struct kmy_ctx {
   std::string evolve_key, evolve_seen;
   int64_t evolve_launches = 0;
   int64_t graph_replays = 0;  // launches of a cached graph (kmy_graph_replays)
+  int fault_wait = 0;  // kmy_set_fault "stage_wait": the next z-streamed stage's waits run out
   // pinned host staging for the per-step reads (clock, tags), grown on demand
   void *h_pin = nullptr;
   size_t h_pin_bytes = 0;

@@ -94,6 +94,11 @@ struct Args {
   int rgroup;        // padded rows per TMA row group (row stride x rgroup is a multiple of 16 bytes)
   int nty;           // tiles per block along y
   int nitems;        // blocks x tiles
+  // the staged-pair wait: iterations of mbarrier.try_wait before it gives up,
+  // and extra bytes the barrier expects beyond what the loads deliver (0; a
+  // test sets it, with a short limit, to make the wait run out)
+  int wait_limit;
+  unsigned tx_extra;
 };
 
 // Shared-memory plan (bytes), the same on host and device: one raw slot (the
@@ -137,9 +142,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
                : "memory");
 }
 // Bounded wait for the phase of the given parity: false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int limit) {
   const uint32_t a = smem_u32(bar);
-  for (int it = 0; it < (1 << 22); it++) {
+  for (int it = 0; it < limit; it++) {
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -482,7 +487,7 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
     auto issue = [&](int pair) {
       if (tid == 0) {
         fence_proxy_async();
-        mbar_expect_tx(&bar[0], unsigned(L.tx_bytes()));
+        mbar_expect_tx(&bar[0], unsigned(L.tx_bytes()) + a.tx_extra);
         tma_load_4d(rawcc, &tm_cc, 0, row0 / a.rgroup, zc0 + 2 * pair, 0, &bar[0]);
         tma_load_3d(rawlo, &tm_lo, 0, row0 / a.rgroup, zc0 + 2 * pair, &bar[0]);
       }
@@ -490,13 +495,13 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
     // thread 0's bounded wait for the pair; the CTA reads the outcome after its
     // next barrier and then acquires the pair with a wait that returns at once
     auto wait_start = [&]() {
-      if (tid == 0) *flag = mbar_wait(&bar[0], phase) ? 0 : 1;
+      if (tid == 0) *flag = mbar_wait(&bar[0], phase, a.wait_limit) ? 0 : 1;
     };
     auto wait_finish = [&]() -> bool {
       const unsigned par = phase;
       phase ^= 1u;
       if (*flag) return false;
-      mbar_wait(&bar[0], par);
+      mbar_wait(&bar[0], par, a.wait_limit);
       return true;
     };
     // own column of a pair -> primitives (float2 over the two planes)

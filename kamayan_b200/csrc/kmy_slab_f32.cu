@@ -154,6 +154,14 @@ int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md
   a.rgroup = row_group(m.np[0]);
   a.nty = m.nx[1] / ty;
   a.nitems = m.nb * a.nty;
+  a.wait_limit = 1 << 22;
+  a.tx_extra = 0;
+  if (c->fault_wait) {
+    // kmy_set_fault(ctx, "stage_wait", 1): this stage's waits run out
+    a.tx_extra = 16;
+    a.wait_limit = 1 << 10;
+    c->fault_wait = 0;
+  }
   const int ctas = ty == 8 ? slab::Tile<8>::CTAS : slab::Tile<16>::CTAS;
   const int grid = std::min(a.nitems, sm_count(c->device) * ctas);
   const size_t smem = size_t(ty == 8 ? slab::Smem<8>(m.np[0]).total() : slab::Smem<16>(m.np[0]).total());

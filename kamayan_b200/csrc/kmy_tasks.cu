@@ -957,6 +957,8 @@ __global__ void k_dt_controller(DevClock *clk, TimeParams tp, int mode, long lon
     clk->dt = big;
     clk->dt_taken = 0.0;
     clk->status = 0;
+    clk->below_min = 0;
+    clk->above_max = 0;
   }
   const double est = dtmin * tp.cfl_over_ndim;
   clk->dt_est = est;
