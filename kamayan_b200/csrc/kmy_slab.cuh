@@ -177,7 +177,8 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
 
 // ---------------------------------------------------------------------------
 // Packed FP32 helpers.
-__device__ __forceinline__ float2 psub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+// a - b as one packed FMA, a + (-1) b
+__device__ __forceinline__ float2 psub2(float2 a, float2 b) { return __ffma2_rn(make_float2(-1.f, -1.f), b, a); }
 __device__ __forceinline__ float rsqrt_approx(float x) {
   float r;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -197,7 +198,9 @@ __device__ __forceinline__ float exp_scale(float x) {
 //    ratios tau / (eps + beta_k) unchanged up to eps;
 //  * each ratio takes one reciprocal and is capped at 1e15 so its square
 //    stays finite in FP32: at that ratio the stencil already holds the whole
-//    weight.
+//    weight.  The clamps run on the ALU pipe, which the stage leaves mostly
+//    idle; an eps scaled to the indicators (no clamps) cost five more
+//    FMA-pipe operations per pair and measured slower.
 __device__ __forceinline__ void WenoZPair(const float2 (&s)[5], float2 &vM, float2 &vP) {
   const float2 a = s[0], b = s[1], c = s[2], d = s[3], e = s[4];
   const float2 m2 = p2(-2.f), m4 = p2(-4.f);
@@ -461,6 +464,9 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
     const int zc0 = b * m.np[2] + m.g[2];  // tensor plane coordinate of interior plane 0
     // this thread's column: interior (x, y) = (lane, oy + wr)
     const long long col = (long long)b * m.P + (long long)(oy + wr + m.g[1]) * np0 + (lane + gx);
+    // whether the column lies within g of an x or y block face (its cells fill face ghosts)
+    const bool px = lane < gx || lane >= NX - gx;
+    const bool py = oy + wr < m.g[1] || oy + wr >= m.nx[1] - m.g[1];
 
     if (done) {
       // a stage queued after the run reached tlim leaves the state as it is
@@ -685,9 +691,15 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
             a.u1[v * NP + n[h]] = gv.v[v];
           }
           a.u1lo[n[h]] = gv.lo;
-          const int pc[3] = {lane + gx, oy + wr + m.g[1], zlo + h + m.g[2]};
-#pragma unroll
-          for (int d = 0; d < 3; d++) ghost_push_axis(a, d, b, lb, pc, gv);
+          // face ghosts: only where the cell lies within g of a block face
+          const int z = zlo + h;
+          const bool pz = z < m.g[2] || z >= nz - m.g[2];
+          if (px | py | pz) {
+            const int pc[3] = {lane + gx, oy + wr + m.g[1], z + m.g[2]};
+            if (px) ghost_push_axis(a, 0, b, lb, pc, gv);
+            if (py) ghost_push_axis(a, 1, b, lb, pc, gv);
+            if (pz) ghost_push_axis(a, 2, b, lb, pc, gv);
+          }
           if (a.last) {
             float V[NV];
             slab_prim(a.gm1, gv.v[0], gv.v[1], gv.v[2], gv.v[3], gv.v[4], gv.lo, V);
