@@ -406,20 +406,49 @@ def workloads_block(a, device: int, stream) -> dict:
         ms, upd, steps = _evolve_run(s, stream, nlim=max(3, a.steps // 4))
         ot[path] = (upd / (ms / 1e3), steps, ms / steps, float(abs(s.interior(s.export("divb"))).max()))
         s.close()
+    # the same solve to t = 0.5 (the configuration's end time) in FP32 and in
+    # FP64: the FP32 run's L1 against FP64 and its div B at t_end
+    t_end = {}
+    for prec in ("fp32", "fp64"):
+        s = solver(configs.ot_3d(n=n3, nb=32, precision=prec), "orszag_tang", "fused")
+        ms, upd, steps = _evolve_run(s, stream, tlim=0.5)
+        t_end[prec] = (upd / (ms / 1e3), steps, ms / 1e3, s.time["time"],
+                       {v: s.interior(s.export(v, c)) for v, c in (("dens", 0), ("ener", 0), ("magc", 0))},
+                       float(abs(s.interior(s.export("divb"))).max()))
+        s.close()
+    l1_ot = {v: float(abs(t_end["fp32"][4][v] - t_end["fp64"][4][v]).sum() / abs(t_end["fp64"][4][v]).sum())
+             for v in t_end["fp64"][4]}
     out["orszag_tang_3d_ct_fp32"] = {
         "cell_updates_per_s": ot["fused"][0], "steps": ot["fused"][1], "ms_per_step": ot["fused"][2],
         "max_abs_divb": ot["fused"][3],
         "tasks_cell_updates_per_s": ot["tasks"][0], "tasks_ms_per_step": ot["tasks"][2],
+        "to_t_end": {"t_end": t_end["fp32"][3], "steps": t_end["fp32"][1], "seconds_fp32": t_end["fp32"][2],
+                     "cell_updates_per_s_fp32": t_end["fp32"][0], "seconds_fp64": t_end["fp64"][2],
+                     "cell_updates_per_s_fp64": t_end["fp64"][0], "l1_fp32_vs_fp64": l1_ot,
+                     "max_abs_divb_fp32": t_end["fp32"][5], "max_abs_divb_fp64": t_end["fp64"][5]},
         "config": f"{n3}^3 in 32^3 blocks, g=4, CT, PPM(MC)+HLL, RK2, CFL 0.3, fused stage"}
-    # c4: blast on an adaptive mesh, 128^2 base in 16^2 blocks, 3 levels, Loehner on density
-    s = solver(configs.blast_2d_amr(), "blast", "tasks")
-    nb0 = s.nblocks
-    ms, upd, steps = _evolve_run(s, stream, tlim=0.2)
-    out["blast_2d_amr_fp64"] = {
-        "cell_updates_per_s": upd / (ms / 1e3), "steps": steps, "seconds": ms / 1e3,
-        "blocks_initial": nb0, "blocks_final": s.nblocks,
-        "config": "128^2 base in 16^2 blocks, 3 levels, Loehner dens 0.3/0.05, PLM(MC)+HLLC, RK2, t=0.2"}
-    s.close()
+    # c4: blast on an adaptive mesh, 128^2 base in 16^2 blocks, 3 levels,
+    # Loehner on density, to t = 0.2, in FP64 and FP32
+    amr = {}
+    for prec in ("fp64", "fp32"):
+        s = solver(configs.blast_2d_amr(precision=prec), "blast", "tasks")
+        nb0 = s.nblocks
+        ms, upd, steps = _evolve_run(s, stream, tlim=0.2)
+        amr[prec] = {"cell_updates_per_s": upd / (ms / 1e3), "steps": steps, "seconds": ms / 1e3,
+                     "blocks_initial": nb0, "blocks_final": s.nblocks, "leaves": s.blocks(),
+                     "dens": s.interior(s.export("dens"))}
+        s.close()
+    a64, a32 = amr["fp64"], amr["fp32"]
+    same = (a64["leaves"][0].shape == a32["leaves"][0].shape and bool((a64["leaves"][0] == a32["leaves"][0]).all())
+            and bool((a64["leaves"][1] == a32["leaves"][1]).all()))
+    out["blast_2d_amr_fp64"] = {k: v for k, v in a64.items() if k not in ("leaves", "dens")}
+    out["blast_2d_amr_fp64"]["config"] = \
+        "128^2 base in 16^2 blocks, 3 levels, Loehner dens 0.3/0.05, PLM(MC)+HLLC, RK2, t=0.2"
+    out["blast_2d_amr_fp64"]["fp32"] = {
+        "cell_updates_per_s": a32["cell_updates_per_s"], "steps": a32["steps"], "blocks_final": a32["blocks_final"],
+        "same_leaves_as_fp64": same,
+        "l1_density_vs_fp64": (float(abs(a32["dens"] - a64["dens"]).sum() / abs(a64["dens"]).sum())
+                               if same else None)}
     return out
 
 
