@@ -226,8 +226,8 @@ int kmy_conserved_sums(kmy_ctx *ctx, const char *md, double *out);
  * functions: out[3i] = vM, out[3i+1] = vP, out[3i+2] = 1 when the two lanes of
  * a packed FP32 form disagreed (else 0).  impl selects the form each stage
  * kernel uses: 0 FP64 per-task kernels, 1 FP64 brick stage (two-division
- * WENO-Z), 2 FP32 per lane, 3 FP32 brick stage (packed), 4 FP32 z-streamed
- * stage (packed).  Needs no context; runs on the current device and
+ * WENO-Z; also the FP64 z-streamed stage, lane by lane), 2 FP32 per lane,
+ * 3 FP32 brick stage (packed), 4 FP32 z-streamed stage (packed).  Needs no context; runs on the current device and
  * synchronises it.  Counterpart of the reference's device-side Reconstruct
  * (src/physics/hydro/reconstruction.hpp:11-142) as its unit tests call it
  * (src/physics/hydro/tests/test_reconstruction.cpp:13-194). */
@@ -251,8 +251,8 @@ int kmy_graph_replays(const kmy_ctx *ctx, int64_t *out);
  * The reference chooses its flux loop strategy by a runtime parameter
  * (<hydro> ReconstructionStrategy, src/physics/hydro/hydro.cpp:75-79).  Here
  * the stage kernel is chosen by measurement: "brick" (brick-tiled fused
- * stage), "slab16" / "slab8" (z-streamed FP32 3D stage with TMA-staged plane
- * pairs, tiles of 16 or 8 rows).  kmy_autotune times every candidate that
+ * stage), "slab16" / "slab8" (z-streamed 3D stage with TMA-staged plane
+ * pairs, tiles of 16 or 8 rows; FP64 runs 8 only).  kmy_autotune times every candidate that
  * applies to the context on its current state (stage 1 into a scratch
  * container, so the solve does not advance), applies the fastest and caches
  * it under (device name, configuration key).  The deck option

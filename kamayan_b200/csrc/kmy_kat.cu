@@ -8,7 +8,7 @@
 // exactness and left/right mirror symmetry) pin the CUDA code, not only the
 // CPU restatement:
 //   impl 0  FP64 Reconstruct                   (per-task kernels, k_face_flux)
-//   impl 1  FP64 two-division WENO-Z           (FP64 brick stage)
+//   impl 1  FP64 two-division WENO-Z           (FP64 brick and z-streamed stages)
 //   impl 2  FP32 Reconstruct                   (per-lane FP32 path)
 //   impl 3  FP32 packed WenoZBoth2 / per lane  (FP32 brick stage)
 //   impl 4  FP32 packed WenoZPair / per lane   (z-streamed FP32 stage)

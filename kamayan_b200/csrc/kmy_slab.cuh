@@ -1,30 +1,32 @@
-// kmy_slab.cuh -- one RK stage of 3D hydro in FP32, streamed through each
-// meshblock along z with TMA-staged plane pairs.
+// kmy_slab.cuh -- one RK stage of 3D hydro, streamed through each meshblock
+// along z with TMA-staged plane pairs, in FP32 or FP64.
 //
 // Work item: one meshblock b and one tile of TY rows (y) by the block's full
 // 32-cell width (x).  A persistent grid strides over the (block, tile) work
-// list: TY = 16 runs one CTA of 512 threads per SM, TY = 8 two CTAs of 256
-// (they fill each other's barrier waits; the staged halo rows cost more).
-// Thread t owns the column
-// (x = t % 32, y = oy + t / 32) and walks it along z two planes at a time, so
-// every FP32 operation of the z sweep works on a float2 of planes (k, k+1)
-// (sm_100's FADD2/FMUL2/FFMA2 issue one instruction for both lanes).
+// list: in FP32, TY = 16 runs one CTA of 512 threads per SM, TY = 8 two CTAs
+// of 256 (they fill each other's barrier waits; the staged halo rows cost
+// more); in FP64 (twice the shared memory per cell) TY = 8 runs one CTA of
+// 256 per SM.  Thread t owns the column (x = t % 32, y = oy + t / 32) and
+// walks it along z two planes at a time: every operation of the z sweep works
+// on a pair of planes (k, k+1).  In FP32 the pair is a float2 and sm_100's
+// FADD2/FMUL2/FFMA2 issue one instruction for both lanes; in FP64 it is a
+// double2 worked lane by lane (two independent dependency chains per thread).
 //
-// Per plane pair, the stage input (5 conserved components and the energy's
-// low word) arrives in shared memory by two cp.async.bulk.tensor loads of
-// the ghost-padded block: a box of 22 rows x the padded row x 2 planes, so
-// the x and y halos are the block's own ghost zones.  The previous stage's
-// epilogue keeps those current (it writes every cell it updates into the
-// face ghosts that hold it, periodic, outflow or reflect as Parthenon's
+// Per plane pair, the stage input (5 conserved components, and in FP32 the
+// energy's low word) arrives in shared memory by cp.async.bulk.tensor loads
+// of the ghost-padded block: a box of TY + 6 rows x the padded row x 2
+// planes, so the x and y halos are the block's own ghost zones.  The previous
+// stage's epilogue keeps those current (it writes every cell it updates into
+// the face ghosts that hold it, periodic, outflow or reflect as Parthenon's
 // boundary exchange would).  The loads of the next pair are issued as soon as
 // the raw slot is converted and land while the CTA works on the current pair
 // (one mbarrier, bounded waits); the staging costs no per-cell address
 // arithmetic.
 //
 // Per pair the CTA then
-//   1. converts the pair to primitives (rho, v, P, e_int; e_int = E - e_kin in
-//      FP64 from the hi/lo energy) into an interleaved float2 buffer, the
-//      thread's own column straight into its z window in registers;
+//   1. converts the pair to primitives (rho, v, P, e_int; in FP32 e_int =
+//      E - e_kin in FP64 from the hi/lo energy) into an interleaved pair
+//      buffer, the thread's own column straight into its z window in registers;
 //   2. x and y sweeps: reconstruction of every (primitive, cell) into shared
 //      memory, then the Riemann flux of every face, then the divergence of the
 //      thread's own two cells, accumulated in registers;
@@ -41,9 +43,11 @@
 //
 // Arithmetic follows the reference expressions (reconstruction.hpp:11-142,
 // riemann_solver.hpp:15-149, primconsflux.hpp:55-138, grid_update.hpp:15-57,
-// grid.cpp:213-283, hydro_time_step.cpp:19-64) in FP32, with the
-// rearrangements documented at each function; the FP32 path is checked
-// against FP64 by its density L1 error.
+// grid.cpp:213-283, hydro_time_step.cpp:19-64).  FP64 calls the per-cell
+// device functions of the other FP64 stages (Reconstruct, WenoZBothTwoDiv,
+// RiemannFlux, Cons2PrimEos) lane by lane and is checked against the oracle;
+// FP32 uses the packed rearrangements documented at each function and is
+// checked against FP64 by its density L1 error.
 #pragma once
 
 #include <cuda.h>
@@ -54,6 +58,12 @@
 #include "kmy_internal.hpp"
 
 namespace kmy {
+
+// Pair arithmetic on double2, lane by lane (the float2 forms are packed
+// instructions, kmy_device.cuh).
+__device__ __forceinline__ double2 padd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 pmul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+
 namespace slab {
 
 constexpr int NX = 32;            // interior cells along x (one warp per row)
@@ -63,30 +73,38 @@ constexpr int NV = 6;             // reconstructed: rho, v0, v1, v2, P, e_int
 constexpr int NCV = 5;            // conserved components
 enum : int { SD = 0, SV0 = 1, SPRES = 4, SEINT = 5 };
 
-// Tile of TY rows (16: one CTA of 512 threads per SM; 8: two CTAs of 256).
+// Pair of two planes' values: packed FP32, or FP64 worked lane by lane.
+template <typename R> struct PairOf;
+template <> struct PairOf<float> { using T = float2; };
+template <> struct PairOf<double> { using T = double2; };
+
+// Tile of TY rows.  FP32: 16 (one CTA of 512 threads per SM) or 8 (two CTAs
+// of 256); FP64: 8 (one CTA of 256).
 // x sweep: reconstruction cells -1 .. 32 (34) per row, 33 faces per row;
 // y sweep: cells -1 .. TY (TY + 2) per column, TY + 1 faces per column.
-template <int TY_>
+template <int TY_, typename R>
 struct Tile {
   static constexpr int TY = TY_;
   static constexpr int NT = NX * TY;      // threads, one column each
   static constexpr int PR = TY + 2 * HH;  // staged rows
-  static constexpr int CTAS = TY == 8 ? 2 : 1;  // CTAs per SM the plan is sized for
+  static constexpr int CTAS = (TY == 8 && sizeof(R) == 4) ? 2 : 1;  // CTAs per SM the plan is sized for
   static constexpr int RXC = NX + 2, RYC = TY + 2;
-  static constexpr int REC_N = RXC * TY > RYC * NX ? RXC * TY : RYC * NX;  // float2 per variable and side
+  static constexpr int REC_N = RXC * TY > RYC * NX ? RXC * TY : RYC * NX;  // pairs per variable and side
   static constexpr int FX_N = (NX + 1) * TY, FY_N = NX * (TY + 1);
-  static constexpr int FLX_N = FX_N > FY_N ? FX_N : FY_N;                  // float2 per component
+  static constexpr int FLX_N = FX_N > FY_N ? FX_N : FY_N;                  // pairs per component
 };
 
+template <typename R>
 struct Args {
   MeshDesc m;
-  float gm1, gam;
+  EosParams eos;     // the FP64 conversion (Cons2PrimEos)
+  R gm1, gam;
   int limiter;
-  const float *u0;   // stage input (its interior cells feed the update)
-  const float *u0lo;
-  const float *ub;   // "base" container of the low-storage scheme
+  const R *u0;       // stage input (its interior cells feed the update)
+  const float *u0lo; // FP32: energy low words (null in FP64)
+  const R *ub;       // "base" container of the low-storage scheme
   const float *ublo;
-  float *u1;         // stage output (interior and face ghosts)
+  R *u1;             // stage output (interior and face ghosts)
   float *u1lo;
   int last;          // last stage: CFL estimate into the device clock
   double beta;
@@ -105,27 +123,30 @@ struct Args {
 // stage input of one plane pair as the tensor loads deliver it), the
 // interleaved primitives of the centre pair, the reconstructed face values
 // and the face fluxes of one sweep, the mbarrier and reduction scratch.
-template <int TY>
+template <int TY, typename R>
 struct Smem {
-  using T = Tile<TY>;
+  using T = Tile<TY, R>;
+  static constexpr int ES = int(sizeof(R));      // bytes per staged value
+  static constexpr int PS = 2 * int(sizeof(R));  // bytes per pair
+  static constexpr bool LO = sizeof(R) == 4;     // FP32 stages the energy low words too
   int np0;
   __host__ __device__ explicit Smem(int np0_) : np0(np0_) {}
   __host__ __device__ static constexpr int rup(int x) { return (x + 127) & ~127; }
-  __host__ __device__ int raw_plane() const { return T::PR * np0; }           // floats
-  __host__ __device__ int raw_var() const { return 2 * raw_plane(); }         // floats
-  __host__ __device__ int cc_bytes() const { return NCV * raw_var() * 4; }
+  __host__ __device__ int raw_plane() const { return T::PR * np0; }           // values
+  __host__ __device__ int raw_var() const { return 2 * raw_plane(); }         // values
+  __host__ __device__ int cc_bytes() const { return NCV * raw_var() * ES; }
   __host__ __device__ int lo_off() const { return rup(cc_bytes()); }
-  __host__ __device__ int lo_bytes() const { return raw_var() * 4; }
+  __host__ __device__ int lo_bytes() const { return LO ? raw_var() * 4 : 0; }
   __host__ __device__ int slot_bytes() const { return rup(lo_off() + lo_bytes()); }
   __host__ __device__ int prim_off() const { return slot_bytes(); }
-  __host__ __device__ static constexpr int prim_bytes() { return NV * T::PR * PC * 8; }
+  __host__ __device__ static constexpr int prim_bytes() { return NV * T::PR * PC * PS; }
   __host__ __device__ int rec_off() const { return prim_off() + prim_bytes(); }
-  __host__ __device__ static constexpr int rec_bytes() { return 2 * NV * T::REC_N * 8; }
+  __host__ __device__ static constexpr int rec_bytes() { return 2 * NV * T::REC_N * PS; }
   __host__ __device__ int flx_off() const { return rec_off() + rec_bytes(); }
-  __host__ __device__ static constexpr int flx_bytes() { return NCV * T::FLX_N * 8; }
+  __host__ __device__ static constexpr int flx_bytes() { return NCV * T::FLX_N * PS; }
   __host__ __device__ int bar_off() const { return flx_off() + flx_bytes(); }
   __host__ __device__ int total() const { return bar_off() + 256; }
-  // bytes one plane pair brings in (both tensor loads)
+  // bytes one plane pair brings in (all tensor loads)
   __host__ __device__ int tx_bytes() const { return cc_bytes() + lo_bytes(); }
 };
 
@@ -176,9 +197,13 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
 }
 
 // ---------------------------------------------------------------------------
-// Packed FP32 helpers.
-// a - b as one packed FMA, a + (-1) b
+// Pair helpers.
+// a - b; in FP32 one packed FMA, a + (-1) b
 __device__ __forceinline__ float2 psub2(float2 a, float2 b) { return __ffma2_rn(make_float2(-1.f, -1.f), b, a); }
+__device__ __forceinline__ double2 psub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
+template <typename R> __device__ __forceinline__ typename PairOf<R>::T splat(R a) { return mk2(a, a); }
 __device__ __forceinline__ float rsqrt_approx(float x) {
   float r;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -250,6 +275,25 @@ __device__ __forceinline__ void ReconPair(int limiter, const float2 (&s)[5], flo
     }
     Reconstruct<RECON, float>(limiter, lo, vM.x, vP.x);
     Reconstruct<RECON, float>(limiter, hi, vM.y, vP.y);
+  }
+}
+
+// FP64: the per-cell reconstructions of the other FP64 stages, lane by lane
+// (WENO-Z in its two-division form).
+template <int RECON>
+__device__ __forceinline__ void ReconPair(int limiter, const double2 (&s)[5], double2 &vM, double2 &vP) {
+  double lo[5], hi[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    lo[k] = s[k].x;
+    hi[k] = s[k].y;
+  }
+  if constexpr (RECON == WENOZ) {
+    WenoZBothTwoDiv<double>(lo, vM.x, vP.x);
+    WenoZBothTwoDiv<double>(hi, vM.y, vP.y);
+  } else {
+    Reconstruct<RECON, double>(limiter, lo, vM.x, vP.x);
+    Reconstruct<RECON, double>(limiter, hi, vM.y, vP.y);
   }
 }
 
@@ -338,6 +382,88 @@ __device__ __forceinline__ void SlabRiemann2(const float2 *vL, const float2 *vR,
   }
 }
 
+// FP64 HLLC at one face (riemann_solver.hpp:59-149) from the six
+// reconstructed primitives of each side.  The reference blends the two star
+// fluxes by max(tiny, sign u*) and -min(-tiny, sign u*); one factor is
+// DBL_MIN, so the flux is the star flux of the side sign(u*) selects (u* = -0
+// selects the right side, as copysign does) and only that state is formed.
+// Its density ratio U*_rho / U_rho is susi (S - u_n), the reference's
+// expression with rho cancelled (one division instead of two per side).
+template <int DIR1>
+__device__ __forceinline__ void hllc64(const double (&L)[NV], const double (&Rv)[NV], double gam, double *F) {
+  constexpr int DIR2 = (DIR1 + 1) % 3, DIR3 = (DIR1 + 2) % 3;
+  const double tiny = DBL_MIN;
+  const double uL = L[SV0 + DIR1], uR = Rv[SV0 + DIR1];
+  // FastSpeed: sqrt(bulk modulus / rho), bulk modulus gamma P
+  const double cfL = sqrt((1.0 / L[SD]) * (gam * L[SPRES]));
+  const double cfR = sqrt((1.0 / Rv[SD]) * (gam * Rv[SPRES]));
+  const double sL = kmin(-tiny, kmin(uL - cfL, uR - cfR));
+  const double sR = kmax(tiny, kmax(uL + cfL, uR + cfR));
+  const double dL = sL - uL, dR = sR - uR;
+  double ustar = Rv[SPRES] - L[SPRES] + (L[SD] * uL) * dL - (Rv[SD] * uR) * dR;
+  ustar = ustar / (L[SD] * dL - Rv[SD] * dR);
+  const double pstar = 0.5 * (L[SPRES] + Rv[SPRES] + L[SD] * dL * (ustar - uL) + Rv[SD] * dR * (ustar - uR));
+  const bool left = !signbit(ustar);
+  const double S = left ? sL : sR;
+  double V[NV];
+#pragma unroll
+  for (int v = 0; v < NV; v++) V[v] = left ? L[v] : Rv[v];
+  const double rho = V[SD], un = V[SV0 + DIR1], pr = V[SPRES];
+  // U and F of that side along DIR1 (primconsflux.hpp:55-138)
+  const double mn = rho * un, mt1 = rho * V[SV0 + DIR2], mt2 = rho * V[SV0 + DIR3];
+  double ekin = 0.0;
+  ekin += V[SV0] * V[SV0];
+  ekin += V[SV0 + 1] * V[SV0 + 1];
+  ekin += V[SV0 + 2] * V[SV0 + 2];
+  const double E = V[SEINT] * rho + ekin * (0.5 * rho);
+  const double susi = 1.0 / (S - ustar + tiny);
+  const double Usr = susi * (S * rho - mn);
+  const double ratio = susi * (S - un);
+  F[CDENS] = mn + S * (Usr - rho);
+  F[CMOM0 + DIR1] = (mn * un + pr) + S * (Usr * ustar - mn);
+  F[CMOM0 + DIR2] = mn * V[SV0 + DIR2] + S * (mt1 * ratio - mt1);
+  F[CMOM0 + DIR3] = mn * V[SV0 + DIR3] + S * (mt2 * ratio - mt2);
+  F[CENER] = (E + pr) * un + S * ((E * ratio + susi * (pstar * ustar - pr * un)) - E);
+}
+
+// FP64 Riemann flux at two faces, lane by lane: HLLC as above, HLL through
+// RiemannFlux (riemann_solver.hpp:20-57) with the face bulk modulus gamma P.
+template <int RIEMANN, int DIR1>
+__device__ __forceinline__ void SlabRiemann2(const double2 *vL, const double2 *vR, double gam, double2 *F) {
+  double fl[2][NCV];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    auto lane = [h](double2 p) { return h ? p.y : p.x; };
+    if constexpr (RIEMANN == HLLC) {
+      double L[NV], Rv[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        L[v] = lane(vL[v]);
+        Rv[v] = lane(vR[v]);
+      }
+      hllc64<DIR1>(L, Rv, gam, fl[h]);
+    } else {
+      double L[7], Rv[7];
+      L[RDENS] = lane(vL[SD]);
+      Rv[RDENS] = lane(vR[SD]);
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        L[RVEL0 + d] = lane(vL[SV0 + d]);
+        Rv[RVEL0 + d] = lane(vR[SV0 + d]);
+      }
+      L[RPRES] = lane(vL[SPRES]);
+      Rv[RPRES] = lane(vR[SPRES]);
+      L[RBMOD] = gam * L[RPRES];
+      Rv[RBMOD] = gam * Rv[RPRES];
+      L[REINT] = lane(vL[SEINT]);
+      Rv[REINT] = lane(vR[SEINT]);
+      RiemannFlux<RIEMANN, false, DIR1, double>(L, Rv, fl[h]);
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NCV; v++) F[v] = make_double2(fl[0][v], fl[1][v]);
+}
+
 // Primitives of one cell from its FP32 conserved state and energy low word
 // (primconsflux.hpp:76-98 with the ideal-gas EOS of equation_of_state.hpp:53-64):
 // e_int = (E_hi + E_lo) - |m|^2 / (2 rho) in FP64, with 1/rho from the FP32
@@ -358,6 +484,19 @@ __device__ __forceinline__ void slab_prim(float gm1, float rho, float m0, float 
   V[SPRES] = fmaxf(0.f, gm1 * rho * sie);
 }
 
+// FP64: Cons2Prim with the ideal-gas EOS exactly as the other FP64 stages
+// evaluate it (Cons2PrimEos).
+__device__ __forceinline__ void slab_prim(const EosParams &eos, double rho, double m0, double m1, double m2,
+                                          double ener, double (&V)[NV]) {
+  double W[7];
+  Cons2PrimEos<false, double>(eos, rho, m0, m1, m2, ener, nullptr, W);
+  V[SD] = W[RDENS];
+#pragma unroll
+  for (int d = 0; d < 3; d++) V[SV0 + d] = W[RVEL0 + d];
+  V[SPRES] = W[RPRES];
+  V[SEINT] = W[REINT];
+}
+
 // ---------------------------------------------------------------------------
 // Face ghosts of the new state.  An interior cell at local index l along axis
 // d is the source of the ghost cells that Parthenon's boundary exchange would
@@ -366,20 +505,23 @@ __device__ __forceinline__ void slab_prim(float gm1, float rho, float m0, float 
 // an outflow or reflecting boundary its own block's ghosts (zero gradient; a
 // mirror with the normal momentum negated).  Only face ghosts (the other two
 // coordinates interior) are written: the sweeps read nothing else.
+template <typename R>
 struct GhostVal {
-  float v[NCV];
-  float lo;
+  R v[NCV];
+  float lo;  // FP32: the energy's low word
 };
 
-__device__ __forceinline__ void ghost_store(const Args &a, long long idx, const GhostVal &gv, int flip_d) {
+template <typename R>
+__device__ __forceinline__ void ghost_store(const Args<R> &a, long long idx, const GhostVal<R> &gv, int flip_d) {
   const long long NP = (long long)a.m.nb * a.m.P;
 #pragma unroll
   for (int v = 0; v < NCV; v++) a.u1[v * NP + idx] = (v == CMOM0 + flip_d) ? -gv.v[v] : gv.v[v];
-  a.u1lo[idx] = gv.lo;
+  if constexpr (sizeof(R) == 4) a.u1lo[idx] = gv.lo;
 }
 
-__device__ __forceinline__ void ghost_push_axis(const Args &a, int d, int b, const int lb[3], const int pc[3],
-                                                const GhostVal &gv) {
+template <typename R>
+__device__ __forceinline__ void ghost_push_axis(const Args<R> &a, int d, int b, const int lb[3], const int pc[3],
+                                                const GhostVal<R> &gv) {
   const MeshDesc &m = a.m;
   const int n = m.nx[d], g = m.g[d], nbd = m.nbx[d];
   const int l = pc[d] - g;
@@ -416,24 +558,34 @@ __device__ __forceinline__ void ghost_push_axis(const Args &a, int d, int b, con
 }
 
 // ---------------------------------------------------------------------------
-template <int TY_, int RECON, int RIEMANN>
-__global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
+#ifndef SLAB_F64_UNROLL
+#define SLAB_F64_UNROLL 1
+#endif
+
+// The stage kernel.  tm_cc maps the stage input's conserved components;
+// tm_lo its energy low words (FP32; unused in FP64).
+template <typename R, int TY_, int RECON, int RIEMANN>
+__global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
     k_slab_stage(const __grid_constant__ CUtensorMap tm_cc, const __grid_constant__ CUtensorMap tm_lo,
-                 const __grid_constant__ Args a) {
-  using T = Tile<TY_>;
+                 const __grid_constant__ Args<R> a) {
+  using T = Tile<TY_, R>;
+  using P = typename PairOf<R>::T;
+  constexpr bool LO = sizeof(R) == 4;
   constexpr int TY = T::TY, NT = T::NT, PR = T::PR, RXC = T::RXC, REC_N = T::REC_N, FLX_N = T::FLX_N;
+  // unrolling of the x and y reconstruction loops over the six variables
+  constexpr int RU = LO ? NV : SLAB_F64_UNROLL;
   extern __shared__ __align__(128) unsigned char smem[];
   const MeshDesc &m = a.m;
-  const Smem<TY_> L(m.np[0]);
+  const Smem<TY_, R> L(m.np[0]);
   const int tid = threadIdx.x, lane = tid & 31, wr = tid >> 5;
   const int np0 = m.np[0], gx = m.g[0], nz = m.nx[2], nz2 = nz / 2;
-  // the raw slot: the conserved box of a plane pair, then its energy low words
-  float *const rawcc = reinterpret_cast<float *>(smem);
+  // the raw slot: the conserved box of a plane pair, then (FP32) its energy low words
+  R *const rawcc = reinterpret_cast<R *>(smem);
   float *const rawlo = reinterpret_cast<float *>(smem + L.lo_off());
-  float2 *prim = reinterpret_cast<float2 *>(smem + L.prim_off());   // [NV][PR][PC]
-  float2 *rm = reinterpret_cast<float2 *>(smem + L.rec_off());      // [NV][REC_N]
-  float2 *rp = rm + NV * REC_N;
-  float2 *flx = reinterpret_cast<float2 *>(smem + L.flx_off());     // [NCV][FLX_N]
+  P *prim = reinterpret_cast<P *>(smem + L.prim_off());   // [NV][PR][PC]
+  P *rm = reinterpret_cast<P *>(smem + L.rec_off());      // [NV][REC_N]
+  P *rp = rm + NV * REC_N;
+  P *flx = reinterpret_cast<P *>(smem + L.flx_off());     // [NCV][FLX_N]
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar_off());
   int *flag = reinterpret_cast<int *>(smem + L.bar_off() + 16);
   double *wmin = reinterpret_cast<double *>(smem + L.bar_off() + 64);
@@ -441,9 +593,9 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
   const bool done = a.clock->done != 0;
   const double dt = a.clock->dt;
   const long long NP = (long long)m.nb * m.P;
-  const float A0 = float(m.area[0]), A1 = float(m.area[1]), A2 = float(m.area[2]);
-  const float vol = float(m.vol);
-  const float bt = float(a.beta);
+  const R A0 = R(m.area[0]), A1 = R(m.area[1]), A2 = R(m.area[2]);
+  const R vol = R(m.vol);
+  const R bt = R(a.beta);
   const int RV = L.raw_var(), RPL = L.raw_plane();
   const long long plane_st = (long long)np0 * m.np[1];
 
@@ -472,14 +624,14 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
       // a stage queued after the run reached tlim leaves the state as it is
       for (int z = 0; z < nz; z++) {
         const long long n = col + (long long)(z + m.g[2]) * plane_st;
-        GhostVal gv;
+        GhostVal<R> gv;
 #pragma unroll
         for (int v = 0; v < NCV; v++) gv.v[v] = a.u0[v * NP + n];
-        gv.lo = a.u0lo[n];
+        gv.lo = LO ? a.u0lo[n] : 0.f;
         if (a.u1 != a.u0) {
 #pragma unroll
           for (int v = 0; v < NCV; v++) a.u1[v * NP + n] = gv.v[v];
-          a.u1lo[n] = gv.lo;
+          if constexpr (LO) a.u1lo[n] = gv.lo;
         }
         const int pc[3] = {lane + gx, oy + wr + m.g[1], z + m.g[2]};
 #pragma unroll
@@ -495,7 +647,7 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
         fence_proxy_async();
         mbar_expect_tx(&bar[0], unsigned(L.tx_bytes()) + a.tx_extra);
         tma_load_4d(rawcc, &tm_cc, 0, row0 / a.rgroup, zc0 + 2 * pair, 0, &bar[0]);
-        tma_load_3d(rawlo, &tm_lo, 0, row0 / a.rgroup, zc0 + 2 * pair, &bar[0]);
+        if constexpr (LO) tma_load_3d(rawlo, &tm_lo, 0, row0 / a.rgroup, zc0 + 2 * pair, &bar[0]);
       }
     };
     // thread 0's bounded wait for the pair; the CTA reads the outcome after its
@@ -510,16 +662,23 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
       mbar_wait(&bar[0], par, a.wait_limit);
       return true;
     };
-    // own column of a pair -> primitives (float2 over the two planes)
-    auto convert_own = [&](float2 (&W)[NV], bool keep) {
-      const float *r = rawcc, *rl = rawlo;
+    // primitives of the staged cell at raw offset o
+    auto cell_prim = [&](int o, R (&V)[NV]) {
+      const R *r = rawcc;
+      if constexpr (LO) {
+        slab_prim(a.gm1, r[o], r[RV + o], r[2 * RV + o], r[3 * RV + o], r[4 * RV + o], rawlo[o], V);
+      } else {
+        slab_prim(a.eos, r[o], r[RV + o], r[2 * RV + o], r[3 * RV + o], r[4 * RV + o], V);
+      }
+    };
+    // own column of a pair -> primitives (a pair over the two planes)
+    auto convert_own = [&](P (&W)[NV], bool keep) {
       const int o = (wr + HH) * np0 + lane + gx;
-      float V0[NV], V1[NV];
-      slab_prim(a.gm1, r[o], r[RV + o], r[2 * RV + o], r[3 * RV + o], r[4 * RV + o], rl[o], V0);
-      slab_prim(a.gm1, r[RPL + o], r[RV + RPL + o], r[2 * RV + RPL + o], r[3 * RV + RPL + o], r[4 * RV + RPL + o],
-                rl[RPL + o], V1);
+      R V0[NV], V1[NV];
+      cell_prim(o, V0);
+      cell_prim(RPL + o, V1);
 #pragma unroll
-      for (int v = 0; v < NV; v++) W[v] = make_float2(V0[v], V1[v]);
+      for (int v = 0; v < NV; v++) W[v] = mk2(V0[v], V1[v]);
       if (keep) {
 #pragma unroll
         for (int v = 0; v < NV; v++) prim[(v * PR + wr + HH) * PC + lane + HH] = W[v];
@@ -527,7 +686,6 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
     };
     // the x and y halo cells of a centre pair
     auto convert_halo = [&]() {
-      const float *r = rawcc, *rl = rawlo;
       if (tid < 6 * TY + 6 * NX) {
         int rr, cc;
         if (tid < 6 * TY) {
@@ -541,54 +699,53 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
           cc = HH + h % NX;
         }
         const int o = rr * np0 + cc - HH + gx;
-        float V0[NV], V1[NV];
-        slab_prim(a.gm1, r[o], r[RV + o], r[2 * RV + o], r[3 * RV + o], r[4 * RV + o], rl[o], V0);
-        slab_prim(a.gm1, r[RPL + o], r[RV + RPL + o], r[2 * RV + RPL + o], r[3 * RV + RPL + o],
-                  r[4 * RV + RPL + o], rl[RPL + o], V1);
+        R V0[NV], V1[NV];
+        cell_prim(o, V0);
+        cell_prim(RPL + o, V1);
 #pragma unroll
-        for (int v = 0; v < NV; v++) prim[(v * PR + rr) * PC + cc] = make_float2(V0[v], V1[v]);
+        for (int v = 0; v < NV; v++) prim[(v * PR + rr) * PC + cc] = mk2(V0[v], V1[v]);
       }
     };
     auto recon_x = [&](int v, int r, int xx) {
-      const float2 *c = prim + (v * PR + r + HH) * PC + xx;
-      float2 s[5];
+      const P *c = prim + (v * PR + r + HH) * PC + xx;
+      P s[5];
 #pragma unroll
       for (int q = 0; q < 5; q++) s[q] = c[q];
-      float2 vm, vp;
+      P vm, vp;
       ReconPair<RECON>(a.limiter, s, vm, vp);
       rm[v * REC_N + r * RXC + xx] = vm;
       rp[v * REC_N + r * RXC + xx] = vp;
     };
     auto riemann_x = [&](int r, int f) {
-      float2 vL[NV], vR[NV];
+      P vL[NV], vR[NV];
 #pragma unroll
       for (int v = 0; v < NV; v++) {
         vL[v] = rp[v * REC_N + r * RXC + f];
         vR[v] = rm[v * REC_N + r * RXC + f + 1];
       }
-      float2 F[NCV];
+      P F[NCV];
       SlabRiemann2<RIEMANN, 0>(vL, vR, a.gam, F);
 #pragma unroll
       for (int v = 0; v < NCV; v++) flx[v * FLX_N + r * (NX + 1) + f] = F[v];
     };
     auto recon_y = [&](int v, int yy, int x) {
-      const float2 *c = prim + (v * PR + yy) * PC + x + HH;
-      float2 s[5];
+      const P *c = prim + (v * PR + yy) * PC + x + HH;
+      P s[5];
 #pragma unroll
       for (int q = 0; q < 5; q++) s[q] = c[q * PC];
-      float2 vm, vp;
+      P vm, vp;
       ReconPair<RECON>(a.limiter, s, vm, vp);
       rm[v * REC_N + yy * NX + x] = vm;
       rp[v * REC_N + yy * NX + x] = vp;
     };
     auto riemann_y = [&](int f, int x) {
-      float2 vL[NV], vR[NV];
+      P vL[NV], vR[NV];
 #pragma unroll
       for (int v = 0; v < NV; v++) {
         vL[v] = rp[v * REC_N + f * NX + x];
         vR[v] = rm[v * REC_N + (f + 1) * NX + x];
       }
-      float2 F[NCV];
+      P F[NCV];
       SlabRiemann2<RIEMANN, 1>(vL, vR, a.gam, F);
 #pragma unroll
       for (int v = 0; v < NCV; v++) flx[v * FLX_N + f * NX + x] = F[v];
@@ -599,22 +756,23 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
     // duc = x+y divergence of cell 2j-1 (both for the pending update of cell
     // 2j-1); du = x+y divergence of the step's planes (y part added in the
     // next step's first phase); zF = the step's z fluxes.
-    float2 W0[NV], W1[NV];
-    float vPc[NV], Fc[NCV], duc[NCV];
-    float2 du[NCV], zF[NCV];
+    P W0[NV], W1[NV];
+    R vPc[NV], Fc[NCV], duc[NCV];
+    P du[NCV], zF[NCV];
 #pragma unroll
-    for (int v = 0; v < NV; v++) vPc[v] = 0.f;
+    for (int v = 0; v < NV; v++) vPc[v] = R(0);
 #pragma unroll
     for (int v = 0; v < NCV; v++) {
-      Fc[v] = duc[v] = 0.f;
-      du[v] = zF[v] = p2(0.f);
+      Fc[v] = duc[v] = R(0);
+      du[v] = zF[v] = splat(R(0));
     }
 
     // inputs of the pending update (cells 2j-3, 2j-2 at step j), loaded at the
     // end of the previous step so the loads complete during its last barrier
     bool ok[2] = {false, false};
     long long n[2] = {0, 0};
-    float zb[2][NCV], z0[2][NCV], zblo[2], z0lo[2];
+    R zb[2][NCV], z0[2][NCV];
+    float zblo[2], z0lo[2];
     auto load_update = [&](int zlo) {
 #pragma unroll
       for (int h = 0; h < 2; h++) {
@@ -627,8 +785,10 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
             zb[h][v] = a.ub[v * NP + n[h]];
             z0[h][v] = a.u0[v * NP + n[h]];
           }
-          zblo[h] = a.ublo[n[h]];
-          z0lo[h] = a.u0lo[n[h]];
+          if constexpr (LO) {
+            zblo[h] = a.ublo[n[h]];
+            z0lo[h] = a.u0lo[n[h]];
+          }
         }
       }
     };
@@ -660,12 +820,12 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
         // y divergence of step j-1's planes
 #pragma unroll
         for (int v = 0; v < NCV; v++) {
-          const float2 lo = flx[v * FLX_N + wr * NX + lane], hi = flx[v * FLX_N + (wr + 1) * NX + lane];
-          du[v] = psub2(du[v], psub2(pmul(p2(A1), hi), pmul(p2(A1), lo)));
+          const P lo = flx[v * FLX_N + wr * NX + lane], hi = flx[v * FLX_N + (wr + 1) * NX + lane];
+          du[v] = psub2(du[v], psub2(pmul(splat(A1), hi), pmul(splat(A1), lo)));
         }
       }
       if (j >= 1) {
-        float dz[2][NCV];
+        R dz[2][NCV];
 #pragma unroll
         for (int v = 0; v < NCV; v++) {
           // z contributions -A (F+ - F-) after x and y, as the reference sums them
@@ -676,21 +836,23 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           if (!ok[h]) continue;
-          GhostVal gv;
+          GhostVal<R> gv;
+          gv.lo = 0.f;
 #pragma unroll
           for (int v = 0; v < NCV; v++) {
-            const float dudt = dz[h][v] / vol;
-            if (v == CENER) {
+            const R dudt = dz[h][v] / vol;
+            if (LO && v == CENER) {
+              // FP32: the energy in FP64 from its hi/lo words
               const double eb = double(zb[h][v]) + double(zblo[h]), e0 = double(z0[h][v]) + double(z0lo[h]);
               const double e1 = (a.beta * eb + (1.0 - a.beta) * e0) + a.beta * dt * double(dudt);
-              gv.v[v] = float(e1);
+              gv.v[v] = R(e1);
               gv.lo = float(e1 - double(gv.v[v]));
             } else {
-              gv.v[v] = (bt * zb[h][v] + (1.f - bt) * z0[h][v]) + bt * float(dt) * dudt;
+              gv.v[v] = (bt * zb[h][v] + (R(1) - bt) * z0[h][v]) + bt * R(dt) * dudt;
             }
             a.u1[v * NP + n[h]] = gv.v[v];
           }
-          a.u1lo[n[h]] = gv.lo;
+          if constexpr (LO) a.u1lo[n[h]] = gv.lo;
           // face ghosts: only where the cell lies within g of a block face
           const int z = zlo + h;
           const bool pz = z < m.g[2] || z >= nz - m.g[2];
@@ -701,14 +863,27 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
             if (pz) ghost_push_axis(a, 2, b, lb, pc, gv);
           }
           if (a.last) {
-            float V[NV];
-            slab_prim(a.gm1, gv.v[0], gv.v[1], gv.v[2], gv.v[3], gv.v[4], gv.lo, V);
+            if constexpr (LO) {
+              float V[NV];
+              slab_prim(a.gm1, gv.v[0], gv.v[1], gv.v[2], gv.v[3], gv.v[4], gv.lo, V);
 #pragma unroll
-            for (int d = 0; d < 3; d++) {
-              const float cf = sqrtf(a.gam * V[SPRES] / V[SD]);
-              double xv = double(float(m.dx[d]) / (fabsf(V[SV0 + d]) + cf));
-              if (xv != xv) xv = 0.0;
-              dtl = xv < dtl ? xv : dtl;
+              for (int d = 0; d < 3; d++) {
+                const float cf = sqrtf(a.gam * V[SPRES] / V[SD]);
+                double xv = double(float(m.dx[d]) / (fabsf(V[SV0 + d]) + cf));
+                if (xv != xv) xv = 0.0;
+                dtl = xv < dtl ? xv : dtl;
+              }
+            } else {
+              // hydro_time_step.cpp:19-64 as the other FP64 stages evaluate it
+              double V[7];
+              Cons2PrimEos<false, double>(a.eos, gv.v[0], gv.v[1], gv.v[2], gv.v[3], gv.v[4], nullptr, V);
+#pragma unroll
+              for (int d = 0; d < 3; d++) {
+                const double cf = FastSpeed<false>(d, V);
+                double xv = m.dx[d] / (fabs(V[RVEL0 + d]) + cf);
+                if (xv != xv) xv = 0.0;
+                dtl = xv < dtl ? xv : dtl;
+              }
             }
           }
         }
@@ -719,11 +894,11 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
       for (int v = 0; v < NCV; v++) {
         Fc[v] = zF[v].y;
         duc[v] = du[v].y;
-        du[v] = p2(0.f);
+        du[v] = splat(R(0));
       }
       issue(j + 1);
       if (centre) {
-#pragma unroll 2
+#pragma unroll(RU)
         for (int v = 0; v < NV; v++) recon_x(v, wr, lane);
         if (tid < NV * TY * 2) recon_x(tid / (2 * TY), (tid % (2 * TY)) >> 1, NX + (tid & 1));
       }
@@ -738,10 +913,10 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
       if (centre) {
 #pragma unroll
         for (int v = 0; v < NCV; v++) {
-          const float2 lo = flx[v * FLX_N + wr * (NX + 1) + lane], hi = flx[v * FLX_N + wr * (NX + 1) + lane + 1];
-          du[v] = psub2(du[v], psub2(pmul(p2(A0), hi), pmul(p2(A0), lo)));
+          const P lo = flx[v * FLX_N + wr * (NX + 1) + lane], hi = flx[v * FLX_N + wr * (NX + 1) + lane + 1];
+          du[v] = psub2(du[v], psub2(pmul(splat(A0), hi), pmul(splat(A0), lo)));
         }
-#pragma unroll 2
+#pragma unroll(RU)
         for (int v = 0; v < NV; v++) recon_y(v, wr, lane);
         for (int it = tid; it < NV * 2 * NX; it += NT) recon_y(it >> 6, TY + ((it >> 5) & 1), lane);
       }
@@ -757,20 +932,20 @@ __global__ void __launch_bounds__(Tile<TY_>::NT, Tile<TY_>::CTAS)
         if (tid < NX) riemann_y(TY, tid);
       }
       const bool next_centre = j + 1 >= 0 && j + 1 < nz2;
-      float2 W2[NV];
+      P W2[NV];
       convert_own(W2, next_centre);
       if (next_centre) convert_halo();
       {
         // cells (2j, 2j+1) of the column, faces 2j - 1/2 and 2j + 1/2
-        float2 vm[NV], vp[NV];
+        P vm[NV], vp[NV];
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-          const float2 s[5] = {W0[v], make_float2(W0[v].y, W1[v].x), W1[v], make_float2(W1[v].y, W2[v].x), W2[v]};
+          const P s[5] = {W0[v], mk2(W0[v].y, W1[v].x), W1[v], mk2(W1[v].y, W2[v].x), W2[v]};
           ReconPair<RECON>(a.limiter, s, vm[v], vp[v]);
         }
-        float2 vL[NV];
+        P vL[NV];
 #pragma unroll
-        for (int v = 0; v < NV; v++) vL[v] = make_float2(vPc[v], vp[v].x);
+        for (int v = 0; v < NV; v++) vL[v] = mk2(vPc[v], vp[v].x);
         SlabRiemann2<RIEMANN, 2>(vL, vm, a.gam, zF);
 #pragma unroll
         for (int v = 0; v < NV; v++) {

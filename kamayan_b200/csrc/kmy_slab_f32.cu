@@ -1,195 +1,11 @@
-// kmy_slab_f32.cu -- host side of the z-streamed FP32 3D hydro stage
-// (kmy_slab.cuh): eligibility, tensor maps over the ghost-padded containers,
-// and the persistent launch over the (block, tile) work list.
-#include <cudaTypedefs.h>
-
-#include <atomic>
-#include <cstring>
-#include <mutex>
-
-#include "../../include/kmy_hydro.h"
-#include "kmy_slab.cuh"
+// FP32 instantiations of the z-streamed stage kernel (tiles of 16 and 8 rows),
+// compiled with the FP32 stages' approximate division and square root.
+#include "kmy_slab_launch.cuh"
 
 namespace kmy {
-
-namespace {
-
-__global__ void k_reset_dtmin_slab(DevClock *clock) { clock->dtmin_bits = 0x7FF0000000000000ull; }
-
-// Padded rows per TMA row group: the group's bytes must be a multiple of 16.
-int row_group(int np0) {
-  if ((np0 * 4) % 16 == 0) return 1;
-  if ((2 * np0 * 4) % 16 == 0) return 2;
-  return 0;
+int slab_dispatch_f32(kmy_ctx *c, const CUtensorMap &mc, const CUtensorMap &ml, const slab::Args<float> &a,
+                      int ty, int grid, size_t smem) {
+  return ty == 8 ? slab::dispatch_ty<float, 8>(c, mc, ml, a, grid, smem)
+                 : slab::dispatch_ty<float, 16>(c, mc, ml, a, grid, smem);
 }
-
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn(std::string *err) {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  });
-  if (!fn && err) *err = "cuTensorMapEncodeTiled is not available from the driver";
-  return fn;
-}
-
-// Tensor map over one container array: dims (row group, row groups, planes of
-// all blocks [, variables]); the box is one tile's staged rows of two planes.
-int make_map(kmy_ctx *c, CUtensorMap *map, const void *base, int nvar, int staged_rows) {
-  const MeshDesc &m = c->m;
-  const int R = row_group(m.np[0]);
-  auto fn = encode_fn(&c->err);
-  if (!fn) return KMY_ERR_CUDA;
-  cuuint64_t dims[4] = {cuuint64_t(R) * m.np[0], cuuint64_t(m.np[1] / R), cuuint64_t(m.np[2]) * m.nb,
-                        cuuint64_t(nvar)};
-  cuuint64_t strides[3] = {cuuint64_t(R) * m.np[0] * 4, cuuint64_t(m.np[0]) * m.np[1] * 4,
-                           cuuint64_t(m.nb) * m.P * 4};
-  cuuint32_t box[4] = {cuuint32_t(R * m.np[0]), cuuint32_t(staged_rows / R), 2u, cuuint32_t(nvar)};
-  cuuint32_t estr[4] = {1, 1, 1, 1};
-  const cuuint32_t rank = nvar > 1 ? 4 : 3;
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<void *>(base), dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    c->err = "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")";
-    return KMY_ERR_CUDA;
-  }
-  return KMY_OK;
-}
-
-int sm_count(int device) {
-  static std::atomic<int> cache[64];
-  if (device < 0 || device >= 64) return 148;
-  int v = cache[device].load();
-  if (v <= 0) {
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0) v = 148;
-    cache[device].store(v);
-  }
-  return v;
-}
-
-template <int TY, int RECON, int RIEMANN>
-int launch_kind(kmy_ctx *c, const CUtensorMap &mc, const CUtensorMap &ml, const slab::Args &a, int grid,
-                size_t smem) {
-  auto kern = slab::k_slab_stage<TY, RECON, RIEMANN>;
-  // the shared-memory opt-in once per device, so a stream capture sees launches only
-  static std::atomic<unsigned long long> opted{0};
-  const unsigned long long bit = c->device < 64 ? 1ull << c->device : 0ull;
-  if (!bit || !(opted.load() & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return cuda_check(c, e, "slab smem attribute");
-    opted.fetch_or(bit);
-  }
-  kern<<<unsigned(grid), slab::Tile<TY>::NT, smem, c->stream>>>(mc, ml, a);
-  c->launches++;
-  return cuda_check(c, cudaGetLastError(), "slab stage");
-}
-
-}  // namespace
-
-// Rows per tile for this context: the deck's (or the tuner's) choice, else 16
-// where the block height allows it (measured faster than 8 on the 256^3
-// WENO-Z workload), else 8.
-int slab_rows(const kmy_ctx *c) {
-  if (c->prm.slab_rows) return c->prm.slab_rows;
-  return c->m.nx[1] % 16 == 0 ? 16 : 8;
-}
-
-const char *slab_unsupported(const kmy_ctx *c) {
-  const MeshDesc &m = c->m;
-  if (c->esz != 4) return "the z-streamed stage is FP32";
-  if (m.ndim != 3) return "the z-streamed stage is 3D";
-  if (c->prm.mhd) return "constrained transport runs the brick stage";
-  if (c->amr.on) return "adaptive meshes run the per-task kernels";
-  if (m.nx[0] != slab::NX) return "the z-streamed stage needs 32 cells per block along x";
-  const int ty = slab_rows(c);
-  if (m.nx[1] % ty != 0) return "the block height is not a multiple of the tile's rows";
-  if (m.nx[2] % 2 != 0) return "the z-streamed stage needs an even block size along z";
-  for (int d = 0; d < 3; d++)
-    if (m.g[d] < slab::HH) return "the z-streamed stage needs 3 or more ghost cells";
-  const int R = row_group(m.np[0]);
-  if (!R) return "padded rows do not group into 16-byte multiples";
-  if ((m.g[1] - slab::HH) % R || (ty + 2 * slab::HH) % R || m.np[1] % R || ty % R)
-    return "staged rows do not align with the row groups";
-  if ((size_t(m.np[0]) * m.np[1] * 4) % 16) return "padded planes are not a multiple of 16 bytes";
-  if ((long long)m.np[2] * m.nb >= (1ll << 31)) return "too many planes for a tensor map";
-  const int need = ty == 8 ? slab::Smem<8>(m.np[0]).total() * 2 : slab::Smem<16>(m.np[0]).total();
-  if (need > 227 * 1024) return "padded rows too long for the shared-memory plan";
-  return nullptr;
-}
-
-int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, bool last) {
-  if (const char *why = slab_unsupported(c)) {
-    c->err = std::string("slab stage: ") + why;
-    return KMY_ERR_BAD_PARAM;
-  }
-  if (!md0.ghosts) {
-    if (const int rc = launch_fill_ghosts(c, md0)) return rc;
-  }
-  const MeshDesc &m = c->m;
-  CUtensorMap mc, ml;
-  std::memset(&mc, 0, sizeof(mc));
-  std::memset(&ml, 0, sizeof(ml));
-  const int ty = slab_rows(c);
-  if (int rc = make_map(c, &mc, md0.cc, slab::NCV, ty + 2 * slab::HH)) return rc;
-  if (int rc = make_map(c, &ml, md0.ener_lo, 1, ty + 2 * slab::HH)) return rc;
-  slab::Args a{};
-  a.m = m;
-  a.gm1 = float(c->eos.gm1);
-  a.gam = float(c->eos.gm1 + 1.0);
-  a.limiter = c->prm.limiter;
-  a.u0 = static_cast<const float *>(md0.cc);
-  a.u0lo = static_cast<const float *>(md0.ener_lo);
-  a.ub = static_cast<const float *>(base.cc);
-  a.ublo = static_cast<const float *>(base.ener_lo);
-  a.u1 = static_cast<float *>(md1.cc);
-  a.u1lo = static_cast<float *>(md1.ener_lo);
-  a.last = last ? 1 : 0;
-  a.beta = beta;
-  a.clock = c->clock;
-  a.rgroup = row_group(m.np[0]);
-  a.nty = m.nx[1] / ty;
-  a.nitems = m.nb * a.nty;
-  a.wait_limit = 1 << 22;
-  a.tx_extra = 0;
-  if (c->fault_wait) {
-    // kmy_set_fault(ctx, "stage_wait", 1): this stage's waits run out
-    a.tx_extra = 16;
-    a.wait_limit = 1 << 10;
-    c->fault_wait = 0;
-  }
-  const int ctas = ty == 8 ? slab::Tile<8>::CTAS : slab::Tile<16>::CTAS;
-  const int grid = std::min(a.nitems, sm_count(c->device) * ctas);
-  const size_t smem = size_t(ty == 8 ? slab::Smem<8>(m.np[0]).total() : slab::Smem<16>(m.np[0]).total());
-  if (last) {
-    k_reset_dtmin_slab<<<1, 1, 0, c->stream>>>(c->clock);
-    c->launches++;
-  }
-  int rc;
-  const int rec = c->prm.recon, rie = c->prm.riemann;
-#define KMY_SLAB_TY(TY, RC)                                                               \
-  rc = rie == HLL ? launch_kind<TY, RC, HLL>(c, mc, ml, a, grid, smem)                    \
-                  : launch_kind<TY, RC, HLLC>(c, mc, ml, a, grid, smem);
-#define KMY_SLAB(RC)                                                                      \
-  if (rec == RC) {                                                                        \
-    if (ty == 8) {                                                                        \
-      KMY_SLAB_TY(8, RC)                                                                  \
-    } else {                                                                              \
-      KMY_SLAB_TY(16, RC)                                                                 \
-    }                                                                                     \
-  } else
-  KMY_SLAB(FOG) KMY_SLAB(PLM) KMY_SLAB(PPM) KMY_SLAB(WENOZ) {
-    c->err = "no slab kernel for this reconstruction";
-    return KMY_ERR_BAD_PARAM;
-  }
-#undef KMY_SLAB
-#undef KMY_SLAB_TY
-  md1.ghosts = rc == KMY_OK;
-  return rc;
-}
-
 }  // namespace kmy

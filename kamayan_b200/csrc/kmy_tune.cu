@@ -7,9 +7,10 @@
 //
 //   brick   -- the brick-tiled fused stage (8^3 / 16^2 / 128 bricks, halos
 //              read from neighbouring interiors through address tables);
-//   slab16  -- the z-streamed FP32 3D stage, TMA-staged plane pairs, tiles of
-//              16 rows (one 512-thread CTA per SM);
-//   slab8   -- the same with tiles of 8 rows (two 256-thread CTAs per SM).
+//   slab16  -- the z-streamed 3D stage, TMA-staged plane pairs, tiles of
+//              16 rows (FP32: one 512-thread CTA per SM);
+//   slab8   -- the same with tiles of 8 rows (FP32: two 256-thread CTAs per
+//              SM; FP64, whose plan does not fit 16 rows: one).
 //
 // A tuning run times every candidate that applies to the context, on its own
 // state: stage 1 (beta = 1) reads "base" and writes a scratch container, so

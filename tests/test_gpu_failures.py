@@ -104,7 +104,7 @@ def test_stage_wait_runs_out(kmy_lib):
 
 
 def test_fault_hook_rejects_unknown_and_inapplicable(kmy_lib):
-    s = K.Solver(configs.kh_3d(n=32, nb=16))  # FP64: no z-streamed stage
+    s = K.Solver(configs.kh_3d(n=32, nb=16))  # 16^3 blocks: no z-streamed stage
     with pytest.raises(K.KmyError):
         s.set_fault("stage_wait")
     with pytest.raises(K.KmyError):
