@@ -126,6 +126,9 @@ static int setup_params(kmy_ctx *c, const char *deck) {
   if (!one_of(ln, {"batched", "per_block"})) return bad("kamayan_b200/launch: " + ln);
   p.per_block = ln == "per_block";
   if (p.per_block && p.stage_kernel == 0) p.stage_kernel = 1;  // the per-block launches are of the brick stage
+  const std::string cu = p.str("kamayan_b200/ct_update", "auto");
+  if (!one_of(cu, {"auto", "streamed", "per_face"})) return bad("kamayan_b200/ct_update: " + cu);
+  p.ct_update = cu == "auto" ? 0 : cu == "streamed" ? 1 : 2;
 
   const std::string integ = p.str("parthenon/time/integrator", "rk2");
   if (integ == "rk1") p.beta = {1.0};
@@ -878,10 +881,11 @@ int kmy_task_stage(kmy_ctx *c, int stage, double dt) {
 // are current (after set-up, an import, the task path or a previous fused
 // stage) and writes those of its output to c->prim_alt; the buffers swap.
 // Constrained transport: the fused stage updates the cells and writes the
-// transverse field fluxes; the face update (edge EMFs, Stokes, ApplyDuDt in
-// one kernel per face direction) and the primitives (which need the new
-// cell-centred field) follow as separate kernels, in the order of the task
-// list (hydro_add_flux_tasks.cpp, grid.cpp:213-241, primconsflux.cpp:82-142).
+// transverse field fluxes; the face update (edge EMFs, Stokes, ApplyDuDt)
+// and the primitives (which need the new cell-centred field) follow, in the order of the task list
+// (hydro_add_flux_tasks.cpp, grid.cpp:213-241, primconsflux.cpp:82-142): in
+// 3D blocks of 32-cell rows as the streamed face update and one cell pass
+// (kmy_ct.cu), else one kernel per face direction and a primitive pass.
 static int fused_stage_ct(kmy_ctx *c, int stage) {
   const auto &nm = c->prm.stage_name;
   const int ns = int(c->prm.beta.size());
@@ -891,11 +895,22 @@ static int fused_stage_ct(kmy_ctx *c, int stage) {
   md1.ghosts = false;
   int rc = launch_fused_stage(c, base, md0, md1, beta, stored, false);
   if (!rc) rc = launch_flux_halo(c);
-  if (!rc) rc = launch_ct_faces(c, base, md0, md1, beta);
-  if (!rc) rc = launch_prepare_primitive(c, md1);
-  if (!rc && stage == ns) {
-    rc = launch_estimate_dt(c, base, true);
-    if (!rc) rc = launch_fill_derived(c, base);
+  if (!ct_stream_unsupported(c)) {
+    // the streamed face update and cell pass (kmy_ct.cu); on the last stage,
+    // whose output is "base", the cell pass also takes the CFL estimate and div B
+    const bool fold = stage == ns && &md1 == &base;
+    if (!rc) rc = launch_ct_stream(c, base, md0, md1, beta, fold);
+    if (!rc && stage == ns && !fold) {
+      rc = launch_estimate_dt(c, base, true);
+      if (!rc) rc = launch_fill_derived(c, base);
+    }
+  } else {
+    if (!rc) rc = launch_ct_faces(c, base, md0, md1, beta);
+    if (!rc) rc = launch_prepare_primitive(c, md1);
+    if (!rc && stage == ns) {
+      rc = launch_estimate_dt(c, base, true);
+      if (!rc) rc = launch_fill_derived(c, base);
+    }
   }
   // interior primitives of md1 are current (ghost zones are not)
   c->prims_interior = !rc;

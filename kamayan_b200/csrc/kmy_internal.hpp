@@ -143,6 +143,10 @@ struct Params {
   // hydro brick stage launched once per meshblock instead of once per mesh
   // (<kamayan_b200> launch = per_block; the plain per-block GPU baseline)
   bool per_block = false;
+  // face update of a constrained-transport stage (<kamayan_b200> ct_update):
+  // 0 auto (streamed where it applies), 1 streamed (kmy_ct.cu), 2 one kernel
+  // per face direction plus the primitive pass (kmy_tasks.cu)
+  int ct_update = 0;
   TimeParams tp{};
   std::map<std::string, std::string> deck;
   double real(const std::string &k, double d) const;
@@ -281,12 +285,19 @@ int launch_set_energy_split(kmy_ctx *c, Container &ct);
 // ---- fused stage (kmy_fused.cu) ----
 int launch_fused_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1,
                        double beta, bool stored_prims, bool last);
-// ---- z-streamed FP32 3D stage (kmy_slab_f32.cu) ----
+// ---- z-streamed 3D stage (kmy_slab_host.cu; kernels in kmy_slab_f32.cu, kmy_slab_f64.cu) ----
 // Why the z-streamed stage cannot run this context, or null.
 const char *slab_unsupported(const kmy_ctx *c);
 // Rows per tile the z-streamed stage uses for this context (8 or 16).
 int slab_rows(const kmy_ctx *c);
 int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, bool last);
+// ---- streamed constrained-transport face update (kmy_ct.cu) ----
+// Why the streamed face update cannot run this context, or null.
+const char *ct_stream_unsupported(const kmy_ctx *c);
+// Edge EMFs, Stokes sums and face update of md1, then the cell-centred field
+// and primitives of md1; with fold_last also the CFL estimate into the clock
+// and div B of md1 (the last stage, md1 being "base").
+int launch_ct_stream(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, bool fold_last);
 // ---- stage-kernel autotuner (kmy_tune.cu) ----
 std::string tune_config_key(const kmy_ctx *c);
 int tune_apply(kmy_ctx *c, const std::string &choice);
