@@ -434,7 +434,11 @@ def workloads_block(a, device: int, stream) -> dict:
         s = solver(configs.blast_2d_amr(precision=prec), "blast", "tasks")
         nb0 = s.nblocks
         ms, upd, steps = _evolve_run(s, stream, tlim=0.2)
+        # the steps' device time as kmy_evolve counted it (host read-backs and
+        # tree updates excluded): the wall-over-device ratio is the host's share
+        dev = s.evolve_device_ms
         amr[prec] = {"cell_updates_per_s": upd / (ms / 1e3), "steps": steps, "seconds": ms / 1e3,
+                     "device_seconds": dev / 1e3, "wall_over_device": ms / dev if dev > 0 else None,
                      "blocks_initial": nb0, "blocks_final": s.nblocks, "leaves": s.blocks(),
                      "dens": s.interior(s.export("dens"))}
         s.close()
@@ -446,6 +450,7 @@ def workloads_block(a, device: int, stream) -> dict:
         "128^2 base in 16^2 blocks, 3 levels, Loehner dens 0.3/0.05, PLM(MC)+HLLC, RK2, t=0.2"
     out["blast_2d_amr_fp64"]["fp32"] = {
         "cell_updates_per_s": a32["cell_updates_per_s"], "steps": a32["steps"], "blocks_final": a32["blocks_final"],
+        "wall_over_device": a32["wall_over_device"],
         "same_leaves_as_fp64": same,
         "l1_density_vs_fp64": (float(abs(a32["dens"] - a64["dens"]).sum() / abs(a64["dens"]).sum())
                                if same else None)}

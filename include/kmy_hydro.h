@@ -57,7 +57,8 @@ typedef struct {
  * ReconstructionVars, ReconstructionStrategy, EMF_averaging), <physics> (MHD),
  * <material/single> (gamma, Abar, eos_type), <eos> (mode_init), plus
  * <kamayan_b200> (precision = fp64|fp32; stage_kernel = auto|brick|slab|tune;
- * slab_rows = auto|8|16; launch = batched|per_block).  Unknown option values
+ * slab_rows = auto|8|16; launch = batched|per_block; ct_update =
+ * auto|streamed|per_face).  Unknown option values
  * fail with KMY_ERR_BAD_PARAM.
  * Adaptive meshes (hydro and CT): <parthenon/mesh> refinement = adaptive, numlevel
  * (<= 8), derefine_count, and <kamayan/refinement0>, <kamayan/refinement1>, ...
@@ -246,6 +247,11 @@ int kmy_set_fault(kmy_ctx *ctx, const char *what, int value);
 /* Number of kmy_evolve chunks (or adaptive steps) that replayed a cached CUDA
  * graph instead of launching their kernels one by one. */
 int kmy_graph_replays(const kmy_ctx *ctx, int64_t *out);
+/* Device time (ms) of the last kmy_evolve call: from before each group of
+ * queued steps to after their last kernel, summed; the host's read-backs and
+ * tree updates between groups are not counted, so wall time over this is the
+ * host's share of the loop. */
+int kmy_evolve_device_ms(const kmy_ctx *ctx, double *ms);
 
 /* ---- stage-kernel autotuner -------------------------------------------------
  * The reference chooses its flux loop strategy by a runtime parameter

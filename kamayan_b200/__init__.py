@@ -39,7 +39,7 @@ EXPORTS = (
     "kmy_zone_cycles",
     "kmy_get_blocks", "kmy_set_dt", "kmy_save_restart", "kmy_load_restart",
     "kmy_set_path", "kmy_vortex_error", "kmy_conserved_sums", "kmy_launch_count",
-    "kmy_graph_replays", "kmy_set_fault", "kmy_reconstruct_stencils", "kmy_autotune", "kmy_stage_kernel", "kmy_tune_key", "kmy_tune_cache_put",
+    "kmy_graph_replays", "kmy_evolve_device_ms", "kmy_set_fault", "kmy_reconstruct_stencils", "kmy_autotune", "kmy_stage_kernel", "kmy_tune_key", "kmy_tune_cache_put",
     "kmy_tune_cache_get", "kmy_tune_cache_clear", "kmy_tune_cache_save", "kmy_tune_cache_load",
     "kmy_conserved_sums_noalloc",
     "kmy_server_create", "kmy_server_destroy", "kmy_server_last_error", "kmy_server_submit",
@@ -118,6 +118,7 @@ def lib() -> ctypes.CDLL:
         L.kmy_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.kmy_zone_cycles.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.kmy_graph_replays.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.kmy_evolve_device_ms.argtypes = [vp, _dp]
         L.kmy_set_fault.argtypes = [vp, cp, i]
         L.kmy_reconstruct_stencils.argtypes = [cp, cp, i, _dp, i, _dp]
         L.kmy_autotune.argtypes = [vp, i, ctypes.POINTER(TuneResult), i, ctypes.POINTER(i)]
@@ -401,6 +402,14 @@ class Solver:
         n = ctypes.c_int64()
         self._check(lib().kmy_graph_replays(self._h, ctypes.byref(n)))
         return n.value
+
+    @property
+    def evolve_device_ms(self) -> float:
+        """Device time (ms) of the last evolve call, host read-backs excluded
+        (kmy_evolve_device_ms)."""
+        v = ctypes.c_double()
+        self._check(lib().kmy_evolve_device_ms(self._h, ctypes.byref(v)))
+        return v.value
 
     def autotune(self, reps: int = 5) -> dict:
         """Time every stage kernel that applies on the current state, apply

@@ -26,6 +26,8 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
+#include <functional>
 #include <map>
 #include <vector>
 
@@ -1361,21 +1363,36 @@ int launch_amr_tag(kmy_ctx *c, Container &ct) {
 // whose members were tagged for derefinement derefine_count times in a row
 // when the merged parent keeps the balance.  New leaves are ordered by the
 // Morton key of their lower corner and get their data from the old mesh.
-int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
+int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out, DevClock *clock_out) {
   AmrHost &a = c->amr;
   MeshDesc &m = c->m;
   const int nd = m.ndim;
   const int nb = m.nb;
   *changed_out = false;
-  int *pin = static_cast<int *>(host_pin(c, sizeof(int) * (size_t(nb) + 1)));
-  if (!pin) return KMY_ERR_OOM;
+  // pinned staging: [the clock] [error flag] [tags]
+  const size_t cb = clock_out ? sizeof(DevClock) : 0;
+  char *stage = static_cast<char *>(host_pin(c, cb + sizeof(int) * (size_t(nb) + 1)));
+  if (!stage) return KMY_ERR_OOM;
+  int *pin = reinterpret_cast<int *>(stage + cb);
   int rc = cuda_check(c, cudaMemcpyAsync(pin + 1, a.d_tags, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream),
                       "amr tags");
   if (!rc) rc = cuda_check(c, cudaMemcpyAsync(pin, a.d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "amr err");
+  if (!rc && clock_out)
+    rc = cuda_check(c, cudaMemcpyAsync(stage, c->clock, sizeof(DevClock), cudaMemcpyDeviceToHost, c->stream),
+                    "amr clock");
   if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "amr tags sync");
   if (rc) return rc;
-  const int err = pin[0];
+  if (clock_out) std::memcpy(clock_out, stage, sizeof(DevClock));
   const std::vector<int> tags(pin + 1, pin + 1 + nb);
+  bool any = false;
+  rc = amr_count_tags(c, tags, pin[0], &any);
+  if (rc || !any) return rc;
+  return amr_remesh_apply(c, allow_derefine, tags, changed_out);
+}
+
+int amr_count_tags(kmy_ctx *c, const std::vector<int> &tags, int err, bool *any_out) {
+  AmrHost &a = c->amr;
+  *any_out = false;
   if (err) {
     c->err = "adaptive mesh: a level-value evaluation exceeded its depth or call budget (mesh not 2:1 balanced)";
     return KMY_ERR_STATE;
@@ -1383,11 +1400,22 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
   // derefinement counts; a step with no split candidate, a balanced tree and
   // no leaf due for derefinement leaves the mesh as it is
   bool any = !a.balanced;
-  for (int b = 0; b < nb; b++) {
+  for (int b = 0; b < c->m.nb; b++) {
     a.cnt[b] = tags[b] == -1 ? a.cnt[b] + 1 : 0;
     if ((tags[b] == 1 && a.lev[b] < a.max_level) || (a.lev[b] > 0 && a.cnt[b] >= a.derefine_count)) any = true;
   }
-  if (!any) return KMY_OK;
+  *any_out = any;
+  return KMY_OK;
+}
+
+int amr_remesh_apply(kmy_ctx *c, bool allow_derefine, const std::vector<int> &tags, bool *changed_out,
+                     const std::function<int()> &before_change) {
+  AmrHost &a = c->amr;
+  MeshDesc &m = c->m;
+  const int nd = m.ndim;
+  const int nb = m.nb;
+  *changed_out = false;
+  int rc = KMY_OK;
   typedef std::array<int, 4> Key;  // level, location
   std::map<Key, int> leaf;         // -> old leaf id, -1 for a new leaf
   for (int b = 0; b < nb; b++) leaf[{a.lev[b], a.loc[3 * b], a.loc[3 * b + 1], a.loc[3 * b + 2]}] = b;
@@ -1479,6 +1507,11 @@ int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed_out) {
     }
   }
   if (!changed) return KMY_OK;
+  // the new tree differs: the caller's last word before the device state is
+  // remapped
+  if (before_change) {
+    if (const int r = before_change()) return r;
+  }
 
   std::vector<std::pair<uint64_t, Key>> order;
   int maxl = 0;

@@ -491,8 +491,15 @@ int kmy_destroy(kmy_ctx *c) {
   if (!c) return KMY_OK;
   cudaSetDevice(c->device);
   if (c->evolve_exec) cudaGraphExecDestroy(c->evolve_exec);
+  for (cudaEvent_t &e : c->ev_evolve)
+    if (e) cudaEventDestroy(e);
+  for (auto &pair : c->pipe_ev)
+    for (cudaEvent_t &e : pair)
+      if (e) cudaEventDestroy(e);
   for (void *p : c->allocations) cudaFreeAsync(p, c->stream);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (char *&p : c->pipe_pin)
+    if (p) cudaFreeHost(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   if (c->h_pin) cudaFreeHost(c->h_pin);
   delete c;
@@ -861,13 +868,23 @@ static int task_stage(kmy_ctx *c, int stage, double dt) {
   return rc;
 }
 
-// After the stages of a step on an adaptive mesh: the tree update and remap,
-// and when the mesh changed the next dt also respects the new blocks' CFL
-// limit (the estimate accumulates into the step's minimum).
+// After the stages of a step on an adaptive mesh (the dt controller has run):
+// the tree update and remap.  The tags and the advanced clock come back in one
+// read, and a step that leaves the mesh as it is keeps that clock for
+// read_clock, so it syncs with the host once.  When the mesh changed, the next
+// dt also respects the new blocks' CFL limit (controller mode 3).
 static int amr_after_step(kmy_ctx *c) {
   bool changed = false;
-  int rc = amr_remesh(c, true, &changed);
-  if (!rc && changed) rc = launch_estimate_dt(c, c->md["base"], false);
+  DevClock h{};
+  int rc = amr_remesh(c, true, &changed, &h);
+  if (rc) return rc;
+  if (changed) {
+    rc = launch_estimate_dt(c, c->md["base"], true);
+    if (!rc) rc = launch_dt_controller(c, 3);
+  } else {
+    c->clock_host = h;
+    c->clock_host_launches = c->launches;
+  }
   return rc;
 }
 
@@ -1056,11 +1073,11 @@ static int stages_async(kmy_ctx *c) {
   return rc;
 }
 
-// After a step's stages: the tree update on an adaptive mesh, then the dt
-// controller, which counts the step's cells (taken before the remesh).
+// After a step's stages: the dt controller, which counts the step's cells,
+// then the tree update on an adaptive mesh.
 static int finish_step(kmy_ctx *c, long long cells) {
-  int rc = c->amr.on ? amr_after_step(c) : KMY_OK;
-  if (!rc) rc = launch_dt_controller(c, 0, cells);
+  int rc = launch_dt_controller(c, 0, cells);
+  if (!rc && c->amr.on) rc = amr_after_step(c);
   return rc;
 }
 
@@ -1071,8 +1088,14 @@ static int step_async(kmy_ctx *c) {
   return rc;
 }
 
-// The device clock through the pinned staging (synchronizes the stream).
+// The device clock through the pinned staging (synchronizes the stream),
+// unless an adaptive step's tag read just brought it back.
 static int read_clock(kmy_ctx *c, DevClock &h, const char *what) {
+  if (c->clock_host_launches == c->launches) {
+    h = c->clock_host;
+    c->clock_host_launches = -1;
+    return KMY_OK;
+  }
   DevClock *pin = static_cast<DevClock *>(host_pin(c, sizeof(DevClock)));
   if (!pin) return KMY_ERR_OOM;
   int rc = cuda_check(c, cudaMemcpyAsync(pin, c->clock, sizeof(DevClock), cudaMemcpyDeviceToHost, c->stream), what);
@@ -1196,6 +1219,174 @@ static int graph_run(kmy_ctx *c, const std::function<int()> &body, bool *ran) {
   return rc;
 }
 
+// ---------------------------------------------------------------------------
+// kmy_evolve on an adaptive mesh.  Each step's stages and dt controller run
+// as one graph; its tags, error flag and clock then come back to the host,
+// which decides whether the mesh changes.  The host queues the next step
+// before it waits for those reads, so the GPU does not idle while the host
+// decides: that step is speculative.  Before it the base state (conserved,
+// energy low words, faces, primitives, div B, clock) is copied aside on the
+// device; when the current step's tags ask for a remesh, or the run ends
+// with it (t_end, the step limit, a status), the speculative step is undone
+// from that copy before the host goes on, so the results are those of
+// stepping one at a time.
+
+// Pinned slots, events and backup arrays for the current mesh (grown by half
+// again when it outgrows them).  Called only with nothing in flight.
+static int pipe_reserve(kmy_ctx *c) {
+  // padded cells (or faces, the larger) of one array over all blocks
+  const size_t cells = size_t(c->m.nb) * size_t(std::max<long long>(c->m.P, c->m.Pf));
+  const size_t nb = size_t(c->m.nb);
+  // pinned slots: [clock][error flag][tags]
+  const size_t pin = sizeof(DevClock) + sizeof(int) * (nb + 1);
+  if (pin > c->pipe_pin_bytes) {
+    const size_t want = pin + pin / 2;
+    for (char *&p : c->pipe_pin) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      if (cudaMallocHost(reinterpret_cast<void **>(&p), want) != cudaSuccess) {
+        cudaGetLastError();
+        c->err = "pinned host allocation failed";
+        return KMY_ERR_OOM;
+      }
+    }
+    c->pipe_pin_bytes = want;
+  }
+  for (auto &pair : c->pipe_ev)
+    for (cudaEvent_t &e : pair)
+      if (!e && cudaEventCreate(&e) != cudaSuccess) return cuda_check(c, cudaGetLastError(), "pipeline event");
+  if (cells > c->bak_cells) {
+    const size_t want = cells + cells / 2;
+    for (void **p : {&c->bak_cc, &c->bak_lo, &c->bak_fc, &c->bak_prim, &c->bak_divb, &c->bak_clock}) {
+      dfree(c, *p);
+      *p = nullptr;
+    }
+    int rc = dalloc(c, &c->bak_cc, c->esz * c->ncc * want);
+    if (!rc && c->esz == 4) rc = dalloc(c, &c->bak_lo, 4 * want);
+    if (!rc && c->prm.mhd) rc = dalloc(c, &c->bak_fc, c->esz * 3 * want);
+    if (!rc) rc = dalloc(c, &c->bak_prim, c->esz * NPRIM * want);
+    if (!rc && c->prm.mhd) rc = dalloc(c, &c->bak_divb, 8 * want);
+    if (!rc) rc = dalloc(c, &c->bak_clock, sizeof(DevClock));
+    if (rc) return rc;
+    c->bak_cells = want;
+  }
+  return KMY_OK;
+}
+
+// copy the base state's step-changed arrays aside (to_bak) or back
+static int pipe_copy(kmy_ctx *c, bool to_bak) {
+  Container &base = c->md["base"];
+  const size_t n = size_t(c->m.nb) * size_t(c->m.P), nf = size_t(c->m.nb) * size_t(c->m.Pf);
+  struct Arr {
+    void *live, *bak;
+    size_t bytes;
+  };
+  const Arr arrs[] = {{base.cc, c->bak_cc, c->esz * c->ncc * n},
+                      {base.ener_lo, c->bak_lo, c->esz == 4 ? 4 * n : 0},
+                      {base.fc, c->bak_fc, c->prm.mhd ? c->esz * 3 * nf : 0},
+                      {c->prim, c->bak_prim, c->esz * NPRIM * n},
+                      {c->divb, c->bak_divb, c->prm.mhd ? 8 * n : 0},
+                      {c->clock, c->bak_clock, sizeof(DevClock)}};
+  for (const Arr &a : arrs) {
+    if (!a.bytes || !a.live) continue;
+    void *dst = to_bak ? a.bak : a.live;
+    const void *src = to_bak ? a.live : a.bak;
+    if (int rc = cuda_check(c, cudaMemcpyAsync(dst, src, a.bytes, cudaMemcpyDeviceToDevice, c->stream), "pipeline copy"))
+      return rc;
+  }
+  return KMY_OK;
+}
+
+static int evolve_amr(kmy_ctx *c, int nlim, int *n_out, DevClock &h) {
+  AmrHost &a = c->amr;
+  int rc = pipe_reserve(c);
+  if (rc) return rc;
+  // queue one step into slot k: timing event, (backup), stages + controller,
+  // the reads of its tags, error flag and clock, timing event
+  auto enqueue = [&](int k, bool speculative) -> int {
+    int r = cuda_check(c, cudaEventRecord(c->pipe_ev[k][0], c->stream), "pipeline event");
+    if (!r && speculative) r = pipe_copy(c, true);
+    const long long cells = interior_cells(c);
+    auto body = [&] {
+      int q = stages_async(c);
+      if (!q) q = launch_dt_controller(c, 0, cells);
+      return q;
+    };
+    bool ran = false;
+    if (!r) r = graph_run(c, body, &ran);
+    if (!r && !ran) r = body();
+    char *pin = c->pipe_pin[k];
+    int *ip = reinterpret_cast<int *>(pin + sizeof(DevClock));
+    if (!r)
+      r = cuda_check(c, cudaMemcpyAsync(pin, c->clock, sizeof(DevClock), cudaMemcpyDeviceToHost, c->stream),
+                     "pipeline clock");
+    if (!r) r = cuda_check(c, cudaMemcpyAsync(ip, a.d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "pipeline err");
+    if (!r)
+      r = cuda_check(c, cudaMemcpyAsync(ip + 1, a.d_tags, sizeof(int) * size_t(c->m.nb), cudaMemcpyDeviceToHost,
+                                        c->stream),
+                     "pipeline tags");
+    if (!r) r = cuda_check(c, cudaEventRecord(c->pipe_ev[k][1], c->stream), "pipeline event");
+    return r;
+  };
+  int n = 0, cur = 0;
+  rc = enqueue(cur, false);
+  while (!rc) {
+    // the speculative next step, unless the current one is the last allowed
+    const bool spec = nlim < 0 || n + 1 < nlim;
+    if (spec) rc = enqueue(1 - cur, true);
+    if (!rc) rc = cuda_check(c, cudaEventSynchronize(c->pipe_ev[cur][1]), "pipeline wait");
+    if (rc) break;
+    float ms = 0.f;
+    rc = cuda_check(c, cudaEventElapsedTime(&ms, c->pipe_ev[cur][0], c->pipe_ev[cur][1]), "pipeline event");
+    if (rc) break;
+    c->evolve_device_ms += double(ms);
+    // the current step's reads
+    const char *pin = c->pipe_pin[cur];
+    std::memcpy(&h, pin, sizeof(DevClock));
+    const int *ip = reinterpret_cast<const int *>(pin + sizeof(DevClock));
+    const int nbt = c->m.nb;
+    const std::vector<int> tags(ip + 1, ip + 1 + nbt);
+    n++;
+    bool any = false;
+    rc = amr_count_tags(c, tags, ip[0], &any);
+    const bool stop = rc || h.status || h.done || (nlim >= 0 && n >= nlim);
+    // undo the speculative step (once): before a remap, or when the run ends
+    bool undone = !spec;
+    auto undo = [&]() -> int {
+      if (undone) return KMY_OK;
+      undone = true;
+      int r = cuda_check(c, cudaStreamSynchronize(c->stream), "pipeline sync");
+      if (!r) r = pipe_copy(c, false);
+      return r;
+    };
+    bool changed = false;
+    if (!rc && any) rc = amr_remesh_apply(c, true, tags, &changed, undo);
+    if (!rc && (stop || changed)) rc = undo();
+    if (!rc && changed) {
+      rc = launch_estimate_dt(c, c->md["base"], true);
+      if (!rc) rc = launch_dt_controller(c, 3);
+      if (!rc) rc = read_clock(c, h, "evolve remesh");
+    }
+    if (rc) {
+      undo();
+      break;
+    }
+    if (!stop && !changed) {
+      // the speculative step stands and becomes the current one
+      cur = 1 - cur;
+      continue;
+    }
+    if (rc || stop || h.status) break;
+    if (!rc) rc = pipe_reserve(c);
+    if (!rc) rc = enqueue(cur, false);
+  }
+  // nothing stays in flight
+  const int r = cuda_check(c, cudaStreamSynchronize(c->stream), "pipeline end");
+  if (!rc) rc = r;
+  *n_out = n;
+  return rc;
+}
+
 int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
   if (!c) return KMY_ERR_BAD_PARAM;
   cudaSetDevice(c->device);
@@ -1203,13 +1394,30 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
   int rc = launch_dt_controller(c, 2);  // clamp the pending dt to tlim
   int n = 0;
   DevClock h{};
+  // device time: from before each iteration's steps to after their last
+  // kernel (the host's read-back and tree update excluded)
+  for (cudaEvent_t &e : c->ev_evolve)
+    if (!rc && !e) rc = cuda_check(c, cudaEventCreate(&e), "evolve event");
+  c->evolve_device_ms = 0.0;
+  if (!rc && c->amr.on) {
+    if (nlim != 0) {
+      rc = evolve_amr(c, nlim, &n, h);
+    } else {
+      rc = read_clock(c, h, "evolve");
+    }
+    if (!rc && h.status) rc = clock_status(c, h.status);
+    if (nsteps) *nsteps = h.ncycle;
+    return rc;
+  }
   while (!rc) {
+    rc = cuda_check(c, cudaEventRecord(c->ev_evolve[0], c->stream), "evolve event");
+    if (rc) break;
+
     // Fused hydro steps queue ahead in chunks: a step queued after the clock
-    // reached tlim leaves the state unchanged.  The per-task kernels
-    // (adaptive meshes, the tasks path, and the face update and primitives
-    // of a constrained-transport stage) do not check the clock, so those
-    // step one at a time; an adaptive mesh reads its tags back every step
-    // anyway.
+    // reached tlim leaves the state unchanged.  The per-task kernels (the
+    // tasks path, and the primitives of a constrained-transport stage) do
+    // not check the clock, so those step one at a time.  Adaptive meshes run
+    // evolve_amr above.
     const int chunk = steps_fused(c) && !c->prm.mhd ? kChunk : 1;
     bool ran = false;
     if (chunk == kChunk && (nlim < 0 || nlim - n >= kChunk)) {
@@ -1219,18 +1427,16 @@ int kmy_evolve(kmy_ctx *c, double tlim, int nlim, int *nsteps) {
         return r;
       }, &ran);
       if (ran) n += kChunk;
-    } else if (c->amr.on && (nlim < 0 || n < nlim)) {
-      const long long cells = interior_cells(c);
-      rc = graph_run(c, [&] { return stages_async(c); }, &ran);
-      if (!rc && !ran) rc = stages_async(c);
-      if (!rc) rc = finish_step(c, cells);
-      n++;
-      ran = true;
     }
     for (int i = 0; !ran && i < chunk && !rc && (nlim < 0 || n < nlim); i++, n++) rc = step_async(c);
+    if (!rc) rc = cuda_check(c, cudaEventRecord(c->ev_evolve[1], c->stream), "evolve event");
     if (rc) break;
     rc = read_clock(c, h, "evolve");
     if (rc) break;
+    float ms = 0.f;
+    rc = cuda_check(c, cudaEventElapsedTime(&ms, c->ev_evolve[0], c->ev_evolve[1]), "evolve event");
+    if (rc) break;
+    c->evolve_device_ms += double(ms);
     if (h.status) {
       rc = clock_status(c, h.status);
       break;
@@ -1385,6 +1591,12 @@ int kmy_set_fault(kmy_ctx *c, const char *what, int value) {
   }
   c->err = std::string("unknown fault ") + what;
   return KMY_ERR_BAD_PARAM;
+}
+
+int kmy_evolve_device_ms(const kmy_ctx *c, double *ms) {
+  if (!c || !ms) return KMY_ERR_BAD_PARAM;
+  *ms = c->evolve_device_ms;
+  return KMY_OK;
 }
 
 int kmy_graph_replays(const kmy_ctx *c, int64_t *out) {

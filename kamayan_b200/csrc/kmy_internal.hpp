@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -237,10 +238,29 @@ struct kmy_ctx {
   std::string evolve_key, evolve_seen;
   int64_t evolve_launches = 0;
   int64_t graph_replays = 0;  // launches of a cached graph (kmy_graph_replays)
+  // kmy_evolve's device time: events around each iteration's queued steps
+  cudaEvent_t ev_evolve[2] = {nullptr, nullptr};
+  double evolve_device_ms = 0.0;
+  // kmy_evolve on an adaptive mesh queues the next step before it reads the
+  // tags of the current one (kmy_api.cu:evolve_amr): the base state before
+  // that speculative step is kept here (conserved, energy low words, faces,
+  // primitives, div B, clock; sized for bak_cells padded cells per array),
+  // and each step in flight has a pinned slot for its tags and clock and a
+  // pair of timing events
+  void *bak_cc = nullptr, *bak_lo = nullptr, *bak_fc = nullptr, *bak_prim = nullptr, *bak_divb = nullptr,
+       *bak_clock = nullptr;
+  size_t bak_cells = 0;
+  char *pipe_pin[2] = {nullptr, nullptr};
+  size_t pipe_pin_bytes = 0;
+  cudaEvent_t pipe_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int fault_wait = 0;  // kmy_set_fault "stage_wait": the next z-streamed stage's waits run out
   // pinned host staging for the per-step reads (clock, tags), grown on demand
   void *h_pin = nullptr;
   size_t h_pin_bytes = 0;
+  // the clock as an adaptive step's tag read brought it back, valid while no
+  // kernel has been launched since (launches == clock_host_launches)
+  kmy::DevClock clock_host{};
+  int64_t clock_host_launches = -1;
   std::string err;
   std::string deck_text;  // the deck the context was created from (restart files carry it)
   std::vector<void *> allocations;
@@ -322,7 +342,17 @@ int launch_amr_fill_ghosts(kmy_ctx *c, Container &ct);
 int launch_flux_correct(kmy_ctx *c);
 int launch_emf_correct(kmy_ctx *c, Container &md0);
 int launch_amr_tag(kmy_ctx *c, Container &ct);
-int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed);
+// The tree update from the last tags; with clock_out, the device clock comes
+// back in the same read (one host sync).
+int amr_remesh(kmy_ctx *c, bool allow_derefine, bool *changed, DevClock *clock_out = nullptr);
+// The two halves of amr_remesh on tags already read back: the derefinement
+// counters and whether anything is due (call once per step's tags), then the
+// tree update and remap.
+int amr_count_tags(kmy_ctx *c, const std::vector<int> &tags, int err, bool *any);
+// before_change runs once the new tree is known to differ, before any device
+// work.
+int amr_remesh_apply(kmy_ctx *c, bool allow_derefine, const std::vector<int> &tags, bool *changed,
+                     const std::function<int()> &before_change = nullptr);
 // Storage for the leaf list already in c->amr (lev, loc, cnt): level tables,
 // every stage container, the primitives and div B at the new block count.
 int amr_adopt_leaves(kmy_ctx *c);

@@ -950,6 +950,18 @@ __global__ void k_dt_controller(DevClock *clk, TimeParams tp, int mode, long lon
     advance_clock(clk, tp);
     clk->zone_cycles += (unsigned long long)cells;
     return;
+  }
+  if (mode == 3) {
+    // after a remesh that followed mode 0: the new blocks' estimate also
+    // bounds the next dt.  min(dt, est) clamped to tlim equals the mode-0
+    // result over the union of both estimates.
+    const double est = dtmin * tp.cfl_over_ndim;
+    if (clk->status == 0 && (!(est > 0.0) || !(est < big))) clk->status = KMY_ERR_NONFINITE;
+    clk->dt_est = fmin(clk->dt_est, est);
+    double nd = fmin(clk->dt, est);
+    if (clk->time < tp.tlim && (tp.tlim - clk->time) < nd) nd = tp.tlim - clk->time;
+    clk->dt = nd;
+    return;
   } else {
     clk->time = 0.0;
     clk->ncycle = 0;

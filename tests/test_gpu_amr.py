@@ -232,3 +232,35 @@ def test_evolve_graph_matches_steps(kmy_lib):
         a, b = sa.export(var, c), sb.export(var, c)
         assert np.array_equal(a, b), f"{var}{c}: max |diff| {np.abs(a - b).max()}"
     assert sa.zone_cycles == sb.zone_cycles
+
+
+def test_evolve_to_tlim_matches_steps(kmy_lib):
+    # kmy_evolve queues each next step before it reads the current step's tags
+    # (a speculative step, undone when the mesh changes or the run ends); to an
+    # end time it gives what stepping one at a time gives, and it counts the
+    # steps' device time
+    from kamayan_b200 import Solver
+
+    deck = configs.blast_2d_amr(n=64, nb=8, derefine_count=2)
+    probe = Solver(deck.text())
+    probe.set_path("tasks")
+    probe.pgen("blast")
+    probe.evolve(1e30, 45)
+    tlim = probe.time["time"] * 0.97  # the last step is clamped to land on tlim
+    probe.close()
+    sa, sb = Solver(deck.text()), Solver(deck.text())
+    for s in (sa, sb):
+        s.set_path("tasks")
+        s.pgen("blast")
+    while sa.time["time"] < tlim:
+        sa.evolve(tlim, 1)
+    sb.evolve(tlim)
+    assert sb.time == sa.time and sb.time["time"] == tlim
+    la, ca = sa.blocks()
+    lb, cb = sb.blocks()
+    assert np.array_equal(la, lb) and np.array_equal(ca, cb)
+    for var, c in CONS + PRIMS:
+        a, b = sa.export(var, c), sb.export(var, c)
+        assert np.array_equal(a, b), f"{var}{c}: max |diff| {np.abs(a - b).max()}"
+    assert sa.zone_cycles == sb.zone_cycles
+    assert sb.evolve_device_ms > 0.0

@@ -49,6 +49,23 @@ def test_key_rejects_a_bad_deck():
         K.tune_key(d)
 
 
+@pytest.mark.parametrize("block,key,value", [("kamayan_b200", "ct_update", "sideways"),
+                                              ("kamayan_b200", "stage_kernel", "fastest"),
+                                              ("kamayan_b200", "slab_rows", "12")])
+def test_key_rejects_unknown_kernel_options(block, key, value):
+    d = configs.ot_3d(n=64, nb=32)
+    d.set(block, key, value)
+    with pytest.raises(K.KmyError):
+        K.tune_key(d)
+
+
+@pytest.mark.parametrize("value", ["auto", "streamed", "per_face"])
+def test_key_accepts_ct_update(value):
+    d = configs.ot_3d(n=64, nb=32)
+    d.set("kamayan_b200", "ct_update", value)
+    assert "ct" in K.tune_key(d)
+
+
 def test_cache_put_get_and_unknown_choice():
     assert K.tune_cache_get("NVIDIA B200 | x") is None
     K.tune_cache_put("NVIDIA B200 | x", "slab16", 1.25)
