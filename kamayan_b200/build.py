@@ -37,6 +37,10 @@ EXTRA_FLAGS = {
     # the z-streamed FP32 stage, and the device reconstruction functions as the
     # FP32 stage kernels compile them
     "kmy_slab_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+    "kmy_slab_mhd.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+    # the streamed CT face update and cell pass: their FP32 instantiations
+    # round as the FP32 stage kernels do (FP64 division is unaffected)
+    "kmy_ct.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "kmy_kat.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     # adaptive mesh: no FMA contraction, so prolongation, restriction and the
     # refinement estimator round exactly as written (tags are threshold tests)

@@ -910,7 +910,15 @@ static int fused_stage_ct(kmy_ctx *c, int stage) {
   const bool stored = c->prims_valid || c->prims_interior;
   const double beta = c->prm.beta[stage - 1];
   md1.ghosts = false;
-  int rc = launch_fused_stage(c, base, md0, md1, beta, stored, false);
+  // the cells: the z-streamed stage (FP32, 3D blocks of 32-cell rows) by
+  // default, else the brick stage; both write the transverse field fluxes
+  const char *no_slab = slab_unsupported(c);
+  if (c->prm.stage_kernel == 2 && no_slab) {
+    c->err = std::string("stage_kernel = slab: ") + no_slab;
+    return KMY_ERR_BAD_PARAM;
+  }
+  int rc = ct_cells_on_slab(c) ? launch_slab_stage(c, base, md0, md1, beta, false)
+                               : launch_fused_stage(c, base, md0, md1, beta, stored, false);
   if (!rc) rc = launch_flux_halo(c);
   if (!ct_stream_unsupported(c)) {
     // the streamed face update and cell pass (kmy_ct.cu); on the last stage,
@@ -929,8 +937,9 @@ static int fused_stage_ct(kmy_ctx *c, int stage) {
       if (!rc) rc = launch_fill_derived(c, base);
     }
   }
-  // interior primitives of md1 are current (ghost zones are not)
-  c->prims_interior = !rc;
+  // interior primitives of md1 are current (ghost zones are not), unless the
+  // z-streamed stage ran the cells (its cell pass stores no primitives)
+  c->prims_interior = !rc && !ct_cells_on_slab(c);
   c->prims_valid = false;
   return rc;
 }

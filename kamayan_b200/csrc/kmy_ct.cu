@@ -8,9 +8,10 @@
 // E_x and E_y on node plane k, E_z on cell plane k), then updates the z faces
 // of plane k and the x and y faces of cell plane k - 1 from them: FluxStokes
 // (grid_update.hpp:80-137) and the low-storage update ApplyDuDt
-// (grid.cpp:213-241), with the expressions of the per-face-direction kernel
-// in the same order (the two compilations may contract a product into an FMA
-// differently, an ulp apart).  Each face is read and written only by the
+// (grid.cpp:213-241; the input container's faces are left as they are),
+// with the expressions of the per-face-direction kernel in the same order
+// (the two compilations may contract a product into an FMA differently, an
+// ulp apart).  Each face is read and written only by the
 // thread that owns it, so an update in place (a stage whose output container
 // is its input) is safe, and an EMF on a block face is formed by the same
 // code in both blocks that share it.  The face inputs are loaded before the
@@ -24,7 +25,9 @@
 // average of primconsflux.cpp:102-129), the primitives (PreparePrimitive,
 // primconsflux.cpp:82-142, with the ideal-gas EOS), and on the last stage the
 // CFL estimate (EstimateTimeStep, hydro_time_step.cpp:19-64) and div B in
-// FP64 (FillDerived, hydro.cpp:150-190) from the same values.
+// FP64 (FillDerived, hydro.cpp:150-190) from the same values.  When the
+// z-streamed stage runs the cells, it writes the field's face ghosts instead
+// of storing the primitives (that stage converts its input itself).
 //
 // Edges on block faces read the ghost-layer fluxes that k_flux_halo copies.
 #include "../../include/kmy_hydro.h"
@@ -75,10 +78,12 @@ __global__ void __launch_bounds__(CT_NX * TY)
   const S ia2 = S(1.) / (S(m.area[2]) + S(1.e-36));
   const double h = *dt_dev;
   const S bt = S(beta);
-  // a face's low-storage update from its base and input values
+  // a face's low-storage update from its base and input values.  The input
+  // container's faces are not rewritten with x0 as ApplyDuDt does: the
+  // low-storage scheme reads a stage's input container only in that stage
+  // (in the first stage it is "base" and x0 equals its value).
   auto finish = [&](long long n, S vb, S v0, S out) {
     const S x0 = bt * vb + (S(1.0) - bt) * v0;
-    f0[n] = x0;
     f1[n] = x0 + bt * S(h) * out;
   };
   // stokes(edge, axis) of the per-face-direction kernel: sign * (L E_a - L E_b)
@@ -153,57 +158,126 @@ __global__ void __launch_bounds__(CT_NX * TY)
   }
 }
 
-// One thread per cell; a CTA is 8 rows of one plane of one block.
+// The face ghosts of a cell's new field components, for a z-streamed stage
+// that stages the next stage's input with its ghost zones: an interior cell
+// within g of a block face fills the ghosts that Parthenon's boundary
+// exchange would fill from it (the high ghosts of the block below along an
+// axis, the low ghosts of the block above, wrapped across a periodic
+// boundary; at an outflow boundary its own block's ghosts; at a reflecting
+// one the mirror with the normal component negated), the rule of the
+// z-streamed stage's epilogue.  pc: the cell's padded coordinates.
+template <typename S>
+__device__ void push_field_ghosts(const MeshDesc &m, S *cc, long long NP, int b, const int pc[3],
+                                  const S (&B)[3]) {
+  const int lb[3] = {b % m.nbx[0], (b / m.nbx[0]) % m.nbx[1], b / (m.nbx[0] * m.nbx[1])};
+  auto store = [&](long long idx, int flip) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) cc[(CMAGC0 + q) * NP + idx] = q == flip ? -B[q] : B[q];
+  };
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const int n = m.nx[d], g = m.g[d], nbd = m.nbx[d];
+    const int l = pc[d] - g;
+    if (l >= g && l < n - g) continue;
+    const long long stride = d == 0 ? 1 : d == 1 ? m.nbx[0] : (long long)m.nbx[0] * m.nbx[1];
+    // element offset of pc with coordinate d replaced by p, in block tb
+    auto at = [&](long long tb, int p) {
+      int q[3] = {pc[0], pc[1], pc[2]};
+      q[d] = p;
+      return tb * m.P + ((long long)q[2] * m.np[1] + q[1]) * m.np[0] + q[0];
+    };
+    if (l < g) {
+      if (lb[d] > 0 || m.bc[d][0] == BC_PERIODIC) {
+        store(at(b + (lb[d] > 0 ? -stride : (long long)(nbd - 1) * stride), n + g + l), -1);
+      } else if (m.bc[d][0] == BC_OUTFLOW) {
+        if (l == 0)
+          for (int p = 0; p < g; p++) store(at(b, p), -1);
+      } else {
+        store(at(b, g - 1 - l), d);
+      }
+    }
+    if (l >= n - g) {
+      if (lb[d] < nbd - 1 || m.bc[d][1] == BC_PERIODIC) {
+        store(at(b + (lb[d] < nbd - 1 ? stride : -(long long)(nbd - 1) * stride), l - n + g), -1);
+      } else if (m.bc[d][1] == BC_OUTFLOW) {
+        if (l == n - 1)
+          for (int p = 0; p < g; p++) store(at(b, n + g + p), -1);
+      } else {
+        store(at(b, g + 2 * n - 1 - l), d);
+      }
+    }
+  }
+}
+
+// One thread per column of a CTA of 8 rows of one block; the CTA walks a
+// chunk of CT_ZC planes (on the last stage one atomic per CTA collects the
+// CFL minimum, so fewer, longer CTAs keep that atomic off the critical path).
 template <typename S, bool LAST>
 __global__ void __launch_bounds__(CT_NX * CT_TY)
     k_ct_cells(MeshDesc m, EosParams eos, S *cc, const float *lo, const S *fc, S *prim, double *divb,
-               DevClock *clock) {
+               DevClock *clock, int push) {
+  // push: the z-streamed stage runs the cells; it stages the next input with
+  // its ghost zones (so the field's face ghosts are written here) and converts
+  // it itself (so the primitives are not stored)
   __shared__ double wmin[CT_TY];
   const int tid = threadIdx.x, lane = tid & 31, wr = tid >> 5;
   const int nty = m.nx[1] / CT_TY;
-  const int k = blockIdx.y, b = blockIdx.x / nty, oy = (blockIdx.x - b * nty) * CT_TY;
-  const int i = lane + m.g[0], j = oy + wr + m.g[1], kp = k + m.g[2];
+  const int b = blockIdx.x / nty, oy = (blockIdx.x - b * nty) * CT_TY;
+  const int k0 = blockIdx.y * CT_ZC, k1 = min(m.nx[2], k0 + CT_ZC);
+  const int i = lane + m.g[0], j = oy + wr + m.g[1];
   const long long NP = (long long)m.nb * m.P, NF = (long long)m.nb * m.Pf, bo = (long long)b * m.Pf;
-  const long long n = (long long)b * m.P + ((long long)kp * m.np[1] + j) * m.np[0] + i;
   auto fo = [&](int kk, int jj, int ii) { return bo + ((long long)kk * m.nf[1] + jj) * m.nf[0] + ii; };
-  const long long f000 = fo(kp, j, i), fx1 = fo(kp, j, i + 1), fy1 = fo(kp, j + 1, i), fz1 = fo(kp + 1, j, i);
-  // the face average (primconsflux.cpp:102-129)
   const S vol = S(m.vol);
   const S a0 = S(m.area[0]), a1 = S(m.area[1]), a2 = S(m.area[2]);
-  S B[3];
-  B[0] = S(0.5) * S(m.dx[0]) * (a0 * fc[fx1] + a0 * fc[f000]) / vol;
-  B[1] = S(0.5) * S(m.dx[1]) * (a1 * fc[NF + fy1] + a1 * fc[NF + f000]) / vol;
-  B[2] = S(0.5) * S(m.dx[2]) * (a2 * fc[2 * NF + fz1] + a2 * fc[2 * NF + f000]) / vol;
+  double dtl = INFINITY;
+  for (int k = k0; k < k1; k++) {
+    const int kp = k + m.g[2];
+    const long long n = (long long)b * m.P + ((long long)kp * m.np[1] + j) * m.np[0] + i;
+    const long long f000 = fo(kp, j, i), fx1 = fo(kp, j, i + 1), fy1 = fo(kp, j + 1, i), fz1 = fo(kp + 1, j, i);
+    // the face average (primconsflux.cpp:102-129)
+    S B[3];
+    B[0] = S(0.5) * S(m.dx[0]) * (a0 * fc[fx1] + a0 * fc[f000]) / vol;
+    B[1] = S(0.5) * S(m.dx[1]) * (a1 * fc[NF + fy1] + a1 * fc[NF + f000]) / vol;
+    B[2] = S(0.5) * S(m.dx[2]) * (a2 * fc[2 * NF + fz1] + a2 * fc[2 * NF + f000]) / vol;
 #pragma unroll
-  for (int d = 0; d < 3; d++) cc[(CMAGC0 + d) * NP + n] = B[d];
-  double ener = double(cc[CENER * NP + n]);
-  if constexpr (sizeof(S) == 4) {
-    if (lo) ener += double(lo[n]);
-  }
-  S V[10];
-  Cons2PrimEos<true, S>(eos, cc[n], cc[CMOM0 * NP + n], cc[CMOM1 * NP + n], cc[CMOM2 * NP + n], ener, B, V);
-  prim[PVEL0 * NP + n] = V[RVEL0];
-  prim[PVEL1 * NP + n] = V[RVEL1];
-  prim[PVEL2 * NP + n] = V[RVEL2];
-  prim[PPRES * NP + n] = V[RPRES];
-  prim[PBMOD * NP + n] = V[RBMOD];
-  prim[PEINT * NP + n] = V[REINT];
-  prim[PTEMP * NP + n] = kmax(S(0), V[REINT] / S(eos.cv));
-  if constexpr (LAST) {
-    // div B in FP64 (hydro.cpp:150-190)
-    double d = 0.;
-    d += m.area[0] * double(fc[fx1]) - m.area[0] * double(fc[f000]);
-    d += m.area[1] * double(fc[NF + fy1]) - m.area[1] * double(fc[NF + f000]);
-    d += m.area[2] * double(fc[2 * NF + fz1]) - m.area[2] * double(fc[2 * NF + f000]);
-    divb[n] = d / m.vol;
-    // CFL estimate (hydro_time_step.cpp:19-64); a NaN propagates
-    double dtl = INFINITY;
-#pragma unroll
-    for (int dir = 0; dir < 3; dir++) {
-      const S cf = FastSpeed<true>(dir, V);
-      const double x = double(S(m.dx[dir]) / (fabs(V[RVEL0 + dir]) + cf));
-      dtl = (x < dtl || x != x) ? x : dtl;
+    for (int d = 0; d < 3; d++) cc[(CMAGC0 + d) * NP + n] = B[d];
+    if (push) {
+      const int pc[3] = {i, j, kp};
+      push_field_ghosts(m, cc, NP, b, pc, B);
     }
+    if (push && !LAST) continue;  // nothing else to do for this cell
+    double ener = double(cc[CENER * NP + n]);
+    if constexpr (sizeof(S) == 4) {
+      if (lo) ener += double(lo[n]);
+    }
+    S V[10];
+    Cons2PrimEos<true, S>(eos, cc[n], cc[CMOM0 * NP + n], cc[CMOM1 * NP + n], cc[CMOM2 * NP + n], ener, B, V);
+    if (!push) {
+      prim[PVEL0 * NP + n] = V[RVEL0];
+      prim[PVEL1 * NP + n] = V[RVEL1];
+      prim[PVEL2 * NP + n] = V[RVEL2];
+      prim[PPRES * NP + n] = V[RPRES];
+      prim[PBMOD * NP + n] = V[RBMOD];
+      prim[PEINT * NP + n] = V[REINT];
+      prim[PTEMP * NP + n] = kmax(S(0), V[REINT] / S(eos.cv));
+    }
+    if constexpr (LAST) {
+      // div B in FP64 (hydro.cpp:150-190)
+      double d = 0.;
+      d += m.area[0] * double(fc[fx1]) - m.area[0] * double(fc[f000]);
+      d += m.area[1] * double(fc[NF + fy1]) - m.area[1] * double(fc[NF + f000]);
+      d += m.area[2] * double(fc[2 * NF + fz1]) - m.area[2] * double(fc[2 * NF + f000]);
+      divb[n] = d / m.vol;
+      // CFL estimate (hydro_time_step.cpp:19-64); a NaN propagates
+#pragma unroll
+      for (int dir = 0; dir < 3; dir++) {
+        const S cf = FastSpeed<true>(dir, V);
+        const double x = double(S(m.dx[dir]) / (fabs(V[RVEL0 + dir]) + cf));
+        dtl = (x < dtl || x != x) ? x : dtl;
+      }
+    }
+  }
+  if constexpr (LAST) {
     for (int o = 16; o > 0; o >>= 1) dtl = fmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, o));
     if (lane == 0) wmin[wr] = dtl;
     __syncthreads();
@@ -226,16 +300,18 @@ int ct_launch(kmy_ctx *c, Container &base, Container &md0, Container &md1, doubl
   k_ct_emf_faces<S, CT_TY><<<fgrid, CT_NX * CT_TY, 0, c->stream>>>(
       m, (const S *)c->flux, (const S *)base.fc, (S *)md0.fc, (S *)md1.fc, beta, &c->clock->dt, c->clock);
   c->launches++;
-  const dim3 grid(tiles, unsigned(m.nx[2]));
+  const dim3 grid(tiles, unsigned((m.nx[2] + CT_ZC - 1) / CT_ZC));
+  // the field's face ghosts, for the z-streamed stage that stages md1 next
+  const int push = ct_cells_on_slab(c) ? 1 : 0;
   const float *lo = c->esz == 4 ? static_cast<const float *>(md1.ener_lo) : nullptr;
   if (fold_last) {
     k_ct_reset_dtmin<<<1, 1, 0, c->stream>>>(c->clock);
     k_ct_cells<S, true><<<grid, CT_NX * CT_TY, 0, c->stream>>>(m, c->eos, (S *)md1.cc, lo, (const S *)md1.fc,
-                                                               (S *)c->prim, c->divb, c->clock);
+                                                               (S *)c->prim, c->divb, c->clock, push);
     c->launches += 2;
   } else {
     k_ct_cells<S, false><<<grid, CT_NX * CT_TY, 0, c->stream>>>(m, c->eos, (S *)md1.cc, lo, (const S *)md1.fc,
-                                                                (S *)c->prim, c->divb, c->clock);
+                                                                (S *)c->prim, c->divb, c->clock, push);
     c->launches++;
   }
   return cuda_check(c, cudaGetLastError(), "ct stream");

@@ -57,6 +57,16 @@
 
 #include "kmy_internal.hpp"
 
+// Unrolling of the constrained-transport stage's loops: the x and y
+// reconstruction loops over the nine variables, and the two lanes of its
+// per-lane MHD Riemann solver.
+#ifndef SLAB_MHD_UNROLL
+#define SLAB_MHD_UNROLL 1
+#endif
+#ifndef SLAB_MHD_LANES
+#define SLAB_MHD_LANES 2
+#endif
+
 namespace kmy {
 
 // Pair arithmetic on double2, lane by lane (the float2 forms are packed
@@ -70,8 +80,15 @@ constexpr int NX = 32;            // interior cells along x (one warp per row)
 constexpr int HH = 3;             // staged halo cells on each side
 constexpr int PC = NX + 2 * HH;   // 38 staged columns
 constexpr int NV = 6;             // reconstructed: rho, v0, v1, v2, P, e_int
-constexpr int NCV = 5;            // conserved components
-enum : int { SD = 0, SV0 = 1, SPRES = 4, SEINT = 5 };
+constexpr int NCV = 5;            // conserved components the stage updates
+enum : int { SD = 0, SV0 = 1, SPRES = 4, SEINT = 5, SB0 = 6 };
+// With constrained transport the cell-centred field is reconstructed too
+// (slots SB0 .. SB0 + 2) and staged with the other conserved components; the
+// stage updates the five hydro components (the field is the faces' business).
+template <bool MHD> struct Vars {
+  static constexpr int NV = MHD ? 9 : 6;   // reconstructed
+  static constexpr int NCC = MHD ? 8 : 5;  // staged conserved components
+};
 
 // Pair of two planes' values: packed FP32, or FP64 worked lane by lane.
 template <typename R> struct PairOf;
@@ -82,12 +99,12 @@ template <> struct PairOf<double> { using T = double2; };
 // of 256); FP64: 8 (one CTA of 256).
 // x sweep: reconstruction cells -1 .. 32 (34) per row, 33 faces per row;
 // y sweep: cells -1 .. TY (TY + 2) per column, TY + 1 faces per column.
-template <int TY_, typename R>
+template <int TY_, typename R, bool MHD = false>
 struct Tile {
   static constexpr int TY = TY_;
   static constexpr int NT = NX * TY;      // threads, one column each
   static constexpr int PR = TY + 2 * HH;  // staged rows
-  static constexpr int CTAS = (TY == 8 && sizeof(R) == 4) ? 2 : 1;  // CTAs per SM the plan is sized for
+  static constexpr int CTAS = (TY == 8 && sizeof(R) == 4 && !MHD) ? 2 : 1;  // CTAs per SM the plan is sized for
   static constexpr int RXC = NX + 2, RYC = TY + 2;
   static constexpr int REC_N = RXC * TY > RYC * NX ? RXC * TY : RYC * NX;  // pairs per variable and side
   static constexpr int FX_N = (NX + 1) * TY, FY_N = NX * (TY + 1);
@@ -117,15 +134,21 @@ struct Args {
   // test sets it, with a short limit, to make the wait run out)
   int wait_limit;
   unsigned tx_extra;
+  // constrained transport: the stage input's face field (the Riemann
+  // problems' normal component) and the face-flux arrays the edge EMFs read,
+  // layout [dir][8][nb * Pf]
+  const R *fc0;
+  R *flux;
 };
 
 // Shared-memory plan (bytes), the same on host and device: one raw slot (the
 // stage input of one plane pair as the tensor loads deliver it), the
 // interleaved primitives of the centre pair, the reconstructed face values
 // and the face fluxes of one sweep, the mbarrier and reduction scratch.
-template <int TY, typename R>
+template <int TY, typename R, bool MHD = false>
 struct Smem {
-  using T = Tile<TY, R>;
+  using T = Tile<TY, R, MHD>;
+  static constexpr int NVK = Vars<MHD>::NV, NCCK = Vars<MHD>::NCC;
   static constexpr int ES = int(sizeof(R));      // bytes per staged value
   static constexpr int PS = 2 * int(sizeof(R));  // bytes per pair
   static constexpr bool LO = sizeof(R) == 4;     // FP32 stages the energy low words too
@@ -134,14 +157,14 @@ struct Smem {
   __host__ __device__ static constexpr int rup(int x) { return (x + 127) & ~127; }
   __host__ __device__ int raw_plane() const { return T::PR * np0; }           // values
   __host__ __device__ int raw_var() const { return 2 * raw_plane(); }         // values
-  __host__ __device__ int cc_bytes() const { return NCV * raw_var() * ES; }
+  __host__ __device__ int cc_bytes() const { return NCCK * raw_var() * ES; }
   __host__ __device__ int lo_off() const { return rup(cc_bytes()); }
   __host__ __device__ int lo_bytes() const { return LO ? raw_var() * 4 : 0; }
   __host__ __device__ int slot_bytes() const { return rup(lo_off() + lo_bytes()); }
   __host__ __device__ int prim_off() const { return slot_bytes(); }
-  __host__ __device__ static constexpr int prim_bytes() { return NV * T::PR * PC * PS; }
+  __host__ __device__ static constexpr int prim_bytes() { return NVK * T::PR * PC * PS; }
   __host__ __device__ int rec_off() const { return prim_off() + prim_bytes(); }
-  __host__ __device__ static constexpr int rec_bytes() { return 2 * NV * T::REC_N * PS; }
+  __host__ __device__ static constexpr int rec_bytes() { return 2 * NVK * T::REC_N * PS; }
   __host__ __device__ int flx_off() const { return rec_off() + rec_bytes(); }
   __host__ __device__ static constexpr int flx_bytes() { return NCV * T::FLX_N * PS; }
   __host__ __device__ int bar_off() const { return flx_off() + flx_bytes(); }
@@ -497,6 +520,71 @@ __device__ __forceinline__ void slab_prim(const EosParams &eos, double rho, doub
   V[SEINT] = W[REINT];
 }
 
+// Constrained transport, FP32: the primitives of a staged cell with its
+// cell-centred field; e_int = (E_hi + E_lo) - |m|^2 / (2 rho) - |B|^2 / 2 in
+// FP64 (primconsflux.hpp:76-98).
+__device__ __forceinline__ void slab_prim_mhd(float gm1, const float (&u)[8], float elo, float (&V)[9]) {
+  const float rho = u[CDENS];
+  const float r0 = rcp_approx(rho);
+  V[SD] = rho;
+#pragma unroll
+  for (int d = 0; d < 3; d++) V[SV0 + d] = u[CMOM0 + d] * r0;
+  const double dd = double(rho), r0d = double(r0);
+  const double id = fma(r0d, fma(-dd, r0d, 1.0), r0d);
+  const double msq = fma(double(u[CMOM0]), double(u[CMOM0]),
+                         fma(double(u[CMOM1]), double(u[CMOM1]), double(u[CMOM2]) * double(u[CMOM2])));
+  const double bsq = fma(double(u[CMAGC0]), double(u[CMAGC0]),
+                         fma(double(u[CMAGC0 + 1]), double(u[CMAGC0 + 1]),
+                             double(u[CMAGC0 + 2]) * double(u[CMAGC0 + 2])));
+  const double eint = ((double(u[CENER]) + double(elo)) - 0.5 * msq * id) - 0.5 * bsq;
+  const float sie = float(eint * id);
+  V[SEINT] = sie;
+  V[SPRES] = fmaxf(0.f, gm1 * rho * sie);
+#pragma unroll
+  for (int d = 0; d < 3; d++) V[SB0 + d] = u[CMAGC0 + d];
+}
+
+// Constrained transport, FP32: the MHD Riemann flux at two faces, lane by lane
+// through RiemannFlux<RIEMANN, MHD> (riemann_solver.hpp:20-149), with the face
+// field bn as the normal component of both states
+// (hydro_add_flux_tasks.cpp:343-346) and the face bulk modulus gamma P.  F
+// gets the five hydro fluxes; Bt[lane][0 / 1] the fluxes of the two
+// transverse field components (DIR1 + 1, DIR1 + 2 mod 3 in increasing axis
+// order), which the edge EMFs read.
+template <int RIEMANN, int DIR1>
+__device__ __forceinline__ void SlabRiemannMHD2(const float2 *vL, const float2 *vR, float gam, float2 bn,
+                                                float2 *F, float (&Bt)[2][2]) {
+  float fl[2][8];
+  constexpr int LANES = SLAB_MHD_LANES;
+#pragma unroll(LANES)
+  for (int h = 0; h < 2; h++) {
+    auto lane = [h](float2 p) { return h ? p.y : p.x; };
+    float L[10], Rv[10];
+    L[RDENS] = lane(vL[SD]);
+    Rv[RDENS] = lane(vR[SD]);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      L[RVEL0 + d] = lane(vL[SV0 + d]);
+      Rv[RVEL0 + d] = lane(vR[SV0 + d]);
+      L[RMAGC0 + d] = lane(vL[SB0 + d]);
+      Rv[RMAGC0 + d] = lane(vR[SB0 + d]);
+    }
+    L[RPRES] = lane(vL[SPRES]);
+    Rv[RPRES] = lane(vR[SPRES]);
+    L[RBMOD] = gam * L[RPRES];
+    Rv[RBMOD] = gam * Rv[RPRES];
+    L[REINT] = lane(vL[SEINT]);
+    Rv[REINT] = lane(vR[SEINT]);
+    L[RMAGC0 + DIR1] = Rv[RMAGC0 + DIR1] = lane(bn);
+    RiemannFlux<RIEMANN, true, DIR1, float>(L, Rv, fl[h]);
+    constexpr int T0 = DIR1 == 0 ? 1 : 0, T1 = DIR1 == 2 ? 1 : 2;
+    Bt[h][0] = fl[h][CMAGC0 + T0];
+    Bt[h][1] = fl[h][CMAGC0 + T1];
+  }
+#pragma unroll
+  for (int v = 0; v < NCV; v++) F[v] = make_float2(fl[0][v], fl[1][v]);
+}
+
 // ---------------------------------------------------------------------------
 // Face ghosts of the new state.  An interior cell at local index l along axis
 // d is the source of the ghost cells that Parthenon's boundary exchange would
@@ -562,21 +650,26 @@ __device__ __forceinline__ void ghost_push_axis(const Args<R> &a, int d, int b, 
 #define SLAB_F64_UNROLL 1
 #endif
 
+
 // The stage kernel.  tm_cc maps the stage input's conserved components;
-// tm_lo its energy low words (FP32; unused in FP64).
-template <typename R, int TY_, int RECON, int RIEMANN>
-__global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
+// tm_lo its energy low words (FP32; unused in FP64).  MHD: constrained
+// transport (FP32): nine reconstructed variables, the face field as the
+// normal B of every Riemann problem, the transverse field fluxes written out.
+template <typename R, int TY_, int RECON, int RIEMANN, bool MHD = false>
+__global__ void __launch_bounds__(Tile<TY_, R, MHD>::NT, Tile<TY_, R, MHD>::CTAS)
     k_slab_stage(const __grid_constant__ CUtensorMap tm_cc, const __grid_constant__ CUtensorMap tm_lo,
                  const __grid_constant__ Args<R> a) {
-  using T = Tile<TY_, R>;
+  using T = Tile<TY_, R, MHD>;
   using P = typename PairOf<R>::T;
   constexpr bool LO = sizeof(R) == 4;
+  static_assert(!MHD || LO, "the constrained-transport stage is FP32");
+  constexpr int NV = Vars<MHD>::NV, NCC = Vars<MHD>::NCC;
   constexpr int TY = T::TY, NT = T::NT, PR = T::PR, RXC = T::RXC, REC_N = T::REC_N, FLX_N = T::FLX_N;
-  // unrolling of the x and y reconstruction loops over the six variables
-  constexpr int RU = LO ? NV : SLAB_F64_UNROLL;
+  // unrolling of the x and y reconstruction loops over the variables
+  constexpr int RU = LO ? (MHD ? SLAB_MHD_UNROLL : NV) : SLAB_F64_UNROLL;
   extern __shared__ __align__(128) unsigned char smem[];
   const MeshDesc &m = a.m;
-  const Smem<TY_, R> L(m.np[0]);
+  const Smem<TY_, R, MHD> L(m.np[0]);
   const int tid = threadIdx.x, lane = tid & 31, wr = tid >> 5;
   const int np0 = m.np[0], gx = m.g[0], nz = m.nx[2], nz2 = nz / 2;
   // the raw slot: the conserved box of a plane pair, then (FP32) its energy low words
@@ -630,7 +723,7 @@ __global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
         gv.lo = LO ? a.u0lo[n] : 0.f;
         if (a.u1 != a.u0) {
 #pragma unroll
-          for (int v = 0; v < NCV; v++) a.u1[v * NP + n] = gv.v[v];
+          for (int v = 0; v < NCC; v++) a.u1[v * NP + n] = a.u0[v * NP + n];
           if constexpr (LO) a.u1lo[n] = gv.lo;
         }
         const int pc[3] = {lane + gx, oy + wr + m.g[1], z + m.g[2]};
@@ -665,7 +758,12 @@ __global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
     // primitives of the staged cell at raw offset o
     auto cell_prim = [&](int o, R (&V)[NV]) {
       const R *r = rawcc;
-      if constexpr (LO) {
+      if constexpr (MHD) {
+        float u[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) u[v] = r[v * RV + o];
+        slab_prim_mhd(a.gm1, u, rawlo[o], V);
+      } else if constexpr (LO) {
         slab_prim(a.gm1, r[o], r[RV + o], r[2 * RV + o], r[3 * RV + o], r[4 * RV + o], rawlo[o], V);
       } else {
         slab_prim(a.eos, r[o], r[RV + o], r[2 * RV + o], r[3 * RV + o], r[4 * RV + o], V);
@@ -706,6 +804,30 @@ __global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
         for (int v = 0; v < NV; v++) prim[(v * PR + rr) * PC + cc] = mk2(V0[v], V1[v]);
       }
     };
+    // constrained transport: face-array offsets of this block (interior
+    // coordinates), and the transverse field fluxes of a face pair written
+    // for the edge EMFs (each face by the tile that owns it)
+    int kz = 0;  // the current pair's first plane
+    const long long NF = (long long)m.nb * m.Pf, fbo = (long long)b * m.Pf;
+    const long long fsk = (long long)m.nf[0] * m.nf[1];
+    auto foff = [&](int k, int jj, int ii) {
+      return fbo + ((long long)(k + m.g[2]) * m.nf[1] + (jj + m.g[1])) * m.nf[0] + (ii + m.g[0]);
+    };
+    auto put_bt = [&](int dir, long long fo, const float (&Bt)[2][2], bool own0, bool own1) {
+      if constexpr (MHD) {
+        const int t0 = dir == 0 ? 1 : 0, t1 = dir == 2 ? 1 : 2;
+        R *F0 = a.flux + ((long long)dir * 8 + CMAGC0 + t0) * NF;
+        R *F1 = a.flux + ((long long)dir * 8 + CMAGC0 + t1) * NF;
+        if (own0) {
+          F0[fo] = Bt[0][0];
+          F1[fo] = Bt[0][1];
+        }
+        if (own1) {
+          F0[fo + fsk] = Bt[1][0];
+          F1[fo + fsk] = Bt[1][1];
+        }
+      }
+    };
     auto recon_x = [&](int v, int r, int xx) {
       const P *c = prim + (v * PR + r + HH) * PC + xx;
       P s[5];
@@ -724,7 +846,15 @@ __global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
         vR[v] = rm[v * REC_N + r * RXC + f + 1];
       }
       P F[NCV];
-      SlabRiemann2<RIEMANN, 0>(vL, vR, a.gam, F);
+      if constexpr (MHD) {
+        // x face f of tile row r on the pair's two planes; every one is this tile's
+        const long long fo = foff(kz, oy + r, f);
+        float Bt[2][2];
+        SlabRiemannMHD2<RIEMANN, 0>(vL, vR, a.gam, mk2(a.fc0[fo], a.fc0[fo + fsk]), F, Bt);
+        put_bt(0, fo, Bt, true, true);
+      } else {
+        SlabRiemann2<RIEMANN, 0>(vL, vR, a.gam, F);
+      }
 #pragma unroll
       for (int v = 0; v < NCV; v++) flx[v * FLX_N + r * (NX + 1) + f] = F[v];
     };
@@ -746,7 +876,16 @@ __global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
         vR[v] = rm[v * REC_N + (f + 1) * NX + x];
       }
       P F[NCV];
-      SlabRiemann2<RIEMANN, 1>(vL, vR, a.gam, F);
+      if constexpr (MHD) {
+        // y face oy + f: the tile's own unless it is the next tile's first row
+        const long long fo = foff(kz, oy + f, x);
+        float Bt[2][2];
+        SlabRiemannMHD2<RIEMANN, 1>(vL, vR, a.gam, mk2(a.fc0[NF + fo], a.fc0[NF + fo + fsk]), F, Bt);
+        const bool own = f < TY || oy + TY == m.nx[1];
+        put_bt(1, fo, Bt, own, own);
+      } else {
+        SlabRiemann2<RIEMANN, 1>(vL, vR, a.gam, F);
+      }
 #pragma unroll
       for (int v = 0; v < NCV; v++) flx[v * FLX_N + f * NX + x] = F[v];
     };
@@ -814,6 +953,7 @@ __global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
 
     for (int j = -1; j <= nz2 + 1; j++) {
       const bool centre = j >= 0 && j < nz2;
+      kz = 2 * j;
       // ---- phase A: the pending update of cells (2j-3, 2j-2), the next
       // pair's loads, x reconstruction of this step's planes ----
       if (j - 1 >= 0 && j - 1 < nz2) {
@@ -862,8 +1002,10 @@ __global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
             if (py) ghost_push_axis(a, 1, b, lb, pc, gv);
             if (pz) ghost_push_axis(a, 2, b, lb, pc, gv);
           }
-          if (a.last) {
-            if constexpr (LO) {
+          // (constrained transport: the cell pass after the face update takes the estimate)
+          if (!MHD && a.last) {
+            if constexpr (MHD) {
+            } else if constexpr (LO) {
               float V[NV];
               slab_prim(a.gm1, gv.v[0], gv.v[1], gv.v[2], gv.v[3], gv.v[4], gv.lo, V);
 #pragma unroll
@@ -946,7 +1088,15 @@ __global__ void __launch_bounds__(Tile<TY_, R>::NT, Tile<TY_, R>::CTAS)
         P vL[NV];
 #pragma unroll
         for (int v = 0; v < NV; v++) vL[v] = mk2(vPc[v], vp[v].x);
-        SlabRiemann2<RIEMANN, 2>(vL, vm, a.gam, zF);
+        if constexpr (MHD) {
+          // z faces 2j and 2j + 1 of the column; those in 0 .. nz are its own
+          const long long fo = foff(2 * j, oy + wr, lane);
+          float Bt[2][2];
+          SlabRiemannMHD2<RIEMANN, 2>(vL, vm, a.gam, mk2(a.fc0[2 * NF + fo], a.fc0[2 * NF + fo + fsk]), zF, Bt);
+          put_bt(2, fo, Bt, 2 * j >= 0 && 2 * j <= nz, 2 * j + 1 >= 0 && 2 * j + 1 <= nz);
+        } else {
+          SlabRiemann2<RIEMANN, 2>(vL, vm, a.gam, zF);
+        }
 #pragma unroll
         for (int v = 0; v < NV; v++) {
           vPc[v] = vp[v].y;

@@ -18,6 +18,8 @@ int slab_dispatch_f32(kmy_ctx *c, const CUtensorMap &mc, const CUtensorMap &ml, 
                       int ty, int grid, size_t smem);
 int slab_dispatch_f64(kmy_ctx *c, const CUtensorMap &mc, const CUtensorMap &ml, const slab::Args<double> &a,
                       int ty, int grid, size_t smem);
+int slab_dispatch_mhd(kmy_ctx *c, const CUtensorMap &mc, const CUtensorMap &ml, const slab::Args<float> &a,
+                      int ty, int grid, size_t smem);
 
 namespace {
 
@@ -86,10 +88,13 @@ int sm_count(int device) {
 // Shared memory of one CTA and CTAs per SM of the plan for this precision and tile.
 int slab_smem(const kmy_ctx *c, int ty) {
   const int np0 = c->m.np[0];
+  if (c->prm.mhd)
+    return ty == 8 ? slab::Smem<8, float, true>(np0).total() : slab::Smem<16, float, true>(np0).total();
   if (c->esz == 4) return ty == 8 ? slab::Smem<8, float>(np0).total() : slab::Smem<16, float>(np0).total();
   return ty == 8 ? slab::Smem<8, double>(np0).total() : slab::Smem<16, double>(np0).total();
 }
 int slab_ctas(const kmy_ctx *c, int ty) {
+  if (c->prm.mhd) return ty == 8 ? slab::Tile<8, float, true>::CTAS : slab::Tile<16, float, true>::CTAS;
   if (c->esz == 4) return ty == 8 ? slab::Tile<8, float>::CTAS : slab::Tile<16, float>::CTAS;
   return ty == 8 ? slab::Tile<8, double>::CTAS : slab::Tile<16, double>::CTAS;
 }
@@ -98,7 +103,8 @@ int slab_ctas(const kmy_ctx *c, int ty) {
 
 // Rows per tile for this context: the deck's (or the tuner's) choice, else
 // in FP32 16 where the block height allows it (measured faster than 8 on the
-// 256^3 WENO-Z workload), else 8; FP64 runs 8.
+// 256^3 WENO-Z workload, and 3.54 against 4.56 ms per step on the 192^3
+// Orszag-Tang workload with constrained transport), else 8; FP64 runs 8.
 int slab_rows(const kmy_ctx *c) {
   if (c->prm.slab_rows) return c->prm.slab_rows;
   if (c->esz == 8) return 8;
@@ -109,7 +115,14 @@ const char *slab_unsupported(const kmy_ctx *c) {
   const MeshDesc &m = c->m;
   if (c->esz != 4 && c->esz != 8) return "the z-streamed stage is FP32 or FP64";
   if (m.ndim != 3) return "the z-streamed stage is 3D";
-  if (c->prm.mhd) return "constrained transport runs the brick stage";
+  if (c->prm.mhd) {
+    if (c->esz != 4) return "constrained transport runs the FP64 brick stage";
+    // the cell pass of the streamed face update keeps the field's face ghosts
+    if (ct_stream_unsupported(c)) return "constrained transport without the streamed face update";
+    for (int d = 0; d < 3; d++)
+      for (int side = 0; side < 2; side++)
+        if (m.bc[d][side] == BC_REFLECT) return "constrained transport with reflecting boundaries";
+  }
   if (c->amr.on) return "adaptive meshes run the per-task kernels";
   if (m.nx[0] != slab::NX) return "the z-streamed stage needs 32 cells per block along x";
   const int ty = slab_rows(c);
@@ -128,6 +141,10 @@ const char *slab_unsupported(const kmy_ctx *c) {
   return nullptr;
 }
 
+bool ct_cells_on_slab(const kmy_ctx *c) {
+  return c->prm.mhd && c->prm.stage_kernel != 1 && !slab_unsupported(c);
+}
+
 int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, bool last) {
   if (const char *why = slab_unsupported(c)) {
     c->err = std::string("slab stage: ") + why;
@@ -136,13 +153,22 @@ int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md
   if (!md0.ghosts) {
     if (const int rc = launch_fill_ghosts(c, md0)) return rc;
   }
+  // constrained transport: the face-flux arrays the edge EMFs read
+  if (c->prm.mhd) {
+    if (const int rc = ensure_flux(c)) return rc;
+    if (!md0.fc || !c->flux) {
+      c->err = "slab stage: constrained transport without face arrays";
+      return KMY_ERR_STATE;
+    }
+  }
   const MeshDesc &m = c->m;
   const bool f32 = c->esz == 4;
   CUtensorMap mc, ml;
   std::memset(&mc, 0, sizeof(mc));
   std::memset(&ml, 0, sizeof(ml));
   const int ty = slab_rows(c);
-  if (int rc = make_map(c, &mc, md0.cc, slab::NCV, ty + 2 * slab::HH, int(c->esz))) return rc;
+  const int ncc = c->prm.mhd ? 8 : slab::NCV;
+  if (int rc = make_map(c, &mc, md0.cc, ncc, ty + 2 * slab::HH, int(c->esz))) return rc;
   if (f32) {
     if (int rc = make_map(c, &ml, md0.ener_lo, 1, ty + 2 * slab::HH, 4)) return rc;
   } else {
@@ -169,6 +195,8 @@ int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md
     a.nitems = m.nb * a.nty;
     a.wait_limit = 1 << 22;
     a.tx_extra = 0;
+    a.fc0 = c->prm.mhd ? static_cast<const R *>(md0.fc) : nullptr;
+    a.flux = c->prm.mhd ? static_cast<R *>(c->flux) : nullptr;
     if (c->fault_wait) {
       // kmy_set_fault(ctx, "stage_wait", 1): this stage's waits run out
       a.tx_extra = 16;
@@ -186,7 +214,7 @@ int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md
   if (f32) {
     slab::Args<float> a{};
     fill(a);
-    rc = slab_dispatch_f32(c, mc, ml, a, ty, grid, smem);
+    rc = c->prm.mhd ? slab_dispatch_mhd(c, mc, ml, a, ty, grid, smem) : slab_dispatch_f32(c, mc, ml, a, ty, grid, smem);
   } else {
     slab::Args<double> a{};
     fill(a);
