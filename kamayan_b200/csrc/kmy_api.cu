@@ -963,13 +963,11 @@ static int adopt_rk1_output(kmy_ctx *c) {
   return rc;
 }
 
-// Whether the hydro stage runs the z-streamed kernel (kmy_slab_f32.cu): by
-// default wherever it applies (FP32, 3D, 32-cell rows), or as the deck's
-// <kamayan_b200> stage_kernel asks.
-static bool use_slab(const kmy_ctx *c) {
-  if (c->prm.stage_kernel == 1) return false;
-  return !slab_unsupported(c);
-}
+// Whether the hydro stage runs the z-streamed kernel (kmy_slab_host.cu): by
+// default where it applies (3D, 32-cell rows) on meshes large enough to fill
+// the GPU with its work items, or as the deck's <kamayan_b200> stage_kernel
+// asks.
+static bool use_slab(const kmy_ctx *c) { return slab_runs(c); }
 
 // One stage through the z-streamed kernel.  rk1 updates base in place, and
 // the kernel reads its input's neighbouring blocks while it writes, so rk1

@@ -311,8 +311,10 @@ const char *slab_unsupported(const kmy_ctx *c);
 // Rows per tile the z-streamed stage uses for this context (8 or 16).
 int slab_rows(const kmy_ctx *c);
 int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, bool last);
-// Whether a constrained-transport stage runs its cells through the
-// z-streamed stage (the deck allows it and it applies).
+// Whether the fused stage runs the z-streamed kernel (it applies, the deck
+// allows it, and in auto mode the mesh has enough work items), and whether a
+// constrained-transport stage runs its cells through it.
+bool slab_runs(const kmy_ctx *c);
 bool ct_cells_on_slab(const kmy_ctx *c);
 // ---- streamed constrained-transport face update (kmy_ct.cu) ----
 // Why the streamed face update cannot run this context, or null.

@@ -141,9 +141,22 @@ const char *slab_unsupported(const kmy_ctx *c) {
   return nullptr;
 }
 
-bool ct_cells_on_slab(const kmy_ctx *c) {
-  return c->prm.mhd && c->prm.stage_kernel != 1 && !slab_unsupported(c);
+// Whether the z-streamed stage runs this context's stages: where it applies,
+// unless the deck asks for the brick stage, and by default (stage_kernel =
+// auto) only on meshes with enough (block, tile) work items to fill the GPU.
+// A work item walks a whole block along z, one CTA per SM: with fewer items
+// than about half the SMs (FP32) or than the SMs (FP64, a slower item) the
+// brick stage, which spreads a block over many CTAs, is faster (a 64^3 mesh
+// of 32^3 blocks has 16 FP32 items).
+bool slab_runs(const kmy_ctx *c) {
+  if (c->prm.stage_kernel == 1 || slab_unsupported(c)) return false;
+  if (c->prm.stage_kernel != 0) return true;
+  const long long items = (long long)c->m.nb * (c->m.nx[1] / slab_rows(c));
+  const int sms = sm_count(c->device);
+  return c->esz == 8 ? items >= sms : 2 * items >= sms;
 }
+
+bool ct_cells_on_slab(const kmy_ctx *c) { return c->prm.mhd && slab_runs(c); }
 
 int launch_slab_stage(kmy_ctx *c, Container &base, Container &md0, Container &md1, double beta, bool last) {
   if (const char *why = slab_unsupported(c)) {

@@ -326,8 +326,17 @@ int launch_compute_fluxes(kmy_ctx *c, Container &md0) {
 // came from, so the flux is copied from there.  One thread per ghost-layer
 // face: face direction a, transverse axis t, side, the a-face index and the
 // remaining axis c.
+// One launch covers every (face direction a, transverse axis t) pair of the
+// mesh: blockIdx.y indexes the pairs ((a, t) in pairs[], na and nc per pair).
+struct FluxHaloPairs {
+  int n;
+  int a[6], t[6], na[6], nc[6];
+};
+
 template <typename S>
-__global__ void k_flux_halo(MeshDesc m, S *flux, int a, int t, int na, int nc) {
+__global__ void k_flux_halo(MeshDesc m, S *flux, FluxHaloPairs pairs) {
+  const int pi = blockIdx.y;
+  const int a = pairs.a[pi], t = pairs.t[pi], na = pairs.na[pi], nc = pairs.nc[pi];
   const int cax = 3 - a - t;
   const long long tt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = 2LL * na * nc;
@@ -361,17 +370,25 @@ __global__ void k_flux_halo(MeshDesc m, S *flux, int a, int t, int na, int nc) {
 
 int launch_flux_halo(kmy_ctx *c) {
   const MeshDesc &m = c->m;
+  FluxHaloPairs p{};
+  long long most = 0;
   for (int a = 0; a < m.ndim; a++)
     for (int t = 0; t < m.ndim; t++) {
       if (t == a) continue;
-      const int na = m.nx[a] + 1, nc = m.nx[3 - a - t];
-      const long long tot = 2LL * na * nc * m.nb;
-      if (c->esz == 8)
-        k_flux_halo<double><<<nblk(tot), kThreads, 0, c->stream>>>(m, (double *)c->flux, a, t, na, nc);
-      else
-        k_flux_halo<float><<<nblk(tot), kThreads, 0, c->stream>>>(m, (float *)c->flux, a, t, na, nc);
-      c->launches++;
+      p.a[p.n] = a;
+      p.t[p.n] = t;
+      p.na[p.n] = m.nx[a] + 1;
+      p.nc[p.n] = m.nx[3 - a - t];
+      most = std::max(most, 2LL * p.na[p.n] * p.nc[p.n] * m.nb);
+      p.n++;
     }
+  if (!p.n) return KMY_OK;
+  const dim3 grid(nblk(most), unsigned(p.n));
+  if (c->esz == 8)
+    k_flux_halo<double><<<grid, kThreads, 0, c->stream>>>(m, (double *)c->flux, p);
+  else
+    k_flux_halo<float><<<grid, kThreads, 0, c->stream>>>(m, (float *)c->flux, p);
+  c->launches++;
   return cuda_check(c, cudaGetLastError(), "flux_halo");
 }
 

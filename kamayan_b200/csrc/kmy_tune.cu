@@ -254,9 +254,8 @@ int kmy_stage_kernel(const kmy_ctx *c, char *name, size_t n) {
   if (!c || !name || n == 0) return KMY_ERR_BAD_PARAM;
   const char *s = "tasks";
   if (c->path == 0 && !c->amr.on) {
-    if (c->prm.stage_kernel == 1 || (c->prm.mhd && slab_unsupported(c))) s = "brick";
-    else if (c->prm.stage_kernel == 3) s = "tune";
-    else if (!slab_unsupported(c)) s = slab_rows(c) == 8 ? "slab8" : "slab16";
+    if (c->prm.stage_kernel == 3 && !c->prm.mhd) s = "tune";
+    else if (slab_runs(c)) s = slab_rows(c) == 8 ? "slab8" : "slab16";
     else s = c->prm.stage_kernel == 2 ? "slab (does not apply)" : "brick";
   }
   std::snprintf(name, n, "%s", s);

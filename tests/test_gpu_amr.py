@@ -223,8 +223,12 @@ def test_evolve_graph_matches_steps(kmy_lib):
         s.pgen("blast")
     for _ in range(60):
         sa.step()
-    sb.evolve(1e30, 60)
+    sb.evolve(1e30, 30)
+    r30 = sb.graph_replays
+    sb.evolve(1e30, 30)
     assert sa.time == sb.time and sa.time["ncycle"] == 60
+    # the steps replayed their captured graphs, also on meshes after a remesh
+    assert r30 > 0 and sb.graph_replays > r30
     la, ca = sa.blocks()
     lb, cb = sb.blocks()
     assert np.array_equal(la, lb) and np.array_equal(ca, cb)

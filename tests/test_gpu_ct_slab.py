@@ -52,9 +52,11 @@ def close(a, b, tol):
         assert err <= tol, ("mag", c, err)
 
 
-def test_default_kernel_is_the_slab(kmy_lib):
-    assert K.Solver(ot(kernel="auto")).stage_kernel == "slab16"
-    assert K.Solver(ot(precision="fp64", kernel="auto")).stage_kernel == "brick"
+def test_default_kernel_is_the_slab_on_large_meshes(kmy_lib):
+    # 192^3: 432 work items of 16 rows; 64^3: 16, too few to fill the GPU
+    assert K.Solver(ot(kernel="auto", n=192)).stage_kernel == "slab16"
+    assert K.Solver(ot(kernel="auto")).stage_kernel == "brick"
+    assert K.Solver(ot(precision="fp64", kernel="auto", n=192)).stage_kernel == "brick"
 
 
 @pytest.mark.parametrize("rows", ["8", "16"])

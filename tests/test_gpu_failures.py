@@ -35,8 +35,13 @@ def _poison(s):
     s.finalize_import()
 
 
-@pytest.mark.parametrize("deck", [configs.kh_3d(n=32, nb=16),                    # FP64 brick
-                                  configs.kh_3d(n=64, nb=32, precision="fp32")],  # FP32 z-streamed
+def _slab(deck):
+    deck.set("kamayan_b200", "stage_kernel", "slab")
+    return deck
+
+
+@pytest.mark.parametrize("deck", [configs.kh_3d(n=32, nb=16),                           # FP64 brick
+                                  _slab(configs.kh_3d(n=64, nb=32, precision="fp32"))],  # FP32 z-streamed
                          ids=["fp64_brick", "fp32_slab"])
 def test_nan_density_returns_nonfinite(kmy_lib, deck):
     s = K.Solver(deck)
@@ -83,6 +88,7 @@ def test_dt_above_dt_max(kmy_lib):
 
 def test_stage_wait_runs_out(kmy_lib):
     deck = configs.kh_3d(n=64, nb=32, precision="fp32")
+    deck.set("kamayan_b200", "stage_kernel", "slab")
     s = K.Solver(deck)
     s.pgen("kelvin_helmholtz")
     assert s.stage_kernel.startswith("slab")

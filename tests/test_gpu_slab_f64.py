@@ -33,9 +33,10 @@ def _check(res: dict, tol: float):
     assert not bad, f"relative L1 above {tol}: {bad}"
 
 
-def test_fp64_default_is_the_slab(kmy_lib):
-    s = K.Solver(kh64(kernel="auto"))
-    assert s.stage_kernel == "slab8"
+def test_fp64_default_is_the_slab_on_large_meshes(kmy_lib):
+    # 192^3: 864 work items of 8 rows; 64^3: 32, too few to fill the GPU
+    assert K.Solver(kh64(kernel="auto", n=192)).stage_kernel == "slab8"
+    assert K.Solver(kh64(kernel="auto")).stage_kernel == "brick"
 
 
 @pytest.mark.parametrize("bcname", list(BCS))
