@@ -85,9 +85,10 @@ def run_stream(requests, nsteps: int, arrivals=None, hbm_fraction: float = 0.7, 
             id_of[srv.submit(requests[k].deck, requests[k].problem, nsteps)] = k
             nxt += 1
         st = srv.stats
-        if st["active"] == 0 and st["queued"] == 0:
-            if nxt < len(order):
-                time.sleep(max(0.0, min(0.002, arr[order[nxt]] - now)))
+        if st["active"] == 0 and st["queued"] == 0 and nxt < len(order):
+            # idle until the next arrival (with every request submitted, tick on:
+            # the tick reports what is left)
+            time.sleep(max(0.0, min(0.002, arr[order[nxt]] - now)))
             continue
         srv.tick()
         t_now = time.perf_counter() - t0
