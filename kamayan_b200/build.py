@@ -34,8 +34,9 @@ EXTRA_FLAGS = {
     # same arithmetic as the single-mesh FP32 stage, so a solve gives the same
     # bits alone and inside a batch
     "kmy_batch_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
-    # the z-streamed FP32 stage, and the device reconstruction functions as the
-    # FP32 stage kernels compile them
+    # the z-streamed stage's FP32 instantiations (hydro and constrained
+    # transport), and the device reconstruction functions as the FP32 stage
+    # kernels compile them
     "kmy_slab_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "kmy_slab_mhd.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     # the streamed CT face update and cell pass: their FP32 instantiations

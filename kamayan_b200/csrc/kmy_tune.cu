@@ -93,7 +93,9 @@ int tune_apply(kmy_ctx *c, const std::string &choice) {
 // the fastest.  results: (name, ms per stage, applies).
 int tune_run(kmy_ctx *c, int reps, std::vector<std::pair<std::string, double>> *results) {
   if (c->prm.mhd || c->amr.on) {
-    // constrained transport runs the brick stage; adaptive meshes the per-task kernels
+    // constrained transport takes the z-streamed stage where it runs (FP32,
+    // enough blocks) and the brick stage elsewhere, without tuning; adaptive
+    // meshes run the per-task kernels
     if (results) results->push_back({"brick", -1.0});
     return tune_apply(c, "brick");
   }
