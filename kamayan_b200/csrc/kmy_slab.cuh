@@ -60,6 +60,9 @@
 // Unrolling of the constrained-transport stage's loops: the x and y
 // reconstruction loops over the nine variables, and the two lanes of its
 // per-lane MHD Riemann solver.
+#ifndef SLAB_Y_EXTRAS_LAST_WARP
+#define SLAB_Y_EXTRAS_LAST_WARP 1
+#endif
 #ifndef SLAB_MHD_UNROLL
 #define SLAB_MHD_UNROLL 1
 #endif
@@ -1071,7 +1074,13 @@ __global__ void __launch_bounds__(Tile<TY_, R, MHD>::NT, Tile<TY_, R, MHD>::CTAS
       }
       if (centre) {
         riemann_y(wr, lane);
+        // the extra face row on the last warp: the first warps also convert
+        // the next pair's halo cells in this phase
+#if SLAB_Y_EXTRAS_LAST_WARP
+        if (tid >= NT - NX) riemann_y(TY, tid - (NT - NX));
+#else
         if (tid < NX) riemann_y(TY, tid);
+#endif
       }
       const bool next_centre = j + 1 >= 0 && j + 1 < nz2;
       P W2[NV];
