@@ -139,7 +139,14 @@ __device__ __forceinline__ void Reconstruct(int limiter, const R (&s)[5], R &vM,
 // cancels: W_k = d_k (A_k + tau^2) prod_{j != k} A_j.  Same value as
 // Reconstruct up to rounding; with eps = 1e-36 the scaled weights stay
 // within [1e-216, 1e+216] for smoothness indicators up to 1e+36.
-template <typename R>
+// The two divisions as IEEE division (Div::div(a, b) = a / b); a stage may
+// pass its own form.
+struct DivIeee {
+  template <typename R>
+  static __device__ __forceinline__ R div(R a, R b) { return a / b; }
+};
+
+template <typename R, typename Div = DivIeee>
 __device__ __forceinline__ void WenoZBothTwoDiv(const R (&s)[5], R &vM, R &vP) {
   const R s0 = s[2];
   const R sixth = R(1.) / R(6.);
@@ -159,11 +166,11 @@ __device__ __forceinline__ void WenoZBothTwoDiv(const R (&s)[5], R &vM, R &vP) {
   const R P01 = A0 * A1, P02 = A0 * A2, P12 = A1 * A2;
   {  // minus face: d = (3, 6, 1) on (beta0, beta1, beta2)
     const R w0 = R(3) * N0 * P12, w1 = R(6) * N1 * P02, w2 = N2 * P01;
-    vM = (w0 * em0 + w1 * em1 + w2 * em2) / (w0 + w1 + w2);
+    vM = Div::div(w0 * em0 + w1 * em1 + w2 * em2, w0 + w1 + w2);
   }
   {  // plus face: d = (3, 6, 1) on (beta2, beta1, beta0)
     const R w0 = R(3) * N2 * P01, w1 = R(6) * N1 * P02, w2 = N0 * P12;
-    vP = (w0 * ep0 + w1 * ep1 + w2 * ep2) / (w0 + w1 + w2);
+    vP = Div::div(w0 * ep0 + w1 * ep1 + w2 * ep2, w0 + w1 + w2);
   }
 }
 

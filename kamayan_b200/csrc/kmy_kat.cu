@@ -8,10 +8,12 @@
 // exactness and left/right mirror symmetry) pin the CUDA code, not only the
 // CPU restatement:
 //   impl 0  FP64 Reconstruct                   (per-task kernels, k_face_flux)
-//   impl 1  FP64 two-division WENO-Z           (FP64 brick and z-streamed stages)
+//   impl 1  FP64 two-division WENO-Z           (FP64 brick stage)
 //   impl 2  FP32 Reconstruct                   (per-lane FP32 path)
 //   impl 3  FP32 packed WenoZBoth2 / per lane  (FP32 brick stage)
 //   impl 4  FP32 packed WenoZPair / per lane   (z-streamed FP32 stage)
+//   impl 5  FP64 ReconPair, lane by lane       (z-streamed FP64 stage: WENO-Z
+//                                               divides by Newton-Raphson reciprocals)
 // This unit compiles with the FP32 stage kernels' flags (approximate
 // division and square root, denormals flushed), so impls 2-4 round as they do.
 #include <string>
@@ -39,6 +41,14 @@ __device__ void kat_one(int impl, int limiter, const double *s, double *out) {
     Reconstruct<RECON, float>(limiter, f, vm, vp);
     out[0] = vm;
     out[1] = vp;
+  } else if (impl == 5) {
+    double2 f[5];
+    for (int k = 0; k < 5; k++) f[k] = make_double2(s[k], s[k]);
+    double2 vm, vp;
+    slab::ReconPair<RECON>(limiter, f, vm, vp);
+    out[0] = vm.x;
+    out[1] = vp.x;
+    out[2] = (vm.x == vm.y && vp.x == vp.y) ? 0.0 : 1.0;
   } else {
     // both lanes carry the case; lane .y must agree with lane .x
     float2 f[5];
@@ -72,7 +82,7 @@ __global__ void k_reconstruct_stencils(int recon, int limiter, int impl, const d
 extern "C" int kmy_reconstruct_stencils(const char *reconstruction, const char *slope_limiter, int impl,
                                         const double *stencils, int n, double *out) {
   using namespace kmy;
-  if (!reconstruction || !slope_limiter || !stencils || !out || n < 0 || impl < 0 || impl > 4)
+  if (!reconstruction || !slope_limiter || !stencils || !out || n < 0 || impl < 0 || impl > 5)
     return KMY_ERR_BAD_PARAM;
   const std::string r(reconstruction), l(slope_limiter);
   const int recon = r == "fog" ? FOG : r == "plm" ? PLM : r == "ppm" ? PPM : r == "wenoz" ? WENOZ : -1;

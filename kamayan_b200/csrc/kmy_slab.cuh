@@ -60,6 +60,11 @@
 // Unrolling of the constrained-transport stage's loops: the x and y
 // reconstruction loops over the nine variables, and the two lanes of its
 // per-lane MHD Riemann solver.
+// FP64 divisions of the z-streamed stage's reconstruction and HLLC as
+// Newton-Raphson reciprocals (rcp_nr) rather than IEEE division
+#ifndef SLAB_F64_NR
+#define SLAB_F64_NR 1
+#endif
 #ifndef SLAB_Y_EXTRAS_LAST_WARP
 #define SLAB_Y_EXTRAS_LAST_WARP 1
 #endif
@@ -304,8 +309,45 @@ __device__ __forceinline__ void ReconPair(int limiter, const float2 (&s)[5], flo
   }
 }
 
+// FP64 reciprocal by Newton-Raphson: the hardware approximation
+// (rcp.approx.ftz.f64, PTX ISA) refined by two iterations r <- r + r (1 - x r),
+// each of which squares the relative error, so the result is within an ulp or
+// two of 1/x for finite, nonzero, normal x (tests/test_gpu_slab_f64.py holds
+// the stage to the oracle at 1e-12).  It takes two fewer dependent FP64
+// operations than IEEE division and no slow-path branch.  Zero and infinite x
+// give NaN (IEEE division gives inf and 0): only states that are already not
+// physical reach them, and the dt controller reports those as non-finite.
+__device__ __forceinline__ double rcp_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  r = fma(r, fma(-x, r, 1.0), r);
+  return fma(r, fma(-x, r, 1.0), r);
+}
+struct DivNR {
+  static __device__ __forceinline__ double div(double a, double b) { return a * rcp_nr(b); }
+};
+// FP64 square root of a >= 0 by Newton-Raphson on the reciprocal square
+// root: the hardware approximation (rsqrt.approx.ftz.f64) refined by two
+// iterations y <- y (3/2 - a y^2 / 2), then sqrt(a) = a y; sqrt(0) = 0.
+__device__ __forceinline__ double sqrt_nr(double a) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  const double h = 0.5 * a;
+  y = y * fma(-h, y * y, 1.5);
+  y = y * fma(-h, y * y, 1.5);
+  return a > 0.0 ? a * y : a;
+}
+#if SLAB_F64_NR
+using SlabDiv64 = DivNR;
+__device__ __forceinline__ double slab_sqrt64(double a) { return sqrt_nr(a); }
+#else
+using SlabDiv64 = DivIeee;
+__device__ __forceinline__ double slab_sqrt64(double a) { return sqrt(a); }
+#endif
+
 // FP64: the per-cell reconstructions of the other FP64 stages, lane by lane
-// (WENO-Z in its two-division form).
+// (WENO-Z in its two-division form, the divisions as Newton-Raphson
+// reciprocals).
 template <int RECON>
 __device__ __forceinline__ void ReconPair(int limiter, const double2 (&s)[5], double2 &vM, double2 &vP) {
   double lo[5], hi[5];
@@ -315,8 +357,8 @@ __device__ __forceinline__ void ReconPair(int limiter, const double2 (&s)[5], do
     hi[k] = s[k].y;
   }
   if constexpr (RECON == WENOZ) {
-    WenoZBothTwoDiv<double>(lo, vM.x, vP.x);
-    WenoZBothTwoDiv<double>(hi, vM.y, vP.y);
+    WenoZBothTwoDiv<double, SlabDiv64>(lo, vM.x, vP.x);
+    WenoZBothTwoDiv<double, SlabDiv64>(hi, vM.y, vP.y);
   } else {
     Reconstruct<RECON, double>(limiter, lo, vM.x, vP.x);
     Reconstruct<RECON, double>(limiter, hi, vM.y, vP.y);
@@ -421,13 +463,13 @@ __device__ __forceinline__ void hllc64(const double (&L)[NV], const double (&Rv)
   const double tiny = DBL_MIN;
   const double uL = L[SV0 + DIR1], uR = Rv[SV0 + DIR1];
   // FastSpeed: sqrt(bulk modulus / rho), bulk modulus gamma P
-  const double cfL = sqrt((1.0 / L[SD]) * (gam * L[SPRES]));
-  const double cfR = sqrt((1.0 / Rv[SD]) * (gam * Rv[SPRES]));
+  const double cfL = slab_sqrt64(SlabDiv64::div(1.0, L[SD]) * (gam * L[SPRES]));
+  const double cfR = slab_sqrt64(SlabDiv64::div(1.0, Rv[SD]) * (gam * Rv[SPRES]));
   const double sL = kmin(-tiny, kmin(uL - cfL, uR - cfR));
   const double sR = kmax(tiny, kmax(uL + cfL, uR + cfR));
   const double dL = sL - uL, dR = sR - uR;
   double ustar = Rv[SPRES] - L[SPRES] + (L[SD] * uL) * dL - (Rv[SD] * uR) * dR;
-  ustar = ustar / (L[SD] * dL - Rv[SD] * dR);
+  ustar = SlabDiv64::div(ustar, L[SD] * dL - Rv[SD] * dR);
   const double pstar = 0.5 * (L[SPRES] + Rv[SPRES] + L[SD] * dL * (ustar - uL) + Rv[SD] * dR * (ustar - uR));
   const bool left = !signbit(ustar);
   const double S = left ? sL : sR;
@@ -442,7 +484,7 @@ __device__ __forceinline__ void hllc64(const double (&L)[NV], const double (&Rv)
   ekin += V[SV0 + 1] * V[SV0 + 1];
   ekin += V[SV0 + 2] * V[SV0 + 2];
   const double E = V[SEINT] * rho + ekin * (0.5 * rho);
-  const double susi = 1.0 / (S - ustar + tiny);
+  const double susi = SlabDiv64::div(1.0, S - ustar + tiny);
   const double Usr = susi * (S * rho - mn);
   const double ratio = susi * (S - un);
   F[CDENS] = mn + S * (Usr - rho);
@@ -510,17 +552,24 @@ __device__ __forceinline__ void slab_prim(float gm1, float rho, float m0, float 
   V[SPRES] = fmaxf(0.f, gm1 * rho * sie);
 }
 
-// FP64: Cons2Prim with the ideal-gas EOS exactly as the other FP64 stages
-// evaluate it (Cons2PrimEos).
+// FP64: Cons2Prim with the ideal-gas EOS (primconsflux.hpp:76-98,
+// equation_of_state.hpp:53-64) in Cons2PrimEos's order, 1/rho through the
+// stage's reciprocal.
 __device__ __forceinline__ void slab_prim(const EosParams &eos, double rho, double m0, double m1, double m2,
                                           double ener, double (&V)[NV]) {
-  double W[7];
-  Cons2PrimEos<false, double>(eos, rho, m0, m1, m2, ener, nullptr, W);
-  V[SD] = W[RDENS];
-#pragma unroll
-  for (int d = 0; d < 3; d++) V[SV0 + d] = W[RVEL0 + d];
-  V[SPRES] = W[RPRES];
-  V[SEINT] = W[REINT];
+  const double idens = SlabDiv64::div(1.0, rho);
+  V[SD] = rho;
+  V[SV0] = idens * m0;
+  V[SV0 + 1] = idens * m1;
+  V[SV0 + 2] = idens * m2;
+  double ekin = 0.0;
+  ekin += V[SV0] * V[SV0];
+  ekin += V[SV0 + 1] * V[SV0 + 1];
+  ekin += V[SV0 + 2] * V[SV0 + 2];
+  ekin *= 0.5 * rho;
+  const double sie = idens * (ener - ekin);
+  V[SEINT] = sie;
+  V[SPRES] = kmax(0.0, eos.gm1 * rho * sie);
 }
 
 // Constrained transport, FP32: the primitives of a staged cell with its

@@ -7,8 +7,8 @@ mirror symmetry on a steep tanh profile (the minus value of the reversed
 stencil equals the plus value within 4 ulps).  The fixtures in
 tests/golden/reconstruction_kat.json restate those inputs; here they run
 through every device form the stage kernels use (kmy_reconstruct_stencils):
-the FP64 per-task and brick forms, and the FP32 per-lane, brick (packed) and
-z-streamed (packed) forms.  FP32 forms are held to the same exactness bound
+the FP64 per-task, brick and z-streamed forms, and the FP32 per-lane, brick
+(packed) and z-streamed (packed) forms.  FP32 forms are held to the same exactness bound
 (their rounding is far below 5e-6 on these values) and to 4 float ulps of
 symmetry; the packed forms' two lanes must agree bit for bit.
 """
@@ -23,7 +23,7 @@ import kamayan_b200 as K
 pytestmark = pytest.mark.gpu
 
 CASES = json.loads((Path(__file__).resolve().parent / "golden" / "reconstruction_kat.json").read_text())
-IMPLS = ["fp64_tasks", "fp64_brick", "fp32_lane", "fp32_brick", "fp32_slab"]
+IMPLS = ["fp64_tasks", "fp64_brick", "fp32_lane", "fp32_brick", "fp32_slab", "fp64_slab"]
 
 
 def ulps(a, b, f32):
