@@ -507,7 +507,7 @@ def main():
                               "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": tot / K,
                               "dtype": "f32" if a.only == "fp32" else "f64", "stage_kernel": kern,
                               "launch_ms_avg": r1["stage_ms_avg"], "config": workload_config(a, ws),
-                              "note": "single-precision profiling run; not the headline line"}),
+                              "note": f"{a.only}-only profiling run; not the headline line"}),
                   flush=True)
         return
 

@@ -229,7 +229,9 @@ int kmy_conserved_sums(kmy_ctx *ctx, const char *md, double *out);
  * kernel uses: 0 FP64 per-task kernels, 1 FP64 brick stage (two-division
  * WENO-Z), 2 FP32 per lane, 3 FP32 brick stage (packed), 4 FP32 z-streamed
  * stage (packed), 5 FP64 z-streamed stage (lane by lane, WENO-Z dividing by
- * Newton-Raphson reciprocals).  Needs no context; runs on the current device and
+ * Newton-Raphson reciprocals); impl 6 returns that stage's Newton-Raphson
+ * reciprocal of stencils[5i] in out[3i] and square root of stencils[5i+1] in
+ * out[3i+1].  Needs no context; runs on the current device and
  * synchronises it.  Counterpart of the reference's device-side Reconstruct
  * (src/physics/hydro/reconstruction.hpp:11-142) as its unit tests call it
  * (src/physics/hydro/tests/test_reconstruction.cpp:13-194). */

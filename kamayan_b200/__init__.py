@@ -546,7 +546,8 @@ def tune_cache_load(path: str) -> None:
 
 
 # ---- the device reconstruction functions on a batch of stencils --------------
-RECON_IMPLS = {"fp64_tasks": 0, "fp64_brick": 1, "fp32_lane": 2, "fp32_brick": 3, "fp32_slab": 4, "fp64_slab": 5}
+RECON_IMPLS = {"fp64_tasks": 0, "fp64_brick": 1, "fp32_lane": 2, "fp32_brick": 3, "fp32_slab": 4, "fp64_slab": 5,
+               "fp64_nr_math": 6}
 
 
 def reconstruct_stencils(reconstruction: str, slope_limiter: str, impl: str, stencils) -> np.ndarray:

@@ -14,6 +14,9 @@
 //   impl 4  FP32 packed WenoZPair / per lane   (z-streamed FP32 stage)
 //   impl 5  FP64 ReconPair, lane by lane       (z-streamed FP64 stage: WENO-Z
 //                                               divides by Newton-Raphson reciprocals)
+//   impl 6  the z-streamed FP64 stage's Newton-Raphson reciprocal of
+//           stencil[0] (out[0]) and square root of stencil[1] (out[1]), for
+//           checking against IEEE division and square root
 // This unit compiles with the FP32 stage kernels' flags (approximate
 // division and square root, denormals flushed), so impls 2-4 round as they do.
 #include <string>
@@ -41,6 +44,9 @@ __device__ void kat_one(int impl, int limiter, const double *s, double *out) {
     Reconstruct<RECON, float>(limiter, f, vm, vp);
     out[0] = vm;
     out[1] = vp;
+  } else if (impl == 6) {
+    out[0] = slab::rcp_nr(s[0]);
+    out[1] = slab::sqrt_nr(s[1]);
   } else if (impl == 5) {
     double2 f[5];
     for (int k = 0; k < 5; k++) f[k] = make_double2(s[k], s[k]);
@@ -82,7 +88,7 @@ __global__ void k_reconstruct_stencils(int recon, int limiter, int impl, const d
 extern "C" int kmy_reconstruct_stencils(const char *reconstruction, const char *slope_limiter, int impl,
                                         const double *stencils, int n, double *out) {
   using namespace kmy;
-  if (!reconstruction || !slope_limiter || !stencils || !out || n < 0 || impl < 0 || impl > 5)
+  if (!reconstruction || !slope_limiter || !stencils || !out || n < 0 || impl < 0 || impl > 6)
     return KMY_ERR_BAD_PARAM;
   const std::string r(reconstruction), l(slope_limiter);
   const int recon = r == "fog" ? FOG : r == "plm" ? PLM : r == "ppm" ? PPM : r == "wenoz" ? WENOZ : -1;

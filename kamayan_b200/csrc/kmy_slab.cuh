@@ -57,17 +57,18 @@
 
 #include "kmy_internal.hpp"
 
-// Unrolling of the constrained-transport stage's loops: the x and y
-// reconstruction loops over the nine variables, and the two lanes of its
-// per-lane MHD Riemann solver.
-// FP64 divisions of the z-streamed stage's reconstruction and HLLC as
-// Newton-Raphson reciprocals (rcp_nr) rather than IEEE division
+// FP64 divisions and square roots of the z-streamed stage (reconstruction,
+// conversion, HLLC) as Newton-Raphson refinements (rcp_nr, sqrt_nr) rather
+// than IEEE division and square root; 0 builds the IEEE form.
 #ifndef SLAB_F64_NR
 #define SLAB_F64_NR 1
 #endif
 #ifndef SLAB_Y_EXTRAS_LAST_WARP
 #define SLAB_Y_EXTRAS_LAST_WARP 1
 #endif
+// Unrolling of the constrained-transport stage's loops: the x and y
+// reconstruction loops over the nine variables, and the two lanes of its
+// per-lane MHD Riemann solver.
 #ifndef SLAB_MHD_UNROLL
 #define SLAB_MHD_UNROLL 1
 #endif
@@ -312,8 +313,9 @@ __device__ __forceinline__ void ReconPair(int limiter, const float2 (&s)[5], flo
 // FP64 reciprocal by Newton-Raphson: the hardware approximation
 // (rcp.approx.ftz.f64, PTX ISA) refined by two iterations r <- r + r (1 - x r),
 // each of which squares the relative error, so the result is within an ulp or
-// two of 1/x for finite, nonzero, normal x (tests/test_gpu_slab_f64.py holds
-// the stage to the oracle at 1e-12).  It takes two fewer dependent FP64
+// two of 1/x for finite, nonzero, normal x (tests/test_gpu_kat.py holds it to
+// 2 ulps of IEEE 1/x; tests/test_gpu_slab_f64.py holds the stage to the oracle
+// at 1e-12).  It takes two fewer dependent FP64
 // operations than IEEE division and no slow-path branch.  Zero and infinite x
 // give NaN (IEEE division gives inf and 0): only states that are already not
 // physical reach them, and the dt controller reports those as non-finite.
@@ -326,16 +328,18 @@ __device__ __forceinline__ double rcp_nr(double x) {
 struct DivNR {
   static __device__ __forceinline__ double div(double a, double b) { return a * rcp_nr(b); }
 };
-// FP64 square root of a >= 0 by Newton-Raphson on the reciprocal square
-// root: the hardware approximation (rsqrt.approx.ftz.f64) refined by two
-// iterations y <- y (3/2 - a y^2 / 2), then sqrt(a) = a y; sqrt(0) = 0.
+// FP64 square root by Newton-Raphson on the reciprocal square root: the
+// hardware approximation (rsqrt.approx.ftz.f64) refined by two iterations
+// y <- y (3/2 - a y^2 / 2), then sqrt(a) = a y, within 3 ulps of IEEE sqrt
+// for normal a > 0 (tests/test_gpu_kat.py); sqrt(0) = 0 and negative a gives
+// NaN, as IEEE sqrt does.
 __device__ __forceinline__ double sqrt_nr(double a) {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
   const double h = 0.5 * a;
   y = y * fma(-h, y * y, 1.5);
   y = y * fma(-h, y * y, 1.5);
-  return a > 0.0 ? a * y : a;
+  return a == 0.0 ? a : a * y;
 }
 #if SLAB_F64_NR
 using SlabDiv64 = DivNR;
