@@ -1,4 +1,7 @@
 // double instantiations of the batched fused stage (separate unit for parallel builds).
+// FP64 divisions and square roots by Newton-Raphson refinement (kdiv, ksqrt
+// in kmy_device.cuh), as in the z-streamed FP64 stage.
+#define KMY_F64_NR 1
 #include "kmy_batch.cuh"
 
 namespace kmy {

@@ -35,6 +35,51 @@ template <typename R> __device__ __forceinline__ R kmin(R a, R b) { return (b < 
 template <typename R> __device__ __forceinline__ R kmax(R a, R b) { return (a < b) ? b : a; }
 template <typename R> __device__ __forceinline__ R sq(R x) { return x * x; }
 
+// FP64 reciprocal by Newton-Raphson: the hardware approximation
+// (rcp.approx.ftz.f64, PTX ISA) refined by two iterations r <- r + r (1 - x r),
+// each of which squares the relative error, so the result is within an ulp or
+// two of 1/x for finite, nonzero, normal x (tests/test_gpu_kat.py holds it to
+// 2 ulps of IEEE 1/x).  It takes two fewer dependent FP64 operations than
+// IEEE division and no slow-path branch.  Zero and infinite x give NaN (IEEE
+// division gives inf and 0): only states that are already not physical reach
+// them, and the dt controller reports those as non-finite.
+__device__ __forceinline__ double rcp_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  r = fma(r, fma(-x, r, 1.0), r);
+  return fma(r, fma(-x, r, 1.0), r);
+}
+// FP64 square root by Newton-Raphson on the reciprocal square root: the
+// hardware approximation (rsqrt.approx.ftz.f64) refined by two iterations
+// y <- y (3/2 - a y^2 / 2), then sqrt(a) = a y, within 3 ulps of IEEE sqrt
+// for normal a > 0 (tests/test_gpu_kat.py); sqrt(0) = 0 and negative a gives
+// NaN, as IEEE sqrt does.
+__device__ __forceinline__ double sqrt_nr(double a) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  const double h = 0.5 * a;
+  y = y * fma(-h, y * y, 1.5);
+  y = y * fma(-h, y * y, 1.5);
+  return a == 0.0 ? a : a * y;
+}
+
+// Division and square root of the per-cell arithmetic below.  A unit that
+// defines KMY_F64_NR as 1 before including this header (the FP64 brick and
+// batched stages) takes the Newton-Raphson forms above in FP64; every other
+// unit (the per-task kernels among them), and FP32 everywhere, takes a / b and
+// sqrt(a) as the unit's compiler flags round them.
+#ifndef KMY_F64_NR
+#define KMY_F64_NR 0
+#endif
+template <typename R> __device__ __forceinline__ R kdiv(R a, R b) {
+  if constexpr (KMY_F64_NR && sizeof(R) == sizeof(double)) return a * rcp_nr(b);
+  else return a / b;
+}
+template <typename R> __device__ __forceinline__ R ksqrt(R a) {
+  if constexpr (KMY_F64_NR && sizeof(R) == sizeof(double)) return sqrt_nr(a);
+  else return sqrt(a);
+}
+
 // reconstruction.hpp:24-39
 template <typename R>
 __device__ __forceinline__ R LimitedSlope(int limiter, R a, R b) {
@@ -42,7 +87,7 @@ __device__ __forceinline__ R LimitedSlope(int limiter, R a, R b) {
     return (copysign(R(1), a) + copysign(R(1), b)) *
            kmin(fabs(a), kmin(R(.25) * fabs(a + b), fabs(b)));
   } else if (limiter == VAN_LEER) {
-    if (a * b > R(0)) return R(2) * a * b / (a + b);
+    if (a * b > R(0)) return kdiv(R(2) * a * b, a + b);
     return R(0);
   }
   return R(0.5) * (copysign(R(1), a) + copysign(R(1), b)) * kmin(fabs(a), fabs(b));
@@ -64,7 +109,7 @@ __host__ __device__ inline int ReconWidthRuntime(int recon) {
 // float range, and at 1e15 that stencil already holds the whole weight.
 template <typename R>
 __device__ __forceinline__ R weno_q(R tau, R beta) {
-  R r = tau / (R(1.e-36) + beta);
+  R r = kdiv(tau, R(1.e-36) + beta);
   if constexpr (sizeof(R) == 4) r = fminf(r, 1.0e15f);
   return R(1) + sq(r);
 }
@@ -123,12 +168,12 @@ __device__ __forceinline__ void Reconstruct(int limiter, const R (&s)[5], R &vM,
     {  // pm = -1: w0 uses beta0, w2 uses beta2
       const R w0 = R(3) * q0, w1 = R(6) * q1, w2 = R(1) * q2;
       const R norm = w0 + w1 + w2;
-      vM = (w0 * em0 + w1 * em1 + w2 * em2) / norm;
+      vM = kdiv(w0 * em0 + w1 * em1 + w2 * em2, norm);
     }
     {  // pm = +1: w0 uses beta2, w2 uses beta0
       const R w0 = R(3) * q2, w1 = R(6) * q1, w2 = R(1) * q0;
       const R norm = w0 + w1 + w2;
-      vP = (w0 * ep0 + w1 * ep1 + w2 * ep2) / norm;
+      vP = kdiv(w0 * ep0 + w1 * ep1 + w2 * ep2, norm);
     }
   }
 }
@@ -139,14 +184,21 @@ __device__ __forceinline__ void Reconstruct(int limiter, const R (&s)[5], R &vM,
 // cancels: W_k = d_k (A_k + tau^2) prod_{j != k} A_j.  Same value as
 // Reconstruct up to rounding; with eps = 1e-36 the scaled weights stay
 // within [1e-216, 1e+216] for smoothness indicators up to 1e+36.
-// The two divisions as IEEE division (Div::div(a, b) = a / b); a stage may
-// pass its own form.
+// The two divisions as the unit's kdiv by default; a stage may pass its own
+// form: DivIeee (a / b) or DivNR (a times the Newton-Raphson reciprocal).
 struct DivIeee {
   template <typename R>
   static __device__ __forceinline__ R div(R a, R b) { return a / b; }
 };
+struct DivNR {
+  static __device__ __forceinline__ double div(double a, double b) { return a * rcp_nr(b); }
+};
+struct DivK {
+  template <typename R>
+  static __device__ __forceinline__ R div(R a, R b) { return kdiv(a, b); }
+};
 
-template <typename R, typename Div = DivIeee>
+template <typename R, typename Div = DivK>
 __device__ __forceinline__ void WenoZBothTwoDiv(const R (&s)[5], R &vM, R &vP) {
   const R s0 = s[2];
   const R sixth = R(1.) / R(6.);
@@ -318,7 +370,7 @@ __device__ __forceinline__ R TotalPres(const R *V) {
 
 template <bool MHD, typename R>
 __device__ __forceinline__ R FastSpeed(int dir1, const R *V) {
-  const R idens = R(1.) / V[RDENS];
+  const R idens = kdiv(R(1.), V[RDENS]);
   const R a2 = idens * V[RBMOD];
   R cfast2;
   if constexpr (!MHD) {
@@ -328,9 +380,9 @@ __device__ __forceinline__ R FastSpeed(int dir1, const R *V) {
     R b2 = R(0);
     for (int dir = 0; dir < 3; dir++) b2 += V[RMAGC0 + dir] * V[RMAGC0 + dir];
     b2 *= idens;
-    cfast2 = R(0.5) * ((a2 + b2) + sqrt((a2 - b2) * (a2 - b2) + R(4) * a2 * (b2 - bb2)));
+    cfast2 = R(0.5) * ((a2 + b2) + ksqrt((a2 - b2) * (a2 - b2) + R(4) * a2 * (b2 - bb2)));
   }
-  return sqrt(cfast2);
+  return ksqrt(cfast2);
 }
 
 template <bool MHD, typename R>
@@ -394,7 +446,7 @@ __device__ __forceinline__ void RiemannFlux(const R *vL, const R *vR, R *flux) {
   const R tiny = Lim<R>::tiny();
   const R sL = kmin(-tiny, kmin(vL[RVEL0 + DIR1] - cfL, vR[RVEL0 + DIR1] - cfR));
   const R sR = kmax(tiny, kmax(vL[RVEL0 + DIR1] + cfL, vR[RVEL0 + DIR1] + cfR));
-  const R sRmsLi = R(1.0) / (sR - sL);
+  const R sRmsLi = kdiv(R(1.0), sR - sL);
   R UL[NC], UR[NC], FL[NC], FR[NC];
   Prim2Cons<MHD>(vL, UL);
   Prim2Cons<MHD>(vR, UR);
@@ -409,23 +461,23 @@ __device__ __forceinline__ void RiemannFlux(const R *vL, const R *vR, R *flux) {
     const R total_presR = TotalPres<MHD>(vR);
     R ustar = total_presR - total_presL + UL[CMOM0 + DIR1] * (sL - vL[RVEL0 + DIR1]) -
               UR[CMOM0 + DIR1] * (sR - vR[RVEL0 + DIR1]);
-    ustar = ustar / (vL[RDENS] * (sL - vL[RVEL0 + DIR1]) - vR[RDENS] * (sR - vR[RVEL0 + DIR1]));
+    ustar = kdiv(ustar, vL[RDENS] * (sL - vL[RVEL0 + DIR1]) - vR[RDENS] * (sR - vR[RVEL0 + DIR1]));
     const R pstar =
         R(0.5) * (total_presL + total_presR +
                   vL[RDENS] * (sL - vL[RVEL0 + DIR1]) * (ustar - vL[RVEL0 + DIR1]) +
                   vR[RDENS] * (sR - vR[RVEL0 + DIR1]) * (ustar - vR[RVEL0 + DIR1]));
     R UsL[NC], UsR[NC];
     auto hllc_state = [&](R S, const R *U, R Pu, R *Us) {
-      const R susi = R(1.) / (S - ustar + tiny);
+      const R susi = kdiv(R(1.), S - ustar + tiny);
       Us[CDENS] = susi * (S * U[CDENS] - U[CMOM0 + DIR1]);
       Us[CMOM0 + DIR1] = Us[CDENS] * ustar;
       // U * Us_dens / U_dens with one shared ratio (one division instead of three)
-      const R rho_ratio = Us[CDENS] / U[CDENS];
+      const R rho_ratio = kdiv(Us[CDENS], U[CDENS]);
       Us[CMOM0 + DIR2] = U[CMOM0 + DIR2] * rho_ratio;
       Us[CMOM0 + DIR3] = U[CMOM0 + DIR3] * rho_ratio;
       Us[CENER] = U[CENER] * rho_ratio + susi * (pstar * ustar - Pu);
       if constexpr (MHD) {
-        const R sRsLi = R(1.) / (sR - sL);
+        const R sRsLi = kdiv(R(1.), sR - sL);
         auto hll = [&](int v) { return sRsLi * (sR * UR[v] - sL * UL[v] + FL[v] - FR[v]); };
         Us[CMAGC0 + DIR1] = hll(CMAGC0 + DIR1);
         Us[CMAGC0 + DIR2] = hll(CMAGC0 + DIR2);
@@ -434,16 +486,16 @@ __device__ __forceinline__ void RiemannFlux(const R *vL, const R *vR, R *flux) {
             (Us[CMAGC0 + DIR1] * Us[CMAGC0 + DIR2] - U[CMAGC0 + DIR1] * U[CMAGC0 + DIR2]) * susi;
         Us[CMOM0 + DIR3] -=
             (Us[CMAGC0 + DIR1] * Us[CMAGC0 + DIR3] - U[CMAGC0 + DIR1] * U[CMAGC0 + DIR3]) * susi;
-        Us[CENER] -= susi * (Us[CMAGC0 + DIR1] *
-                                 (Us[CMAGC0 + DIR1] * hll(CMOM0 + DIR1) +
-                                  Us[CMAGC0 + DIR2] * hll(CMOM0 + DIR2) +
-                                  Us[CMAGC0 + DIR3] * hll(CMOM0 + DIR3)) /
-                                 hll(CDENS) -
-                             U[CMAGC0 + DIR1] *
-                                 (U[CMAGC0 + DIR1] * U[CMOM0 + DIR1] +
-                                  U[CMAGC0 + DIR2] * U[CMOM0 + DIR2] +
-                                  U[CMAGC0 + DIR3] * U[CMOM0 + DIR3]) /
-                                 U[CDENS]);
+        Us[CENER] -= susi * (kdiv(Us[CMAGC0 + DIR1] *
+                                      (Us[CMAGC0 + DIR1] * hll(CMOM0 + DIR1) +
+                                       Us[CMAGC0 + DIR2] * hll(CMOM0 + DIR2) +
+                                       Us[CMAGC0 + DIR3] * hll(CMOM0 + DIR3)),
+                                  hll(CDENS)) -
+                             kdiv(U[CMAGC0 + DIR1] *
+                                      (U[CMAGC0 + DIR1] * U[CMOM0 + DIR1] +
+                                       U[CMAGC0 + DIR2] * U[CMOM0 + DIR2] +
+                                       U[CMAGC0 + DIR3] * U[CMOM0 + DIR3]),
+                                  U[CDENS]));
       }
     };
     hllc_state(sL, UL, total_presL * vL[RVEL0 + DIR1], UsL);
@@ -540,7 +592,7 @@ __device__ __forceinline__ void EosEner(const EosParams &e, R rho, R sie, R &tem
                                         R &bmod) {
   const R gm1 = R(e.gm1);
   pres = kmax(R(0), gm1 * rho * sie);
-  temp = kmax(R(0), sie / R(e.cv));
+  temp = kmax(R(0), kdiv(sie, R(e.cv)));
   bmod = kmax(R(0), (gm1 + R(1)) * gm1 * rho * sie);
 }
 
@@ -549,7 +601,7 @@ __device__ __forceinline__ void EosEner(const EosParams &e, R rho, R sie, R &tem
 template <bool MHD, typename R>
 __device__ __forceinline__ void Cons2PrimEos(const EosParams &eos, R dens, R m0, R m1, R m2,
                                              double ener, const R *B, R *V) {
-  const R idens = R(1.0) / dens;
+  const R idens = kdiv(R(1.0), dens);
   V[RDENS] = dens;
   V[RVEL0] = idens * m0;
   V[RVEL1] = idens * m1;

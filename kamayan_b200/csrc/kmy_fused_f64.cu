@@ -1,4 +1,7 @@
 // FP64 instantiations of the fused stage kernel (separate unit for parallel builds).
+// FP64 divisions and square roots by Newton-Raphson refinement (kdiv, ksqrt
+// in kmy_device.cuh), as in the z-streamed FP64 stage.
+#define KMY_F64_NR 1
 #include "kmy_fused.cuh"
 
 namespace kmy {

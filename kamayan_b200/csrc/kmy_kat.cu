@@ -8,13 +8,14 @@
 // exactness and left/right mirror symmetry) pin the CUDA code, not only the
 // CPU restatement:
 //   impl 0  FP64 Reconstruct                   (per-task kernels, k_face_flux)
-//   impl 1  FP64 two-division WENO-Z           (FP64 brick stage)
+//   impl 1  FP64 two-division WENO-Z, dividing by Newton-Raphson
+//           reciprocals                        (FP64 brick and batched stages)
 //   impl 2  FP32 Reconstruct                   (per-lane FP32 path)
 //   impl 3  FP32 packed WenoZBoth2 / per lane  (FP32 brick stage)
 //   impl 4  FP32 packed WenoZPair / per lane   (z-streamed FP32 stage)
 //   impl 5  FP64 ReconPair, lane by lane       (z-streamed FP64 stage: WENO-Z
 //                                               divides by Newton-Raphson reciprocals)
-//   impl 6  the z-streamed FP64 stage's Newton-Raphson reciprocal of
+//   impl 6  the FP64 stages' Newton-Raphson reciprocal of
 //           stencil[0] (out[0]) and square root of stencil[1] (out[1]), for
 //           checking against IEEE division and square root
 // This unit compiles with the FP32 stage kernels' flags (approximate
@@ -33,7 +34,7 @@ __device__ void kat_one(int impl, int limiter, const double *s, double *out) {
     double d[5];
     for (int k = 0; k < 5; k++) d[k] = s[k];
     double vm, vp;
-    if (impl == 1 && RECON == WENOZ) WenoZBothTwoDiv<double>(d, vm, vp);
+    if (impl == 1 && RECON == WENOZ) WenoZBothTwoDiv<double, DivNR>(d, vm, vp);
     else Reconstruct<RECON, double>(limiter, d, vm, vp);
     out[0] = vm;
     out[1] = vp;
@@ -45,8 +46,8 @@ __device__ void kat_one(int impl, int limiter, const double *s, double *out) {
     out[0] = vm;
     out[1] = vp;
   } else if (impl == 6) {
-    out[0] = slab::rcp_nr(s[0]);
-    out[1] = slab::sqrt_nr(s[1]);
+    out[0] = rcp_nr(s[0]);
+    out[1] = sqrt_nr(s[1]);
   } else if (impl == 5) {
     double2 f[5];
     for (int k = 0; k < 5; k++) f[k] = make_double2(s[k], s[k]);

@@ -310,37 +310,8 @@ __device__ __forceinline__ void ReconPair(int limiter, const float2 (&s)[5], flo
   }
 }
 
-// FP64 reciprocal by Newton-Raphson: the hardware approximation
-// (rcp.approx.ftz.f64, PTX ISA) refined by two iterations r <- r + r (1 - x r),
-// each of which squares the relative error, so the result is within an ulp or
-// two of 1/x for finite, nonzero, normal x (tests/test_gpu_kat.py holds it to
-// 2 ulps of IEEE 1/x; tests/test_gpu_slab_f64.py holds the stage to the oracle
-// at 1e-12).  It takes two fewer dependent FP64
-// operations than IEEE division and no slow-path branch.  Zero and infinite x
-// give NaN (IEEE division gives inf and 0): only states that are already not
-// physical reach them, and the dt controller reports those as non-finite.
-__device__ __forceinline__ double rcp_nr(double x) {
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-  r = fma(r, fma(-x, r, 1.0), r);
-  return fma(r, fma(-x, r, 1.0), r);
-}
-struct DivNR {
-  static __device__ __forceinline__ double div(double a, double b) { return a * rcp_nr(b); }
-};
-// FP64 square root by Newton-Raphson on the reciprocal square root: the
-// hardware approximation (rsqrt.approx.ftz.f64) refined by two iterations
-// y <- y (3/2 - a y^2 / 2), then sqrt(a) = a y, within 3 ulps of IEEE sqrt
-// for normal a > 0 (tests/test_gpu_kat.py); sqrt(0) = 0 and negative a gives
-// NaN, as IEEE sqrt does.
-__device__ __forceinline__ double sqrt_nr(double a) {
-  double y;
-  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
-  const double h = 0.5 * a;
-  y = y * fma(-h, y * y, 1.5);
-  y = y * fma(-h, y * y, 1.5);
-  return a == 0.0 ? a : a * y;
-}
+// FP64 division and square root: the Newton-Raphson forms (rcp_nr, sqrt_nr,
+// DivNR in kmy_device.cuh) or IEEE.
 #if SLAB_F64_NR
 using SlabDiv64 = DivNR;
 __device__ __forceinline__ double slab_sqrt64(double a) { return sqrt_nr(a); }
