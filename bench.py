@@ -61,6 +61,9 @@ def args():
     ap.add_argument("--serve", type=int, default=120,
                     help="requests in the serving-stream measurement (0: skip; 2000 = full stream)")
     ap.add_argument("--serve-steps", type=int, default=100)
+    ap.add_argument("--serve-seq", type=int, default=240,
+                    help="requests solved one after another for the batched/sequential ratio "
+                         "(the first N of the stream; all of them when N >= --serve)")
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the vortex / Orszag-Tang / adaptive-blast measurements")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
@@ -341,7 +344,7 @@ def serving_block(a, device: int) -> dict:
     arrivals = serving.poisson_arrivals(len(reqs), rate, seed=11)
     poi = serving.run_stream(reqs, a.serve_steps, arrivals=arrivals, device=device)
     # the same requests, one after another, each on its own context (no batching)
-    nseq = len(reqs) if len(reqs) <= 240 else 240
+    nseq = min(len(reqs), a.serve_seq)
     seq = serving.run_sequential(reqs[:nseq], a.serve_steps, device=device)
     return {
         "workload": f"{a.serve} requests (seeded mix of vortex/blast, 64^2..128^3, PLM/HLL, PPM/HLLC, "
