@@ -226,11 +226,12 @@ int kmy_conserved_sums(kmy_ctx *ctx, const char *md, double *out);
  * .. 5i+4] = cells i-2 .. i+2) from the library's device reconstruction
  * functions: out[3i] = vM, out[3i+1] = vP, out[3i+2] = 1 when the two lanes of
  * a packed FP32 form disagreed (else 0).  impl selects the form each stage
- * kernel uses: 0 FP64 per-task kernels, 1 FP64 brick stage (two-division
- * WENO-Z), 2 FP32 per lane, 3 FP32 brick stage (packed), 4 FP32 z-streamed
- * stage (packed), 5 FP64 z-streamed stage (lane by lane, WENO-Z dividing by
- * Newton-Raphson reciprocals); impl 6 returns that stage's Newton-Raphson
- * reciprocal of stencils[5i] in out[3i] and square root of stencils[5i+1] in
+ * kernel uses: 0 FP64 per-task kernels, 1 FP64 brick and batched stages
+ * (two-division WENO-Z, Newton-Raphson reciprocals), 2 FP32 per lane,
+ * 3 FP32 brick stage (packed), 4 FP32 z-streamed stage (packed), 5 FP64
+ * z-streamed stage (lane by lane, WENO-Z dividing by Newton-Raphson
+ * reciprocals); impl 6 returns the FP64 stages' Newton-Raphson reciprocal
+ * of stencils[5i] in out[3i] and square root of stencils[5i+1] in
  * out[3i+1].  Needs no context; runs on the current device and
  * synchronises it.  Counterpart of the reference's device-side Reconstruct
  * (src/physics/hydro/reconstruction.hpp:11-142) as its unit tests call it
