@@ -6,6 +6,7 @@ _build/, then everything links into kamayan_b200/lib/libkmy_hydro.so.
 from __future__ import annotations
 
 import os
+import shlex
 import shutil
 import subprocess
 import sys
@@ -60,6 +61,13 @@ def host_cxx() -> str:
     return "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
 
 
+def user_flags() -> list[str]:
+    """Extra nvcc flags for every unit from KMY_NVCC_FLAGS, for example
+    "-DSLAB_F64_NR=0 -DKMY_F64_NR=0" (IEEE division and square root in the
+    fused FP64 stages).  A change of these flags rebuilds every unit."""
+    return shlex.split(os.environ.get("KMY_NVCC_FLAGS", ""))
+
+
 def sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu"))
 
@@ -72,12 +80,12 @@ def _stale(obj: Path, src: Path) -> bool:
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 
-def compile_one(src: Path, verbose_ptxas: bool = False) -> Path:
+def compile_one(src: Path, verbose_ptxas: bool = False, force: bool = False) -> Path:
     obj = BUILD / (src.stem + ".o")
-    if not _stale(obj, src) and not verbose_ptxas:
+    if not force and not _stale(obj, src) and not verbose_ptxas:
         return obj
-    cmd = [nvcc(), "-ccbin", host_cxx(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src.name, []), "-c", str(src),
-           "-o", str(obj)]
+    cmd = [nvcc(), "-ccbin", host_cxx(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src.name, []), *user_flags(), "-c",
+           str(src), "-o", str(obj)]
     if verbose_ptxas:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -93,8 +101,13 @@ def build(jobs: int | None = None, verbose_ptxas: bool = False) -> Path:
     LIBDIR.mkdir(exist_ok=True)
     srcs = sources()
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
+    # the user flags the objects were built with; a change rebuilds them all
+    stamp = BUILD / "user_flags.txt"
+    flags = " ".join(user_flags())
+    force = (stamp.read_text() if stamp.exists() else "") != flags
     with ThreadPoolExecutor(jobs) as ex:
-        objs = list(ex.map(lambda s: compile_one(s, verbose_ptxas), srcs))
+        objs = list(ex.map(lambda s: compile_one(s, verbose_ptxas, force), srcs))
+    stamp.write_text(flags)
     newest = max(o.stat().st_mtime for o in objs)
     if not LIB.exists() or LIB.stat().st_mtime < newest:
         cmd = [nvcc(), "-ccbin", host_cxx(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a",

@@ -1,7 +1,10 @@
 // double instantiations of the batched fused stage (separate unit for parallel builds).
 // FP64 divisions and square roots by Newton-Raphson refinement (kdiv, ksqrt
-// in kmy_device.cuh), as in the z-streamed FP64 stage.
+// in kmy_device.cuh), as in the z-streamed FP64 stage; -DKMY_F64_NR=0 builds
+// IEEE division and square root.
+#ifndef KMY_F64_NR
 #define KMY_F64_NR 1
+#endif
 #include "kmy_batch.cuh"
 
 namespace kmy {
