@@ -81,8 +81,20 @@ def workload_config(a, n_gpus):
         "cells": a.n ** 3,
         "meshblocks": nb,
         "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU",
-        "cache": "inputs larger than L2 (256^3 state: 671 MB FP64, 336 MB FP32)",
+        "cache": state_vs_l2(a.n, a.nb),
     }
+
+
+def state_vs_l2(n: int, nb: int, ghosts: int = 3) -> str:
+    """The line's cache note: the conserved state (5 words per interior cell)
+    and a stage's working set (it reads two containers and writes a third,
+    ghost zones included) against the 126 MB L2."""
+    f64, f32 = 40 * n ** 3 / 1e6, 20 * n ** 3 / 1e6
+    padded = (n // nb) ** 3 * (nb + 2 * ghosts) ** 3
+    w64, w32 = 3 * 40 * padded / 1e6, 3 * 20 * padded / 1e6
+    side = "larger" if w32 > 126.0 else "smaller"
+    return (f"inputs {side} than L2 ({n}^3 state: {f64:.0f} MB FP64, {f32:.0f} MB FP32; a stage's three "
+            f"containers with ghost zones: {w64:.0f} MB FP64, {w32:.0f} MB FP32)")
 
 
 # ---------------------------------------------------------------------------
